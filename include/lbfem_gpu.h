@@ -1,0 +1,237 @@
+/*
+ * lbfem_gpu.h -- C ABI of the B200 (sm_100a) implementation of the
+ * per-time-step hot path of lbm-fem: the matrix-free Taylor-Galerkin streaming
+ * operator, the consistent (Jacobi-PCG) or lumped mass solve and the nodal BGK
+ * collision, for the Lee-Lin predictor-corrector and the Bardow-Karlin-Gusev
+ * collide-then-stream schemes.
+ *
+ * Conventions
+ *  - Plain C types only; no CUDA or torch types cross this boundary.
+ *  - Every function returns an int status (LBFEM_OK = 0). No exception crosses
+ *    the ABI; the message of the last failure is lbfem_gpu_last_error(ctx).
+ *  - Host buffers belong to the caller; device memory belongs to the context.
+ *  - Population vectors are structure-of-arrays: block a (population a,
+ *    a = 0..8, D2Q9 numbering of include/lbfem/d2q9.h:18-22) occupies
+ *    [a*n_dofs, (a+1)*n_dofs) and is indexed by the caller's DoF numbers.
+ *    Increment / right-hand-side vectors of the moving populations have 8
+ *    blocks (block a-1 holds population a), as in include/lbfem/streaming.h.
+ *  - One host thread per context; calls are ordered on the context's stream.
+ *
+ * Each entry point names the reference interface it replaces (file:line in
+ * the lbm-fem sources).
+ */
+#ifndef LBFEM_GPU_H
+#define LBFEM_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  LBFEM_OK = 0,
+  LBFEM_ERR_ARG = 1,            /* bad argument (AssertThrow / ExcMessage in the reference) */
+  LBFEM_ERR_NO_CONVERGENCE = 2, /* CG hit its iteration cap: SolverControl::NoConvergence, mass.h:38-43 */
+  LBFEM_ERR_NONFINITE = 3,      /* NaN or Inf met in a residual norm */
+  LBFEM_ERR_CUDA = 4,           /* a CUDA runtime call failed */
+  LBFEM_ERR_UNSUPPORTED = 5,    /* option or mesh the implementation does not handle */
+  LBFEM_ERR_TIMEOUT = 6,        /* a bounded device-side wait gave up */
+  LBFEM_ERR_STATE = 7           /* call out of order (e.g. step before set_time_step) */
+};
+
+enum { LBFEM_SCHEME_LEELIN = 0, LBFEM_SCHEME_BARDOW = 1 };             /* schemes.h:379,406 */
+enum { LBFEM_MASS_CG = 0, LBFEM_MASS_LUMPED = 1, LBFEM_MASS_RICHARDSON = 2 }; /* mass.h:26-31 */
+enum { LBFEM_STREAMING_TG2 = 0, LBFEM_STREAMING_TG3 = 1, LBFEM_STREAMING_TG3_SPLIT = 2 }; /* streaming.h:25-30 */
+enum { LBFEM_PRECISION_FP64 = 0, LBFEM_PRECISION_MIXED = 1 };
+enum { LBFEM_ADVECTION_TAYLOR_GALERKIN = 0, LBFEM_ADVECTION_LEELIN = 1 }; /* advection.h:211,256 */
+
+/*
+ * The discretisation, exported once from the host-side mesh builder (deal.II's
+ * Discretization::reinit, discretization.h:78-144, in the reference).
+ *
+ * The mesh is the tensor-product box the reference builds: n_cells_x x
+ * n_cells_y axis-parallel cells with vertex coordinates vertex_x[0..n_cells_x]
+ * and vertex_y[0..n_cells_y] (uniform, tanh-stretched or any increasing
+ * sequence), FE_Q(degree) on Gauss-Lobatto support points.
+ *
+ * Structured node (i, j), 0 <= i <= degree*n_cells_x, 0 <= j <= degree*n_cells_y,
+ * is the support point at vertex_x[i/degree] + (i%degree-th Gauss-Lobatto point)
+ * and likewise in y. In a periodic direction the last node column (row) is the
+ * periodic image of the first: its DoF is constrained to the first one, as
+ * make_periodicity_constraints does (discretization.h:110-112).
+ *
+ * dof_index[j*(degree*n_cells_x+1) + i] is the caller's DoF number of node
+ * (i, j); NULL means the structured numbering itself (n_dofs must then be
+ * (degree*n_cells_x+1)*(degree*n_cells_y+1)). Every DoF must appear once.
+ *
+ * Walls (discretization.h:63-67, Walls): the DoF of each wall node and the
+ * velocity (2 doubles) of its wall. Wall nodes must lie on a non-periodic side
+ * of the box.
+ */
+typedef struct lbfem_mesh_desc {
+  int32_t degree;                /* p = 1..4 */
+  int32_t n_cells_x, n_cells_y;  /* >= 2 in a periodic direction, >= 1 otherwise */
+  int32_t periodic_x, periodic_y;
+  const double *vertex_x;        /* n_cells_x + 1 increasing coordinates */
+  const double *vertex_y;        /* n_cells_y + 1 increasing coordinates */
+  int64_t n_dofs;
+  const int64_t *dof_index;      /* NULL or (p*nx+1)*(p*ny+1) entries */
+  int64_t n_walls;
+  const int64_t *wall_dof;       /* n_walls caller DoF numbers */
+  const double *wall_velocity;   /* 2*n_walls */
+} lbfem_mesh_desc;
+
+/*
+ * Settings of the scheme and of its streaming step (StreamingSettings,
+ * MassSettings: streaming.h:32-36, mass.h:33-48).
+ */
+typedef struct lbfem_params {
+  int32_t scheme;                /* LBFEM_SCHEME_* */
+  int32_t mass;                  /* LBFEM_MASS_* */
+  int32_t richardson;            /* passes of LBFEM_MASS_RICHARDSON (reference default 2) */
+  int32_t streaming;             /* LBFEM_STREAMING_* (TG2 implemented) */
+  int32_t precision;             /* LBFEM_PRECISION_* */
+  int32_t cg_max_iterations;     /* reference default 200 */
+  double cg_tolerance;           /* relative to |r|, reference default 1e-8 */
+  int32_t remove_wall_mass_flux; /* -1: scheme default (Bardow 1, Lee-Lin 0), advection.h:182-199 */
+  int32_t device;                /* CUDA device ordinal */
+} lbfem_params;
+
+typedef struct lbfem_gpu_ctx lbfem_gpu_ctx;
+
+/* Fills *params with the reference defaults (Bardow, CG, 1e-8, 200 its, TG2, FP64). */
+void lbfem_gpu_default_params(lbfem_params *params);
+
+/* Human-readable text of a status code. */
+const char *lbfem_gpu_status_string(int status);
+
+/* The message of the last failure on ctx ("" if none). */
+const char *lbfem_gpu_last_error(const lbfem_gpu_ctx *ctx);
+
+/* Number of CUDA devices visible (0 without a GPU); never fails. */
+int lbfem_gpu_device_count(void);
+
+/*
+ * Creates a context: exports the discretisation to flat device arrays and
+ * builds the operators (Discretization::reinit + Scheme constructor,
+ * discretization.h:78-144, schemes.h:85-90,111-116, streaming.h:41-60).
+ */
+int lbfem_gpu_create(const lbfem_mesh_desc *mesh, const lbfem_params *params, lbfem_gpu_ctx **ctx);
+int lbfem_gpu_destroy(lbfem_gpu_ctx *ctx);
+
+/* Scheme::set_time_step (schemes.h:40-44): dt fixed, lambda = nu / c_s^2. */
+int lbfem_gpu_set_time_step(lbfem_gpu_ctx *ctx, double dt, double lambda);
+
+/*
+ * Scheme::set_initial_populations (schemes.h:51-59, Bardow: 129-141): loads the
+ * physical populations f (host, 9 blocks) and applies the scheme's initial
+ * transform (Bardow: g = f + dt/(2 lambda) (f - feq(f))). Resets the CG
+ * extrapolation history. Needs the time step.
+ */
+int lbfem_gpu_set_initial_populations(lbfem_gpu_ctx *ctx, const double *f);
+
+/* Raw copies of the scheme's populations Scheme::f (schemes.h:63), 9 blocks, host. */
+int lbfem_gpu_set_populations(lbfem_gpu_ctx *ctx, const double *f);
+int lbfem_gpu_get_populations(lbfem_gpu_ctx *ctx, double *f);
+
+/* Scheme::step (LeeLin schemes.h:92-98, Bardow schemes.h:118-124), n_steps times, device-resident. */
+int lbfem_gpu_step(lbfem_gpu_ctx *ctx, int32_t n_steps);
+
+/*
+ * The host-buffer form of the same call: f (host, 9 blocks, caller numbering)
+ * is uploaded, n_steps steps are taken, and f is downloaded again.
+ */
+int lbfem_gpu_step_host(lbfem_gpu_ctx *ctx, double *f, int32_t n_steps);
+
+/* Waits for all work queued on ctx; returns the first deferred device-side failure. */
+int lbfem_gpu_synchronize(lbfem_gpu_ctx *ctx);
+
+/*
+ * AdvectionOperator::apply (advection.h:49-58) with TaylorGalerkinAdvection
+ * (kind = LBFEM_ADVECTION_TAYLOR_GALERKIN, advection.h:219-241) or
+ * LeeLinAdvection (kind = LBFEM_ADVECTION_LEELIN, feq required, advection.h:263-289):
+ * rhs (8 blocks) <- r_alpha of f (and feq), lattice velocities e (9 x 2,
+ * Directions), time step {dt, lambda}. remove_wall_mass_flux: -1 = default of
+ * the kind (1 for Taylor-Galerkin as Bardow builds it, 0 for Lee-Lin).
+ * Host buffers. Constrained (periodic image) entries of rhs are zero.
+ */
+int lbfem_gpu_advection(lbfem_gpu_ctx *ctx, const double *f, const double *feq, const double *e, double dt,
+                        double lambda, int32_t kind, int32_t remove_wall_mass_flux, double *rhs);
+
+/*
+ * MassSolver::solve (mass.h:185-213): x <- A^{-1} r with A = M (+ tg3 K_e(e),
+ * not implemented: tg3_coefficient must be 0). One block of n_dofs values.
+ * CG starts from x (input) and stops at |r - A x| <= cg_tolerance |r|;
+ * lumped and Richardson overwrite x. Returns LBFEM_ERR_NO_CONVERGENCE when the
+ * iteration cap is hit (x then holds the last iterate). Host buffers.
+ */
+int lbfem_gpu_mass_solve(lbfem_gpu_ctx *ctx, double *x, const double *r, const double *e, double tg3_coefficient);
+
+/* y <- M x, the MassOperator vmult (discretization.h:51), constrained rows the identity. Host buffers. */
+int lbfem_gpu_mass_vmult(lbfem_gpu_ctx *ctx, double *y, const double *x);
+
+/* CG iterations of all solves so far (MassSolver::cg_iterations, mass.h:215). */
+int lbfem_gpu_cg_iterations(const lbfem_gpu_ctx *ctx, int64_t *iterations);
+
+/* collide_bgk (collision.h:152-168): g (9 blocks, in place) <- BGK collision with rate omega. Host buffers. */
+int lbfem_gpu_collide_bgk(lbfem_gpu_ctx *ctx, double *g, double omega);
+
+/* compute_equilibrium (collision.h:105-113): feq (9 blocks) <- equilibrium of f, wall velocity imposed. */
+int lbfem_gpu_compute_equilibrium(lbfem_gpu_ctx *ctx, const double *f, double *feq);
+
+/* predictor_corrector (collision.h:119-145): f (9 blocks, in place), feq (9), incr (8), theta = dt/lambda. */
+int lbfem_gpu_predictor_corrector(lbfem_gpu_ctx *ctx, double *f, const double *feq, const double *incr,
+                                  double theta);
+
+/* Discretization::node_weight (discretization.h:164-169): the lumped mass diagonal, n_dofs values (1 on periodic images). */
+int lbfem_gpu_node_weight(lbfem_gpu_ctx *ctx, double *w);
+
+/* The Jacobi diagonal of the mass matrix (MassOperator::compute_diagonal), n_dofs values (1 on periodic images). */
+int lbfem_gpu_jacobi_diagonal(lbfem_gpu_ctx *ctx, double *d);
+
+/*
+ * Moments of the current populations at every DoF (D2Q9::moments, d2q9.h:30-41):
+ * rho, ux, uy (host, n_dofs each; any may be NULL). Periodic images carry the
+ * value of their source node.
+ */
+int lbfem_gpu_moments(lbfem_gpu_ctx *ctx, double *rho, double *ux, double *uy);
+
+/*
+ * FP64 conservation sums over the independent nodes with the lumped-mass
+ * weights w (cgdbe.cc:353-368): out[0] = sum w, out[1] = sum w rho,
+ * out[2] = sum w rho ux, out[3] = sum w rho uy, out[4] = sum w |u|^2.
+ */
+int lbfem_gpu_conservation(lbfem_gpu_ctx *ctx, double out[5]);
+
+/* Page-locked host memory for fast host<->device copies (NULL on failure). */
+void *lbfem_gpu_host_alloc(size_t bytes);
+void lbfem_gpu_host_free(void *ptr);
+
+/*
+ * Device-side timing on the context's stream: lbfem_gpu_event_record(ctx, k)
+ * records event k (0..15); lbfem_gpu_event_elapsed(ctx, a, b, &ms) waits for b
+ * and returns the time between a and b in milliseconds.
+ */
+int lbfem_gpu_event_record(lbfem_gpu_ctx *ctx, int32_t slot);
+int lbfem_gpu_event_elapsed(lbfem_gpu_ctx *ctx, int32_t a, int32_t b, float *ms);
+
+/*
+ * The streaming right-hand side of the scheme on the device-resident
+ * populations, into the context's own rhs buffer (no host copies): the kernel
+ * that lbfem_gpu_step launches first (Bardow: collide + advection fused and
+ * the collided populations written back; Lee-Lin: advection with the nodal
+ * equilibria computed on the fly). For timing and profiling of that kernel.
+ */
+int lbfem_gpu_advection_resident(lbfem_gpu_ctx *ctx);
+
+/* Statistics of the last lbfem_gpu_step call: CG iterations per solve (mean) and kernel launches. */
+int lbfem_gpu_last_step_stats(const lbfem_gpu_ctx *ctx, double *cg_iterations_per_solve, int64_t *kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBFEM_GPU_H */

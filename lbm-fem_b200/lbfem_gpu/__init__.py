@@ -1,0 +1,67 @@
+"""Host side of the B200 implementation of lbm-fem's per-time-step hot path.
+
+The compute lives in the CUDA library ``liblbfem_gpu.so`` (sources in
+``../csrc``, C ABI in ``include/lbfem_gpu.h``); this package binds it with
+ctypes and mirrors the reference's host interface:
+
+* ``Solver`` -- one context: Scheme::set_time_step / set_initial_populations /
+  step (schemes.h), AdvectionOperator::apply (advection.h), MassSolver::solve
+  (mass.h), collide_bgk / compute_equilibrium / predictor_corrector
+  (collision.h), node_weight (discretization.h).
+* ``cases`` -- the TestCase flows and the tensor-product mesh export.
+
+The library must be built (``__graft_entry__.build()`` or ``make -C csrc``);
+there is no CPU fallback: without the library or a GPU, ``Solver`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import cases, d2q9
+from ._abi import LbfemError, NoConvergence, make_params
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "liblbfem_gpu.so")
+
+_lib = None
+
+
+def library():
+    """The loaded CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise LbfemError(4, f"{LIB_PATH} is missing: build it with __graft_entry__.build()")
+        from . import _abi
+
+        lib = C.CDLL(LIB_PATH)
+        _abi.declare(lib, "lbfem_gpu_")
+        lib.lbfem_gpu_last_error.restype = C.c_char_p
+        lib.lbfem_gpu_last_error.argtypes = [C.c_void_p]
+        lib.lbfem_gpu_device_count.restype = C.c_int
+        lib.lbfem_gpu_device_count.argtypes = []
+        lib.lbfem_gpu_host_alloc.restype = C.c_void_p
+        lib.lbfem_gpu_host_alloc.argtypes = [C.c_size_t]
+        lib.lbfem_gpu_host_free.restype = None
+        lib.lbfem_gpu_host_free.argtypes = [C.c_void_p]
+        lib.lbfem_gpu_status_string.restype = C.c_char_p
+        lib.lbfem_gpu_status_string.argtypes = [C.c_int]
+        _lib = lib
+    return _lib
+
+
+def device_count():
+    return library().lbfem_gpu_device_count()
+
+
+class Solver:
+    """A context of the CUDA library; same methods as the oracle's handle."""
+
+    def __new__(cls, mesh, params, dof_index=None):
+        from ._abi import Handle
+
+        return Handle(library(), "lbfem_gpu_", mesh, params, dof_index=dof_index)
+
+
+__all__ = ["Solver", "cases", "d2q9", "make_params", "LbfemError", "NoConvergence", "library", "device_count"]

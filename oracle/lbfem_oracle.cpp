@@ -1,0 +1,1138 @@
+// CPU FP64 oracle of the lbm-fem hot path -- TEST INFRASTRUCTURE ONLY.
+//
+// The checker the CUDA path is compared against (tests/, the smoke check and
+// the CPU-baseline leg of bench.py). It restates the reference's matrix-free
+// algorithm without deal.II, in the reference's order of operations:
+//
+//   * FE_Q(p) on Gauss-Lobatto support points, QGauss(p+1) cell and face
+//     quadrature, cartesian cells (diagonal Jacobian per cell): deal.II's
+//     conventions behind discretization.h:114-121.
+//   * Cell loop of weak_form::integrate_cells (advection.h:93-124): gather the
+//     8 moving populations (periodic images read their source node, as
+//     read_dof_values resolves the constraints), sum-factorised gradients at
+//     the Gauss points, the point operation of TaylorGalerkinAdvection
+//     (advection.h:228-239) or LeeLinAdvection (advection.h:275-287),
+//     integrate values and gradients, scatter-add to the source nodes
+//     (distribute_local_to_global).
+//   * Wall faces, weak_form::integrate_boundary_faces + wall_surface_term
+//     (advection.h:126-146,182-199).
+//   * MassOperator vmult with identity rows on constrained DoFs, row-sum lumped
+//     diagonal and Jacobi diagonal (discretization.h:123-125).
+//   * SolverCG with the Jacobi preconditioner in deal.II's order of updates,
+//     absolute tolerance cg_tolerance * |r| (mass.h:204-211).
+//   * nodal_map semantics of collision.h:78-102 (wall nodes with the wall
+//     velocity imposed on their moments), collide_bgk, compute_equilibrium,
+//     predictor_corrector (collision.h:105-168).
+//   * TaylorGalerkin::increment / stream with the extrapolated CG start
+//     2 x^n - x^{n-1} (streaming.h:66-100) and the two schemes
+//     (schemes.h:92-98,118-141).
+//
+// Cells are processed in four colours (no two cells of a colour share a node)
+// so that the OpenMP scatter-add is race-free; dot products use a fixed chunking
+// so that every result is independent of the thread count.
+#include "lbfem_oracle.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#  include <omp.h>
+#endif
+
+namespace
+{
+  constexpr int Q = 9;
+  constexpr int NM = 8; // moving populations
+  constexpr int MAXP = 4;
+  constexpr int MAXN = MAXP + 1;
+
+  // d2q9.h:18-22
+  constexpr double EX[Q] = {0, 1, 1, 0, -1, -1, -1, 0, 1};
+  constexpr double EY[Q] = {0, 0, 1, 1, 1, 0, -1, -1, -1};
+  constexpr double W[Q] = {4. / 9., 1. / 9., 1. / 36., 1. / 9., 1. / 36., 1. / 9., 1. / 36., 1. / 9., 1. / 36.};
+
+  struct Moments
+  {
+    double rho, ux, uy;
+  };
+
+  // D2Q9::moments, d2q9.h:30-41
+  inline Moments
+  moments(const double *f)
+  {
+    double rho = 0, mx = 0, my = 0;
+    for (int a = 0; a < Q; ++a)
+      {
+        rho += f[a];
+        mx += EX[a] * f[a];
+        my += EY[a] * f[a];
+      }
+    return {rho, mx / rho, my / rho};
+  }
+
+  // D2Q9::equilibrium, d2q9.h:44-55
+  inline void
+  equilibrium(const Moments &m, double *feq)
+  {
+    const double uu = m.ux * m.ux + m.uy * m.uy;
+    for (int a = 0; a < Q; ++a)
+      {
+        const double eu = EX[a] * m.ux + EY[a] * m.uy;
+        feq[a] = W[a] * m.rho * (1. + 3. * eu + 4.5 * eu * eu - 1.5 * uu);
+      }
+  }
+
+  // ---------------------------------------------------------------- 1-D basis
+  long double
+  legendre(int n, long double t, long double *dp)
+  {
+    long double p0 = 1, p1 = t;
+    if (n == 0)
+      {
+        *dp = 0;
+        return 1;
+      }
+    for (int k = 1; k < n; ++k)
+      {
+        const long double p2 = ((2 * k + 1) * t * p1 - k * p0) / (k + 1);
+        p0 = p1;
+        p1 = p2;
+      }
+    *dp = n * (t * p1 - p0) / (t * t - 1);
+    return p1;
+  }
+
+  struct Basis
+  {
+    int p = 1;
+    double xi[MAXN];            // Gauss-Lobatto support points on [0,1]
+    double qx[MAXN], qw[MAXN];  // Gauss points and weights on [0,1]
+    double S[MAXN][MAXN];       // S[q][a] = l_a(q)
+    double D[MAXN][MAXN];       // D[q][a] = l_a'(q)
+    double D0[MAXN], D1[MAXN];  // l_a'(0), l_a'(1)
+
+    explicit Basis(int p_)
+      : p(p_)
+    {
+      const int n = p + 1;
+      const long double pi = 3.141592653589793238462643383279502884L;
+      // Gauss-Legendre: roots of P_{p+1}
+      for (int k = 0; k < n; ++k)
+        {
+          long double t = -std::cos(pi * (k + 0.75L) / (n + 0.5L));
+          for (int it = 0; it < 100; ++it)
+            {
+              long double dp;
+              const long double v = legendre(n, t, &dp);
+              const long double dt = v / dp;
+              t -= dt;
+              if (std::fabs(dt) < 1e-19L)
+                break;
+            }
+          long double dp;
+          legendre(n, t, &dp);
+          qx[k] = double((t + 1) / 2);
+          qw[k] = double(1 / ((1 - t * t) * dp * dp)); // 2/((1-t^2)P'^2) / 2
+        }
+      // Gauss-Lobatto: endpoints and roots of P_p'
+      xi[0] = 0.;
+      xi[p] = 1.;
+      for (int k = 1; k < p; ++k)
+        {
+          long double t = -std::cos(pi * k / p);
+          for (int it = 0; it < 100; ++it)
+            {
+              long double dp;
+              const long double v = legendre(p, t, &dp);
+              const long double d2 = (2 * t * dp - p * (p + 1) * v) / (1 - t * t);
+              const long double dt = dp / d2;
+              t -= dt;
+              if (std::fabs(dt) < 1e-19L)
+                break;
+            }
+          xi[k] = double((t + 1) / 2);
+        }
+      for (int q = 0; q < n; ++q)
+        for (int a = 0; a < n; ++a)
+          {
+            S[q][a] = lagrange(a, qx[q]);
+            D[q][a] = dlagrange(a, qx[q]);
+          }
+      for (int a = 0; a < n; ++a)
+        {
+          D0[a] = dlagrange(a, 0.);
+          D1[a] = dlagrange(a, 1.);
+        }
+    }
+
+    double
+    lagrange(int a, double x) const
+    {
+      long double v = 1;
+      for (int b = 0; b <= p; ++b)
+        if (b != a)
+          v *= ((long double)x - xi[b]) / ((long double)xi[a] - xi[b]);
+      return double(v);
+    }
+
+    double
+    dlagrange(int a, double x) const
+    {
+      long double sum = 0;
+      for (int c = 0; c <= p; ++c)
+        {
+          if (c == a)
+            continue;
+          long double v = 1 / ((long double)xi[a] - xi[c]);
+          for (int b = 0; b <= p; ++b)
+            if (b != a && b != c)
+              v *= ((long double)x - xi[b]) / ((long double)xi[a] - xi[b]);
+          sum += v;
+        }
+      return double(sum);
+    }
+  };
+
+  // ------------------------------------------------------------------ oracle
+  struct WallU
+  {
+    bool wall = false;
+    double ux = 0, uy = 0;
+  };
+
+} // namespace
+
+struct lbfem_oracle
+{
+  int p = 1, ncx = 0, ncy = 0, px = 0, py = 0, nfx = 0, nfy = 0;
+  int64_t N = 0;
+  std::vector<double> vx, vy;
+  std::unique_ptr<Basis> basis;
+  std::vector<WallU> wall;         // per node
+  std::vector<int64_t> wall_nodes; // nodes with a wall velocity
+  std::vector<uint8_t> constrained; // periodic images
+  std::vector<double> lumped, inv_lumped, jacobi, inv_jacobi;
+  lbfem_params prm{};
+  double dt = 0, lambda = 0;
+  bool have_ts = false;
+  std::vector<double> f, feq, rhs, x0, x1, cg_r, cg_p, cg_v, cg_z;
+  int64_t cg_its = 0;
+
+  int64_t
+  master(int i, int j) const
+  {
+    if (px && i == p * ncx)
+      i = 0;
+    if (py && j == p * ncy)
+      j = 0;
+    return int64_t(j) * nfx + i;
+  }
+};
+
+namespace
+{
+  int
+  colour_of(int c, int n, bool periodic)
+  {
+    if (periodic && (n % 2 == 1) && c == n - 1)
+      return 2;
+    return c % 2;
+  }
+
+  template <typename F>
+  void
+  for_cells_coloured(const lbfem_oracle &o, F &&body)
+  {
+    for (int colour_y = 0; colour_y < 3; ++colour_y)
+      for (int colour_x = 0; colour_x < 3; ++colour_x)
+        {
+          std::vector<std::pair<int, int>> cells;
+          for (int cy = 0; cy < o.ncy; ++cy)
+            if (colour_of(cy, o.ncy, o.py) == colour_y)
+              for (int cx = 0; cx < o.ncx; ++cx)
+                if (colour_of(cx, o.ncx, o.px) == colour_x)
+                  cells.push_back({cx, cy});
+          const int64_t n = cells.size();
+#pragma omp parallel for schedule(static)
+          for (int64_t k = 0; k < n; ++k)
+            body(cells[k].first, cells[k].second);
+        }
+  }
+
+  // Fixed-chunk deterministic dot product.
+  double
+  dot(const double *a, const double *b, int64_t n)
+  {
+    constexpr int64_t CH = 4096;
+    const int64_t nch = (n + CH - 1) / CH;
+    std::vector<double> part(nch, 0.);
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < nch; ++c)
+      {
+        double s = 0;
+        const int64_t e = std::min(n, (c + 1) * CH);
+        for (int64_t i = c * CH; i < e; ++i)
+          s += a[i] * b[i];
+        part[c] = s;
+      }
+    double s = 0;
+    for (double v : part)
+      s += v;
+    return s;
+  }
+
+  // ------------------------------------------------------- advection (K1)
+  // rhs (8 blocks) <- cell integrals of the point operation over f (and feq)
+  // + wall-face integrals of the surface term.
+  template <int P>
+  void
+  advection_impl(const lbfem_oracle &o, const double *f, const double *feq, const double *e, double a, double b,
+                 double c, double dt, bool remove_flux, double *rhs)
+  {
+    constexpr int n = P + 1;
+    const Basis &B = *o.basis;
+    const int64_t N = o.N;
+    std::fill(rhs, rhs + NM * N, 0.);
+    const bool two = feq != nullptr;
+    double ex[NM], ey[NM];
+    for (int al = 0; al < NM; ++al)
+      {
+        ex[al] = e[2 * (al + 1)];
+        ey[al] = e[2 * (al + 1) + 1];
+      }
+
+    for_cells_coloured(o, [&](int cx, int cy) {
+      const double hx = o.vx[cx + 1] - o.vx[cx], hy = o.vy[cy + 1] - o.vy[cy];
+      int64_t idx[n][n];
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+          idx[j][i] = o.master(cx * P + i, cy * P + j);
+      double V[NM][n][n], FX[NM][n][n], FY[NM][n][n]; // at Gauss points [q2][q1]
+      for (int al = 0; al < NM; ++al)
+        {
+          double gxf[n][n], gyf[n][n], gxe[n][n], gye[n][n];
+          for (int s = 0; s < (two ? 2 : 1); ++s)
+            {
+              const double *src = (s == 0 ? f : feq) + int64_t(al + 1) * N;
+              double u[n][n];
+              for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i)
+                  u[j][i] = src[idx[j][i]];
+              double tx[n][n], tv[n][n]; // [b][q1]
+              for (int bb = 0; bb < n; ++bb)
+                for (int q1 = 0; q1 < n; ++q1)
+                  {
+                    double sd = 0, sv = 0;
+                    for (int aa = 0; aa < n; ++aa)
+                      {
+                        sd += B.D[q1][aa] * u[bb][aa];
+                        sv += B.S[q1][aa] * u[bb][aa];
+                      }
+                    tx[bb][q1] = sd;
+                    tv[bb][q1] = sv;
+                  }
+              double(*gx)[n] = s == 0 ? gxf : gxe;
+              double(*gy)[n] = s == 0 ? gyf : gye;
+              for (int q2 = 0; q2 < n; ++q2)
+                for (int q1 = 0; q1 < n; ++q1)
+                  {
+                    double sx = 0, sy = 0;
+                    for (int bb = 0; bb < n; ++bb)
+                      {
+                        sx += B.S[q2][bb] * tx[bb][q1];
+                        sy += B.D[q2][bb] * tv[bb][q1];
+                      }
+                    gx[q2][q1] = sx / hx;
+                    gy[q2][q1] = sy / hy;
+                  }
+            }
+          for (int q2 = 0; q2 < n; ++q2)
+            for (int q1 = 0; q1 < n; ++q1)
+              {
+                const double JxW = B.qw[q1] * B.qw[q2] * hx * hy;
+                const double s = ex[al] * gxf[q2][q1] + ey[al] * gyf[q2][q1];
+                double val = a * s;
+                if (two)
+                  val += b * (ex[al] * gxe[q2][q1] + ey[al] * gye[q2][q1]);
+                V[al][q2][q1] = val * JxW;
+                FX[al][q2][q1] = (c * ex[al]) * s * JxW / hx;
+                FY[al][q2][q1] = (c * ey[al]) * s * JxW / hy;
+              }
+        }
+      for (int al = 0; al < NM; ++al)
+        {
+          double A1[n][n], A2[n][n]; // [q1][b]
+          for (int q1 = 0; q1 < n; ++q1)
+            for (int bb = 0; bb < n; ++bb)
+              {
+                double s1 = 0, s2 = 0;
+                for (int q2 = 0; q2 < n; ++q2)
+                  {
+                    s1 += B.S[q2][bb] * V[al][q2][q1] + B.D[q2][bb] * FY[al][q2][q1];
+                    s2 += B.S[q2][bb] * FX[al][q2][q1];
+                  }
+                A1[q1][bb] = s1;
+                A2[q1][bb] = s2;
+              }
+          double *dst = rhs + int64_t(al) * N;
+          for (int bb = 0; bb < n; ++bb)
+            for (int aa = 0; aa < n; ++aa)
+              {
+                double s = 0;
+                for (int q1 = 0; q1 < n; ++q1)
+                  s += B.S[q1][aa] * A1[q1][bb] + B.D[q1][aa] * A2[q1][bb];
+                dst[idx[bb][aa]] += s;
+              }
+        }
+    });
+
+    // Wall faces (all non-periodic sides of the box), serial: O(sqrt N).
+    const double half_dt2 = 0.5 * dt * dt;
+    auto face = [&](int cx, int cy, int side) {
+      // side: 0 bottom (y=0), 1 top (y=L), 2 left (x=0), 3 right (x=L)
+      const double hx = o.vx[cx + 1] - o.vx[cx], hy = o.vy[cy + 1] - o.vy[cy];
+      int64_t idx[n][n];
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+          idx[j][i] = o.master(cx * P + i, cy * P + j);
+      const double nx = side == 2 ? -1. : side == 3 ? 1. : 0.;
+      const double ny = side == 0 ? -1. : side == 1 ? 1. : 0.;
+      const bool horizontal = side < 2; // face along x
+      const double hface = horizontal ? hx : hy;
+      double val[NM][n];
+      for (int al = 0; al < NM; ++al)
+        {
+          const double *src = f + int64_t(al + 1) * N;
+          double u[n][n];
+          for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i)
+              u[j][i] = src[idx[j][i]];
+          for (int q = 0; q < n; ++q)
+            {
+              double gx = 0, gy = 0;
+              if (horizontal)
+                {
+                  const int jb = side == 0 ? 0 : P;
+                  const double *dn = side == 0 ? B.D0 : B.D1;
+                  for (int aa = 0; aa < n; ++aa)
+                    {
+                      gx += B.D[q][aa] * u[jb][aa];
+                      double t = 0;
+                      for (int bb = 0; bb < n; ++bb)
+                        t += dn[bb] * u[bb][aa];
+                      gy += B.S[q][aa] * t;
+                    }
+                }
+              else
+                {
+                  const int ib = side == 2 ? 0 : P;
+                  const double *dn = side == 2 ? B.D0 : B.D1;
+                  for (int bb = 0; bb < n; ++bb)
+                    {
+                      gy += B.D[q][bb] * u[bb][ib];
+                      double t = 0;
+                      for (int aa = 0; aa < n; ++aa)
+                        t += dn[aa] * u[bb][aa];
+                      gx += B.S[q][bb] * t;
+                    }
+                }
+              gx /= hx;
+              gy /= hy;
+              val[al][q] = half_dt2 * (ex[al] * nx + ey[al] * ny) * (ex[al] * gx + ey[al] * gy);
+            }
+        }
+      if (remove_flux)
+        for (int q = 0; q < n; ++q)
+          {
+            double flux = 0;
+            for (int al = 0; al < NM; ++al)
+              flux += val[al][q];
+            for (int al = 0; al < NM; ++al)
+              val[al][q] -= (W[al + 1] / (1. - W[0])) * flux;
+          }
+      for (int al = 0; al < NM; ++al)
+        {
+          double *dst = rhs + int64_t(al) * N;
+          for (int k = 0; k < n; ++k)
+            {
+              double s = 0;
+              for (int q = 0; q < n; ++q)
+                s += B.S[q][k] * (val[al][q] * (B.qw[q] * hface));
+              if (horizontal)
+                dst[idx[side == 0 ? 0 : P][k]] += s;
+              else
+                dst[idx[k][side == 2 ? 0 : P]] += s;
+            }
+        }
+    };
+    if (!o.py)
+      for (int cx = 0; cx < o.ncx; ++cx)
+        {
+          face(cx, 0, 0);
+          face(cx, o.ncy - 1, 1);
+        }
+    if (!o.px)
+      for (int cy = 0; cy < o.ncy; ++cy)
+        {
+          face(0, cy, 2);
+          face(o.ncx - 1, cy, 3);
+        }
+  }
+
+  void
+  advection(const lbfem_oracle &o, const double *f, const double *feq, const double *e, double a, double b, double c,
+            double dt, bool remove_flux, double *rhs)
+  {
+    switch (o.p)
+      {
+        case 1:
+          advection_impl<1>(o, f, feq, e, a, b, c, dt, remove_flux, rhs);
+          break;
+        case 2:
+          advection_impl<2>(o, f, feq, e, a, b, c, dt, remove_flux, rhs);
+          break;
+        case 3:
+          advection_impl<3>(o, f, feq, e, a, b, c, dt, remove_flux, rhs);
+          break;
+        default:
+          advection_impl<4>(o, f, feq, e, a, b, c, dt, remove_flux, rhs);
+      }
+  }
+
+  // ----------------------------------------------------------- mass matrix
+  // dst = M src over the cells (no constraint rows); mode 0: the action,
+  // mode 1: the diagonal of the cell matrices (src unused).
+  template <int P>
+  void
+  mass_cells(const lbfem_oracle &o, const double *src, double *dst, int mode)
+  {
+    constexpr int n = P + 1;
+    const Basis &B = *o.basis;
+    std::fill(dst, dst + o.N, 0.);
+    for_cells_coloured(o, [&](int cx, int cy) {
+      const double hx = o.vx[cx + 1] - o.vx[cx], hy = o.vy[cy + 1] - o.vy[cy];
+      int64_t idx[n][n];
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+          idx[j][i] = o.master(cx * P + i, cy * P + j);
+      if (mode == 1)
+        {
+          for (int bb = 0; bb < n; ++bb)
+            for (int aa = 0; aa < n; ++aa)
+              {
+                double s = 0;
+                for (int q2 = 0; q2 < n; ++q2)
+                  for (int q1 = 0; q1 < n; ++q1)
+                    {
+                      const double phi = B.S[q1][aa] * B.S[q2][bb];
+                      s += phi * phi * (B.qw[q1] * B.qw[q2] * hx * hy);
+                    }
+                dst[idx[bb][aa]] += s;
+              }
+          return;
+        }
+      double u[n][n];
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+          u[j][i] = src[idx[j][i]];
+      double t[n][n]; // [b][q1]
+      for (int bb = 0; bb < n; ++bb)
+        for (int q1 = 0; q1 < n; ++q1)
+          {
+            double s = 0;
+            for (int aa = 0; aa < n; ++aa)
+              s += B.S[q1][aa] * u[bb][aa];
+            t[bb][q1] = s;
+          }
+      double vq[n][n]; // [q2][q1]
+      for (int q2 = 0; q2 < n; ++q2)
+        for (int q1 = 0; q1 < n; ++q1)
+          {
+            double s = 0;
+            for (int bb = 0; bb < n; ++bb)
+              s += B.S[q2][bb] * t[bb][q1];
+            vq[q2][q1] = s * (B.qw[q1] * B.qw[q2] * hx * hy);
+          }
+      double a1[n][n]; // [q1][b]
+      for (int q1 = 0; q1 < n; ++q1)
+        for (int bb = 0; bb < n; ++bb)
+          {
+            double s = 0;
+            for (int q2 = 0; q2 < n; ++q2)
+              s += B.S[q2][bb] * vq[q2][q1];
+            a1[q1][bb] = s;
+          }
+      for (int bb = 0; bb < n; ++bb)
+        for (int aa = 0; aa < n; ++aa)
+          {
+            double s = 0;
+            for (int q1 = 0; q1 < n; ++q1)
+              s += B.S[q1][aa] * a1[q1][bb];
+            dst[idx[bb][aa]] += s;
+          }
+    });
+  }
+
+  void
+  mass_cells_dispatch(const lbfem_oracle &o, const double *src, double *dst, int mode)
+  {
+    switch (o.p)
+      {
+        case 1:
+          mass_cells<1>(o, src, dst, mode);
+          break;
+        case 2:
+          mass_cells<2>(o, src, dst, mode);
+          break;
+        case 3:
+          mass_cells<3>(o, src, dst, mode);
+          break;
+        default:
+          mass_cells<4>(o, src, dst, mode);
+      }
+  }
+
+  // MassOperator vmult: cell loop, then the identity on constrained rows.
+  void
+  mass_vmult(const lbfem_oracle &o, double *dst, const double *src)
+  {
+    mass_cells_dispatch(o, src, dst, 0);
+    for (int64_t i = 0; i < o.N; ++i)
+      if (o.constrained[i])
+        dst[i] = src[i];
+  }
+
+  // deal.II SolverCG with the Jacobi preconditioner, in its order of updates.
+  int
+  cg_solve(lbfem_oracle &o, double *x, const double *b, int64_t *its)
+  {
+    const int64_t N = o.N;
+    double *r = o.cg_r.data(), *p = o.cg_p.data(), *v = o.cg_v.data(), *z = o.cg_z.data();
+    const double tol = o.prm.cg_tolerance * std::sqrt(dot(b, b, N));
+    bool zero = true;
+    for (int64_t i = 0; i < N && zero; ++i)
+      zero = x[i] == 0.;
+    if (!zero)
+      {
+        mass_vmult(o, r, x);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < N; ++i)
+          r[i] = -r[i] + b[i];
+      }
+    else
+      std::copy(b, b + N, r);
+    double res = std::sqrt(dot(r, r, N));
+    int64_t it = 0;
+    *its = 0;
+    if (std::isnan(res))
+      return LBFEM_ERR_NONFINITE;
+    if (res <= tol)
+      return LBFEM_OK;
+    double rz = 0;
+    while (true)
+      {
+        ++it;
+        const double *inv = o.inv_jacobi.data();
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < N; ++i)
+          z[i] = inv[i] * r[i];
+        const double rz_prev = rz;
+        rz = dot(r, z, N);
+        const double beta = it > 1 ? rz / rz_prev : 0.;
+        if (it > 1)
+          {
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < N; ++i)
+              p[i] = beta * p[i] + z[i];
+          }
+        else
+          std::copy(z, z + N, p);
+        mass_vmult(o, v, p);
+        const double pAp = dot(p, v, N);
+        const double alpha = rz / pAp;
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < N; ++i)
+          {
+            x[i] += alpha * p[i];
+            r[i] += -alpha * v[i];
+          }
+        res = std::sqrt(dot(r, r, N));
+        *its = it;
+        if (std::isnan(res))
+          return LBFEM_ERR_NONFINITE;
+        if (res <= tol)
+          return LBFEM_OK;
+        if (it >= o.prm.cg_max_iterations)
+          return LBFEM_ERR_NO_CONVERGENCE;
+      }
+  }
+
+  int
+  mass_solve(lbfem_oracle &o, double *x, const double *r)
+  {
+    if (o.prm.mass == LBFEM_MASS_LUMPED)
+      {
+        const double *inv = o.inv_lumped.data();
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < o.N; ++i)
+          x[i] = inv[i] * r[i];
+        return LBFEM_OK;
+      }
+    if (o.prm.mass == LBFEM_MASS_RICHARDSON)
+      {
+        // x_0 = M_L^{-1} r, x_{j+1} = x_j + M_L^{-1} (r - M x_j) (mass.h:193-202)
+        const double *inv = o.inv_lumped.data();
+        for (int64_t i = 0; i < o.N; ++i)
+          x[i] = inv[i] * r[i];
+        for (int k = 0; k < o.prm.richardson; ++k)
+          {
+            mass_vmult(o, o.cg_v.data(), x);
+            for (int64_t i = 0; i < o.N; ++i)
+              x[i] += inv[i] * (r[i] - o.cg_v[i]);
+          }
+        return LBFEM_OK;
+      }
+    int64_t its = 0;
+    const int st = cg_solve(o, x, r, &its);
+    o.cg_its += its;
+    return st;
+  }
+
+  // ---------------------------------------------------------- nodal maps
+  template <typename Op>
+  void
+  nodal_map(const lbfem_oracle &o, Op &&op)
+  {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < o.N; ++i)
+      op(i, o.wall[i]);
+  }
+
+  inline Moments
+  impose(Moments m, const WallU &w)
+  {
+    if (w.wall)
+      {
+        m.ux = w.ux;
+        m.uy = w.uy;
+      }
+    return m;
+  }
+
+  void
+  collide_bgk(const lbfem_oracle &o, double *g, double omega)
+  {
+    const int64_t N = o.N;
+    nodal_map(o, [&](int64_t i, const WallU &w) {
+      double gi[Q], geq[Q], geqt[Q];
+      for (int a = 0; a < Q; ++a)
+        gi[a] = g[a * N + i];
+      const Moments m = moments(gi);
+      equilibrium(m, geq);
+      equilibrium(impose(m, w), geqt);
+      for (int a = 0; a < Q; ++a)
+        g[a * N + i] = geqt[a] + (1. - omega) * (gi[a] - geq[a]);
+    });
+  }
+
+  void
+  compute_equilibrium(const lbfem_oracle &o, const double *f, double *feq)
+  {
+    const int64_t N = o.N;
+    nodal_map(o, [&](int64_t i, const WallU &w) {
+      double fi[Q], fe[Q];
+      for (int a = 0; a < Q; ++a)
+        fi[a] = f[a * N + i];
+      equilibrium(impose(moments(fi), w), fe);
+      for (int a = 0; a < Q; ++a)
+        feq[a * N + i] = fe[a];
+    });
+  }
+
+  void
+  predictor_corrector(const lbfem_oracle &o, double *f, const double *feq, const double *x, double theta)
+  {
+    const int64_t N = o.N;
+    const double inv = 1. / (1. + theta);
+    nodal_map(o, [&](int64_t i, const WallU &w) {
+      double fh[Q], eqh[Q];
+      fh[0] = inv * (f[i] + theta * feq[i]);
+      for (int a = 1; a < Q; ++a)
+        fh[a] = inv * (f[a * N + i] + theta * feq[a * N + i] + x[(a - 1) * N + i]);
+      equilibrium(impose(moments(fh), w), eqh);
+      for (int a = 0; a < Q; ++a)
+        f[a * N + i] = fh[a] + theta * (eqh[a] - feq[a * N + i]);
+    });
+  }
+
+  int
+  increment(lbfem_oracle &o, const double *f, const double *feq, double a, double b, double c, bool remove_flux)
+  {
+    double e[2 * Q];
+    for (int k = 0; k < Q; ++k)
+      {
+        e[2 * k] = EX[k];
+        e[2 * k + 1] = EY[k];
+      }
+    advection(o, f, feq, e, a, b, c, o.dt, remove_flux, o.rhs.data());
+    const bool extrapolate = o.prm.mass == LBFEM_MASS_CG;
+    const int64_t N = o.N;
+    for (int al = 0; al < NM; ++al)
+      {
+        double *xa = o.x0.data() + al * N, *xb = o.x1.data() + al * N;
+        if (extrapolate)
+          {
+            // x[1].block(a).sadd(-1., 2., xa); xa.swap(x[1].block(a)) (streaming.h:76-80)
+            for (int64_t i = 0; i < N; ++i)
+              xb[i] = -xb[i] + 2. * xa[i];
+            std::swap_ranges(xa, xa + N, xb);
+          }
+        const int st = mass_solve(o, xa, o.rhs.data() + al * N);
+        if (st != LBFEM_OK)
+          return st;
+      }
+    return LBFEM_OK;
+  }
+
+  int
+  step(lbfem_oracle &o)
+  {
+    const int64_t N = o.N;
+    const bool bardow = o.prm.scheme == LBFEM_SCHEME_BARDOW;
+    const int rm = o.prm.remove_wall_mass_flux;
+    if (bardow)
+      {
+        // Bardow::step, schemes.h:118-124
+        collide_bgk(o, o.f.data(), o.dt / (o.lambda + 0.5 * o.dt));
+        const int st = increment(o, o.f.data(), nullptr, -o.dt, 0., -0.5 * o.dt * o.dt, rm < 0 ? true : rm != 0);
+        if (st != LBFEM_OK)
+          return st;
+        for (int al = 0; al < NM; ++al)
+          {
+            double *fa = o.f.data() + (al + 1) * N;
+            const double *xa = o.x0.data() + al * N;
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < N; ++i)
+              fa[i] += xa[i];
+          }
+        return LBFEM_OK;
+      }
+    // LeeLin::step, schemes.h:92-98
+    compute_equilibrium(o, o.f.data(), o.feq.data());
+    const double bb = -0.5 * o.dt * o.dt / o.lambda;
+    const int st =
+      increment(o, o.f.data(), o.feq.data(), -o.dt - bb, bb, -0.5 * o.dt * o.dt, rm < 0 ? false : rm != 0);
+    if (st != LBFEM_OK)
+      return st;
+    predictor_corrector(o, o.f.data(), o.feq.data(), o.x0.data(), o.dt / o.lambda);
+    return LBFEM_OK;
+  }
+} // namespace
+
+extern "C" {
+
+int
+lbfem_oracle_set_threads(int32_t n)
+{
+#ifdef _OPENMP
+  if (n > 0)
+    omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
+
+int
+lbfem_oracle_basis_1d(int32_t p, double *support, double *gp, double *gw)
+{
+  if (p < 1 || p > MAXP)
+    return LBFEM_ERR_ARG;
+  Basis B(p);
+  for (int k = 0; k <= p; ++k)
+    {
+      if (support)
+        support[k] = B.xi[k];
+      if (gp)
+        gp[k] = B.qx[k];
+      if (gw)
+        gw[k] = B.qw[k];
+    }
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_oracle **h)
+{
+  if (!m || !prm || !h)
+    return LBFEM_ERR_ARG;
+  if (m->degree < 1 || m->degree > MAXP || m->n_cells_x < 1 || m->n_cells_y < 1 || m->dof_index)
+    return LBFEM_ERR_ARG;
+  if ((m->periodic_x && m->n_cells_x < 2) || (m->periodic_y && m->n_cells_y < 2))
+    return LBFEM_ERR_ARG;
+  auto o = std::make_unique<lbfem_oracle>();
+  o->p = m->degree;
+  o->ncx = m->n_cells_x;
+  o->ncy = m->n_cells_y;
+  o->px = m->periodic_x != 0;
+  o->py = m->periodic_y != 0;
+  o->nfx = o->p * o->ncx + 1;
+  o->nfy = o->p * o->ncy + 1;
+  o->N = int64_t(o->nfx) * o->nfy;
+  if (m->n_dofs != o->N)
+    return LBFEM_ERR_ARG;
+  o->vx.assign(m->vertex_x, m->vertex_x + o->ncx + 1);
+  o->vy.assign(m->vertex_y, m->vertex_y + o->ncy + 1);
+  o->basis = std::make_unique<Basis>(o->p);
+  o->prm = *prm;
+  const int64_t N = o->N;
+  o->wall.assign(N, WallU{});
+  for (int64_t k = 0; k < m->n_walls; ++k)
+    {
+      const int64_t d = m->wall_dof[k];
+      if (d < 0 || d >= N)
+        return LBFEM_ERR_ARG;
+      o->wall[d] = {true, m->wall_velocity[2 * k], m->wall_velocity[2 * k + 1]};
+    }
+  o->constrained.assign(N, 0);
+  for (int j = 0; j < o->nfy; ++j)
+    for (int i = 0; i < o->nfx; ++i)
+      if (o->master(i, j) != int64_t(j) * o->nfx + i)
+        o->constrained[int64_t(j) * o->nfx + i] = 1;
+  // lumped diagonal: M applied to ones (constraints resolved), constrained = 1
+  std::vector<double> ones(N, 1.);
+  o->lumped.assign(N, 0.);
+  mass_cells_dispatch(*o, ones.data(), o->lumped.data(), 0);
+  o->jacobi.assign(N, 0.);
+  mass_cells_dispatch(*o, nullptr, o->jacobi.data(), 1);
+  o->inv_lumped.resize(N);
+  o->inv_jacobi.resize(N);
+  for (int64_t i = 0; i < N; ++i)
+    {
+      if (o->constrained[i])
+        {
+          o->lumped[i] = 1.;
+          o->jacobi[i] = 1.;
+        }
+      o->inv_lumped[i] = o->lumped[i] == 0. ? 1. : 1. / o->lumped[i];
+      o->inv_jacobi[i] = o->jacobi[i] == 0. ? 1. : 1. / o->jacobi[i];
+    }
+  o->f.assign(Q * N, 0.);
+  o->feq.assign(Q * N, 0.);
+  o->rhs.assign(NM * N, 0.);
+  o->x0.assign(NM * N, 0.);
+  o->x1.assign(NM * N, 0.);
+  o->cg_r.assign(N, 0.);
+  o->cg_p.assign(N, 0.);
+  o->cg_v.assign(N, 0.);
+  o->cg_z.assign(N, 0.);
+  *h = o.release();
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_destroy(lbfem_oracle *h)
+{
+  delete h;
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_set_time_step(lbfem_oracle *h, double dt, double lambda)
+{
+  if (!h || !(dt > 0) || !(lambda > 0))
+    return LBFEM_ERR_ARG;
+  h->dt = dt;
+  h->lambda = lambda;
+  h->have_ts = true;
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_set_populations(lbfem_oracle *h, const double *f)
+{
+  if (!h || !f)
+    return LBFEM_ERR_ARG;
+  std::copy(f, f + Q * h->N, h->f.begin());
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_get_populations(lbfem_oracle *h, double *f)
+{
+  if (!h || !f)
+    return LBFEM_ERR_ARG;
+  std::copy(h->f.begin(), h->f.end(), f);
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_set_initial_populations(lbfem_oracle *h, const double *f)
+{
+  if (!h || !f)
+    return LBFEM_ERR_ARG;
+  if (!h->have_ts)
+    return LBFEM_ERR_STATE;
+  const int64_t N = h->N;
+  std::copy(f, f + Q * N, h->f.begin());
+  std::fill(h->x0.begin(), h->x0.end(), 0.);
+  std::fill(h->x1.begin(), h->x1.end(), 0.);
+  if (h->prm.scheme == LBFEM_SCHEME_BARDOW)
+    {
+      // Bardow::set_initial_populations, schemes.h:129-141
+      const double scale = 0.5 * h->dt / h->lambda;
+      for (int64_t i = 0; i < N; ++i)
+        {
+          double fi[Q], fe[Q];
+          for (int a = 0; a < Q; ++a)
+            fi[a] = h->f[a * N + i];
+          equilibrium(moments(fi), fe);
+          for (int a = 0; a < Q; ++a)
+            h->f[a * N + i] = fi[a] + scale * (fi[a] - fe[a]);
+        }
+    }
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_step(lbfem_oracle *h, int32_t n_steps)
+{
+  if (!h || n_steps < 0)
+    return LBFEM_ERR_ARG;
+  if (!h->have_ts)
+    return LBFEM_ERR_STATE;
+  for (int s = 0; s < n_steps; ++s)
+    {
+      const int st = step(*h);
+      if (st != LBFEM_OK)
+        return st;
+    }
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_advection(lbfem_oracle *h, const double *f, const double *feq, const double *e, double dt,
+                       double lambda, int32_t kind, int32_t remove, double *rhs)
+{
+  if (!h || !f || !e || !rhs || !(dt > 0))
+    return LBFEM_ERR_ARG;
+  if (kind == LBFEM_ADVECTION_LEELIN)
+    {
+      if (!feq || !(lambda > 0))
+        return LBFEM_ERR_ARG;
+      const double b = -0.5 * dt * dt / lambda;
+      advection(*h, f, feq, e, -dt - b, b, -0.5 * dt * dt, dt, remove < 0 ? false : remove != 0, rhs);
+      return LBFEM_OK;
+    }
+  if (kind != LBFEM_ADVECTION_TAYLOR_GALERKIN)
+    return LBFEM_ERR_ARG;
+  advection(*h, f, nullptr, e, -dt, 0., -0.5 * dt * dt, dt, remove < 0 ? true : remove != 0, rhs);
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_mass_solve(lbfem_oracle *h, double *x, const double *r, const double *, double tg3)
+{
+  if (!h || !x || !r)
+    return LBFEM_ERR_ARG;
+  if (tg3 != 0.)
+    return LBFEM_ERR_UNSUPPORTED;
+  return mass_solve(*h, x, r);
+}
+
+int
+lbfem_oracle_mass_vmult(lbfem_oracle *h, double *y, const double *x)
+{
+  if (!h || !x || !y)
+    return LBFEM_ERR_ARG;
+  mass_vmult(*h, y, x);
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_cg_iterations(const lbfem_oracle *h, int64_t *its)
+{
+  if (!h || !its)
+    return LBFEM_ERR_ARG;
+  *its = h->cg_its;
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_collide_bgk(lbfem_oracle *h, double *g, double omega)
+{
+  if (!h || !g)
+    return LBFEM_ERR_ARG;
+  collide_bgk(*h, g, omega);
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_compute_equilibrium(lbfem_oracle *h, const double *f, double *feq)
+{
+  if (!h || !f || !feq)
+    return LBFEM_ERR_ARG;
+  compute_equilibrium(*h, f, feq);
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_predictor_corrector(lbfem_oracle *h, double *f, const double *feq, const double *incr, double theta)
+{
+  if (!h || !f || !feq || !incr)
+    return LBFEM_ERR_ARG;
+  predictor_corrector(*h, f, feq, incr, theta);
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_node_weight(lbfem_oracle *h, double *w)
+{
+  if (!h || !w)
+    return LBFEM_ERR_ARG;
+  std::copy(h->lumped.begin(), h->lumped.end(), w);
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_jacobi_diagonal(lbfem_oracle *h, double *d)
+{
+  if (!h || !d)
+    return LBFEM_ERR_ARG;
+  std::copy(h->jacobi.begin(), h->jacobi.end(), d);
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_conservation(lbfem_oracle *h, double out[5])
+{
+  if (!h || !out)
+    return LBFEM_ERR_ARG;
+  const int64_t N = h->N;
+  double s[5] = {0, 0, 0, 0, 0};
+  for (int64_t i = 0; i < N; ++i)
+    {
+      if (h->constrained[i])
+        continue;
+      double fi[Q];
+      for (int a = 0; a < Q; ++a)
+        fi[a] = h->f[a * N + i];
+      const Moments m = moments(fi);
+      const double w = h->lumped[i];
+      s[0] += w;
+      s[1] += w * m.rho;
+      s[2] += w * m.rho * m.ux;
+      s[3] += w * m.rho * m.uy;
+      s[4] += w * (m.ux * m.ux + m.uy * m.uy);
+    }
+  std::copy(s, s + 5, out);
+  return LBFEM_OK;
+}
+
+} // extern "C"

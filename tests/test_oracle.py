@@ -1,0 +1,198 @@
+"""The CPU oracle pinned against the reference: its compile-time lattice
+identities, the element stencils of analysis/stencils.py, the amplification
+factors of analysis/tg_spectral.py, the check value of
+benchmarks/stencil_bench.cc, and the accuracy tables of docs/results.md."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from helpers import directions, rel_l2, setup_case, tgv, unit_mesh
+from lbfem_gpu import _abi, cases, d2q9, make_params
+
+
+# ------------------------------------------------------------- lattice KATs
+def test_lattice_isotropy():
+    """d2q9.h:80-88: sum_a w_a e..e = 1, 0, cs2 delta, 0, cs4 (delta delta + ...)."""
+    cs2 = d2q9.CS2
+    assert abs(d2q9.lattice_tensor() - 1) < 1e-14
+    for i in (0, 1):
+        assert abs(d2q9.lattice_tensor(i)) < 1e-14
+    assert abs(d2q9.lattice_tensor(0, 0) - cs2) < 1e-14 and abs(d2q9.lattice_tensor(1, 1) - cs2) < 1e-14
+    assert abs(d2q9.lattice_tensor(0, 1)) < 1e-14
+    assert abs(d2q9.lattice_tensor(0, 0, 0)) < 1e-14 and abs(d2q9.lattice_tensor(0, 1, 1)) < 1e-14
+    assert abs(d2q9.lattice_tensor(0, 0, 0, 0) - 3 * cs2 * cs2) < 1e-14
+    assert abs(d2q9.lattice_tensor(0, 0, 1, 1) - cs2 * cs2) < 1e-14
+    assert abs(d2q9.lattice_tensor(0, 0, 0, 1)) < 1e-14
+
+
+def test_equilibrium_roundtrip_oracle(oracle_mod):
+    """d2q9.h:89-92: moments(equilibrium(1.1, 0.05, -0.02)) round trip, through the oracle's nodal map."""
+    m = unit_mesh(2, 1)
+    o = oracle_mod.Oracle(m, make_params())
+    f = np.tile(d2q9.equilibrium(1.1, 0.05, -0.02)[:, None], (1, m.n_dofs))
+    feq = o.compute_equilibrium(f)
+    rho, ux, uy = d2q9.moments(feq)
+    assert np.all(np.abs(rho - 1.1) < 1e-14)
+    assert np.all(np.abs(ux - 0.05) < 1e-14) and np.all(np.abs(uy + 0.02) < 1e-14)
+
+
+# ----------------------------------------------------------- stencil KATs
+def _stencil_rows(o, m, node, dt_pair=(1.0, 2.0)):
+    """Rows of M, C_e, K_e at `node` for e = e_1..e_4, by applying the oracle to unit vectors."""
+    p = m.degree
+    e = directions()
+    out = {"M": {}, "C": {a: {} for a in range(4)}, "K": {a: {} for a in range(4)}}
+    i0, j0 = node
+    for dy in range(-p, p + 1):
+        for dx in range(-p, p + 1):
+            u = np.zeros(m.n_dofs)
+            u[(j0 + dy) * m.nfx + (i0 + dx)] = 1.0
+            Mu = o.mass_vmult(u)
+            out["M"][(dx, dy)] = Mu[j0 * m.nfx + i0]
+            f = np.tile(u, (9, 1))
+            r1 = o.advection(f, e, dt_pair[0], 1.0)
+            r2 = o.advection(f, e, dt_pair[1], 1.0)
+            for a in range(4):
+                a1, a2 = r1[a, j0 * m.nfx + i0], r2[a, j0 * m.nfx + i0]
+                K = 2 * a1 - a2  # r(dt) = -dt C u - dt^2/2 K u
+                out["K"][a][(dx, dy)] = K
+                out["C"][a][(dx, dy)] = -a1 - K / 2
+    return out
+
+
+@pytest.mark.parametrize("p", [1, 2])
+def test_element_stencils(oracle_mod, p):
+    """Assembled M, C_e, K_e stencils equal the reference's sympy stencils (analysis/stencils.py)."""
+    gold = json.load(open(os.path.join(GOLDEN, "stencils.json")))
+    m = unit_mesh(6, p)  # cell size 1: the stencils at h = 1
+    o = oracle_mod.Oracle(m, make_params())
+    names = {0: "(1,0)", 1: "(1,1)", 2: "(0,1)", 3: "(-1,1)"}
+    for tx in range(p):
+        for ty in range(p):
+            rows = _stencil_rows(o, m, (2 * p + tx, 2 * p + ty))
+            g = gold[f"Q{p} M"][f"{tx},{ty}"]
+            for (dx, dy), v in rows["M"].items():
+                assert abs(v - g.get(f"{dx},{dy}", 0.0)) < 1e-13, ("M", tx, ty, dx, dy)
+            for a, en in names.items():
+                for lab in ("C", "K"):
+                    g = gold[f"Q{p} {lab} e={en}"][f"{tx},{ty}"]
+                    for (dx, dy), v in rows[lab][a].items():
+                        assert abs(v - g.get(f"{dx},{dy}", 0.0)) < 1e-12, (lab, en, tx, ty, dx, dy, v)
+
+
+def test_amplification_factor(oracle_mod):
+    """One TG2 streaming step of a Fourier mode (consistent mass) equals G_2d of analysis/tg_spectral.py."""
+    gold = json.load(open(os.path.join(GOLDEN, "tg_spectral.json")))["cases"]
+    n = 16
+    m = unit_mesh(n, 1)
+    o = oracle_mod.Oracle(m, make_params(cg_tolerance=1e-14, cg_max_iterations=500))
+    e = directions()
+    I, J = np.meshgrid(np.arange(m.nfx), np.arange(m.nfy))
+    I, J = I.ravel() % n, J.ravel() % n
+    ind = m.independent()
+    checked = 0
+    for c in gold:
+        if c["tg3"]:
+            continue
+        alpha = [k for k in range(1, 9) if tuple(d2q9.E[k]) == (c["ex"], c["ey"])][0]
+        phi = 2 * np.pi * (c["mx"] * I + c["my"] * J) / n
+        u = np.cos(phi)
+        f = np.tile(u, (9, 1))
+        r = o.advection(f, e, c["C"], 1.0)
+        x = o.mass_solve(r[alpha - 1])
+        up = u + x
+        cs, sn = np.cos(phi[ind]), np.sin(phi[ind])
+        g_re = np.dot(up[ind], cs) / np.dot(cs, cs)
+        g_im = -np.dot(up[ind], sn) / np.dot(sn, sn)
+        assert abs(g_re - c["G_re"]) < 1e-12 and abs(g_im - c["G_im"]) < 1e-12, c
+        checked += 1
+    assert checked >= 60
+
+
+def test_stencil_bench_check_value(oracle_mod):
+    """Q1 lumped streaming increment on a periodic grid reproduces stencil_bench.cc's check value."""
+    gold = json.load(open(os.path.join(GOLDEN, "stencil_bench.json")))
+    for row in gold["rows"]:
+        N = row["N"]
+        m = unit_mesh(N, 1, h=1.0 / N)
+        o = oracle_mod.Oracle(m, make_params(mass="lumped"))
+        I, J = np.meshgrid(np.arange(m.nfx), np.arange(m.nfy))
+        idx = (J.ravel() % N) * N + (I.ravel() % N)
+        fu = 1.0 + 1e-3 * ((idx * 7919) % 13)
+        f = np.tile(fu, (9, 1))
+        r = o.advection(f, directions(), 0.25 / N, 1.0, remove_wall_mass_flux=0)
+        node = 1 * m.nfx + 1
+        chk = sum(o.mass_solve(r[a])[node] for a in range(8))
+        assert abs(chk - row["chk"]) <= 5e-6 * abs(row["chk"]), (N, chk, row["chk"])
+
+
+# ------------------------------------------------------ accuracy tables
+def _tgv_error(oracle_mod, N, scheme, mass, p=1):
+    tc, m = tgv(N, p=p)
+    dt, n = cases.run_length(tc, m, 0.25, 0.25)
+    o = setup_case(oracle_mod.Oracle, tc, m, make_params(scheme, mass), dt, tc.relaxation_time())
+    o.step(n)
+    return cases.diagnostics(tc, m, o.node_weight(), o.get_populations(), n * dt)["rel_l2_u"]
+
+
+@pytest.mark.parametrize("N,scheme,mass,p,expected", [
+    (32, "bardow", "cg", 1, 5.8e-2),
+    (32, "leelin", "cg", 1, 6.4e-2),
+    (32, "bardow", "lumped", 1, 1.0e-1),
+    (64, "bardow", "lumped", 1, 8.8e-3),
+    (16, "bardow", "cg", 2, 1.7e-2),
+])
+def test_tgv_error_table(oracle_mod, N, scheme, mass, p, expected):
+    """docs/results.md:54-59 (modes (1,4), Re 100, CFL 0.25, t = t_ref/4, Ma 0.05), to the printed digits."""
+    err = _tgv_error(oracle_mod, N, scheme, mass, p)
+    assert float(f"{err:.1e}") == expected, err
+
+
+def test_couette_steady_profile(oracle_mod):
+    """docs/results.md:253-260: the steady linear profile to solver tolerance (16 elements, Re 10, t = 2 L^2/nu)."""
+    tc = cases.CouetteFlow(0.1)
+    tc.set_reynolds(10)
+    m = cases.build_mesh(tc, 16, 1)
+    dt, n = cases.run_length(tc, m, 0.25, 2.0)
+    for scheme in ("bardow", "leelin"):
+        o = setup_case(oracle_mod.Oracle, tc, m, make_params(scheme, "lumped"), dt, tc.relaxation_time())
+        o.step(n)
+        d = cases.diagnostics(tc, m, o.node_weight(), o.get_populations(), n * dt)
+        assert d["rel_l2_u"] < 1e-9, (scheme, d["rel_l2_u"])
+        assert abs(d["mass_drift"]) < 1e-10
+
+
+def test_cg_no_convergence(oracle_mod):
+    """The iteration cap raises NoConvergence (SolverControl, mass.h:38-43)."""
+    tc, m = tgv(8)
+    o = oracle_mod.Oracle(m, make_params(cg_tolerance=1e-14, cg_max_iterations=1))
+    r = np.sin(np.arange(m.n_dofs) * 0.37)
+    r[m.constrained()] = 0
+    with pytest.raises(_abi.NoConvergence):
+        o.mass_solve(r)
+
+
+def test_cg_zero_rhs_zero_iterations(oracle_mod):
+    """A zero right-hand side with a zero start converges at step 0 (tol = 0, |r| = 0)."""
+    tc, m = tgv(8)
+    o = oracle_mod.Oracle(m, make_params())
+    x = o.mass_solve(np.zeros(m.n_dofs))
+    assert np.all(x == 0) and o.cg_iterations() == 0
+
+
+def test_bardow_cavity_conserves_mass(oracle_mod):
+    """Bardow with the wall mass flux removed conserves the mean density to round-off with the lumped mass."""
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    tc.set_reynolds(400)
+    m = cases.build_mesh(tc, 16, 1)
+    o = setup_case(oracle_mod.Oracle, tc, m, make_params("bardow", "lumped"), m.time_step(0.4),
+                   tc.relaxation_time())
+    c0 = o.conservation()
+    o.step(300)
+    c1 = o.conservation()
+    assert abs(c1[1] / c1[0] - c0[1] / c0[0]) < 1e-13
+    assert c1[4] > 0  # the lid has set the fluid in motion
