@@ -1,0 +1,309 @@
+"""Throughput of the lbm-fem hot path on B200.
+
+Workload (default): the Taylor-Green throughput scan -- periodic unit square,
+Q3 elements on 1024 x 1024 cells (3072^2 = 9,437,184 distinct nodes), D2Q9,
+Lee-Lin predictor-corrector, consistent mass solved by Jacobi-PCG to 1e-12,
+Re 100, U0 = 0.05, CFL 0.5, u = U0 sin(2 pi x) cos(2 pi y) with the matching
+pressure, f = feq. Synthetic (analytic) input, state resident in HBM (about
+7 GB, far larger than L2, so no flush is needed between steps).
+
+A step is one Scheme::step of the whole mesh. Metric: Q.DoF updates/s =
+9 x distinct nodes x steps / seconds.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the CPU implementation of the same path on the host
+cores (the deal.II reference cannot be built here; the FP64 oracle port of its
+algorithm, OpenMP on all cores, stands in for it).
+Under torchrun each rank runs an independent replica (the path is not
+sharded across GPUs yet): value = units of all ranks / max-over-ranks time.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "lbm-fem_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Q·DoF updates/s, mixed vs FP64 on 1 B200 at ≤1e-5 rel. L2; % HBM roofline"
+UNIT = "Q·DoF updates/s"
+
+
+def workload(args):
+    from lbfem_gpu import cases, d2q9
+
+    tc = cases.TaylorGreenVortex(0.05 / math.sqrt(d2q9.CS2), 1, 1, shift=(0.25, 0.25), chapman_enskog=False)
+    tc.set_reynolds(100)
+    mesh = cases.build_mesh(tc, args.cells, args.degree)
+    dt, lam = mesh.time_step(0.5), tc.relaxation_time()
+    x, y = mesh.nodes()
+    f0 = tc.initial_populations(x, y, lam)
+    cfg = {
+        "workload": f"taylor-green periodic, Q{args.degree} {args.cells}x{args.cells} cells, "
+                    f"{args.scheme} predictor-corrector, consistent mass (Jacobi-PCG 1e-12)",
+        "degree": args.degree, "cells": args.cells, "nodes_distinct": mesh.n_unique(), "nodes_stored": mesh.n_dofs,
+        "scheme": args.scheme, "mass": "cg", "cg_tolerance": 1e-12, "Re": 100, "U0": 0.05, "cfl": 0.5,
+        "precision": "fp64", "l2": "state > L2 (no flush needed)",
+    }
+    return tc, mesh, dt, lam, f0, cfg
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device, self.proc, self.path = device, None, None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(rows[0][2]),
+                "samples": len(rows), "reasons": reasons}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def allreduce_max(pg, v):
+    if pg is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def cpu_run(tc, mesh, dt, lam, f0, args, budget_s, max_steps):
+    """The FP64 oracle port on the host cores: warm-up 1 step, then steps until budget_s or max_steps."""
+    import oracle
+    from lbfem_gpu import make_params
+
+    threads = oracle.set_threads(os.cpu_count() or 1)
+    h = oracle.Oracle(mesh, make_params(args.scheme, "cg", cg_tolerance=1e-12))
+    h.set_time_step(dt, lam)
+    h.set_initial_populations(f0)
+    h.step(1)
+    n, t0 = 0, time.perf_counter()
+    while n < max_steps:
+        h.step(1)
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    sec = time.perf_counter() - t0
+    h.close()
+    return 9 * mesh.n_unique() * n / sec, n, sec, threads
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args):
+    world, rank, local, pg = dist_setup()
+    if rank != 0:
+        return 0
+    tc, mesh, dt, lam, f0, cfg = workload(args)
+    budget = float(os.environ.get("LBFEM_CPU_BUDGET_S", "150"))
+    value, n, sec, threads = cpu_run(tc, mesh, dt, lam, f0, args, budget, args.steps)
+    sample = (f"{n} Lee-Lin steps of the full {args.cells}x{args.cells} Q{args.degree} mesh after 1 warm-up step "
+              f"(bounded to {budget:.0f} s), CPU FP64 oracle port, {threads} OpenMP threads, {cpu_model()}")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": n,
+            "warmup": 1, "ms_per_step": 1e3 * sec / max(n, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import lbfem_gpu
+    from lbfem_gpu import make_params
+
+    world, rank, local, pg = dist_setup()
+    tc, mesh, dt, lam, f0, cfg = workload(args)
+    lib = lbfem_gpu.library()
+    prm = make_params(args.scheme, "cg", cg_tolerance=1e-12, device=local)
+    h = lbfem_gpu.Solver(mesh, prm)
+    h.set_time_step(dt, lam)
+    h.set_initial_populations(f0)
+    ctx = h.h
+
+    def elapsed(a, b):
+        ms = C.c_float()
+        h._call("event_elapsed", ctx, a, b, C.byref(ms))
+        return ms.value * 1e-3
+
+    # warm-up
+    h.step(args.warmup)
+    lib.lbfem_gpu_synchronize(ctx)
+    barrier(pg)
+    with Clocks(local) as clocks:
+        lib.lbfem_gpu_synchronize(ctx)
+        h._call("event_record", ctx, 0)
+        h.step(args.steps)
+        h._call("event_record", ctx, 1)
+        lib.lbfem_gpu_synchronize(ctx)
+    sec = allreduce_max(pg, elapsed(0, 1))
+    barrier(pg)
+    its, launches = C.c_double(), C.c_int64()
+    h._call("last_step_stats", ctx, C.byref(its), C.byref(launches))
+    units = 9 * mesh.n_unique() * args.steps * world
+    value = units / sec
+
+    # roofline of the streaming kernel (K1), timed alone on the context's stream
+    reps = 10
+    h._call("advection_resident", ctx)
+    lib.lbfem_gpu_synchronize(ctx)
+    h._call("event_record", ctx, 2)
+    for _ in range(reps):
+        h._call("advection_resident", ctx)
+    h._call("event_record", ctx, 3)
+    k1 = elapsed(2, 3) / reps
+    n_reads = 9
+    n_writes = 8 if args.scheme == "leelin" else 17
+    alg_bytes = 8 * mesh.n_dofs * (n_reads + n_writes)
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / k1 / 1e9
+
+    # end to end through the host-buffer C ABI call: upload f, one step, download f
+    n_e2e = max(1, min(args.steps, 5))
+    fbuf_ptr = lib.lbfem_gpu_host_alloc(9 * mesh.n_dofs * 8)
+    fbuf = np.ctypeslib.as_array((C.c_double * (9 * mesh.n_dofs)).from_address(fbuf_ptr))
+    fbuf[:] = h.get_populations().ravel()
+    P = C.POINTER(C.c_double)
+    lib.lbfem_gpu_synchronize(ctx)
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        h._call("step_host", ctx, C.cast(fbuf_ptr, P), 1)
+    e2e_sec = allreduce_max(pg, time.perf_counter() - t0)
+    e2e_value = 9 * mesh.n_unique() * n_e2e * world / e2e_sec
+    lib.lbfem_gpu_host_free(fbuf_ptr)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        budget = float(os.environ.get("LBFEM_CPU_BUDGET_S", "20"))
+        cval, cn, csec, threads = cpu_run(tc, mesh, dt, lam, f0, args, budget, 1000)
+        cpu = {"value": cval, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{cn} step(s) of the full mesh after 1 warm-up step ({csec:.1f} s), CPU FP64 oracle port, "
+                         f"{threads} OpenMP threads, {cpu_model()}"}
+    h.close()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Taylor-Green initial state)",
+        "config": dict(cfg, parallelism=f"replicas x{world}" if world > 1 else "single GPU",
+                       cg_iterations_per_solve=its.value),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": f"k_advection<{args.degree}, {args.scheme} fused>",
+                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": 1e3 * k1,
+                     "peak_kind": f"{peak_kind} copy bandwidth (burst)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 9 * 8 * mesh.n_dofs,
+                "d2h_bytes_per_step": 9 * 8 * mesh.n_dofs, "steps": n_e2e,
+                "call": "lbfem_gpu_step_host (pinned host populations in, one step, populations out)"},
+        "clocks": clocks.summary(),
+        "gpu_launches": int(launches.value),
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=1024)
+    ap.add_argument("--degree", type=int, default=3)
+    ap.add_argument("--scheme", default="leelin", choices=["leelin", "bardow"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    return run_reference(args) if args.impl == "reference" else run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

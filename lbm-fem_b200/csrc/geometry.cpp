@@ -1,0 +1,173 @@
+#include "geometry.h"
+
+#include <cmath>
+
+namespace lbfem_gpu
+{
+  namespace
+  {
+    // Legendre P_n(t) and its derivative (three-term recurrence).
+    long double
+    legendre(int n, long double t, long double *dp)
+    {
+      long double p0 = 1, p1 = t;
+      if (n == 0)
+        {
+          *dp = 0;
+          return 1;
+        }
+      for (int k = 1; k < n; ++k)
+        {
+          const long double p2 = ((2 * k + 1) * t * p1 - k * p0) / (k + 1);
+          p0 = p1;
+          p1 = p2;
+        }
+      *dp = n * (t * p1 - p0) / (t * t - 1);
+      return p1;
+    }
+
+    struct Lagrange
+    {
+      int p;
+      long double x[MAXP + 1];
+      long double
+      value(int a, long double t) const
+      {
+        long double v = 1;
+        for (int b = 0; b <= p; ++b)
+          if (b != a)
+            v *= (t - x[b]) / (x[a] - x[b]);
+        return v;
+      }
+      long double
+      deriv(int a, long double t) const
+      {
+        long double sum = 0;
+        for (int c = 0; c <= p; ++c)
+          {
+            if (c == a)
+              continue;
+            long double v = 1 / (x[a] - x[c]);
+            for (int b = 0; b <= p; ++b)
+              if (b != a && b != c)
+                v *= (t - x[b]) / (x[a] - x[b]);
+            sum += v;
+          }
+        return sum;
+      }
+    };
+  } // namespace
+
+  Basis1D::Basis1D(int p_)
+    : p(p_)
+  {
+    const long double pi = 3.141592653589793238462643383279502884L;
+    Lagrange L{p, {}};
+    // support points: 0, 1 and the roots of P_p' (Newton on P_p' with P_p'')
+    L.x[0] = 0;
+    L.x[p] = 1;
+    for (int k = 1; k < p; ++k)
+      {
+        long double t = -std::cos(pi * k / p);
+        for (int it = 0; it < 100; ++it)
+          {
+            long double dp;
+            const long double v = legendre(p, t, &dp);
+            const long double d2 = (2 * t * dp - p * (p + 1) * v) / (1 - t * t);
+            const long double step = dp / d2;
+            t -= step;
+            if (std::fabs(step) < 1e-19L)
+              break;
+          }
+        L.x[k] = (t + 1) / 2;
+      }
+    // Gauss points (roots of P_{p+1}) and weights on [0,1]
+    const int nq = p + 1;
+    long double qx[MAXP + 1], qw[MAXP + 1];
+    for (int k = 0; k < nq; ++k)
+      {
+        long double t = -std::cos(pi * (k + 0.75L) / (nq + 0.5L));
+        for (int it = 0; it < 100; ++it)
+          {
+            long double dp;
+            const long double v = legendre(nq, t, &dp);
+            const long double step = v / dp;
+            t -= step;
+            if (std::fabs(step) < 1e-19L)
+              break;
+          }
+        long double dp;
+        legendre(nq, t, &dp);
+        qx[k] = (t + 1) / 2;
+        qw[k] = 1 / ((1 - t * t) * dp * dp);
+      }
+    for (int a = 0; a <= p; ++a)
+      {
+        xi[a] = double(L.x[a]);
+        d0[a] = double(L.deriv(a, 0));
+        d1[a] = double(L.deriv(a, 1));
+        for (int b = 0; b <= p; ++b)
+          {
+            long double m = 0, c = 0, k = 0;
+            for (int q = 0; q < nq; ++q)
+              {
+                m += qw[q] * L.value(a, qx[q]) * L.value(b, qx[q]);
+                c += qw[q] * L.value(a, qx[q]) * L.deriv(b, qx[q]);
+                k += qw[q] * L.deriv(a, qx[q]) * L.deriv(b, qx[q]);
+              }
+            Mh[a][b] = double(m);
+            Ch[a][b] = double(c);
+            Kh[a][b] = double(k);
+          }
+      }
+  }
+
+  Axis
+  make_axis(const Basis1D &b, const double *vertex, int n_cells, bool periodic)
+  {
+    Axis ax;
+    const int p = b.p, K = 2 * p + 1;
+    ax.p = p;
+    ax.n_cells = n_cells;
+    ax.periodic = periodic;
+    ax.n_nodes = p * n_cells + 1;
+    ax.n_unique = periodic ? p * n_cells : ax.n_nodes;
+    ax.vertex.assign(vertex, vertex + n_cells + 1);
+    ax.h_first = vertex[1] - vertex[0];
+    ax.h_last = vertex[n_cells] - vertex[n_cells - 1];
+    std::vector<long double> acc(size_t(4) * ax.n_nodes * K, 0.0L);
+    auto at = [&](int m, int i, int k) -> long double & { return acc[(size_t(m) * ax.n_nodes + i) * K + k]; };
+    for (int c = 0; c < n_cells; ++c)
+      {
+        const long double h = (long double)vertex[c + 1] - vertex[c];
+        for (int a = 0; a <= p; ++a)
+          {
+            int i = c * p + a;
+            if (periodic && i == ax.n_unique)
+              i = 0; // the image row is assembled into its source
+            for (int bb = 0; bb <= p; ++bb)
+              {
+                const int k = bb - a + p;
+                at(0, i, k) += h * b.Mh[a][bb];
+                at(1, i, k) += b.Ch[a][bb];
+                at(2, i, k) += b.Ch[bb][a];
+                at(3, i, k) += b.Kh[a][bb] / h;
+              }
+          }
+      }
+    ax.rows.resize(acc.size());
+    for (size_t t = 0; t < acc.size(); ++t)
+      ax.rows[t] = double(acc[t]);
+    ax.diag.assign(ax.n_nodes, 1.0);
+    ax.lump.assign(ax.n_nodes, 1.0);
+    for (int i = 0; i < ax.n_unique; ++i)
+      {
+        long double s = 0;
+        for (int k = 0; k < K; ++k)
+          s += at(0, i, k);
+        ax.diag[i] = double(at(0, i, p));
+        ax.lump[i] = double(s);
+      }
+    return ax;
+  }
+} // namespace lbfem_gpu

@@ -1,0 +1,51 @@
+// Host-side geometry of the tensor-product discretisation: the 1-D FE_Q(p)
+// basis on Gauss-Lobatto points, its exactly integrated reference matrices, and
+// the assembled 1-D operators of one mesh axis.
+//
+// On an axis-parallel cell the 2-D element matrices of the reference factor
+// into 1-D ones (advection.h:6-10, mass.h: M, C_e = int N e.grad N^T,
+// K_e = int (e.grad N)(e.grad N^T)), and so do their assembled forms:
+//
+//   M   = My (x) Mx
+//   C_e = ex My (x) Cx + ey Cy (x) Mx
+//   K_e = ex^2 My (x) Kx + ey^2 Ky (x) Mx + ex ey (Cy (x) Cx^T + Cy^T (x) Cx)
+//
+// with, per axis, M = sum_cells h Mhat, C = sum_cells Chat, K = sum_cells Khat / h
+// (Mhat_ab = int_0^1 l_a l_b, Chat_ab = int_0^1 l_a l_b', Khat_ab = int_0^1 l_a' l_b',
+// exact with the p+1 Gauss points the reference integrates with). Periodic
+// axes wrap (the last node is the image of the first).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace lbfem_gpu
+{
+  constexpr int MAXP = 4;
+
+  struct Basis1D
+  {
+    int p = 1;
+    double xi[MAXP + 1];          // Gauss-Lobatto support points on [0,1]
+    double Mh[MAXP + 1][MAXP + 1]; // int l_a l_b
+    double Ch[MAXP + 1][MAXP + 1]; // int l_a l_b'
+    double Kh[MAXP + 1][MAXP + 1]; // int l_a' l_b'
+    double d0[MAXP + 1], d1[MAXP + 1]; // l_a'(0), l_a'(1)
+    explicit Basis1D(int p);
+  };
+
+  // The assembled 1-D operators of one axis, as rows of 2p+1 coefficients:
+  // row[m][i][k] couples node i to node i+k-p (m: 0 = M, 1 = C, 2 = C^T, 3 = K).
+  struct Axis
+  {
+    int p = 1, n_cells = 0, n_nodes = 0, n_unique = 0;
+    bool periodic = false;
+    std::vector<double> vertex;
+    std::vector<double> rows; // [4][n_nodes][2p+1]
+    std::vector<double> diag; // Jacobi: diagonal of M (images: 1)
+    std::vector<double> lump; // row sums of M (images: 1)
+    double h_first = 0, h_last = 0;
+  };
+
+  Axis make_axis(const Basis1D &b, const double *vertex, int n_cells, bool periodic);
+} // namespace lbfem_gpu

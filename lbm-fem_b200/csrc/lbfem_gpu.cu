@@ -1,0 +1,1059 @@
+// C ABI of the B200 hot path of lbm-fem (include/lbfem_gpu.h): the context,
+// its device buffers, and the launch sequences of Scheme::step and of the
+// operator entry points.
+#include "lbfem_gpu.h"
+
+#include "geometry.h"
+#include "operators.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <utility>
+#include <vector>
+
+using namespace lbfem_gpu;
+
+struct lbfem_gpu_ctx
+{
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[16] = {};
+  lbfem_params prm{};
+  int P = 1;
+  Grid grid{};
+  int64_t n_dofs = 0;
+  bool identity = true;
+  std::unique_ptr<Basis1D> basis;
+  Axis ax, ay;
+  // discretisation on the device
+  double *d_rowx = nullptr, *d_rowy = nullptr, *d_diagx = nullptr, *d_diagy = nullptr, *d_lumpx = nullptr,
+         *d_lumpy = nullptr;
+  uint8_t *d_wall = nullptr;
+  double *d_wall_u = nullptr;
+  long long *d_dof = nullptr; // structured node -> caller DoF
+  int4 *d_bnode = nullptr;
+  int n_bnodes = 0;
+  // state
+  double *d_f[2] = {nullptr, nullptr};
+  int cur = 0;
+  double *d_rhs = nullptr, *d_x[3] = {nullptr, nullptr, nullptr};
+  int x_cur = 0, x_prev = 1, x_new = 2;
+  double *d_r = nullptr, *d_p[2] = {nullptr, nullptr}, *d_v = nullptr;
+  double *d_feq = nullptr, *d_stage = nullptr;
+  double *d_partials = nullptr, *d_sums = nullptr;
+  size_t partial_cap = 0;
+  CgState *d_cg = nullptr;
+  CgState *h_cg = nullptr; // pinned mirror
+  double dt = 0, lambda = 0;
+  bool have_ts = false;
+  int64_t cg_its = 0;
+  double last_its_per_solve = 0;
+  int64_t launches = 0, last_launches = 0;
+  std::string err;
+};
+
+namespace
+{
+  int
+  fail(lbfem_gpu_ctx *c, int status, const char *fmt, ...)
+  {
+    if (c)
+      {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        c->err = buf;
+      }
+    return status;
+  }
+
+#define CK(call)                                                                                          \
+  do                                                                                                      \
+    {                                                                                                     \
+      const cudaError_t e_ = (call);                                                                      \
+      if (e_ != cudaSuccess)                                                                              \
+        return fail(ctx, LBFEM_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    }                                                                                                     \
+  while (0)
+
+#define LAUNCHED()                                                                                        \
+  do                                                                                                      \
+    {                                                                                                     \
+      ++ctx->launches;                                                                                    \
+      CK(cudaGetLastError());                                                                             \
+    }                                                                                                     \
+  while (0)
+
+  Geo
+  geo_of(const lbfem_gpu_ctx *ctx)
+  {
+    return Geo{ctx->grid, ctx->d_rowx, ctx->d_rowy, ctx->d_diagx, ctx->d_diagy, ctx->d_lumpx, ctx->d_lumpy,
+               ctx->d_wall, ctx->d_wall_u};
+  }
+
+  int
+  n_pointwise_blocks(long long N)
+  {
+    const long long b = (N + THREADS - 1) / THREADS;
+    return int(std::max(1LL, std::min(b, 148LL * 8)));
+  }
+
+  template <int P>
+  dim3
+  tile_grid(const Grid &g)
+  {
+    return dim3((g.nfx + Tile<P>::TX - 1) / Tile<P>::TX, (g.nfy + Tile<P>::TY - 1) / Tile<P>::TY);
+  }
+
+  template <typename F>
+  int
+  with_degree(int P, F &&f)
+  {
+    switch (P)
+      {
+        case 1:
+          return f(std::integral_constant<int, 1>());
+        case 2:
+          return f(std::integral_constant<int, 2>());
+        case 3:
+          return f(std::integral_constant<int, 3>());
+        default:
+          return f(std::integral_constant<int, 4>());
+      }
+  }
+
+  template <int P>
+  int
+  set_smem_attributes(lbfem_gpu_ctx *ctx)
+  {
+    CK(cudaFuncSetAttribute(k_advection<P, ADV_TG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            int(advection_smem<P, ADV_TG>())));
+    CK(cudaFuncSetAttribute(k_advection<P, ADV_TG_COLLIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            int(advection_smem<P, ADV_TG_COLLIDE>())));
+    CK(cudaFuncSetAttribute(k_advection<P, ADV_LEELIN_FEQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            int(advection_smem<P, ADV_LEELIN_FEQ>())));
+    CK(cudaFuncSetAttribute(k_advection<P, ADV_LEELIN_FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            int(advection_smem<P, ADV_LEELIN_FUSED>())));
+    CK(cudaFuncSetAttribute(k_mass_vmult<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>())));
+    CK(cudaFuncSetAttribute(k_cg_start<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>())));
+    CK(cudaFuncSetAttribute(k_cg_pv<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>())));
+    return LBFEM_OK;
+  }
+
+  int
+  reduce(lbfem_gpu_ctx *ctx, int n_blocks, int nq)
+  {
+    k_reduce_partials<<<1, 1024, 0, ctx->stream>>>(ctx->d_partials, n_blocks, nq, ctx->d_sums);
+    LAUNCHED();
+    return LBFEM_OK;
+  }
+
+  // --------------------------------------------------- streaming RHS (K1)
+  AdvCoef
+  adv_coef(double a, double b, double c, const double *e, double omega)
+  {
+    AdvCoef ac{};
+    ac.a = a;
+    ac.b = b;
+    ac.c = c;
+    for (int al = 0; al < NM; ++al)
+      {
+        ac.ex[al] = e[2 * (al + 1)];
+        ac.ey[al] = e[2 * (al + 1) + 1];
+      }
+    ac.omega = omega;
+    return ac;
+  }
+
+  const double *
+  d2q9_e()
+  {
+    static const double e[18] = {0, 0, 1, 0, 1, 1, 0, 1, -1, 1, -1, 0, -1, -1, 0, -1, 1, -1};
+    return e;
+  }
+
+  int
+  launch_advection(lbfem_gpu_ctx *ctx, int mode, const double *f, const double *feq, double *fout, double *rhs,
+                   const AdvCoef &ac)
+  {
+    const Geo geo = geo_of(ctx);
+    return with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      const dim3 grid = tile_grid<P>(ctx->grid);
+      switch (mode)
+        {
+          case ADV_TG:
+            k_advection<P, ADV_TG><<<grid, THREADS, advection_smem<P, ADV_TG>(), ctx->stream>>>(geo, f, feq, fout,
+                                                                                               rhs, ac);
+            break;
+          case ADV_TG_COLLIDE:
+            k_advection<P, ADV_TG_COLLIDE>
+              <<<grid, THREADS, advection_smem<P, ADV_TG_COLLIDE>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
+            break;
+          case ADV_LEELIN_FEQ:
+            k_advection<P, ADV_LEELIN_FEQ>
+              <<<grid, THREADS, advection_smem<P, ADV_LEELIN_FEQ>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
+            break;
+          default:
+            k_advection<P, ADV_LEELIN_FUSED>
+              <<<grid, THREADS, advection_smem<P, ADV_LEELIN_FUSED>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
+        }
+      LAUNCHED();
+      return LBFEM_OK;
+    });
+  }
+
+  int
+  launch_wall_faces(lbfem_gpu_ctx *ctx, const double *f, double *rhs, const double *e, double dt, bool remove)
+  {
+    if (ctx->n_bnodes == 0)
+      return LBFEM_OK;
+    FaceCoef fc{};
+    fc.half_dt2 = 0.5 * dt * dt;
+    for (int al = 0; al < NM; ++al)
+      {
+        fc.ex[al] = e[2 * (al + 1)];
+        fc.ey[al] = e[2 * (al + 1) + 1];
+      }
+    fc.remove = remove ? 1 : 0;
+    for (int a = 0; a <= ctx->P; ++a)
+      {
+        fc.d0[a] = ctx->basis->d0[a];
+        fc.d1[a] = ctx->basis->d1[a];
+      }
+    fc.hx0 = ctx->ax.h_first;
+    fc.hx1 = ctx->ax.h_last;
+    fc.hy0 = ctx->ay.h_first;
+    fc.hy1 = ctx->ay.h_last;
+    const Geo geo = geo_of(ctx);
+    return with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      k_wall_faces<P><<<(ctx->n_bnodes + 127) / 128, 128, 0, ctx->stream>>>(geo, f, rhs, ctx->d_bnode,
+                                                                           ctx->n_bnodes, fc);
+      LAUNCHED();
+      return LBFEM_OK;
+    });
+  }
+
+  // ------------------------------------------------------ mass solve (K2-K4)
+  // x_new <- A^{-1} b for nsys systems (extrapolated start or the given x_new).
+  int
+  cg_solve(lbfem_gpu_ctx *ctx, const double *b, double *x_new, const double *x_cur, const double *x_prev,
+           int extrapolate, int nsys, int64_t *its_out)
+  {
+    const Geo geo = geo_of(ctx);
+    const Grid &g = ctx->grid;
+    const double tol = ctx->prm.cg_tolerance;
+    const int max_its = ctx->prm.cg_max_iterations;
+    CK(cudaMemsetAsync(ctx->d_cg, 0, sizeof(CgState), ctx->stream));
+    int n_tiles = 0;
+    int st = with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      const dim3 grid = tile_grid<P>(g);
+      n_tiles = int(grid.x * grid.y);
+      k_cg_start<P><<<grid, THREADS, mass_smem<P>(), ctx->stream>>>(geo, b, x_cur, x_prev, x_new, ctx->d_r,
+                                                                      extrapolate, nsys, ctx->d_partials);
+      LAUNCHED();
+      return LBFEM_OK;
+    });
+    if (st)
+      return st;
+    if ((st = reduce(ctx, n_tiles, 3 * NM)))
+      return st;
+    k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nsys, 0, tol, max_its);
+    LAUNCHED();
+    int pi = 0;
+    const int nb = n_pointwise_blocks(g.N);
+    for (int it = 0;; ++it)
+      {
+        CK(cudaMemcpyAsync(ctx->h_cg, ctx->d_cg, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (ctx->h_cg->n_active == 0)
+          break;
+        st = with_degree(ctx->P, [&](auto PP) -> int {
+          constexpr int P = decltype(PP)::value;
+          k_cg_pv<P><<<tile_grid<P>(g), THREADS, mass_smem<P>(), ctx->stream>>>(
+            geo, ctx->d_r, ctx->d_p[pi], ctx->d_p[1 - pi], ctx->d_v, ctx->d_cg, nsys, ctx->d_partials);
+          LAUNCHED();
+          return LBFEM_OK;
+        });
+        if (st)
+          return st;
+        if ((st = reduce(ctx, n_tiles, NM)))
+          return st;
+        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nsys, 1, tol, max_its);
+        LAUNCHED();
+        pi = 1 - pi;
+        k_cg_update<<<nb, THREADS, 0, ctx->stream>>>(geo, x_new, ctx->d_r, ctx->d_p[pi], ctx->d_v, ctx->d_cg, nsys,
+                                                     ctx->d_partials);
+        LAUNCHED();
+        if ((st = reduce(ctx, nb, 2 * NM)))
+          return st;
+        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nsys, 2, tol, max_its);
+        LAUNCHED();
+      }
+    if (its_out)
+      *its_out = ctx->h_cg->total_its;
+    ctx->cg_its += ctx->h_cg->total_its;
+    if (ctx->h_cg->status == 2)
+      return fail(ctx, LBFEM_ERR_NO_CONVERGENCE, "CG: iteration cap %d reached", max_its);
+    if (ctx->h_cg->status == 3)
+      return fail(ctx, LBFEM_ERR_NONFINITE, "CG: non-finite residual");
+    return LBFEM_OK;
+  }
+
+  int
+  mass_solve_dev(lbfem_gpu_ctx *ctx, const double *b, double *x_new, const double *x_cur, const double *x_prev,
+                 int extrapolate, int nsys, int64_t *its)
+  {
+    if (ctx->prm.mass == LBFEM_MASS_LUMPED)
+      {
+        k_lumped<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), b, x_new, nsys);
+        LAUNCHED();
+        if (its)
+          *its = 0;
+        return LBFEM_OK;
+      }
+    if (ctx->prm.mass != LBFEM_MASS_CG)
+      return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass solve: only cg and lumped are implemented");
+    return cg_solve(ctx, b, x_new, x_cur, x_prev, extrapolate, nsys, its);
+  }
+
+  // ------------------------------------------------------- host <-> device
+  // Copies nb blocks of a caller-numbered host vector into structured device storage.
+  int
+  upload(lbfem_gpu_ctx *ctx, const double *host, double *dst, int nb)
+  {
+    const long long N = ctx->grid.N;
+    if (ctx->identity)
+      {
+        CK(cudaMemcpyAsync(dst, host, sizeof(double) * nb * N, cudaMemcpyHostToDevice, ctx->stream));
+        return LBFEM_OK;
+      }
+    CK(cudaMemcpyAsync(ctx->d_stage, host, sizeof(double) * nb * ctx->n_dofs, cudaMemcpyHostToDevice, ctx->stream));
+    k_gather<<<n_pointwise_blocks(N), THREADS, 0, ctx->stream>>>(ctx->d_stage, ctx->d_dof, dst, N, ctx->n_dofs, nb);
+    LAUNCHED();
+    return LBFEM_OK;
+  }
+
+  int
+  download(lbfem_gpu_ctx *ctx, const double *src, double *host, int nb)
+  {
+    const long long N = ctx->grid.N;
+    if (ctx->identity)
+      {
+        CK(cudaMemcpyAsync(host, src, sizeof(double) * nb * N, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        return LBFEM_OK;
+      }
+    k_scatter<<<n_pointwise_blocks(N), THREADS, 0, ctx->stream>>>(src, ctx->d_dof, ctx->d_stage, N, ctx->n_dofs, nb);
+    LAUNCHED();
+    CK(cudaMemcpyAsync(host, ctx->d_stage, sizeof(double) * nb * ctx->n_dofs, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return LBFEM_OK;
+  }
+
+  // ------------------------------------------------------------ one step
+  int
+  step_once(lbfem_gpu_ctx *ctx, int64_t *its)
+  {
+    const Geo geo = geo_of(ctx);
+    const double dt = ctx->dt, lam = ctx->lambda;
+    const double *e = d2q9_e();
+    const long long N = ctx->grid.N;
+    const int nb = n_pointwise_blocks(N);
+    const int rm = ctx->prm.remove_wall_mass_flux;
+    const bool cg = ctx->prm.mass == LBFEM_MASS_CG;
+    double *f = ctx->d_f[ctx->cur];
+    int st;
+    if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
+      {
+        // Bardow::step (schemes.h:118-124): collide, then stream (streaming.h:88-100)
+        double *g = ctx->d_f[1 - ctx->cur];
+        const AdvCoef ac = adv_coef(-dt, 0., -0.5 * dt * dt, e, dt / (lam + 0.5 * dt));
+        if ((st = launch_advection(ctx, ADV_TG_COLLIDE, f, nullptr, g, ctx->d_rhs, ac)))
+          return st;
+        if ((st = launch_wall_faces(ctx, g, ctx->d_rhs, e, dt, rm < 0 ? true : rm != 0)))
+          return st;
+        double *xn = ctx->d_x[cg ? ctx->x_new : ctx->x_cur];
+        if ((st = mass_solve_dev(ctx, ctx->d_rhs, xn, ctx->d_x[ctx->x_cur], ctx->d_x[ctx->x_prev], 1, NM, its)))
+          return st;
+        if (cg)
+          {
+            const int old_prev = ctx->x_prev;
+            ctx->x_prev = ctx->x_cur;
+            ctx->x_cur = ctx->x_new;
+            ctx->x_new = old_prev;
+          }
+        k_add_increment<<<nb, THREADS, 0, ctx->stream>>>(geo, g, ctx->d_x[ctx->x_cur]);
+        LAUNCHED();
+        ctx->cur = 1 - ctx->cur;
+        return LBFEM_OK;
+      }
+    // LeeLin::step (schemes.h:92-98): equilibria, increment, predictor-corrector
+    const double b = -0.5 * dt * dt / lam;
+    const AdvCoef ac = adv_coef(-dt - b, b, -0.5 * dt * dt, e, 0.);
+    if ((st = launch_advection(ctx, ADV_LEELIN_FUSED, f, nullptr, nullptr, ctx->d_rhs, ac)))
+      return st;
+    if ((st = launch_wall_faces(ctx, f, ctx->d_rhs, e, dt, rm < 0 ? false : rm != 0)))
+      return st;
+    double *xn = ctx->d_x[cg ? ctx->x_new : ctx->x_cur];
+    if ((st = mass_solve_dev(ctx, ctx->d_rhs, xn, ctx->d_x[ctx->x_cur], ctx->d_x[ctx->x_prev], 1, NM, its)))
+      return st;
+    if (cg)
+      {
+        const int old_prev = ctx->x_prev;
+        ctx->x_prev = ctx->x_cur;
+        ctx->x_cur = ctx->x_new;
+        ctx->x_new = old_prev;
+      }
+    k_predictor_corrector<<<nb, THREADS, 0, ctx->stream>>>(geo, f, nullptr, ctx->d_x[ctx->x_cur], dt / lam);
+    LAUNCHED();
+    return LBFEM_OK;
+  }
+
+  int
+  check_ctx(lbfem_gpu_ctx *ctx)
+  {
+    if (!ctx)
+      return LBFEM_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    return LBFEM_OK;
+  }
+} // namespace
+
+extern "C" {
+
+void
+lbfem_gpu_default_params(lbfem_params *p)
+{
+  if (!p)
+    return;
+  p->scheme = LBFEM_SCHEME_BARDOW;
+  p->mass = LBFEM_MASS_CG;
+  p->richardson = 2;
+  p->streaming = LBFEM_STREAMING_TG2;
+  p->precision = LBFEM_PRECISION_FP64;
+  p->cg_max_iterations = 200;
+  p->cg_tolerance = 1e-8;
+  p->remove_wall_mass_flux = -1;
+  p->device = 0;
+}
+
+const char *
+lbfem_gpu_status_string(int s)
+{
+  switch (s)
+    {
+      case LBFEM_OK:
+        return "ok";
+      case LBFEM_ERR_ARG:
+        return "bad argument";
+      case LBFEM_ERR_NO_CONVERGENCE:
+        return "CG did not converge within the iteration cap";
+      case LBFEM_ERR_NONFINITE:
+        return "non-finite value";
+      case LBFEM_ERR_CUDA:
+        return "CUDA error";
+      case LBFEM_ERR_UNSUPPORTED:
+        return "unsupported option";
+      case LBFEM_ERR_TIMEOUT:
+        return "device-side wait timed out";
+      case LBFEM_ERR_STATE:
+        return "call out of order";
+      default:
+        return "unknown status";
+    }
+}
+
+const char *
+lbfem_gpu_last_error(const lbfem_gpu_ctx *ctx)
+{
+  return ctx ? ctx->err.c_str() : "";
+}
+
+int
+lbfem_gpu_device_count(void)
+{
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess)
+    {
+      cudaGetLastError();
+      return 0;
+    }
+  return n;
+}
+
+void *
+lbfem_gpu_host_alloc(size_t bytes)
+{
+  void *p = nullptr;
+  if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess)
+    {
+      cudaGetLastError();
+      return nullptr;
+    }
+  return p;
+}
+
+void
+lbfem_gpu_host_free(void *p)
+{
+  if (p)
+    cudaFreeHost(p);
+}
+
+int
+lbfem_gpu_destroy(lbfem_gpu_ctx *ctx)
+{
+  if (!ctx)
+    return LBFEM_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream)
+    cudaStreamSynchronize(ctx->stream);
+  void *bufs[] = {ctx->d_rowx, ctx->d_rowy, ctx->d_diagx, ctx->d_diagy, ctx->d_lumpx, ctx->d_lumpy, ctx->d_wall,
+                  ctx->d_wall_u, ctx->d_dof, ctx->d_bnode, ctx->d_f[0], ctx->d_f[1], ctx->d_rhs, ctx->d_x[0],
+                  ctx->d_x[1], ctx->d_x[2], ctx->d_r, ctx->d_p[0], ctx->d_p[1], ctx->d_v, ctx->d_feq, ctx->d_stage,
+                  ctx->d_partials, ctx->d_sums, ctx->d_cg};
+  for (void *b : bufs)
+    if (b)
+      cudaFree(b);
+  if (ctx->h_cg)
+    cudaFreeHost(ctx->h_cg);
+  for (auto &e : ctx->ev)
+    if (e)
+      cudaEventDestroy(e);
+  if (ctx->stream)
+    cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ctx **out)
+{
+  if (!m || !prm || !out)
+    return LBFEM_ERR_ARG;
+  *out = nullptr;
+  if (m->degree < 1 || m->degree > MAXP || m->n_cells_x < 1 || m->n_cells_y < 1 || !m->vertex_x || !m->vertex_y)
+    return LBFEM_ERR_ARG;
+  if ((m->periodic_x && m->n_cells_x < 2) || (m->periodic_y && m->n_cells_y < 2))
+    return LBFEM_ERR_ARG;
+  for (int i = 0; i < m->n_cells_x; ++i)
+    if (!(m->vertex_x[i + 1] > m->vertex_x[i]))
+      return LBFEM_ERR_ARG;
+  for (int i = 0; i < m->n_cells_y; ++i)
+    if (!(m->vertex_y[i + 1] > m->vertex_y[i]))
+      return LBFEM_ERR_ARG;
+  if (prm->scheme != LBFEM_SCHEME_BARDOW && prm->scheme != LBFEM_SCHEME_LEELIN)
+    return LBFEM_ERR_ARG;
+  if (prm->streaming != LBFEM_STREAMING_TG2 || prm->precision != LBFEM_PRECISION_FP64 ||
+      (prm->mass != LBFEM_MASS_CG && prm->mass != LBFEM_MASS_LUMPED))
+    return LBFEM_ERR_UNSUPPORTED;
+  if (!(prm->cg_tolerance >= 0) || prm->cg_max_iterations < 1)
+    return LBFEM_ERR_ARG;
+  const int P = m->degree;
+  const int nfx = P * m->n_cells_x + 1, nfy = P * m->n_cells_y + 1;
+  const long long N = (long long)nfx * nfy;
+  if (m->dof_index == nullptr && m->n_dofs != N)
+    return LBFEM_ERR_ARG;
+  if (m->dof_index != nullptr && m->n_dofs != N)
+    return LBFEM_ERR_ARG; // every DoF appears once: n_dofs is the node count
+  if (m->n_walls < 0 || (m->n_walls > 0 && (!m->wall_dof || !m->wall_velocity)))
+    return LBFEM_ERR_ARG;
+
+  auto ctx = new lbfem_gpu_ctx();
+  std::unique_ptr<lbfem_gpu_ctx, int (*)(lbfem_gpu_ctx *)> guard(ctx, lbfem_gpu_destroy);
+  ctx->device = prm->device;
+  ctx->prm = *prm;
+  ctx->P = P;
+  ctx->n_dofs = m->n_dofs;
+  ctx->identity = m->dof_index == nullptr;
+  ctx->grid = Grid{nfx, nfy, m->periodic_x ? nfx - 1 : nfx, m->periodic_y ? nfy - 1 : nfy, m->periodic_x ? 1 : 0,
+                   m->periodic_y ? 1 : 0, N};
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  for (auto &e : ctx->ev)
+    CK(cudaEventCreate(&e));
+  ctx->basis = std::make_unique<Basis1D>(P);
+  ctx->ax = make_axis(*ctx->basis, m->vertex_x, m->n_cells_x, m->periodic_x != 0);
+  ctx->ay = make_axis(*ctx->basis, m->vertex_y, m->n_cells_y, m->periodic_y != 0);
+
+  auto put = [&](double **d, const std::vector<double> &h) -> int {
+    CK(cudaMalloc(d, sizeof(double) * h.size()));
+    CK(cudaMemcpy(*d, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+    return LBFEM_OK;
+  };
+  int st;
+  if ((st = put(&ctx->d_rowx, ctx->ax.rows)) || (st = put(&ctx->d_rowy, ctx->ay.rows)) ||
+      (st = put(&ctx->d_diagx, ctx->ax.diag)) || (st = put(&ctx->d_diagy, ctx->ay.diag)) ||
+      (st = put(&ctx->d_lumpx, ctx->ax.lump)) || (st = put(&ctx->d_lumpy, ctx->ay.lump)))
+    return st;
+
+  // numbering: structured node -> caller DoF, and its inverse for the wall list
+  std::vector<long long> node_of_dof;
+  if (!ctx->identity)
+    {
+      node_of_dof.assign(N, -1);
+      std::vector<long long> dof(m->dof_index, m->dof_index + N);
+      for (long long s = 0; s < N; ++s)
+        {
+          if (dof[s] < 0 || dof[s] >= N || node_of_dof[dof[s]] >= 0)
+            return fail(ctx, LBFEM_ERR_ARG, "dof_index is not a permutation");
+          node_of_dof[dof[s]] = s;
+        }
+      CK(cudaMalloc(&ctx->d_dof, sizeof(long long) * N));
+      CK(cudaMemcpy(ctx->d_dof, dof.data(), sizeof(long long) * N, cudaMemcpyHostToDevice));
+    }
+
+  // walls: one class per distinct velocity
+  if (m->n_walls > 0)
+    {
+      std::vector<uint8_t> cls(N, 0);
+      std::map<std::pair<double, double>, int> classes;
+      std::vector<double> table;
+      for (int64_t k = 0; k < m->n_walls; ++k)
+        {
+          const int64_t d = m->wall_dof[k];
+          if (d < 0 || d >= N)
+            return fail(ctx, LBFEM_ERR_ARG, "wall DoF %lld out of range", (long long)d);
+          const long long s = ctx->identity ? d : node_of_dof[d];
+          const auto key = std::make_pair(m->wall_velocity[2 * k], m->wall_velocity[2 * k + 1]);
+          auto it = classes.find(key);
+          if (it == classes.end())
+            {
+              if (classes.size() >= 255)
+                return fail(ctx, LBFEM_ERR_UNSUPPORTED, "more than 255 distinct wall velocities");
+              it = classes.emplace(key, int(classes.size()) + 1).first;
+              table.push_back(key.first);
+              table.push_back(key.second);
+            }
+          cls[s] = uint8_t(it->second);
+        }
+      CK(cudaMalloc(&ctx->d_wall, N));
+      CK(cudaMemcpy(ctx->d_wall, cls.data(), N, cudaMemcpyHostToDevice));
+      if ((st = put(&ctx->d_wall_u, table)))
+        return st;
+    }
+
+  // boundary nodes of the non-periodic sides (images excluded: their face integrals belong to the source)
+  {
+    std::vector<int4> bn;
+    const Grid &g = ctx->grid;
+    for (int j = 0; j < nfy; ++j)
+      for (int i = 0; i < nfx; ++i)
+        {
+          int sides = 0;
+          if (!g.py && j == 0)
+            sides |= 1;
+          if (!g.py && j == nfy - 1)
+            sides |= 2;
+          if (!g.px && i == 0)
+            sides |= 4;
+          if (!g.px && i == nfx - 1)
+            sides |= 8;
+          const bool image = (g.px && i == g.nux) || (g.py && j == g.nuy);
+          if (sides && !image)
+            bn.push_back(make_int4(i, j, sides, 0));
+        }
+    ctx->n_bnodes = int(bn.size());
+    if (!bn.empty())
+      {
+        CK(cudaMalloc(&ctx->d_bnode, sizeof(int4) * bn.size()));
+        CK(cudaMemcpy(ctx->d_bnode, bn.data(), sizeof(int4) * bn.size(), cudaMemcpyHostToDevice));
+      }
+  }
+
+  // state and scratch
+  auto zeros = [&](double **d, size_t n) -> int {
+    CK(cudaMalloc(d, sizeof(double) * n));
+    CK(cudaMemset(*d, 0, sizeof(double) * n));
+    return LBFEM_OK;
+  };
+  if ((st = zeros(&ctx->d_f[0], Q * N)) || (st = zeros(&ctx->d_f[1], Q * N)) || (st = zeros(&ctx->d_rhs, NM * N)) ||
+      (st = zeros(&ctx->d_x[0], NM * N)) || (st = zeros(&ctx->d_x[1], NM * N)) ||
+      (st = zeros(&ctx->d_x[2], NM * N)) || (st = zeros(&ctx->d_r, NM * N)) || (st = zeros(&ctx->d_p[0], NM * N)) ||
+      (st = zeros(&ctx->d_p[1], NM * N)) || (st = zeros(&ctx->d_v, NM * N)) || (st = zeros(&ctx->d_feq, Q * N)))
+    return st;
+  if (!ctx->identity && (st = zeros(&ctx->d_stage, Q * N)))
+    return st;
+  const long long tiles = (long long)((nfx + 31) / 32) * ((nfy + 15) / 16);
+  ctx->partial_cap = size_t(std::max<long long>(tiles, 148 * 8)) * 3 * NM;
+  if ((st = zeros(&ctx->d_partials, ctx->partial_cap)) || (st = zeros(&ctx->d_sums, 64)))
+    return st;
+  CK(cudaMalloc(&ctx->d_cg, sizeof(CgState)));
+  CK(cudaHostAlloc(&ctx->h_cg, sizeof(CgState), cudaHostAllocDefault));
+  if ((st = with_degree(P, [&](auto PP) -> int { return set_smem_attributes<decltype(PP)::value>(ctx); })))
+    return st;
+  *out = guard.release();
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_set_time_step(lbfem_gpu_ctx *ctx, double dt, double lambda)
+{
+  if (!ctx)
+    return LBFEM_ERR_ARG;
+  if (!(dt > 0) || !(lambda > 0) || !std::isfinite(dt) || !std::isfinite(lambda))
+    return fail(ctx, LBFEM_ERR_ARG, "set_time_step: dt and lambda must be positive");
+  ctx->dt = dt;
+  ctx->lambda = lambda;
+  ctx->have_ts = true;
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_set_populations(lbfem_gpu_ctx *ctx, const double *f)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!f)
+    return fail(ctx, LBFEM_ERR_ARG, "set_populations: null buffer");
+  return upload(ctx, f, ctx->d_f[ctx->cur], Q);
+}
+
+int
+lbfem_gpu_get_populations(lbfem_gpu_ctx *ctx, double *f)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!f)
+    return fail(ctx, LBFEM_ERR_ARG, "get_populations: null buffer");
+  return download(ctx, ctx->d_f[ctx->cur], f, Q);
+}
+
+int
+lbfem_gpu_set_initial_populations(lbfem_gpu_ctx *ctx, const double *f)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!f)
+    return fail(ctx, LBFEM_ERR_ARG, "set_initial_populations: null buffer");
+  if (!ctx->have_ts)
+    return fail(ctx, LBFEM_ERR_STATE, "set_initial_populations needs the time step");
+  if ((st = upload(ctx, f, ctx->d_f[ctx->cur], Q)))
+    return st;
+  const long long N = ctx->grid.N;
+  for (int k = 0; k < 3; ++k)
+    CK(cudaMemsetAsync(ctx->d_x[k], 0, sizeof(double) * NM * N, ctx->stream));
+  if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
+    {
+      k_bardow_transform<<<n_pointwise_blocks(N), THREADS, 0, ctx->stream>>>(geo_of(ctx), ctx->d_f[ctx->cur],
+                                                                             0.5 * ctx->dt / ctx->lambda);
+      LAUNCHED();
+    }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_step(lbfem_gpu_ctx *ctx, int32_t n_steps)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (n_steps < 0)
+    return fail(ctx, LBFEM_ERR_ARG, "step: negative count");
+  if (!ctx->have_ts)
+    return fail(ctx, LBFEM_ERR_STATE, "step needs the time step");
+  const int64_t launches0 = ctx->launches;
+  int64_t its_total = 0;
+  for (int s = 0; s < n_steps; ++s)
+    {
+      int64_t its = 0;
+      if ((st = step_once(ctx, &its)))
+        return st;
+      its_total += its;
+    }
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->last_launches = ctx->launches - launches0;
+  ctx->last_its_per_solve = n_steps > 0 ? double(its_total) / (double(n_steps) * NM) : 0.0;
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_step_host(lbfem_gpu_ctx *ctx, double *f, int32_t n_steps)
+{
+  int st;
+  if ((st = lbfem_gpu_set_populations(ctx, f)))
+    return st;
+  if ((st = lbfem_gpu_step(ctx, n_steps)))
+    return st;
+  return lbfem_gpu_get_populations(ctx, f);
+}
+
+int
+lbfem_gpu_synchronize(lbfem_gpu_ctx *ctx)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_advection(lbfem_gpu_ctx *ctx, const double *f, const double *feq, const double *e, double dt, double lambda,
+                    int32_t kind, int32_t remove, double *rhs)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!f || !e || !rhs || !(dt > 0))
+    return fail(ctx, LBFEM_ERR_ARG, "advection: bad argument");
+  const bool leelin = kind == LBFEM_ADVECTION_LEELIN;
+  if (!leelin && kind != LBFEM_ADVECTION_TAYLOR_GALERKIN)
+    return fail(ctx, LBFEM_ERR_ARG, "advection: unknown kind %d", kind);
+  if (leelin && (!feq || !(lambda > 0)))
+    return fail(ctx, LBFEM_ERR_ARG, "LeeLinAdvection needs the equilibria");
+  double *fs = ctx->d_f[1 - ctx->cur];
+  if ((st = upload(ctx, f, fs, Q)))
+    return st;
+  if (leelin && (st = upload(ctx, feq, ctx->d_feq, Q)))
+    return st;
+  AdvCoef ac;
+  if (leelin)
+    {
+      const double b = -0.5 * dt * dt / lambda;
+      ac = adv_coef(-dt - b, b, -0.5 * dt * dt, e, 0.);
+    }
+  else
+    ac = adv_coef(-dt, 0., -0.5 * dt * dt, e, 0.);
+  if ((st = launch_advection(ctx, leelin ? ADV_LEELIN_FEQ : ADV_TG, fs, ctx->d_feq, nullptr, ctx->d_rhs, ac)))
+    return st;
+  const bool rmv = remove < 0 ? !leelin : remove != 0;
+  if ((st = launch_wall_faces(ctx, fs, ctx->d_rhs, e, dt, rmv)))
+    return st;
+  return download(ctx, ctx->d_rhs, rhs, NM);
+}
+
+int
+lbfem_gpu_advection_resident(lbfem_gpu_ctx *ctx)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!ctx->have_ts)
+    return fail(ctx, LBFEM_ERR_STATE, "advection_resident needs the time step");
+  const double dt = ctx->dt, lam = ctx->lambda;
+  if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
+    return launch_advection(ctx, ADV_TG_COLLIDE, ctx->d_f[ctx->cur], nullptr, ctx->d_f[1 - ctx->cur], ctx->d_rhs,
+                            adv_coef(-dt, 0., -0.5 * dt * dt, d2q9_e(), dt / (lam + 0.5 * dt)));
+  const double b = -0.5 * dt * dt / lam;
+  return launch_advection(ctx, ADV_LEELIN_FUSED, ctx->d_f[ctx->cur], nullptr, nullptr, ctx->d_rhs,
+                          adv_coef(-dt - b, b, -0.5 * dt * dt, d2q9_e(), 0.));
+}
+
+int
+lbfem_gpu_mass_solve(lbfem_gpu_ctx *ctx, double *x, const double *r, const double *, double tg3)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!x || !r)
+    return fail(ctx, LBFEM_ERR_ARG, "mass_solve: null buffer");
+  if (tg3 != 0.)
+    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve: the TG3 left-hand side is not implemented");
+  double *xn = ctx->d_x[ctx->x_new];
+  if ((st = upload(ctx, r, ctx->d_rhs, 1)) || (st = upload(ctx, x, xn, 1)))
+    return st;
+  const int solve_st = mass_solve_dev(ctx, ctx->d_rhs, xn, nullptr, nullptr, 0, 1, nullptr);
+  if (solve_st != LBFEM_OK && solve_st != LBFEM_ERR_NO_CONVERGENCE && solve_st != LBFEM_ERR_NONFINITE)
+    return solve_st;
+  if ((st = download(ctx, xn, x, 1)))
+    return st;
+  return solve_st;
+}
+
+int
+lbfem_gpu_mass_vmult(lbfem_gpu_ctx *ctx, double *y, const double *x)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!x || !y)
+    return fail(ctx, LBFEM_ERR_ARG, "mass_vmult: null buffer");
+  if ((st = upload(ctx, x, ctx->d_r, 1)))
+    return st;
+  const Geo geo = geo_of(ctx);
+  st = with_degree(ctx->P, [&](auto PP) -> int {
+    constexpr int P = decltype(PP)::value;
+    k_mass_vmult<P><<<tile_grid<P>(ctx->grid), THREADS, mass_smem<P>(), ctx->stream>>>(geo, ctx->d_r, ctx->d_v, 1);
+    LAUNCHED();
+    return LBFEM_OK;
+  });
+  if (st)
+    return st;
+  return download(ctx, ctx->d_v, y, 1);
+}
+
+int
+lbfem_gpu_cg_iterations(const lbfem_gpu_ctx *ctx, int64_t *its)
+{
+  if (!ctx || !its)
+    return LBFEM_ERR_ARG;
+  *its = ctx->cg_its;
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_collide_bgk(lbfem_gpu_ctx *ctx, double *g, double omega)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!g)
+    return fail(ctx, LBFEM_ERR_ARG, "collide_bgk: null buffer");
+  double *d = ctx->d_f[1 - ctx->cur];
+  if ((st = upload(ctx, g, d, Q)))
+    return st;
+  k_collide<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), d, omega);
+  LAUNCHED();
+  return download(ctx, d, g, Q);
+}
+
+int
+lbfem_gpu_compute_equilibrium(lbfem_gpu_ctx *ctx, const double *f, double *feq)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!f || !feq)
+    return fail(ctx, LBFEM_ERR_ARG, "compute_equilibrium: null buffer");
+  double *d = ctx->d_f[1 - ctx->cur];
+  if ((st = upload(ctx, f, d, Q)))
+    return st;
+  k_equilibrium<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), d, ctx->d_feq);
+  LAUNCHED();
+  return download(ctx, ctx->d_feq, feq, Q);
+}
+
+int
+lbfem_gpu_predictor_corrector(lbfem_gpu_ctx *ctx, double *f, const double *feq, const double *incr, double theta)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!f || !feq || !incr)
+    return fail(ctx, LBFEM_ERR_ARG, "predictor_corrector: null buffer");
+  double *d = ctx->d_f[1 - ctx->cur];
+  if ((st = upload(ctx, f, d, Q)) || (st = upload(ctx, feq, ctx->d_feq, Q)) || (st = upload(ctx, incr, ctx->d_r, NM)))
+    return st;
+  k_predictor_corrector<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), d, ctx->d_feq,
+                                                                                      ctx->d_r, theta);
+  LAUNCHED();
+  return download(ctx, d, f, Q);
+}
+
+int
+lbfem_gpu_node_weight(lbfem_gpu_ctx *ctx, double *w)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!w)
+    return fail(ctx, LBFEM_ERR_ARG, "node_weight: null buffer");
+  k_diagonal<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), ctx->d_v, 0);
+  LAUNCHED();
+  return download(ctx, ctx->d_v, w, 1);
+}
+
+int
+lbfem_gpu_jacobi_diagonal(lbfem_gpu_ctx *ctx, double *d)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!d)
+    return fail(ctx, LBFEM_ERR_ARG, "jacobi_diagonal: null buffer");
+  k_diagonal<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), ctx->d_v, 1);
+  LAUNCHED();
+  return download(ctx, ctx->d_v, d, 1);
+}
+
+int
+lbfem_gpu_moments(lbfem_gpu_ctx *ctx, double *rho, double *ux, double *uy)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  const long long N = ctx->grid.N;
+  double *d = ctx->d_r; // 3 of its 8 blocks
+  k_moments<<<n_pointwise_blocks(N), THREADS, 0, ctx->stream>>>(geo_of(ctx), ctx->d_f[ctx->cur], d, d + N, d + 2 * N);
+  LAUNCHED();
+  double *outs[3] = {rho, ux, uy};
+  for (int k = 0; k < 3; ++k)
+    if (outs[k] && (st = download(ctx, d + k * N, outs[k], 1)))
+      return st;
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_conservation(lbfem_gpu_ctx *ctx, double out[5])
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!out)
+    return fail(ctx, LBFEM_ERR_ARG, "conservation: null buffer");
+  const int nb = n_pointwise_blocks(ctx->grid.N);
+  k_conservation<<<nb, THREADS, 0, ctx->stream>>>(geo_of(ctx), ctx->d_f[ctx->cur], ctx->d_partials);
+  LAUNCHED();
+  if ((st = reduce(ctx, nb, 5)))
+    return st;
+  CK(cudaMemcpyAsync(out, ctx->d_sums, 5 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_event_record(lbfem_gpu_ctx *ctx, int32_t slot)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (slot < 0 || slot >= 16)
+    return fail(ctx, LBFEM_ERR_ARG, "event slot out of range");
+  CK(cudaEventRecord(ctx->ev[slot], ctx->stream));
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_event_elapsed(lbfem_gpu_ctx *ctx, int32_t a, int32_t b, float *ms)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (a < 0 || a >= 16 || b < 0 || b >= 16 || !ms)
+    return fail(ctx, LBFEM_ERR_ARG, "event slot out of range");
+  CK(cudaEventSynchronize(ctx->ev[b]));
+  CK(cudaEventElapsedTime(ms, ctx->ev[a], ctx->ev[b]));
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_last_step_stats(const lbfem_gpu_ctx *ctx, double *its, int64_t *launches)
+{
+  if (!ctx)
+    return LBFEM_ERR_ARG;
+  if (its)
+    *its = ctx->last_its_per_solve;
+  if (launches)
+    *launches = ctx->last_launches;
+  return LBFEM_OK;
+}
+
+} // extern "C"

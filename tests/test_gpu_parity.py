@@ -1,0 +1,194 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle on the same
+seeded inputs: every operator of the hot path, then whole runs of both schemes.
+FP64 bar: relative L2 <= 1e-12 (rounding order differs; CG stops on the same
+tolerance), element-wise nodal maps <= 1e-14."""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import directions, random_populations, rel_l2, setup_case, tgv, unit_mesh
+from lbfem_gpu import _abi, cases, d2q9, make_params
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu(mesh, params, dof_index=None):
+    import lbfem_gpu
+
+    return lbfem_gpu.Solver(mesh, params, dof_index=dof_index)
+
+
+def _meshes():
+    out = []
+    tc = cases.TaylorGreenVortex(0.05, 1, 4)
+    tc.set_reynolds(100)
+    out.append(("tgv", tc, 1, 12))
+    tc = cases.CouetteFlow(0.1)
+    tc.set_reynolds(10)
+    out.append(("couette", tc, 1, 10))
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    tc.set_reynolds(400)
+    out.append(("cavity", tc, 1, 9))
+    return out
+
+
+MESHES = _meshes()
+
+
+@pytest.mark.parametrize("name,tc,_p,n", MESHES, ids=[m[0] for m in MESHES])
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_nodal_maps(gpu_lib, oracle_mod, name, tc, _p, n, p):
+    m = cases.build_mesh(tc, n, p)
+    f = random_populations(m, seed=p)
+    feq_in = random_populations(m, seed=p + 10)
+    incr = 1e-3 * np.random.default_rng(p).standard_normal((8, m.n_dofs))
+    g, o = _gpu(m, make_params()), oracle_mod.Oracle(m, make_params())
+    for fn, args in (("collide_bgk", (f, 1.3)), ("compute_equilibrium", (f,)),
+                     ("predictor_corrector", (f, feq_in, incr, 0.7))):
+        a, b = getattr(g, fn)(*args), getattr(o, fn)(*args)
+        assert np.max(np.abs(a - b)) <= 1e-14 * np.max(np.abs(b)), (fn, np.max(np.abs(a - b)))
+
+
+@pytest.mark.parametrize("name,tc,_p,n", MESHES, ids=[m[0] for m in MESHES])
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+@pytest.mark.parametrize("kind", ["taylor_galerkin", "leelin"])
+def test_advection(gpu_lib, oracle_mod, name, tc, _p, n, p, kind):
+    m = cases.build_mesh(tc, n, p)
+    f = random_populations(m, seed=3 * p)
+    feq = d2q9.equilibrium(*d2q9.moments(f)) if kind == "leelin" else None
+    dt, lam = m.time_step(0.3), 2e-3
+    g, o = _gpu(m, make_params()), oracle_mod.Oracle(m, make_params())
+    for rm in (-1, 0, 1):
+        a = g.advection(f, directions(), dt, lam, kind=kind, feq=feq, remove_wall_mass_flux=rm)
+        b = o.advection(f, directions(), dt, lam, kind=kind, feq=feq, remove_wall_mass_flux=rm)
+        for al in range(8):
+            assert rel_l2(a[al], b[al]) <= 1e-12, (al, rm, rel_l2(a[al], b[al]))
+        assert np.all(a[:, m.constrained()] == 0)
+
+
+@pytest.mark.parametrize("name,tc,_p,n", MESHES, ids=[m[0] for m in MESHES])
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_mass_operator(gpu_lib, oracle_mod, name, tc, _p, n, p):
+    m = cases.build_mesh(tc, n, p)
+    g, o = _gpu(m, make_params()), oracle_mod.Oracle(m, make_params())
+    assert rel_l2(g.node_weight(), o.node_weight()) <= 1e-14
+    assert rel_l2(g.jacobi_diagonal(), o.jacobi_diagonal()) <= 1e-14
+    x = np.random.default_rng(7).standard_normal(m.n_dofs)
+    assert rel_l2(g.mass_vmult(x), o.mass_vmult(x)) <= 1e-14
+
+
+@pytest.mark.parametrize("name,tc,_p,n", MESHES, ids=[m[0] for m in MESHES])
+@pytest.mark.parametrize("p", [1, 2])
+@pytest.mark.parametrize("mass", ["cg", "lumped"])
+def test_mass_solve(gpu_lib, oracle_mod, name, tc, _p, n, p, mass):
+    m = cases.build_mesh(tc, n, p)
+    prm = make_params(mass=mass, cg_tolerance=1e-13)
+    g, o = _gpu(m, prm), oracle_mod.Oracle(m, prm)
+    rng = np.random.default_rng(11)
+    r = rng.standard_normal(m.n_dofs)
+    r[m.constrained()] = 0
+    x0 = 0.1 * rng.standard_normal(m.n_dofs)
+    x0[m.constrained()] = 0
+    a, b = g.mass_solve(r, x=x0), o.mass_solve(r, x=x0)
+    assert rel_l2(a, b) <= 1e-12
+    assert abs(g.cg_iterations() - o.cg_iterations()) <= 1
+
+
+def test_cg_no_convergence(gpu_lib):
+    tc, m = tgv(8)
+    g = _gpu(m, make_params(cg_tolerance=1e-14, cg_max_iterations=1))
+    r = np.sin(np.arange(m.n_dofs) * 0.37)
+    r[m.constrained()] = 0
+    with pytest.raises(_abi.NoConvergence):
+        g.mass_solve(r)
+
+
+def test_state_and_argument_errors(gpu_lib):
+    tc, m = tgv(8)
+    g = _gpu(m, make_params())
+    with pytest.raises(_abi.LbfemError) as ei:
+        g.set_initial_populations(np.ones((9, m.n_dofs)))
+    assert ei.value.status == _abi.LBFEM_ERR_STATE
+    with pytest.raises(_abi.LbfemError) as ei:
+        g.set_time_step(-1.0, 1.0)
+    assert ei.value.status == _abi.LBFEM_ERR_ARG
+
+
+def _run_pair(oracle_mod, tc, m, prm, dt, steps, lam=None):
+    lam = tc.relaxation_time() if lam is None else lam
+    g = setup_case(_gpu, tc, m, prm, dt, lam)
+    o = setup_case(oracle_mod.Oracle, tc, m, prm, dt, lam)
+    g.step(steps)
+    o.step(steps)
+    return g, o
+
+
+@pytest.mark.parametrize("scheme,mass,case,p,n,steps", [
+    ("bardow", "cg", "tgv", 1, 24, 60),
+    ("leelin", "cg", "tgv", 2, 10, 40),
+    ("bardow", "lumped", "cavity", 2, 8, 80),
+    ("leelin", "cg", "couette", 1, 12, 80),
+    ("bardow", "cg", "cavity", 1, 12, 60),
+    ("leelin", "lumped", "cavity", 3, 5, 40),
+    ("bardow", "cg", "couette", 3, 4, 40),
+])
+def test_step(gpu_lib, oracle_mod, scheme, mass, case, p, n, steps):
+    if case == "tgv":
+        tc = cases.TaylorGreenVortex(0.05, 1, 4)
+        tc.set_reynolds(100)
+    elif case == "couette":
+        tc = cases.CouetteFlow(0.1)
+        tc.set_reynolds(10)
+    else:
+        tc = cases.LidDrivenCavity(0.1, 1.2)
+        tc.set_reynolds(400)
+    m = cases.build_mesh(tc, n, p)
+    prm = make_params(scheme, mass, cg_tolerance=1e-12)
+    g, o = _run_pair(oracle_mod, tc, m, prm, m.time_step(0.3), steps)
+    a, b = g.get_populations(), o.get_populations()
+    assert rel_l2(a, b) <= 1e-12, rel_l2(a, b)
+    if mass == "cg":
+        assert abs(g.cg_iterations() - o.cg_iterations()) <= steps // 10
+    ca, cb = g.conservation(), o.conservation()
+    assert np.allclose(ca, cb, rtol=1e-12, atol=1e-15)
+
+
+def test_tgv_plain_fp64_2000_steps(gpu_lib, oracle_mod):
+    """Periodic TGV, 64 x 64 Q1, Bardow, consistent mass (Jacobi-PCG to 1e-12), Re 100,
+    U0 = 0.05, CFL 0.5 on h, u = U0 sin(2 pi x) cos(2 pi y), f = feq, 2000 steps."""
+    tc = cases.TaylorGreenVortex(0.05 / math.sqrt(d2q9.CS2), 1, 1, shift=(0.25, 0.25), chapman_enskog=False)
+    tc.set_reynolds(100)
+    m = cases.build_mesh(tc, 64, 1)
+    prm = make_params("bardow", "cg", cg_tolerance=1e-12)
+    g, o = _run_pair(oracle_mod, tc, m, prm, m.time_step(0.5), 2000)
+    a, b = g.get_populations(), o.get_populations()
+    err = rel_l2(a, b)
+    assert err <= 1e-12, err
+    ua = d2q9.moments(a[:, m.independent()])
+    ub = d2q9.moments(b[:, m.independent()])
+    assert rel_l2(np.stack(ua[1:]), np.stack(ub[1:])) <= 1e-12
+
+
+def test_dof_permutation(gpu_lib):
+    """A caller numbering (a permutation of the structured nodes) gives the same results."""
+    tc, m = tgv(10, p=2)
+    rng = np.random.default_rng(5)
+    perm = rng.permutation(m.n_dofs).astype(np.int64)  # structured node s -> caller DoF perm[s]
+    prm = make_params("bardow", "cg", cg_tolerance=1e-12)
+    dt, lam = m.time_step(0.25), tc.relaxation_time()
+    x, y = m.nodes()
+    f0 = tc.initial_populations(x, y, lam)
+    ref = _gpu(m, prm)
+    ref.set_time_step(dt, lam)
+    ref.set_initial_populations(f0)
+    ref.step(20)
+    # the same mesh with permuted numbering: walls would also be given by caller DoF
+    g = _gpu(m, prm, dof_index=perm)
+    fc = np.empty_like(f0)
+    fc[:, perm] = f0
+    g.set_time_step(dt, lam)
+    g.set_initial_populations(fc)
+    g.step(20)
+    out = g.get_populations()
+    assert np.array_equal(out[:, perm], ref.get_populations())

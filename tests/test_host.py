@@ -1,0 +1,91 @@
+"""CPU checks of the boundary and the host-side set-up: the C-ABI library loads
+and exports every symbol include/lbfem_gpu.h declares (no compute call needs
+a GPU here), its defaults are the reference's, and the test-case set-up
+(mesh, walls, time step) follows test_cases.h / discretization.h."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from lbfem_gpu import _abi, cases
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "lbfem_gpu.h")).read()
+    return sorted(set(re.findall(r"\b(lbfem_gpu_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    import lbfem_gpu
+
+    lib = lbfem_gpu.library()
+    names = header_functions()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings_and_defaults():
+    import lbfem_gpu
+
+    lib = lbfem_gpu.library()
+    for s in range(8):
+        assert lib.lbfem_gpu_status_string(s)
+    p = _abi.Params()
+    lib.lbfem_gpu_default_params.restype = None
+    lib.lbfem_gpu_default_params(C.byref(p))
+    # MassSettings / StreamingSettings defaults (mass.h:33-48, streaming.h:32-36), Bardow (cgdbe.cc:65)
+    assert (p.scheme, p.mass, p.richardson, p.streaming, p.cg_max_iterations) == (1, 0, 2, 0, 200)
+    assert p.cg_tolerance == 1e-8 and p.remove_wall_mass_flux == -1
+
+
+def test_no_gpu_fails_loudly():
+    import lbfem_gpu
+
+    if lbfem_gpu.device_count() > 0:
+        pytest.skip("a GPU is present")
+    tc = cases.TaylorGreenVortex(0.1, 1, 1)
+    tc.set_reynolds(100)
+    with pytest.raises(_abi.LbfemError) as ei:
+        lbfem_gpu.Solver(cases.build_mesh(tc, 4, 1), lbfem_gpu.make_params())
+    assert ei.value.status == _abi.LBFEM_ERR_CUDA
+
+
+def test_gauss_lobatto_points_match_oracle(oracle_mod):
+    for p in (1, 2, 3, 4):
+        s, _, _ = oracle_mod.basis_1d(p)
+        assert np.allclose(cases.gauss_lobatto(p), s, atol=1e-15)
+
+
+def test_cavity_walls_and_time_step():
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    tc.set_reynolds(400)
+    m = cases.build_mesh(tc, 8, 2)
+    x, y = m.nodes()
+    # every boundary node is a wall; the lid moves except at its corners (test_cases.h:310-323)
+    on = (x < 1e-12) | (x > 1 - 1e-12) | (y < 1e-12) | (y > 1 - 1e-12)
+    assert set(m.wall_dof) == set(np.nonzero(on)[0])
+    moving = m.wall_dof[m.wall_velocity[:, 0] > 0]
+    assert np.all(y[moving] > 1 - 1e-12) and np.all((x[moving] > 1e-12) & (x[moving] < 1 - 1e-12))
+    # h_min is the clustered first cell; dt = cfl h_min / p^2 (discretization.h:158-162)
+    assert abs(m.h_min - (m.vertex_x[1] - m.vertex_x[0])) < 1e-15
+    assert abs(m.time_step(0.4) - 0.4 * m.h_min / 4) < 1e-18
+
+
+def test_couette_walls_include_periodic_images():
+    tc = cases.CouetteFlow(0.1)
+    tc.set_reynolds(10)
+    m = cases.build_mesh(tc, 4, 1)
+    assert len(m.wall_dof) == 2 * m.nfx  # both rows, images included (the reference tags by coordinate)
+    assert m.constrained().sum() == m.nfy
+
+
+def test_run_length_hits_t_end():
+    tc = cases.TaylorGreenVortex(0.05, 1, 4)
+    tc.set_reynolds(100)
+    m = cases.build_mesh(tc, 32, 1)
+    dt, n = cases.run_length(tc, m, 0.25, 0.25)
+    assert n == 166 and abs(n * dt - 0.25 * tc.reference_time()) < 1e-12
