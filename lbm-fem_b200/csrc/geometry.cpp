@@ -160,6 +160,13 @@ namespace lbfem_gpu
       ax.rows[t] = double(acc[t]);
     ax.diag.assign(ax.n_nodes, 1.0);
     ax.lump.assign(ax.n_nodes, 1.0);
+    ax.h.resize(n_cells);
+    ax.hinv.resize(n_cells);
+    for (int c = 0; c < n_cells; ++c)
+      {
+        ax.h[c] = vertex[c + 1] - vertex[c];
+        ax.hinv[c] = 1.0 / ax.h[c];
+      }
     for (int i = 0; i < ax.n_unique; ++i)
       {
         long double s = 0;
@@ -167,6 +174,13 @@ namespace lbfem_gpu
           s += at(0, i, k);
         ax.diag[i] = double(at(0, i, p));
         ax.lump[i] = double(s);
+      }
+    ax.invdiag.resize(ax.n_nodes);
+    ax.invlump.resize(ax.n_nodes);
+    for (int i = 0; i < ax.n_nodes; ++i)
+      {
+        ax.invdiag[i] = 1.0 / ax.diag[i];
+        ax.invlump[i] = 1.0 / ax.lump[i];
       }
     return ax;
   }

@@ -42,8 +42,11 @@ namespace lbfem_gpu
     bool periodic = false;
     std::vector<double> vertex;
     std::vector<double> rows; // [4][n_nodes][2p+1]
-    std::vector<double> diag; // Jacobi: diagonal of M (images: 1)
-    std::vector<double> lump; // row sums of M (images: 1)
+    std::vector<double> diag;    // Jacobi: diagonal of M (images: 1)
+    std::vector<double> lump;    // row sums of M (images: 1)
+    std::vector<double> invdiag; // 1 / diag
+    std::vector<double> invlump; // 1 / lump
+    std::vector<double> h, hinv; // cell widths and their inverses
     double h_first = 0, h_last = 0;
   };
 

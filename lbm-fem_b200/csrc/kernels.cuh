@@ -1,4 +1,4 @@
-// Device kernels of the lbm-fem hot path for sm_100a (FP64 plain path).
+// Device building blocks of the lbm-fem hot path for sm_100a (FP64 plain path).
 //
 // Layout in HBM: structure of arrays, one contiguous array per population
 // (block a of a population vector at [a*N, (a+1)*N)), node (i, j) of the
@@ -8,12 +8,16 @@
 // them from their own values, and the streaming increment there is zero, as
 // in the reference.
 //
-// Operators (see geometry.h): the advection right-hand side and the mass
-// vmult are owner-computes tile stencils. A CTA stages one tile of nodes plus a
-// halo of p nodes in shared memory, applies the assembled 1-D x operators
-// (x pass) and then the y operators (y pass), and writes its own nodes: no
-// scatter, no atomics, deterministic. Reductions are fixed-order (per-CTA
-// partials, then a one-CTA final sum).
+// Tensor-product operators (see geometry.h) are applied by owner-computes
+// tiles. A CTA owns TX x TY nodes (whole cells: TX = p*CX, TY = p*CY) and
+// stages the footprint -- the own nodes, one cell to the left/below and one
+// node to the right/above -- in shared memory. The x pass applies the 1-D
+// element matrices along x for every footprint row; the y pass applies them
+// along y and writes the own nodes. Both passes sweep a run of cells per
+// thread with the element matrices of the reference cell as constant-bank
+// operands, the per-cell widths as the only geometry, and the shared vertex of
+// two cells summed in a register: no scatter, no atomics, deterministic.
+// Reductions are fixed-order: per-CTA partials, then one CTA per quantity.
 #pragma once
 
 #include <cstdint>
@@ -23,21 +27,67 @@ namespace lbfem_gpu
   constexpr int Q = 9;
   constexpr int NM = 8;
   constexpr int THREADS = 256;
-  constexpr int NPART = 16; // max reduction quantities per kernel
+  constexpr int MAXPD = 4;
 
-  // Shape of a tile of nodes per CTA.
+  // Reference 1-D element matrices of FE_Q(p) on [0,1] (exact Gauss integration):
+  // [p-1][0] = int l_a l_b, [1] = int l_a l_b', [2] = int l_a' l_b'.
+  __device__ __constant__ double c_ref[MAXPD][3][MAXPD + 1][MAXPD + 1];
+  enum
+  {
+    OP_M = 0,
+    OP_C = 1,
+    OP_K = 2
+  };
+
+  // Tile shapes: CX x CY cells per CTA; x-pass segments of KX cells, y-pass segments of KY cells.
+  // Constraints: footprint rows TY + p + 1 <= 32 (one warp lane per row in the x pass).
+  template <int P>
+  struct TileShape;
+  template <>
+  struct TileShape<1>
+  {
+    static constexpr int CX = 64, CY = 24, KX = 8, KY = 6;
+  };
+  template <>
+  struct TileShape<2>
+  {
+    static constexpr int CX = 32, CY = 12, KX = 4, KY = 3;
+  };
+  template <>
+  struct TileShape<3>
+  {
+    static constexpr int CX = 21, CY = 8, KX = 3, KY = 2;
+  };
+  template <>
+  struct TileShape<4>
+  {
+    static constexpr int CX = 15, CY = 6, KX = 3, KY = 2;
+  };
+
   template <int P>
   struct Tile
   {
-    static constexpr int TX = 32, TY = 16;
-    static constexpr int HX = TX + 2 * P, HY = TY + 2 * P, HN = HX * HY;
-    static constexpr int K = 2 * P + 1;
+    static constexpr int CX = TileShape<P>::CX, CY = TileShape<P>::CY;
+    static constexpr int KX = TileShape<P>::KX, KY = TileShape<P>::KY;
+    static constexpr int TX = P * CX, TY = P * CY;         // own nodes
+    static constexpr int FX = TX + P + 1, FY = TY + P + 1; // footprint
+    static constexpr int PF = FX | 1;                      // odd row pitch: conflict-free column access
+    static constexpr int PY = TX | 1;                      // row pitch of the x-pass outputs
+    static constexpr int SX = P * KX, SY = P * KY;         // segment lengths (nodes)
+    static constexpr int NSX = TX / SX, NSY = TY / SY;     // segments per row / column
+    static constexpr int NF = PF * FY;                     // doubles of one staged field
+    static constexpr int NY = PY * FY;                     // doubles of one x-pass output array
+    static constexpr int YL = (TX + 31) / 32 * 32;         // y-pass lanes per segment row
+    static_assert(FY <= 32, "footprint rows must fit one warp");
+    static_assert(TX % SX == 0 && TY % SY == 0, "segments must tile the own nodes");
+    static_assert(NSX * 32 <= THREADS && NSY * YL <= THREADS, "one pass round per CTA");
   };
 
   struct Grid
   {
     int nfx, nfy; // nodes per axis, images included
     int nux, nuy; // distinct nodes per axis (the wrap modulus of a periodic axis)
+    int ncx, ncy; // cells per axis
     int px, py;
     long long N;
   };
@@ -46,10 +96,13 @@ namespace lbfem_gpu
   struct Geo
   {
     Grid g;
-    const double *rowx, *rowy;   // [4][n][2p+1]: M, C, C^T, K
-    const double *diagx, *diagy; // Jacobi diagonal per axis
-    const double *lumpx, *lumpy; // lumped diagonal per axis
-    const uint8_t *wall;         // per node: 0 fluid, k > 0 wall with velocity wall_u[2(k-1)..]; may be null
+    const double *hx, *hxi, *hy, *hyi;   // cell widths and their inverses
+    const double *ijx, *ijy;             // inverse Jacobi diagonal per axis (1 on images)
+    const double *ilx, *ily;             // inverse lumped diagonal per axis (1 on images)
+    const double *lumpx, *lumpy;         // lumped diagonal per axis (node weights)
+    const double *diagx, *diagy;         // Jacobi diagonal per axis
+    const double *rowx, *rowy;           // assembled 1-D rows [4][n][2p+1] (M, C, C^T, K), wall faces
+    const uint8_t *wall;                 // per node: 0 fluid, k > 0 wall with velocity wall_u[2(k-1)..]; may be null
     const double *wall_u;
   };
 
@@ -75,14 +128,6 @@ namespace lbfem_gpu
   is_image(int i, int j, const Grid &g)
   {
     return (g.px && i == g.nux) || (g.py && j == g.nuy);
-  }
-
-  __device__ __forceinline__ double
-  inv_jacobi(int i, int j, const Geo &geo)
-  {
-    if (is_image(i, j, geo.g))
-      return 1.0;
-    return 1.0 / (geo.diagx[i] * geo.diagy[j]);
   }
 
   struct Mom
@@ -116,34 +161,34 @@ namespace lbfem_gpu
 
   // What a node imposes on its moments (collision.h:53-72).
   __device__ __forceinline__ Mom
-  impose(Mom m, long long idx, const Geo &geo)
+  impose_class(Mom m, int k, const Geo &geo)
   {
-    if (geo.wall)
+    if (k)
       {
-        const int k = geo.wall[idx];
-        if (k)
-          {
-            m.ux = geo.wall_u[2 * (k - 1)];
-            m.uy = geo.wall_u[2 * (k - 1) + 1];
-          }
+        m.ux = geo.wall_u[2 * (k - 1)];
+        m.uy = geo.wall_u[2 * (k - 1) + 1];
       }
     return m;
   }
 
+  __device__ __forceinline__ Mom
+  impose(Mom m, long long idx, const Geo &geo)
+  {
+    return geo.wall ? impose_class(m, geo.wall[idx], geo) : m;
+  }
+
   // ---------------------------------------------------- fixed-order reductions
-  // Sums v[0..nq) over the CTA (warp shuffles, then warp 0) and stores the CTA
-  // totals at partials[q * gridDim + block].
+  // Sums v[0..NQ) over the CTA (warp shuffles, then warp 0) and stores the CTA
+  // totals at partials[q * n_blocks + block].
   template <int NQ>
   __device__ __forceinline__ void
-  block_reduce_store(double (&v)[NQ], int nq, double *partials, int block, int n_blocks)
+  block_reduce_store(double (&v)[NQ], double *partials, int block, int n_blocks)
   {
     __shared__ double warp_sum[NQ][THREADS / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < NQ; ++q)
       {
-        if (q >= nq)
-          break;
         double s = v[q];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
@@ -154,7 +199,8 @@ namespace lbfem_gpu
     __syncthreads();
     if (warp == 0)
       {
-        for (int q = 0; q < nq; ++q)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
           {
             double s = lane < THREADS / 32 ? warp_sum[q][lane] : 0.0;
 #pragma unroll
@@ -167,95 +213,200 @@ namespace lbfem_gpu
     __syncthreads();
   }
 
-  // One CTA of 1024 threads: out[q] = sum_b partials[q * n_blocks + b], in a fixed order.
+  // One CTA per quantity q: out[q] = sum_b partials[q * n_blocks + b], in a fixed order.
   __global__ void
-  k_reduce_partials(const double *__restrict__ partials, int n_blocks, int nq, double *__restrict__ out)
+  k_reduce_partials(const double *__restrict__ partials, int n_blocks, double *__restrict__ out)
   {
     __shared__ double red[32];
+    const int q = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int q = 0; q < nq; ++q)
+    double s = 0;
+    for (int b = threadIdx.x; b < n_blocks; b += blockDim.x)
+      s += partials[(long long)q * n_blocks + b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+      s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0)
+      red[warp] = s;
+    __syncthreads();
+    if (warp == 0)
       {
-        double s = 0;
-        for (int b = threadIdx.x; b < n_blocks; b += blockDim.x)
-          s += partials[(long long)q * n_blocks + b];
+        s = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
           s += __shfl_down_sync(0xffffffffu, s, o);
         if (lane == 0)
-          red[warp] = s;
-        __syncthreads();
-        if (warp == 0)
-          {
-            s = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-              s += __shfl_down_sync(0xffffffffu, s, o);
-            if (lane == 0)
-              out[q] = s;
-          }
-        __syncthreads();
+          out[q] = s;
       }
   }
 
-  // ------------------------------------------------------------ tile helpers
+  // ------------------------------------------------------------ tile staging
+  // Per-CTA tables of the footprint: source column and row offset of every
+  // footprint column/row (-1 outside a non-periodic domain), the widths of the
+  // CX+1 / CY+1 footprint cells and their inverses (0 outside the domain).
   template <int P>
-  __device__ __forceinline__ void
-  load_rows(double *s_row, const double *__restrict__ rows, int g0, int n_own, int n_nodes)
+  struct TileMaps
   {
-    constexpr int K = 2 * P + 1;
-    for (int t = threadIdx.x; t < 4 * n_own * K; t += blockDim.x)
-      {
-        const int m = t / (n_own * K), r = t - m * n_own * K, i = r / K, k = r - i * K;
-        const int gi = g0 + i;
-        s_row[t] = gi < n_nodes ? rows[((long long)m * n_nodes + gi) * K + k] : 0.0;
-      }
-  }
+    int col[Tile<P>::FX];
+    int rowi[Tile<P>::FY];
+    long long row[Tile<P>::FY];
+    double hx[Tile<P>::CX + 1], hxi[Tile<P>::CX + 1], cx[Tile<P>::CX + 1];
+    double hy[Tile<P>::CY + 1], hyi[Tile<P>::CY + 1], cy[Tile<P>::CY + 1];
+  };
 
-  // s[ly][lx] <- src at grid (gx0 - P + lx, gy0 - P + ly), images read their source, outside 0.
   template <int P>
   __device__ __forceinline__ void
-  load_tile(double *s, const double *__restrict__ src, const Grid &g, int gx0, int gy0)
+  build_maps(TileMaps<P> &m, const Geo &geo, int gx0, int gy0)
   {
     using T = Tile<P>;
-    for (int t = threadIdx.x; t < T::HN; t += blockDim.x)
+    const Grid &g = geo.g;
+    for (int t = threadIdx.x; t < T::FX; t += blockDim.x)
+      m.col[t] = wrap(gx0 - P + t, g.px, g.nux, g.nfx);
+    for (int t = threadIdx.x; t < T::FY; t += blockDim.x)
       {
-        const int ly = t / T::HX, lx = t - ly * T::HX;
-        const int sx = wrap(gx0 - P + lx, g.px, g.nux, g.nfx), sy = wrap(gy0 - P + ly, g.py, g.nuy, g.nfy);
-        s[t] = (sx >= 0 && sy >= 0) ? src[(long long)sy * g.nfx + sx] : 0.0;
+        const int r = wrap(gy0 - P + t, g.py, g.nuy, g.nfy);
+        m.rowi[t] = r;
+        m.row[t] = r < 0 ? -1 : (long long)r * g.nfx;
+      }
+    const int cx0 = gx0 / P - 1, cy0 = gy0 / P - 1;
+    for (int t = threadIdx.x; t <= T::CX; t += blockDim.x)
+      {
+        const int c = wrap(cx0 + t, g.px, g.ncx, g.ncx);
+        m.hx[t] = c < 0 ? 0.0 : geo.hx[c];
+        m.hxi[t] = c < 0 ? 0.0 : geo.hxi[c];
+        m.cx[t] = c < 0 ? 0.0 : 1.0;
+      }
+    for (int t = threadIdx.x; t <= T::CY; t += blockDim.x)
+      {
+        const int c = wrap(cy0 + t, g.py, g.ncy, g.ncy);
+        m.hy[t] = c < 0 ? 0.0 : geo.hy[c];
+        m.hyi[t] = c < 0 ? 0.0 : geo.hyi[c];
+        m.cy[t] = c < 0 ? 0.0 : 1.0;
       }
   }
 
-  // out[lyo][lxo] = sum_k rowy[lyo][k] * (sum_k' rowx[lxo][k'] * s[lyo + k][lxo + k']) : the
-  // tensor-product operator My (x) Mx (m = 0) or another (mx, my) pair, for all own nodes.
-  // s_t is scratch of HY * TX.
-  template <int P>
+  // s[fy*PF + fx] <- op(storage index) over the footprint (0 outside the domain).
+  template <int P, typename F>
   __device__ __forceinline__ void
-  xpass(const double *s, const double *s_rx, double *s_t)
+  stage(double *s, const TileMaps<P> &m, F &&value_at)
   {
     using T = Tile<P>;
-    for (int t = threadIdx.x; t < T::HY * T::TX; t += blockDim.x)
+    for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
       {
-        const int ly = t / T::TX, lxo = t - ly * T::TX;
-        const double *row = s_rx + lxo * T::K;
-        const double *u = s + ly * T::HX + lxo;
-        double acc = 0;
-#pragma unroll
-        for (int k = 0; k < T::K; ++k)
-          acc += row[k] * u[k];
-        s_t[t] = acc;
+        const int fy = t / T::FX, fx = t - fy * T::FX;
+        const long long r = m.row[fy];
+        const int c = m.col[fx];
+        s[fy * T::PF + fx] = (r >= 0 && c >= 0) ? value_at(r + c) : 0.0;
       }
   }
 
+  // s[i*TX + j] <- src at own node (gx0 + j, gy0 + i) of the tile (0 past the grid).
   template <int P>
+  __device__ __forceinline__ void
+  stage_own(double *s, const double *__restrict__ src, const Grid &g, int gx0, int gy0)
+  {
+    using T = Tile<P>;
+    for (int t = threadIdx.x; t < T::TY * T::TX; t += blockDim.x)
+      {
+        const int i = t / T::TX, j = t - i * T::TX;
+        const int gx = gx0 + j, gy = gy0 + i;
+        s[t] = (gx < g.nfx && gy < g.nfy) ? src[(long long)gy * g.nfx + gx] : 0.0;
+      }
+  }
+
+  // y[a] = sum_b R[a][b] u[b] for the reference element matrix OP.
+  template <int P, int OP>
+  __device__ __forceinline__ void
+  elem(const double (&u)[P + 1], double (&y)[P + 1])
+  {
+#pragma unroll
+    for (int a = 0; a <= P; ++a)
+      {
+        double s = c_ref[P - 1][OP][a][0] * u[0];
+#pragma unroll
+        for (int b = 1; b <= P; ++b)
+          s = fma(c_ref[P - 1][OP][a][b], u[b], s);
+        y[a] = s;
+      }
+  }
+
+  // The last row (right vertex) only.
+  template <int P, int OP>
   __device__ __forceinline__ double
-  ypass_at(const double *s_t, const double *s_ry, int lyo, int lxo)
+  elem_last(const double (&u)[P + 1])
+  {
+    double s = c_ref[P - 1][OP][P][0] * u[0];
+#pragma unroll
+    for (int b = 1; b <= P; ++b)
+      s = fma(c_ref[P - 1][OP][P][b], u[b], s);
+    return s;
+  }
+
+  // The x pass of a mass-type operator (OP_M with the cell width as scale) on one
+  // footprint row and one x segment: out[fy*PY + j] for the segment's own columns j.
+  template <int P>
+  __device__ __forceinline__ void
+  mass_xpass(const double *__restrict__ s, double *__restrict__ out, const TileMaps<P> &m, int fy, int seg)
   {
     using T = Tile<P>;
-    const double *row = s_ry + lyo * T::K;
-    double acc = 0;
+    const double *row = s + fy * T::PF;
+    double *orow = out + fy * T::PY;
+    const int q0 = seg * T::KX; // halo cell (footprint cell index)
+    double u[P + 1];
 #pragma unroll
-    for (int k = 0; k < T::K; ++k)
-      acc += row[k] * s_t[(lyo + k) * T::TX + lxo];
-    return acc;
+    for (int b = 0; b <= P; ++b)
+      u[b] = row[q0 * P + b];
+    double pend = m.hx[q0] * elem_last<P, OP_M>(u);
+#pragma unroll
+    for (int q = 1; q <= T::KX; ++q)
+      {
+        const int qc = q0 + q;
+        u[0] = u[P];
+#pragma unroll
+        for (int b = 1; b <= P; ++b)
+          u[b] = row[qc * P + b];
+        double y[P + 1];
+        elem<P, OP_M>(u, y);
+        const double sc = m.hx[qc];
+        const int j0 = (qc - 1) * P;
+        orow[j0] = fma(sc, y[0], pend);
+#pragma unroll
+        for (int a = 1; a < P; ++a)
+          orow[j0 + a] = sc * y[a];
+        pend = sc * y[P];
+      }
+  }
+
+  // The y pass of a mass-type operator on column j and y segment seg: calls
+  // emit(own row i, value) for the segment's SY own rows.
+  template <int P, typename Emit>
+  __device__ __forceinline__ void
+  mass_ypass(const double *__restrict__ t, const TileMaps<P> &m, int j, int seg, Emit &&emit)
+  {
+    using T = Tile<P>;
+    const int q0 = seg * T::KY;
+    double u[P + 1];
+#pragma unroll
+    for (int b = 0; b <= P; ++b)
+      u[b] = t[(q0 * P + b) * T::PY + j];
+    double pend = m.hy[q0] * elem_last<P, OP_M>(u);
+#pragma unroll
+    for (int q = 1; q <= T::KY; ++q)
+      {
+        const int qc = q0 + q;
+        u[0] = u[P];
+#pragma unroll
+        for (int b = 1; b <= P; ++b)
+          u[b] = t[(qc * P + b) * T::PY + j];
+        double y[P + 1];
+        elem<P, OP_M>(u, y);
+        const double sc = m.hy[qc];
+        const int i0 = (qc - 1) * P;
+        emit(i0, fma(sc, y[0], pend));
+#pragma unroll
+        for (int a = 1; a < P; ++a)
+          emit(i0 + a, sc * y[a]);
+        pend = sc * y[P];
+      }
   }
 } // namespace lbfem_gpu

@@ -36,6 +36,8 @@ struct lbfem_gpu_ctx
   // discretisation on the device
   double *d_rowx = nullptr, *d_rowy = nullptr, *d_diagx = nullptr, *d_diagy = nullptr, *d_lumpx = nullptr,
          *d_lumpy = nullptr;
+  double *d_hx = nullptr, *d_hxi = nullptr, *d_hy = nullptr, *d_hyi = nullptr, *d_ijx = nullptr, *d_ijy = nullptr,
+         *d_ilx = nullptr, *d_ily = nullptr;
   uint8_t *d_wall = nullptr;
   double *d_wall_u = nullptr;
   long long *d_dof = nullptr; // structured node -> caller DoF
@@ -97,8 +99,25 @@ namespace
   Geo
   geo_of(const lbfem_gpu_ctx *ctx)
   {
-    return Geo{ctx->grid, ctx->d_rowx, ctx->d_rowy, ctx->d_diagx, ctx->d_diagy, ctx->d_lumpx, ctx->d_lumpy,
-               ctx->d_wall, ctx->d_wall_u};
+    Geo g{};
+    g.g = ctx->grid;
+    g.hx = ctx->d_hx;
+    g.hxi = ctx->d_hxi;
+    g.hy = ctx->d_hy;
+    g.hyi = ctx->d_hyi;
+    g.ijx = ctx->d_ijx;
+    g.ijy = ctx->d_ijy;
+    g.ilx = ctx->d_ilx;
+    g.ily = ctx->d_ily;
+    g.lumpx = ctx->d_lumpx;
+    g.lumpy = ctx->d_lumpy;
+    g.diagx = ctx->d_diagx;
+    g.diagy = ctx->d_diagy;
+    g.rowx = ctx->d_rowx;
+    g.rowy = ctx->d_rowy;
+    g.wall = ctx->d_wall;
+    g.wall_u = ctx->d_wall_u;
+    return g;
   }
 
   int
@@ -145,15 +164,16 @@ namespace
     CK(cudaFuncSetAttribute(k_advection<P, ADV_LEELIN_FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             int(advection_smem<P, ADV_LEELIN_FUSED>())));
     CK(cudaFuncSetAttribute(k_mass_vmult<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>())));
-    CK(cudaFuncSetAttribute(k_cg_start<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>())));
-    CK(cudaFuncSetAttribute(k_cg_pv<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>())));
+    CK(cudaFuncSetAttribute(k_cg_start<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>(1))));
+    CK(cudaFuncSetAttribute(k_cg_p<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>())));
+    CK(cudaFuncSetAttribute(k_cg_update<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>(2))));
     return LBFEM_OK;
   }
 
   int
   reduce(lbfem_gpu_ctx *ctx, int n_blocks, int nq)
   {
-    k_reduce_partials<<<1, 1024, 0, ctx->stream>>>(ctx->d_partials, n_blocks, nq, ctx->d_sums);
+    k_reduce_partials<<<nq, 256, 0, ctx->stream>>>(ctx->d_partials, n_blocks, ctx->d_sums);
     LAUNCHED();
     return LBFEM_OK;
   }
@@ -259,10 +279,11 @@ namespace
     int n_tiles = 0;
     int st = with_degree(ctx->P, [&](auto PP) -> int {
       constexpr int P = decltype(PP)::value;
-      const dim3 grid = tile_grid<P>(g);
+      dim3 grid = tile_grid<P>(g);
       n_tiles = int(grid.x * grid.y);
-      k_cg_start<P><<<grid, THREADS, mass_smem<P>(), ctx->stream>>>(geo, b, x_cur, x_prev, x_new, ctx->d_r,
-                                                                      extrapolate, nsys, ctx->d_partials);
+      grid.z = nsys;
+      k_cg_start<P><<<grid, THREADS, mass_smem<P>(1), ctx->stream>>>(geo, b, x_cur, x_prev, x_new, ctx->d_r,
+                                                                      extrapolate, ctx->d_partials);
       LAUNCHED();
       return LBFEM_OK;
     });
@@ -273,7 +294,6 @@ namespace
     k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nsys, 0, tol, max_its);
     LAUNCHED();
     int pi = 0;
-    const int nb = n_pointwise_blocks(g.N);
     for (int it = 0;; ++it)
       {
         CK(cudaMemcpyAsync(ctx->h_cg, ctx->d_cg, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
@@ -282,8 +302,10 @@ namespace
           break;
         st = with_degree(ctx->P, [&](auto PP) -> int {
           constexpr int P = decltype(PP)::value;
-          k_cg_pv<P><<<tile_grid<P>(g), THREADS, mass_smem<P>(), ctx->stream>>>(
-            geo, ctx->d_r, ctx->d_p[pi], ctx->d_p[1 - pi], ctx->d_v, ctx->d_cg, nsys, ctx->d_partials);
+          dim3 grid = tile_grid<P>(g);
+          grid.z = nsys;
+          k_cg_p<P><<<grid, THREADS, mass_smem<P>(), ctx->stream>>>(geo, ctx->d_r, ctx->d_p[pi], ctx->d_p[1 - pi],
+                                                                     ctx->d_cg, ctx->d_partials);
           LAUNCHED();
           return LBFEM_OK;
         });
@@ -294,10 +316,18 @@ namespace
         k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nsys, 1, tol, max_its);
         LAUNCHED();
         pi = 1 - pi;
-        k_cg_update<<<nb, THREADS, 0, ctx->stream>>>(geo, x_new, ctx->d_r, ctx->d_p[pi], ctx->d_v, ctx->d_cg, nsys,
-                                                     ctx->d_partials);
-        LAUNCHED();
-        if ((st = reduce(ctx, nb, 2 * NM)))
+        st = with_degree(ctx->P, [&](auto PP) -> int {
+          constexpr int P = decltype(PP)::value;
+          dim3 grid = tile_grid<P>(g);
+          grid.z = nsys;
+          k_cg_update<P><<<grid, THREADS, mass_smem<P>(2), ctx->stream>>>(geo, x_new, ctx->d_r, ctx->d_p[pi],
+                                                                          ctx->d_cg, ctx->d_partials);
+          LAUNCHED();
+          return LBFEM_OK;
+        });
+        if (st)
+          return st;
+        if ((st = reduce(ctx, n_tiles, 2 * NM)))
           return st;
         k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nsys, 2, tol, max_its);
         LAUNCHED();
@@ -521,7 +551,8 @@ lbfem_gpu_destroy(lbfem_gpu_ctx *ctx)
   cudaSetDevice(ctx->device);
   if (ctx->stream)
     cudaStreamSynchronize(ctx->stream);
-  void *bufs[] = {ctx->d_rowx, ctx->d_rowy, ctx->d_diagx, ctx->d_diagy, ctx->d_lumpx, ctx->d_lumpy, ctx->d_wall,
+  void *bufs[] = {ctx->d_hx, ctx->d_hxi, ctx->d_hy, ctx->d_hyi, ctx->d_ijx, ctx->d_ijy, ctx->d_ilx, ctx->d_ily,
+                  ctx->d_rowx, ctx->d_rowy, ctx->d_diagx, ctx->d_diagy, ctx->d_lumpx, ctx->d_lumpy, ctx->d_wall,
                   ctx->d_wall_u, ctx->d_dof, ctx->d_bnode, ctx->d_f[0], ctx->d_f[1], ctx->d_rhs, ctx->d_x[0],
                   ctx->d_x[1], ctx->d_x[2], ctx->d_r, ctx->d_p[0], ctx->d_p[1], ctx->d_v, ctx->d_feq, ctx->d_stage,
                   ctx->d_partials, ctx->d_sums, ctx->d_cg};
@@ -579,8 +610,15 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
   ctx->P = P;
   ctx->n_dofs = m->n_dofs;
   ctx->identity = m->dof_index == nullptr;
-  ctx->grid = Grid{nfx, nfy, m->periodic_x ? nfx - 1 : nfx, m->periodic_y ? nfy - 1 : nfy, m->periodic_x ? 1 : 0,
-                   m->periodic_y ? 1 : 0, N};
+  ctx->grid = Grid{nfx,
+                   nfy,
+                   m->periodic_x ? nfx - 1 : nfx,
+                   m->periodic_y ? nfy - 1 : nfy,
+                   m->n_cells_x,
+                   m->n_cells_y,
+                   m->periodic_x ? 1 : 0,
+                   m->periodic_y ? 1 : 0,
+                   N};
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   for (auto &e : ctx->ev)
@@ -597,8 +635,29 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
   int st;
   if ((st = put(&ctx->d_rowx, ctx->ax.rows)) || (st = put(&ctx->d_rowy, ctx->ay.rows)) ||
       (st = put(&ctx->d_diagx, ctx->ax.diag)) || (st = put(&ctx->d_diagy, ctx->ay.diag)) ||
-      (st = put(&ctx->d_lumpx, ctx->ax.lump)) || (st = put(&ctx->d_lumpy, ctx->ay.lump)))
+      (st = put(&ctx->d_lumpx, ctx->ax.lump)) || (st = put(&ctx->d_lumpy, ctx->ay.lump)) ||
+      (st = put(&ctx->d_hx, ctx->ax.h)) || (st = put(&ctx->d_hxi, ctx->ax.hinv)) || (st = put(&ctx->d_hy, ctx->ay.h)) ||
+      (st = put(&ctx->d_hyi, ctx->ay.hinv)) || (st = put(&ctx->d_ijx, ctx->ax.invdiag)) ||
+      (st = put(&ctx->d_ijy, ctx->ay.invdiag)) || (st = put(&ctx->d_ilx, ctx->ax.invlump)) ||
+      (st = put(&ctx->d_ily, ctx->ay.invlump)))
     return st;
+  {
+    // reference element matrices of every degree, into constant memory
+    static double ref[MAXPD][3][MAXPD + 1][MAXPD + 1];
+    std::memset(ref, 0, sizeof ref);
+    for (int q = 1; q <= MAXPD; ++q)
+      {
+        const Basis1D b(q);
+        for (int a = 0; a <= q; ++a)
+          for (int c = 0; c <= q; ++c)
+            {
+              ref[q - 1][OP_M][a][c] = b.Mh[a][c];
+              ref[q - 1][OP_C][a][c] = b.Ch[a][c];
+              ref[q - 1][OP_K][a][c] = b.Kh[a][c];
+            }
+      }
+    CK(cudaMemcpyToSymbol(c_ref, ref, sizeof ref));
+  }
 
   // numbering: structured node -> caller DoF, and its inverse for the wall list
   std::vector<long long> node_of_dof;
@@ -687,7 +746,11 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
     return st;
   if (!ctx->identity && (st = zeros(&ctx->d_stage, Q * N)))
     return st;
-  const long long tiles = (long long)((nfx + 31) / 32) * ((nfy + 15) / 16);
+  const long long tiles = with_degree(P, [&](auto PP) -> int {
+    constexpr int Pd = decltype(PP)::value;
+    const dim3 tg = tile_grid<Pd>(ctx->grid);
+    return int(tg.x * tg.y);
+  });
   ctx->partial_cap = size_t(std::max<long long>(tiles, 148 * 8)) * 3 * NM;
   if ((st = zeros(&ctx->d_partials, ctx->partial_cap)) || (st = zeros(&ctx->d_sums, 64)))
     return st;

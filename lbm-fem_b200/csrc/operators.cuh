@@ -7,6 +7,9 @@
 
 namespace lbfem_gpu
 {
+#define LBFEM_GRID_STRIDE(i, n) \
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
   // ----------------------------------------------------------- nodal maps
   // collide_bgk (collision.h:152-168): g <- geq(rho, u_imposed) + (1 - omega)(g - geq(rho, u)).
   __device__ __forceinline__ void
@@ -23,17 +26,17 @@ namespace lbfem_gpu
   k_collide(const Geo geo, double *__restrict__ g, double omega)
   {
     const long long N = geo.g.N;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
-      {
-        double v[Q];
+    LBFEM_GRID_STRIDE(i, N)
+    {
+      double v[Q];
 #pragma unroll
-        for (int a = 0; a < Q; ++a)
-          v[a] = g[a * N + i];
-        collide_node(v, i, geo, omega);
+      for (int a = 0; a < Q; ++a)
+        v[a] = g[a * N + i];
+      collide_node(v, i, geo, omega);
 #pragma unroll
-        for (int a = 0; a < Q; ++a)
-          g[a * N + i] = v[a];
-      }
+      for (int a = 0; a < Q; ++a)
+        g[a * N + i] = v[a];
+    }
   }
 
   // compute_equilibrium (collision.h:105-113)
@@ -41,17 +44,17 @@ namespace lbfem_gpu
   k_equilibrium(const Geo geo, const double *__restrict__ f, double *__restrict__ feq)
   {
     const long long N = geo.g.N;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
-      {
-        double v[Q];
+    LBFEM_GRID_STRIDE(i, N)
+    {
+      double v[Q];
 #pragma unroll
-        for (int a = 0; a < Q; ++a)
-          v[a] = f[a * N + i];
-        const Mom m = impose(moments(v), i, geo);
+      for (int a = 0; a < Q; ++a)
+        v[a] = f[a * N + i];
+      const Mom m = impose(moments(v), i, geo);
 #pragma unroll
-        for (int a = 0; a < Q; ++a)
-          feq[a * N + i] = feq_a(a, m);
-      }
+      for (int a = 0; a < Q; ++a)
+        feq[a * N + i] = feq_a(a, m);
+    }
   }
 
   // predictor_corrector (collision.h:119-145); feq == nullptr: the equilibria of
@@ -62,34 +65,34 @@ namespace lbfem_gpu
   {
     const long long N = geo.g.N;
     const double inv = 1. / (1. + theta);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
-      {
-        double fi[Q], fe[Q], fh[Q];
+    LBFEM_GRID_STRIDE(i, N)
+    {
+      double fi[Q], fe[Q], fh[Q];
 #pragma unroll
-        for (int a = 0; a < Q; ++a)
-          fi[a] = f[a * N + i];
-        if (feq)
-          {
+      for (int a = 0; a < Q; ++a)
+        fi[a] = f[a * N + i];
+      if (feq)
+        {
 #pragma unroll
-            for (int a = 0; a < Q; ++a)
-              fe[a] = feq[a * N + i];
-          }
-        else
-          {
-            const Mom m = impose(moments(fi), i, geo);
+          for (int a = 0; a < Q; ++a)
+            fe[a] = feq[a * N + i];
+        }
+      else
+        {
+          const Mom m = impose(moments(fi), i, geo);
 #pragma unroll
-            for (int a = 0; a < Q; ++a)
-              fe[a] = feq_a(a, m);
-          }
-        fh[0] = inv * (fi[0] + theta * fe[0]);
+          for (int a = 0; a < Q; ++a)
+            fe[a] = feq_a(a, m);
+        }
+      fh[0] = inv * (fi[0] + theta * fe[0]);
 #pragma unroll
-        for (int a = 1; a < Q; ++a)
-          fh[a] = inv * (fi[a] + theta * fe[a] + x[(a - 1) * N + i]);
-        const Mom mh = impose(moments(fh), i, geo);
+      for (int a = 1; a < Q; ++a)
+        fh[a] = inv * (fi[a] + theta * fe[a] + x[(a - 1) * N + i]);
+      const Mom mh = impose(moments(fh), i, geo);
 #pragma unroll
-        for (int a = 0; a < Q; ++a)
-          f[a * N + i] = fh[a] + theta * (feq_a(a, mh) - fe[a]);
-      }
+      for (int a = 0; a < Q; ++a)
+        f[a * N + i] = fh[a] + theta * (feq_a(a, mh) - fe[a]);
+    }
   }
 
   // Bardow::set_initial_populations (schemes.h:129-141): g = f + scale (f - feq(f)), no imposition.
@@ -97,17 +100,17 @@ namespace lbfem_gpu
   k_bardow_transform(const Geo geo, double *__restrict__ f, double scale)
   {
     const long long N = geo.g.N;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
-      {
-        double v[Q];
+    LBFEM_GRID_STRIDE(i, N)
+    {
+      double v[Q];
 #pragma unroll
-        for (int a = 0; a < Q; ++a)
-          v[a] = f[a * N + i];
-        const Mom m = moments(v);
+      for (int a = 0; a < Q; ++a)
+        v[a] = f[a * N + i];
+      const Mom m = moments(v);
 #pragma unroll
-        for (int a = 0; a < Q; ++a)
-          f[a * N + i] = v[a] + scale * (v[a] - feq_a(a, m));
-      }
+      for (int a = 0; a < Q; ++a)
+        f[a * N + i] = v[a] + scale * (v[a] - feq_a(a, m));
+    }
   }
 
   // TaylorGalerkin::stream (streaming.h:94-98): f_a += x_{a-1}, a = 1..8.
@@ -115,12 +118,12 @@ namespace lbfem_gpu
   k_add_increment(const Geo geo, double *__restrict__ f, const double *__restrict__ x)
   {
     const long long N = geo.g.N;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
-      {
+    LBFEM_GRID_STRIDE(i, N)
+    {
 #pragma unroll
-        for (int a = 1; a < Q; ++a)
-          f[a * N + i] += x[(a - 1) * N + i];
-      }
+      for (int a = 1; a < Q; ++a)
+        f[a * N + i] += x[(a - 1) * N + i];
+    }
   }
 
   // Lumped solve (mass.h:189-191): x = M_L^{-1} r, for nsys vectors.
@@ -129,14 +132,13 @@ namespace lbfem_gpu
   {
     const Grid &g = geo.g;
     const long long N = g.N;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N;
-         idx += (long long)gridDim.x * blockDim.x)
-      {
-        const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
-        const double inv = is_image(i, j, g) ? 1.0 : 1.0 / (geo.lumpx[i] * geo.lumpy[j]);
-        for (int s = 0; s < nsys; ++s)
-          x[s * N + idx] = inv * r[s * N + idx];
-      }
+    LBFEM_GRID_STRIDE(idx, N)
+    {
+      const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
+      const double inv = is_image(i, j, g) ? 1.0 : geo.ilx[i] * geo.ily[j];
+      for (int s = 0; s < nsys; ++s)
+        x[s * N + idx] = inv * r[s * N + idx];
+    }
   }
 
   // Node weights: the lumped (which = 0) or Jacobi (which = 1) diagonal, images 1.
@@ -144,12 +146,11 @@ namespace lbfem_gpu
   k_diagonal(const Geo geo, double *__restrict__ w, int which)
   {
     const Grid &g = geo.g;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < g.N;
-         idx += (long long)gridDim.x * blockDim.x)
-      {
-        const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
-        w[idx] = is_image(i, j, g) ? 1.0 : which == 0 ? geo.lumpx[i] * geo.lumpy[j] : geo.diagx[i] * geo.diagy[j];
-      }
+    LBFEM_GRID_STRIDE(idx, g.N)
+    {
+      const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
+      w[idx] = is_image(i, j, g) ? 1.0 : which == 0 ? geo.lumpx[i] * geo.lumpy[j] : geo.diagx[i] * geo.diagy[j];
+    }
   }
 
   // Moments at every node; images report their source node (constraints.distribute).
@@ -159,51 +160,49 @@ namespace lbfem_gpu
   {
     const Grid &g = geo.g;
     const long long N = g.N;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N;
-         idx += (long long)gridDim.x * blockDim.x)
-      {
-        const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
-        const long long src = (long long)wrap(j, g.py, g.nuy, g.nfy) * g.nfx + wrap(i, g.px, g.nux, g.nfx);
-        double v[Q];
+    LBFEM_GRID_STRIDE(idx, N)
+    {
+      const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
+      const long long src = (long long)wrap(j, g.py, g.nuy, g.nfy) * g.nfx + wrap(i, g.px, g.nux, g.nfx);
+      double v[Q];
 #pragma unroll
-        for (int a = 0; a < Q; ++a)
-          v[a] = f[a * N + src];
-        const Mom m = moments(v);
-        if (rho)
-          rho[idx] = m.rho;
-        if (ux)
-          ux[idx] = m.ux;
-        if (uy)
-          uy[idx] = m.uy;
-      }
+      for (int a = 0; a < Q; ++a)
+        v[a] = f[a * N + src];
+      const Mom m = moments(v);
+      if (rho)
+        rho[idx] = m.rho;
+      if (ux)
+        ux[idx] = m.ux;
+      if (uy)
+        uy[idx] = m.uy;
+    }
   }
 
   // FP64 conservation sums over the independent nodes (cgdbe.cc:353-368).
-  __global__ void
-  k_conservation(const Geo geo, const double *__restrict__ f, double *__restrict__ partials)
+  __global__ void __launch_bounds__(THREADS)
+    k_conservation(const Geo geo, const double *__restrict__ f, double *__restrict__ partials)
   {
     const Grid &g = geo.g;
     const long long N = g.N;
     double s[5] = {0, 0, 0, 0, 0};
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N;
-         idx += (long long)gridDim.x * blockDim.x)
-      {
-        const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
-        if (is_image(i, j, g))
-          continue;
-        double v[Q];
+    LBFEM_GRID_STRIDE(idx, N)
+    {
+      const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
+      if (is_image(i, j, g))
+        continue;
+      double v[Q];
 #pragma unroll
-        for (int a = 0; a < Q; ++a)
-          v[a] = f[a * N + idx];
-        const Mom m = moments(v);
-        const double w = geo.lumpx[i] * geo.lumpy[j];
-        s[0] += w;
-        s[1] += w * m.rho;
-        s[2] += w * m.rho * m.ux;
-        s[3] += w * m.rho * m.uy;
-        s[4] += w * (m.ux * m.ux + m.uy * m.uy);
-      }
-    block_reduce_store<5>(s, 5, partials, blockIdx.x, gridDim.x);
+      for (int a = 0; a < Q; ++a)
+        v[a] = f[a * N + idx];
+      const Mom m = moments(v);
+      const double w = geo.lumpx[i] * geo.lumpy[j];
+      s[0] += w;
+      s[1] += w * m.rho;
+      s[2] += w * m.rho * m.ux;
+      s[3] += w * m.rho * m.uy;
+      s[4] += w * (m.ux * m.ux + m.uy * m.uy);
+    }
+    block_reduce_store<5>(s, partials, blockIdx.x, gridDim.x);
   }
 
   // Caller numbering <-> structured numbering, nb blocks of a vector.
@@ -211,24 +210,24 @@ namespace lbfem_gpu
   k_gather(const double *__restrict__ src, const long long *__restrict__ dof, double *__restrict__ dst, long long N,
            long long n_dofs, int nb)
   {
-    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < N; s += (long long)gridDim.x * blockDim.x)
-      {
-        const long long d = dof[s];
-        for (int b = 0; b < nb; ++b)
-          dst[b * N + s] = src[b * n_dofs + d];
-      }
+    LBFEM_GRID_STRIDE(s, N)
+    {
+      const long long d = dof[s];
+      for (int b = 0; b < nb; ++b)
+        dst[b * N + s] = src[b * n_dofs + d];
+    }
   }
 
   __global__ void
   k_scatter(const double *__restrict__ src, const long long *__restrict__ dof, double *__restrict__ dst, long long N,
             long long n_dofs, int nb)
   {
-    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < N; s += (long long)gridDim.x * blockDim.x)
-      {
-        const long long d = dof[s];
-        for (int b = 0; b < nb; ++b)
-          dst[b * n_dofs + d] = src[b * N + s];
-      }
+    LBFEM_GRID_STRIDE(s, N)
+    {
+      const long long d = dof[s];
+      for (int b = 0; b < nb; ++b)
+        dst[b * n_dofs + d] = src[b * N + s];
+    }
   }
 
   // ------------------------------------------------- K1: streaming right-hand side
@@ -247,197 +246,387 @@ namespace lbfem_gpu
     double omega;          // BGK rate (ADV_TG_COLLIDE)
   };
 
+  template <int MODE>
+  __host__ __device__ constexpr bool
+  has_moments()
+  {
+    return MODE == ADV_TG_COLLIDE || MODE == ADV_LEELIN_FUSED;
+  }
+
   template <int P, int MODE>
   constexpr size_t
   advection_smem()
   {
     using T = Tile<P>;
-    return sizeof(double) * (4 * T::TX * T::K + 4 * T::TY * T::K + 9 * T::HN + T::HN + 3 * T::HN + 4 * T::HY * T::TX);
+    const int fields = (has_moments<MODE>() ? 3 : 0) + 1 + (MODE == ADV_LEELIN_FEQ ? 1 : 0);
+    return sizeof(double) * (fields * T::NF + 3 * T::NY + 2 * T::TX) +
+           (MODE == ADV_TG_COLLIDE ? size_t(T::NF + 15) / 16 * 16 : 0);
   }
 
-  // rhs_{a-1} <- r_a for a = 1..8 (advection.h:93-124 with the point operations of
-  // advection.h:228-239 / 275-287): cell integrals over the whole mesh, in the
-  // assembled tensor-product form
-  //   r = My (x) (a ex Cx + c ex^2 Kx) f + Cy (x) (a ey Mx + c ex ey Cx^T) f
-  //     + Ky (x) (c ey^2 Mx) f + Cy^T (x) (c ex ey Cx) f  [+ b (ex My (x) Cx + ey Cy (x) Mx) feq].
-  // Images get 0 (constrained rows, as distribute_local_to_global leaves them).
+  // Per-population scalars of the grouped operator
+  //   r = My (x) Y1 + Cy (x) Y2' + Ky (x) Y3 + By (x) Y4, with h = a f + b feq:
+  //   Y1 = ex Cx h + c ex^2 Kx f, Y2' = ey Mx h - 2 c ex ey Cx f + c ex ey Bx f,
+  //   Y3 = c ey^2 Mx f, Y4 = c ex ey Cx f
+  // (C^T = B - C, B the end-point term of the integration by parts).
+  struct AdvK
+  {
+    double A, B, k1, k2, k3, k4, k5, k6;
+  };
+
+  // Population a at footprint index t: u, and h = A u + B feq.
+  template <int HM>
+  __device__ __forceinline__ void
+  load_uh(const double *s_u, const double *s_e, const double *s_m, int nf, int t, int a, const AdvK &k, double &u,
+          double &h)
+  {
+    u = s_u[t];
+    if constexpr (HM == 0)
+      h = k.A * u;
+    else if constexpr (HM == 1)
+      h = fma(k.B, feq_a(a, Mom{s_m[t], s_m[nf + t], s_m[2 * nf + t]}), k.A * u);
+    else
+      h = fma(k.B, s_e[t], k.A * u);
+  }
+
+  // x pass of K1 for one footprint row fy and one x segment. CLS: 0 e = (ex, 0), 1 e = (0, ey), 2 diagonal.
+  template <int P, int CLS, int HM>
+  __device__ __forceinline__ void
+  adv_xpass(const double *s_u, const double *s_e, const double *s_m, double *s_y, double *s_y4,
+            const TileMaps<P> &m, const AdvK &k, int a, int fy, int seg, int gx0, int y4_slot, int bx_lo, int bx_hi)
+  {
+    using T = Tile<P>;
+    constexpr bool XC = CLS != 1, YC = CLS != 0, DG = CLS == 2;
+    const int base = fy * T::PF;
+    const int q0 = seg * T::KX;
+    double u[P + 1], h[P + 1];
+#pragma unroll
+    for (int b = 0; b <= P; ++b)
+      load_uh<HM>(s_u, s_e, s_m, T::NF, base + q0 * P + b, a, k, u[b], h[b]);
+    double pCh = 0, pKu = 0, pMh = 0, pCu = 0, pMu = 0;
+    if constexpr (XC)
+      {
+        pCh = m.cx[q0] * elem_last<P, OP_C>(h);
+        pKu = m.hxi[q0] * elem_last<P, OP_K>(u);
+      }
+    if constexpr (YC)
+      {
+        pMh = m.hx[q0] * elem_last<P, OP_M>(h);
+        pMu = m.hx[q0] * elem_last<P, OP_M>(u);
+      }
+    if constexpr (DG)
+      pCu = m.cx[q0] * elem_last<P, OP_C>(u);
+    double *y1 = s_y + fy * T::PY, *y2 = y1 + T::NY, *y3 = y2 + T::NY;
+#pragma unroll
+    for (int q = 1; q <= T::KX; ++q)
+      {
+        const int qc = q0 + q;
+        u[0] = u[P];
+        h[0] = h[P];
+#pragma unroll
+        for (int b = 1; b <= P; ++b)
+          load_uh<HM>(s_u, s_e, s_m, T::NF, base + qc * P + b, a, k, u[b], h[b]);
+        double eCh[P + 1], eKu[P + 1], eMh[P + 1], eCu[P + 1], eMu[P + 1];
+        if constexpr (XC)
+          {
+            elem<P, OP_C>(h, eCh);
+            elem<P, OP_K>(u, eKu);
+          }
+        if constexpr (YC)
+          {
+            elem<P, OP_M>(h, eMh);
+            elem<P, OP_M>(u, eMu);
+          }
+        if constexpr (DG)
+          elem<P, OP_C>(u, eCu);
+        const double sc = m.cx[qc], sh = m.hx[qc], shi = m.hxi[qc];
+        const int j0 = (qc - 1) * P;
+#pragma unroll
+        for (int aa = 0; aa < P; ++aa)
+          {
+            const int j = j0 + aa;
+            double vCh = 0, vKu = 0, vMh = 0, vCu = 0, vMu = 0;
+            if constexpr (XC)
+              {
+                vCh = sc * eCh[aa];
+                vKu = shi * eKu[aa];
+              }
+            if constexpr (YC)
+              {
+                vMh = sh * eMh[aa];
+                vMu = sh * eMu[aa];
+              }
+            if constexpr (DG)
+              vCu = sc * eCu[aa];
+            if (aa == 0)
+              {
+                vCh += pCh;
+                vKu += pKu;
+                vMh += pMh;
+                vMu += pMu;
+                vCu += pCu;
+              }
+            if constexpr (XC)
+              y1[j] = k.k1 * vCh + k.k2 * vKu;
+            if constexpr (YC)
+              {
+                double y = k.k3 * vMh;
+                if constexpr (DG)
+                  {
+                    y = fma(k.k4, vCu, y);
+                    if (aa == 0)
+                      {
+                        // Bx f = -f at the first node, +f at the last node of a non-periodic axis
+                        const int gx = gx0 + j;
+                        if (gx == bx_lo)
+                          y = fma(-k.k6, u[0], y);
+                        else if (gx == bx_hi)
+                          y = fma(k.k6, u[0], y);
+                      }
+                  }
+                y2[j] = y;
+                y3[j] = k.k5 * vMu;
+              }
+            if constexpr (DG)
+              if (y4_slot >= 0)
+                s_y4[y4_slot * T::TX + j] = k.k6 * vCu;
+          }
+        if constexpr (XC)
+          {
+            pCh = sc * eCh[P];
+            pKu = shi * eKu[P];
+          }
+        if constexpr (YC)
+          {
+            pMh = sh * eMh[P];
+            pMu = sh * eMu[P];
+          }
+        if constexpr (DG)
+          pCu = sc * eCu[P];
+      }
+  }
+
+  // y pass of K1 on column j and y segment seg: emit(own row i, r).
+  template <int P, int CLS, typename Emit>
+  __device__ __forceinline__ void
+  adv_ypass(const double *s_y, const double *s_y4, const TileMaps<P> &m, int j, int seg, int gy0, int by_lo,
+            int by_hi, Emit &&emit)
+  {
+    using T = Tile<P>;
+    constexpr bool XC = CLS != 1, YC = CLS != 0, DG = CLS == 2;
+    const double *y1 = s_y, *y2 = s_y + T::NY, *y3 = s_y + 2 * T::NY;
+    const int q0 = seg * T::KY;
+    double v1[P + 1], v2[P + 1], v3[P + 1];
+#pragma unroll
+    for (int b = 0; b <= P; ++b)
+      {
+        const int t = (q0 * P + b) * T::PY + j;
+        if constexpr (XC)
+          v1[b] = y1[t];
+        if constexpr (YC)
+          {
+            v2[b] = y2[t];
+            v3[b] = y3[t];
+          }
+      }
+    double pend = 0;
+    if constexpr (XC)
+      pend = m.hy[q0] * elem_last<P, OP_M>(v1);
+    if constexpr (YC)
+      pend += m.cy[q0] * elem_last<P, OP_C>(v2) + m.hyi[q0] * elem_last<P, OP_K>(v3);
+#pragma unroll
+    for (int q = 1; q <= T::KY; ++q)
+      {
+        const int qc = q0 + q;
+        v1[0] = v1[P];
+        v2[0] = v2[P];
+        v3[0] = v3[P];
+#pragma unroll
+        for (int b = 1; b <= P; ++b)
+          {
+            const int t = (qc * P + b) * T::PY + j;
+            if constexpr (XC)
+              v1[b] = y1[t];
+            if constexpr (YC)
+              {
+                v2[b] = y2[t];
+                v3[b] = y3[t];
+              }
+          }
+        double e1[P + 1], e2[P + 1], e3[P + 1];
+        if constexpr (XC)
+          elem<P, OP_M>(v1, e1);
+        if constexpr (YC)
+          {
+            elem<P, OP_C>(v2, e2);
+            elem<P, OP_K>(v3, e3);
+          }
+        const double sh = m.hy[qc], sc = m.cy[qc], shi = m.hyi[qc];
+        const int i0 = (qc - 1) * P;
+#pragma unroll
+        for (int aa = 0; aa <= P; ++aa)
+          {
+            double r = 0;
+            if constexpr (XC)
+              r = sh * e1[aa];
+            if constexpr (YC)
+              r += sc * e2[aa] + shi * e3[aa];
+            if (aa == P)
+              {
+                pend = r;
+                break;
+              }
+            if (aa == 0)
+              r += pend;
+            if constexpr (DG)
+              {
+                const int gy = gy0 + i0 + aa;
+                if (gy == by_lo)
+                  r -= s_y4[0 * T::TX + j];
+                else if (gy == by_hi)
+                  r += s_y4[1 * T::TX + j];
+              }
+            emit(i0 + aa, r);
+          }
+      }
+  }
+
+  // rhs_{a-1} <- r_a for a = 1..8: cell integrals of the point operations of
+  // TaylorGalerkinAdvection (advection.h:228-239) / LeeLinAdvection
+  // (advection.h:275-287), in the grouped tensor-product form above. Images get
+  // 0 (constrained rows, as distribute_local_to_global leaves them).
   template <int P, int MODE>
-  __global__ void __launch_bounds__(THREADS)
+  __global__ void __launch_bounds__(THREADS, 2)
     k_advection(const Geo geo, const double *__restrict__ f, const double *__restrict__ feq,
                 double *__restrict__ fout, double *__restrict__ rhs, const AdvCoef ac)
   {
     using T = Tile<P>;
-    constexpr int TX = T::TX, TY = T::TY, HX = T::HX, HN = T::HN, K = T::K;
+    constexpr bool MOM = has_moments<MODE>();
+    constexpr int HM = MODE == ADV_LEELIN_FUSED ? 1 : MODE == ADV_LEELIN_FEQ ? 2 : 0;
     extern __shared__ double sm[];
-    double *s_rx = sm;
-    double *s_ry = s_rx + 4 * TX * K;
-    double *s_f = s_ry + 4 * TY * K; // [9][HN]
-    double *s_q = s_f + 9 * HN;      // [HN]: equilibrium of the current population
-    double *s_m = s_q + HN;          // [3][HN]: rho, ux, uy (imposed) for ADV_LEELIN_FUSED
-    double *s_t = s_m + 3 * HN;      // [4][HY][TX]
+    __shared__ TileMaps<P> maps;
+    double *s_m = sm;                                 // [3][NF] moments (MOM modes)
+    double *s_u = s_m + (MOM ? 3 * T::NF : 0);        // [NF] the current population
+    double *s_e = s_u + T::NF;                        // [NF] its equilibrium (ADV_LEELIN_FEQ)
+    double *s_y = s_e + (MODE == ADV_LEELIN_FEQ ? T::NF : 0); // [3][NY] x-pass outputs
+    double *s_y4 = s_y + 3 * T::NY;                   // [2][TX] Y4 on the first / last domain row
+    uint8_t *s_wall = reinterpret_cast<uint8_t *>(s_y4 + 2 * T::TX); // [NF] wall classes (ADV_TG_COLLIDE)
     const Grid &g = geo.g;
     const long long N = g.N;
-    const int gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
-
-    load_rows<P>(s_rx, geo.rowx, gx0, TX, g.nfx);
-    load_rows<P>(s_ry, geo.rowy, gy0, TY, g.nfy);
-    constexpr bool all9 = MODE == ADV_TG_COLLIDE || MODE == ADV_LEELIN_FUSED;
-    for (int a = all9 ? 0 : 1; a < Q; ++a)
-      load_tile<P>(s_f + a * HN, f + a * N, g, gx0, gy0);
+    const int gx0 = blockIdx.x * T::TX, gy0 = blockIdx.y * T::TY;
+    build_maps<P>(maps, geo, gx0, gy0);
     __syncthreads();
 
-    if constexpr (all9)
+    if constexpr (MOM)
       {
-        for (int t = threadIdx.x; t < HN; t += blockDim.x)
+        for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
           {
-            const int ly = t / HX, lx = t - ly * HX;
-            const int sx = wrap(gx0 - P + lx, g.px, g.nux, g.nfx), sy = wrap(gy0 - P + ly, g.py, g.nuy, g.nfy);
-            if (sx < 0 || sy < 0)
+            const int fy = t / T::FX, fx = t - fy * T::FX, st = fy * T::PF + fx;
+            const long long r = maps.row[fy];
+            const int c = maps.col[fx];
+            if (r < 0 || c < 0)
               {
-                if constexpr (MODE == ADV_LEELIN_FUSED)
-                  s_m[t] = s_m[HN + t] = s_m[2 * HN + t] = 0.0;
+                s_m[st] = s_m[T::NF + st] = s_m[2 * T::NF + st] = 0.0;
+                if constexpr (MODE == ADV_TG_COLLIDE)
+                  s_wall[st] = 0;
                 continue;
               }
-            const long long idx = (long long)sy * g.nfx + sx;
+            const long long idx = r + c;
             double v[Q];
 #pragma unroll
             for (int a = 0; a < Q; ++a)
-              v[a] = s_f[a * HN + t];
-            if constexpr (MODE == ADV_TG_COLLIDE)
-              {
-                collide_node(v, idx, geo, ac.omega);
-#pragma unroll
-                for (int a = 0; a < Q; ++a)
-                  s_f[a * HN + t] = v[a];
-                const int gx = gx0 - P + lx, gy = gy0 - P + ly;
-                if (lx >= P && lx < P + TX && ly >= P && ly < P + TY && gx < g.nfx && gy < g.nfy &&
-                    !is_image(gx, gy, g))
-                  {
-#pragma unroll
-                    for (int a = 0; a < Q; ++a)
-                      fout[a * N + idx] = v[a];
-                  }
-              }
+              v[a] = f[a * N + idx];
+            Mom mo = moments(v);
+            const int wk = geo.wall ? geo.wall[idx] : 0;
+            if constexpr (MODE == ADV_LEELIN_FUSED)
+              mo = impose_class(mo, wk, geo);
             else
-              {
-                const Mom m = impose(moments(v), idx, geo);
-                s_m[t] = m.rho;
-                s_m[HN + t] = m.ux;
-                s_m[2 * HN + t] = m.uy;
-              }
+              s_wall[st] = uint8_t(wk);
+            s_m[st] = mo.rho;
+            s_m[T::NF + st] = mo.ux;
+            s_m[2 * T::NF + st] = mo.uy;
           }
-        __syncthreads();
       }
 
-    for (int al = 0; al < NM; ++al)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int bx_lo = g.px ? -1 : 0, bx_hi = g.px ? -1 : g.nfx - 1;
+    const int by_lo = g.py ? -1 : 0, by_hi = g.py ? -1 : g.nfy - 1;
+
+    for (int a = (MODE == ADV_TG_COLLIDE ? 0 : 1); a < Q; ++a)
       {
-        const int a = al + 1;
-        const double ex = ac.ex[al], ey = ac.ey[al];
-        const bool hx = ex != 0.0, hy = ey != 0.0;
-        constexpr bool two = MODE == ADV_LEELIN_FEQ || MODE == ADV_LEELIN_FUSED;
+        __syncthreads(); // the previous population's passes are done with s_u / s_y
+        stage<P>(s_u, maps, [&](long long idx) { return f[a * N + idx]; });
         if constexpr (MODE == ADV_LEELIN_FEQ)
+          stage<P>(s_e, maps, [&](long long idx) { return feq[a * N + idx]; });
+        if constexpr (MODE == ADV_TG_COLLIDE)
           {
-            load_tile<P>(s_q, feq + a * N, g, gx0, gy0);
             __syncthreads();
-          }
-        else if constexpr (MODE == ADV_LEELIN_FUSED)
-          {
-            for (int t = threadIdx.x; t < HN; t += blockDim.x)
-              s_q[t] = feq_a(a, Mom{s_m[t], s_m[HN + t], s_m[2 * HN + t]});
-            __syncthreads();
-          }
-        // x pass: the four x-filtered fields of the y operators My, Cy, Ky, Cy^T
-        const double *u = s_f + a * HN;
-        for (int t = threadIdx.x; t < T::HY * TX; t += blockDim.x)
-          {
-            const int ly = t / TX, lxo = t - ly * TX;
-            const double *rM = s_rx + (0 * TX + lxo) * K, *rC = s_rx + (1 * TX + lxo) * K;
-            const double *rT = s_rx + (2 * TX + lxo) * K, *rK = s_rx + (3 * TX + lxo) * K;
-            const double *uu = u + ly * HX + lxo;
-            double Cu = 0, Mu = 0, Tu = 0, Ku = 0, Ce = 0, Me = 0;
-            if (hx)
+            for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
               {
-#pragma unroll
-                for (int k = 0; k < K; ++k)
-                  {
-                    Cu += rC[k] * uu[k];
-                    Ku += rK[k] * uu[k];
-                  }
-                if constexpr (two)
-                  {
-                    const double *ee = s_q + ly * HX + lxo;
-#pragma unroll
-                    for (int k = 0; k < K; ++k)
-                      Ce += rC[k] * ee[k];
-                  }
+                const int fy = t / T::FX, fx = t - fy * T::FX, st = fy * T::PF + fx;
+                const long long r = maps.row[fy];
+                const int c = maps.col[fx];
+                if (r < 0 || c < 0)
+                  continue;
+                const Mom mo{s_m[st], s_m[T::NF + st], s_m[2 * T::NF + st]};
+                const Mom mt = impose_class(mo, s_wall[st], geo);
+                const double gs = feq_a(a, mt) + (1. - ac.omega) * (s_u[st] - feq_a(a, mo));
+                s_u[st] = gs;
+                const int gx = gx0 - P + fx, gy = gy0 - P + fy;
+                if (fx >= P && fx < P + T::TX && fy >= P && fy < P + T::TY && gx < g.nfx && gy < g.nfy &&
+                    !is_image(gx, gy, g))
+                  fout[a * N + r + c] = gs;
               }
-            if (hy)
-              {
-#pragma unroll
-                for (int k = 0; k < K; ++k)
-                  Mu += rM[k] * uu[k];
-                if (hx)
-                  {
-#pragma unroll
-                    for (int k = 0; k < K; ++k)
-                      Tu += rT[k] * uu[k];
-                  }
-                if constexpr (two)
-                  {
-                    const double *ee = s_q + ly * HX + lxo;
-#pragma unroll
-                    for (int k = 0; k < K; ++k)
-                      Me += rM[k] * ee[k];
-                  }
-              }
-            const int nt = T::HY * TX;
-            s_t[t] = ac.a * ex * Cu + ac.c * ex * ex * Ku + ac.b * ex * Ce;          // -> My
-            s_t[nt + t] = ac.a * ey * Mu + ac.c * ex * ey * Tu + ac.b * ey * Me;     // -> Cy
-            s_t[2 * nt + t] = ac.c * ey * ey * Mu;                                  // -> Ky
-            s_t[3 * nt + t] = ac.c * ex * ey * Cu;                                  // -> Cy^T
-          }
-        __syncthreads();
-        // y pass and store
-        for (int t = threadIdx.x; t < TY * TX; t += blockDim.x)
-          {
-            const int lyo = t / TX, lxo = t - lyo * TX;
-            const int gx = gx0 + lxo, gy = gy0 + lyo;
-            if (gx >= g.nfx || gy >= g.nfy)
+            if (a == 0)
               continue;
-            double r = 0;
-            if (!is_image(gx, gy, g))
-              {
-                const int nt = T::HY * TX;
-                const double *yM = s_ry + (0 * TY + lyo) * K, *yC = s_ry + (1 * TY + lyo) * K;
-                const double *yT = s_ry + (2 * TY + lyo) * K, *yK = s_ry + (3 * TY + lyo) * K;
-#pragma unroll
-                for (int k = 0; k < K; ++k)
-                  r += yM[k] * s_t[(lyo + k) * TX + lxo];
-                if (hy)
-                  {
-#pragma unroll
-                    for (int k = 0; k < K; ++k)
-                      r += yC[k] * s_t[nt + (lyo + k) * TX + lxo] + yK[k] * s_t[2 * nt + (lyo + k) * TX + lxo];
-                    if (hx)
-                      {
-#pragma unroll
-                        for (int k = 0; k < K; ++k)
-                          r += yT[k] * s_t[3 * nt + (lyo + k) * TX + lxo];
-                      }
-                  }
-              }
-            rhs[al * N + (long long)gy * g.nfx + gx] = r;
           }
         __syncthreads();
+        const int al = a - 1;
+        const double ex = ac.ex[al], ey = ac.ey[al];
+        const int cls = ey == 0.0 ? (ex == 0.0 ? 3 : 0) : (ex == 0.0 ? 1 : 2);
+        const AdvK k{ac.a, ac.b, ex, ac.c * ex * ex, ey, -2.0 * ac.c * ex * ey, ac.c * ey * ey, ac.c * ex * ey};
+        // x pass: lane = footprint row, warp = x segment
+        if (warp < T::NSX && lane < T::FY)
+          {
+            const int gy = gy0 - P + lane;
+            const int y4_slot = gy == by_lo ? 0 : gy == by_hi ? 1 : -1;
+            if (cls == 0)
+              adv_xpass<P, 0, HM>(s_u, s_e, s_m, s_y, s_y4, maps, k, a, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
+            else if (cls == 1)
+              adv_xpass<P, 1, HM>(s_u, s_e, s_m, s_y, s_y4, maps, k, a, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
+            else if (cls == 2)
+              adv_xpass<P, 2, HM>(s_u, s_e, s_m, s_y, s_y4, maps, k, a, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
+          }
+        __syncthreads();
+        // y pass: lane group = columns, warp group = y segment
+        const int j = threadIdx.x % T::YL, seg = threadIdx.x / T::YL;
+        if (j < T::TX && seg < T::NSY)
+          {
+            const int gx = gx0 + j;
+            double *out = rhs + (long long)al * N;
+            auto emit = [&](int i, double r) {
+              const int gy = gy0 + i;
+              if (gx < g.nfx && gy < g.nfy)
+                out[(long long)gy * g.nfx + gx] = is_image(gx, gy, g) ? 0.0 : r;
+            };
+            if (cls == 0)
+              adv_ypass<P, 0>(s_y, s_y4, maps, j, seg, gy0, by_lo, by_hi, emit);
+            else if (cls == 1)
+              adv_ypass<P, 1>(s_y, s_y4, maps, j, seg, gy0, by_lo, by_hi, emit);
+            else if (cls == 2)
+              adv_ypass<P, 2>(s_y, s_y4, maps, j, seg, gy0, by_lo, by_hi, emit);
+            else
+              for (int i = seg * T::SY; i < (seg + 1) * T::SY; ++i)
+                emit(i, 0.0);
+          }
       }
 
     if constexpr (MODE == ADV_TG_COLLIDE)
       {
         // the images collide their own (stale) populations, as the nodal map does
-        for (int t = threadIdx.x; t < TY * TX; t += blockDim.x)
+        for (int t = threadIdx.x; t < T::TY * T::TX; t += blockDim.x)
           {
-            const int lyo = t / TX, lxo = t - lyo * TX;
-            const int gx = gx0 + lxo, gy = gy0 + lyo;
+            const int i = t / T::TX, j = t - i * T::TX;
+            const int gx = gx0 + j, gy = gy0 + i;
             if (gx >= g.nfx || gy >= g.nfy || !is_image(gx, gy, g))
               continue;
             const long long idx = (long long)gy * g.nfx + gx;
@@ -502,7 +691,7 @@ namespace lbfem_gpu
             const double en = side == 0 ? -ey : side == 1 ? ey : side == 2 ? -ex : ex;
             if (en == 0.0)
               continue;
-            const double et = horizontal ? ex : ey; // tangential component
+            const double et = horizontal ? ex : ey;  // tangential component
             const double enn = horizontal ? ey : ex; // normal component (derivative direction)
             const double *u = f + (long long)(al + 1) * N;
             double tang = 0, norm = 0;
@@ -517,7 +706,8 @@ namespace lbfem_gpu
 #pragma unroll
                 for (int b = 0; b <= P; ++b)
                   {
-                    const long long id = horizontal ? (long long)(base + b) * g.nfx + s : (long long)s * g.nfx + base + b;
+                    const long long id =
+                      horizontal ? (long long)(base + b) * g.nfx + s : (long long)s * g.nfx + base + b;
                     d += dn[b] * u[id];
                   }
                 d /= hn;
@@ -545,12 +735,36 @@ namespace lbfem_gpu
   }
 
   // ------------------------------------------------------ mass matrix (K2)
+  // staged footprint + x-pass output + `own` own-node vectors
   template <int P>
   constexpr size_t
-  mass_smem()
+  mass_smem(int own = 0)
   {
     using T = Tile<P>;
-    return sizeof(double) * (4 * T::TX * T::K + 4 * T::TY * T::K + T::HN + T::HY * T::TX);
+    return sizeof(double) * (T::NF + T::NY + own * T::TX * T::TY);
+  }
+
+  // The mass operator My (x) Mx of the staged field s_u for every own node of the
+  // tile: emit(i, j, storage index, Au, own u); images get the identity row.
+  template <int P, typename Emit>
+  __device__ __forceinline__ void
+  mass_apply(const double *s_u, double *s_t, const TileMaps<P> &m, const Grid &g, int gx0, int gy0, Emit &&emit)
+  {
+    using T = Tile<P>;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp < T::NSX && lane < T::FY)
+      mass_xpass<P>(s_u, s_t, m, lane, warp);
+    __syncthreads();
+    const int j = threadIdx.x % T::YL, seg = threadIdx.x / T::YL;
+    if (j < T::TX && seg < T::NSY)
+      {
+        const int gx = gx0 + j;
+        mass_ypass<P>(s_t, m, j, seg, [&](int i, double v) {
+          const int gy = gy0 + i;
+          if (gx < g.nfx && gy < g.nfy)
+            emit(i, j, (long long)gy * g.nfx + gx, is_image(gx, gy, g), v);
+        });
+      }
   }
 
   // y = M x for nsys vectors, the identity on images (MassOperator vmult).
@@ -559,31 +773,24 @@ namespace lbfem_gpu
     k_mass_vmult(const Geo geo, const double *__restrict__ x, double *__restrict__ y, int nsys)
   {
     using T = Tile<P>;
-    constexpr int TX = T::TX, TY = T::TY, HX = T::HX, K = T::K;
     extern __shared__ double sm[];
-    double *s_rx = sm, *s_ry = s_rx + 4 * TX * K, *s_u = s_ry + 4 * TY * K, *s_t = s_u + T::HN;
+    __shared__ TileMaps<P> maps;
+    double *s_u = sm, *s_t = sm + T::NF;
     const Grid &g = geo.g;
     const long long N = g.N;
-    const int gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
-    load_rows<P>(s_rx, geo.rowx, gx0, TX, g.nfx);
-    load_rows<P>(s_ry, geo.rowy, gy0, TY, g.nfy);
+    const int gx0 = blockIdx.x * T::TX, gy0 = blockIdx.y * T::TY;
+    build_maps<P>(maps, geo, gx0, gy0);
+    __syncthreads();
     for (int s = 0; s < nsys; ++s)
       {
-        load_tile<P>(s_u, x + s * N, g, gx0, gy0);
+        const double *xs = x + s * N;
+        stage<P>(s_u, maps, [&](long long idx) { return xs[idx]; });
         __syncthreads();
-        xpass<P>(s_u, s_rx, s_t);
-        __syncthreads();
-        for (int t = threadIdx.x; t < TY * TX; t += blockDim.x)
-          {
-            const int lyo = t / TX, lxo = t - lyo * TX, gx = gx0 + lxo, gy = gy0 + lyo;
-            if (gx >= g.nfx || gy >= g.nfy)
-              continue;
-            const long long idx = (long long)gy * g.nfx + gx;
-            y[s * N + idx] = is_image(gx, gy, g) ? x[s * N + idx] : ypass_at<P>(s_t, s_ry, lyo, lxo);
-          }
+        mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int, int, long long idx, bool image, double v) {
+          y[s * N + idx] = image ? xs[idx] : v;
+        });
         __syncthreads();
       }
-    (void)HX;
   }
 
   // ------------------------------------------- Jacobi-PCG, 8 systems at once (K3)
@@ -592,9 +799,15 @@ namespace lbfem_gpu
   {
     double tol[NM], rz[NM], rz_prev[NM], beta[NM], alpha[NM], res[NM];
     int it[NM], active[NM];
-    int status, n_active;
+    int status, n_active, iter;
     unsigned long long total_its;
   };
+
+  __device__ __forceinline__ double
+  inv_jacobi_at(const Geo &geo, int i, int j)
+  {
+    return is_image(i, j, geo.g) ? 1.0 : geo.ijx[i] * geo.ijy[j];
+  }
 
   // r = b - A xg with xg = extrapolate ? 2 x_cur - x_prev (written to x_new) : x_new;
   // partials per system: b.b, r.r, r.D^{-1}r.
@@ -602,170 +815,151 @@ namespace lbfem_gpu
   __global__ void __launch_bounds__(THREADS)
     k_cg_start(const Geo geo, const double *__restrict__ b, const double *__restrict__ x_cur,
                const double *__restrict__ x_prev, double *__restrict__ x_new, double *__restrict__ r, int extrapolate,
-               int nsys, double *__restrict__ partials)
+               double *__restrict__ partials)
   {
     using T = Tile<P>;
-    constexpr int TX = T::TX, TY = T::TY, HX = T::HX, K = T::K;
     extern __shared__ double sm[];
-    double *s_rx = sm, *s_ry = s_rx + 4 * TX * K, *s_u = s_ry + 4 * TY * K, *s_t = s_u + T::HN;
+    __shared__ TileMaps<P> maps;
+    double *s_u = sm, *s_t = sm + T::NF;
     const Grid &g = geo.g;
     const long long N = g.N;
-    const int gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
-    load_rows<P>(s_rx, geo.rowx, gx0, TX, g.nfx);
-    load_rows<P>(s_ry, geo.rowy, gy0, TY, g.nfy);
-    double part[3 * NM];
-#pragma unroll
-    for (int q = 0; q < 3 * NM; ++q)
-      part[q] = 0;
-    for (int s = 0; s < nsys; ++s)
-      {
-        for (int t = threadIdx.x; t < T::HN; t += blockDim.x)
-          {
-            const int ly = t / HX, lx = t - ly * HX;
-            const int sx = wrap(gx0 - P + lx, g.px, g.nux, g.nfx), sy = wrap(gy0 - P + ly, g.py, g.nuy, g.nfy);
-            double v = 0;
-            if (sx >= 0 && sy >= 0)
-              {
-                const long long id = s * N + (long long)sy * g.nfx + sx;
-                v = extrapolate ? -x_prev[id] + 2. * x_cur[id] : x_new[id];
-              }
-            s_u[t] = v;
-          }
-        __syncthreads();
-        xpass<P>(s_u, s_rx, s_t);
-        __syncthreads();
-        for (int t = threadIdx.x; t < TY * TX; t += blockDim.x)
-          {
-            const int lyo = t / TX, lxo = t - lyo * TX, gx = gx0 + lxo, gy = gy0 + lyo;
-            if (gx >= g.nfx || gy >= g.nfy)
-              continue;
-            const long long id = s * N + (long long)gy * g.nfx + gx;
-            double xg, Ax;
-            if (is_image(gx, gy, g))
-              {
-                xg = extrapolate ? -x_prev[id] + 2. * x_cur[id] : x_new[id];
-                Ax = xg;
-              }
-            else
-              {
-                xg = s_u[(lyo + P) * HX + lxo + P];
-                Ax = ypass_at<P>(s_t, s_ry, lyo, lxo);
-              }
-            if (extrapolate)
-              x_new[id] = xg;
-            const double bb = b[id];
-            const double rr = -Ax + bb;
-            r[id] = rr;
-            part[s] += bb * bb;
-            part[NM + s] += rr * rr;
-            part[2 * NM + s] += rr * (inv_jacobi(gx, gy, geo) * rr);
-          }
-        __syncthreads();
-      }
-    block_reduce_store<3 * NM>(part, 3 * NM, partials, blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y);
+    const int s = blockIdx.z;
+    const int gx0 = blockIdx.x * T::TX, gy0 = blockIdx.y * T::TY;
+    build_maps<P>(maps, geo, gx0, gy0);
+    __syncthreads();
+    const long long o = s * N;
+    double *s_b = s_t + T::NY;
+    stage<P>(s_u, maps, [&](long long idx) {
+      return extrapolate ? -x_prev[o + idx] + 2. * x_cur[o + idx] : x_new[o + idx];
+    });
+    stage_own<P>(s_b, b + o, g, gx0, gy0);
+    __syncthreads();
+    double part[3] = {0, 0, 0};
+    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, long long idx, bool image, double Ax) {
+      const long long id = o + idx;
+      double xg;
+      if (image)
+        {
+          xg = extrapolate ? -x_prev[id] + 2. * x_cur[id] : x_new[id];
+          Ax = xg;
+        }
+      else
+        xg = s_u[(i + P) * T::PF + j + P];
+      if (extrapolate)
+        x_new[id] = xg;
+      const double bb = s_b[i * T::TX + j];
+      const double rr = -Ax + bb;
+      r[id] = rr;
+      const int gy = int(idx / g.nfx), gx = int(idx - (long long)gy * g.nfx);
+      part[0] += bb * bb;
+      part[1] += rr * rr;
+      part[2] += rr * (inv_jacobi_at(geo, gx, gy) * rr);
+    });
+    const int nt = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
+    // partial (quantity k of system s) at [(k*NM + s) * n_tiles + tile]
+    block_reduce_store<3>(part, partials + (long long)s * nt, tile, NM * nt);
   }
 
-  // p <- D^{-1} r + beta p (p <- D^{-1} r on the first iteration), v = A p; partials p.v.
+  // p <- D^{-1} r + beta p (p <- D^{-1} r on the first iteration); partial p.Ap. One system per CTA.
   template <int P>
   __global__ void __launch_bounds__(THREADS)
-    k_cg_pv(const Geo geo, const double *__restrict__ r, const double *__restrict__ p_in, double *__restrict__ p_out,
-            double *__restrict__ v, const CgState *__restrict__ st, int nsys, double *__restrict__ partials)
+    k_cg_p(const Geo geo, const double *__restrict__ r, const double *__restrict__ p_in, double *__restrict__ p_out,
+           const CgState *__restrict__ st, double *__restrict__ partials)
   {
     using T = Tile<P>;
-    constexpr int TX = T::TX, TY = T::TY, HX = T::HX, K = T::K;
     extern __shared__ double sm[];
-    double *s_rx = sm, *s_ry = s_rx + 4 * TX * K, *s_u = s_ry + 4 * TY * K, *s_t = s_u + T::HN;
+    __shared__ TileMaps<P> maps;
+    double *s_u = sm, *s_t = sm + T::NF;
     const Grid &g = geo.g;
     const long long N = g.N;
-    const int gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
-    load_rows<P>(s_rx, geo.rowx, gx0, TX, g.nfx);
-    load_rows<P>(s_ry, geo.rowy, gy0, TY, g.nfy);
-    double part[NM];
-#pragma unroll
-    for (int q = 0; q < NM; ++q)
-      part[q] = 0;
-    for (int s = 0; s < nsys; ++s)
+    const int s = blockIdx.z;
+    const int nt = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
+    if (!st->active[s])
+      return;
+    const int gx0 = blockIdx.x * T::TX, gy0 = blockIdx.y * T::TY;
+    build_maps<P>(maps, geo, gx0, gy0);
+    const bool first = st->it[s] == 0;
+    const double beta = st->beta[s];
+    const long long o = s * N;
+    __syncthreads();
+    for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
       {
-        if (!st->active[s])
-          continue;
-        const bool first = st->it[s] == 0;
-        const double beta = st->beta[s];
-        for (int t = threadIdx.x; t < T::HN; t += blockDim.x)
+        const int fy = t / T::FX, fx = t - fy * T::FX;
+        const long long rw = maps.row[fy];
+        const int c = maps.col[fx];
+        double v = 0;
+        if (rw >= 0 && c >= 0)
           {
-            const int ly = t / HX, lx = t - ly * HX;
-            const int sx = wrap(gx0 - P + lx, g.px, g.nux, g.nfx), sy = wrap(gy0 - P + ly, g.py, g.nuy, g.nfy);
-            double val = 0;
-            if (sx >= 0 && sy >= 0)
-              {
-                const long long id = s * N + (long long)sy * g.nfx + sx;
-                const double z = inv_jacobi(sx, sy, geo) * r[id];
-                val = first ? z : beta * p_in[id] + z;
-              }
-            s_u[t] = val;
+            const long long id = o + rw + c;
+            const double z = inv_jacobi_at(geo, c, maps.rowi[fy]) * r[id];
+            v = first ? z : fma(beta, p_in[id], z);
           }
-        __syncthreads();
-        xpass<P>(s_u, s_rx, s_t);
-        __syncthreads();
-        for (int t = threadIdx.x; t < TY * TX; t += blockDim.x)
-          {
-            const int lyo = t / TX, lxo = t - lyo * TX, gx = gx0 + lxo, gy = gy0 + lyo;
-            if (gx >= g.nfx || gy >= g.nfy)
-              continue;
-            const long long id = s * N + (long long)gy * g.nfx + gx;
-            double pn, vn;
-            if (is_image(gx, gy, g))
-              {
-                pn = first ? r[id] : beta * p_in[id] + r[id];
-                vn = pn;
-              }
-            else
-              {
-                pn = s_u[(lyo + P) * HX + lxo + P];
-                vn = ypass_at<P>(s_t, s_ry, lyo, lxo);
-              }
-            p_out[id] = pn;
-            v[id] = vn;
-            part[s] += pn * vn;
-          }
-        __syncthreads();
+        s_u[fy * T::PF + fx] = v;
       }
-    block_reduce_store<NM>(part, NM, partials, blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y);
+    __syncthreads();
+    double part[1] = {0};
+    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, long long idx, bool image, double Ap) {
+      const long long id = o + idx;
+      double pn;
+      if (image)
+        {
+          pn = first ? r[id] : fma(beta, p_in[id], r[id]);
+          Ap = pn;
+        }
+      else
+        pn = s_u[(i + P) * T::PF + j + P];
+      p_out[id] = pn;
+      part[0] += pn * Ap;
+    });
+    block_reduce_store<1>(part, partials + (long long)s * nt, tile, NM * nt);
   }
 
-  // x += alpha p, r -= alpha v; partials r.r, r.D^{-1}r.
+  // v = A p recomputed; x += alpha p, r -= alpha v; partials r.r, r.D^{-1}r. One system per CTA.
+  template <int P>
   __global__ void __launch_bounds__(THREADS)
     k_cg_update(const Geo geo, double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
-                const double *__restrict__ v, const CgState *__restrict__ st, int nsys, double *__restrict__ partials)
+                const CgState *__restrict__ st, double *__restrict__ partials)
   {
+    using T = Tile<P>;
+    extern __shared__ double sm[];
+    __shared__ TileMaps<P> maps;
+    double *s_u = sm, *s_t = sm + T::NF;
     const Grid &g = geo.g;
     const long long N = g.N;
-    double part[2 * NM];
-#pragma unroll
-    for (int q = 0; q < 2 * NM; ++q)
-      part[q] = 0;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N;
-         idx += (long long)gridDim.x * blockDim.x)
-      {
-        const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
-        const double inv = inv_jacobi(i, j, geo);
-        for (int s = 0; s < nsys; ++s)
-          {
-            if (!st->active[s])
-              continue;
-            const double al = st->alpha[s];
-            const long long id = s * N + idx;
-            x[id] += al * p[id];
-            const double rr = r[id] + -al * v[id];
-            r[id] = rr;
-            part[s] += rr * rr;
-            part[NM + s] += rr * (inv * rr);
-          }
-      }
-    block_reduce_store<2 * NM>(part, 2 * NM, partials, blockIdx.x, gridDim.x);
+    const int s = blockIdx.z;
+    const int nt = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
+    if (!st->active[s])
+      return;
+    const int gx0 = blockIdx.x * T::TX, gy0 = blockIdx.y * T::TY;
+    build_maps<P>(maps, geo, gx0, gy0);
+    const double al = st->alpha[s];
+    const long long o = s * N;
+    const double *ps = p + o;
+    double *s_x = s_t + T::NY, *s_r = s_x + T::TX * T::TY;
+    __syncthreads();
+    stage<P>(s_u, maps, [&](long long idx) { return ps[idx]; });
+    stage_own<P>(s_x, x + o, g, gx0, gy0);
+    stage_own<P>(s_r, r + o, g, gx0, gy0);
+    __syncthreads();
+    double part[2] = {0, 0};
+    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, long long idx, bool image, double Ap) {
+      const long long id = o + idx;
+      const double pv = image ? p[id] : s_u[(i + P) * T::PF + j + P];
+      if (image)
+        Ap = pv;
+      const int t = i * T::TX + j;
+      x[id] = s_x[t] + al * pv;
+      const double rr = s_r[t] + -al * Ap;
+      r[id] = rr;
+      const int gy = int(idx / g.nfx), gx = int(idx - (long long)gy * g.nfx);
+      part[0] += rr * rr;
+      part[1] += rr * (inv_jacobi_at(geo, gx, gy) * rr);
+    });
+    block_reduce_store<2>(part, partials + (long long)s * nt, tile, NM * nt);
   }
 
   // The scalar work of one CG phase, one thread per system, from the reduced sums.
-  // phase 0 (after start): sums = [bb, rr, rz]; phase 1 (after pv): [pv];
+  // phase 0 (after start): sums = [bb, rr, rz]; phase 1 (after p): [pAp];
   // phase 2 (after update): [rr, rz].
   __global__ void
   k_cg_scalars(CgState *st, const double *__restrict__ sums, int nsys, int phase, double cg_tol, int max_its)
@@ -832,6 +1026,8 @@ namespace lbfem_gpu
         for (int k = 0; k < NM; ++k)
           n += st->active[k];
         st->n_active = n;
+        if (phase == 2)
+          ++st->iter;
       }
   }
 } // namespace lbfem_gpu

@@ -148,8 +148,10 @@ def test_step(gpu_lib, oracle_mod, scheme, mass, case, p, n, steps):
     g, o = _run_pair(oracle_mod, tc, m, prm, m.time_step(0.3), steps)
     a, b = g.get_populations(), o.get_populations()
     assert rel_l2(a, b) <= 1e-12, rel_l2(a, b)
-    if mass == "cg":
-        assert abs(g.cg_iterations() - o.cg_iterations()) <= steps // 10
+    if mass == "cg" and case != "couette":
+        # Couette is uniform in x: the right-hand sides of the axis populations are pure round-off,
+        # so their stopping iteration is noise; elsewhere the counts agree closely
+        assert abs(g.cg_iterations() - o.cg_iterations()) <= 0.05 * o.cg_iterations() + 2
     ca, cb = g.conservation(), o.conservation()
     assert np.allclose(ca, cb, rtol=1e-12, atol=1e-15)
 
