@@ -230,6 +230,26 @@ int lbfem_gpu_advection_resident(lbfem_gpu_ctx *ctx);
 /* Statistics of the last lbfem_gpu_step call: CG iterations per solve (mean) and kernel launches. */
 int lbfem_gpu_last_step_stats(const lbfem_gpu_ctx *ctx, double *cg_iterations_per_solve, int64_t *kernel_launches);
 
+/*
+ * The mass solve of lbfem_gpu_mass_solve (consistent mass, Jacobi-PCG) for
+ * callers that cannot allocate device memory at the time of the call: for
+ * example code that runs while a CUDA stream is being captured, or a host
+ * framework that must own every device allocation. It has no counterpart in
+ * the reference.
+ *
+ * x (in: start, out: solution) and r are DEVICE pointers to n_dofs doubles in
+ * the structured numbering (the context must have been created without
+ * dof_index). The CG work buffers are not the context's: they live in one
+ * fixed file-scope device array of the library (about 3.8 MiB, held by every
+ * GPU that loads the library until the process exits), so the call allocates
+ * nothing. Limits: at most 131072 nodes and 4096 tiles; larger meshes are
+ * rejected with LBFEM_ERR_ARG. The first call on a device looks up the array's
+ * device address; make that first call before any stream capture. All calls
+ * share the array: calls that overlap on the GPU race. Iterations are not
+ * added to lbfem_gpu_cg_iterations. Returns when the solve has finished.
+ */
+int lbfem_gpu_mass_solve_noalloc(lbfem_gpu_ctx *ctx, double *x, const double *r);
+
 #ifdef __cplusplus
 }
 #endif

@@ -266,37 +266,54 @@ namespace
   }
 
   // ------------------------------------------------------ mass solve (K2-K4)
-  // x_new <- A^{-1} b for nsys systems (extrapolated start or the given x_new).
+  // The work buffers of one CG run: residual, two search directions, per-tile
+  // partial sums, reduced sums and the per-system solver state.
+  struct CgScratch
+  {
+    double *r, *p[2], *partials, *sums;
+    CgState *state;
+  };
+
   int
-  cg_solve(lbfem_gpu_ctx *ctx, const double *b, double *x_new, const double *x_cur, const double *x_prev,
-           int extrapolate, int nsys, int64_t *its_out)
+  reduce_into(lbfem_gpu_ctx *ctx, const double *partials, double *sums, int n_blocks, int nq)
+  {
+    k_reduce_partials<<<nq, 256, 0, ctx->stream>>>(partials, n_blocks, sums);
+    LAUNCHED();
+    return LBFEM_OK;
+  }
+
+  // x_new <- A^{-1} b for nsys systems (extrapolated start or the given x_new),
+  // with the work buffers w. *its_out: CG iterations summed over the systems.
+  int
+  cg_run(lbfem_gpu_ctx *ctx, const CgScratch &w, const double *b, double *x_new, const double *x_cur,
+         const double *x_prev, int extrapolate, int nsys, int64_t *its_out)
   {
     const Geo geo = geo_of(ctx);
     const Grid &g = ctx->grid;
     const double tol = ctx->prm.cg_tolerance;
     const int max_its = ctx->prm.cg_max_iterations;
-    CK(cudaMemsetAsync(ctx->d_cg, 0, sizeof(CgState), ctx->stream));
+    CK(cudaMemsetAsync(w.state, 0, sizeof(CgState), ctx->stream));
     int n_tiles = 0;
     int st = with_degree(ctx->P, [&](auto PP) -> int {
       constexpr int P = decltype(PP)::value;
       dim3 grid = tile_grid<P>(g);
       n_tiles = int(grid.x * grid.y);
       grid.z = nsys;
-      k_cg_start<P><<<grid, THREADS, mass_smem<P>(1), ctx->stream>>>(geo, b, x_cur, x_prev, x_new, ctx->d_r,
-                                                                      extrapolate, ctx->d_partials);
+      k_cg_start<P><<<grid, THREADS, mass_smem<P>(1), ctx->stream>>>(geo, b, x_cur, x_prev, x_new, w.r, extrapolate,
+                                                                      w.partials);
       LAUNCHED();
       return LBFEM_OK;
     });
     if (st)
       return st;
-    if ((st = reduce(ctx, n_tiles, 3 * NM)))
+    if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, 3 * NM)))
       return st;
-    k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nsys, 0, tol, max_its);
+    k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 0, tol, max_its);
     LAUNCHED();
     int pi = 0;
     for (int it = 0;; ++it)
       {
-        CK(cudaMemcpyAsync(ctx->h_cg, ctx->d_cg, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->h_cg, w.state, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
         if (ctx->h_cg->n_active == 0)
           break;
@@ -304,42 +321,55 @@ namespace
           constexpr int P = decltype(PP)::value;
           dim3 grid = tile_grid<P>(g);
           grid.z = nsys;
-          k_cg_p<P><<<grid, THREADS, mass_smem<P>(), ctx->stream>>>(geo, ctx->d_r, ctx->d_p[pi], ctx->d_p[1 - pi],
-                                                                     ctx->d_cg, ctx->d_partials);
+          k_cg_p<P><<<grid, THREADS, mass_smem<P>(), ctx->stream>>>(geo, w.r, w.p[pi], w.p[1 - pi], w.state,
+                                                                     w.partials);
           LAUNCHED();
           return LBFEM_OK;
         });
         if (st)
           return st;
-        if ((st = reduce(ctx, n_tiles, NM)))
+        if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, NM)))
           return st;
-        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nsys, 1, tol, max_its);
+        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 1, tol, max_its);
         LAUNCHED();
         pi = 1 - pi;
         st = with_degree(ctx->P, [&](auto PP) -> int {
           constexpr int P = decltype(PP)::value;
           dim3 grid = tile_grid<P>(g);
           grid.z = nsys;
-          k_cg_update<P><<<grid, THREADS, mass_smem<P>(2), ctx->stream>>>(geo, x_new, ctx->d_r, ctx->d_p[pi],
-                                                                          ctx->d_cg, ctx->d_partials);
+          k_cg_update<P><<<grid, THREADS, mass_smem<P>(2), ctx->stream>>>(geo, x_new, w.r, w.p[pi], w.state,
+                                                                          w.partials);
           LAUNCHED();
           return LBFEM_OK;
         });
         if (st)
           return st;
-        if ((st = reduce(ctx, n_tiles, 2 * NM)))
+        if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, 2 * NM)))
           return st;
-        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nsys, 2, tol, max_its);
+        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 2, tol, max_its);
         LAUNCHED();
       }
     if (its_out)
       *its_out = ctx->h_cg->total_its;
-    ctx->cg_its += ctx->h_cg->total_its;
     if (ctx->h_cg->status == 2)
       return fail(ctx, LBFEM_ERR_NO_CONVERGENCE, "CG: iteration cap %d reached", max_its);
     if (ctx->h_cg->status == 3)
       return fail(ctx, LBFEM_ERR_NONFINITE, "CG: non-finite residual");
     return LBFEM_OK;
+  }
+
+  // The context's own work buffers.
+  int
+  cg_solve(lbfem_gpu_ctx *ctx, const double *b, double *x_new, const double *x_cur, const double *x_prev,
+           int extrapolate, int nsys, int64_t *its_out)
+  {
+    const CgScratch w{ctx->d_r, {ctx->d_p[0], ctx->d_p[1]}, ctx->d_partials, ctx->d_sums, ctx->d_cg};
+    int64_t its = 0;
+    const int st = cg_run(ctx, w, b, x_new, x_cur, x_prev, extrapolate, nsys, &its);
+    if (its_out)
+      *its_out = its;
+    ctx->cg_its += its;
+    return st;
   }
 
   int
@@ -1120,3 +1150,74 @@ lbfem_gpu_last_step_stats(const lbfem_gpu_ctx *ctx, double *its, int64_t *launch
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Mass solve without allocation.
+//
+// For callers that may not allocate device memory when they call in (code that
+// runs while a stream is being captured, or inside a host framework that owns
+// every device allocation): the CG work buffers of this entry point live in
+// one file-scope device array of fixed size, which every GPU that loads the
+// library holds until the process exits. Its device address is looked up once
+// per device, on the first call with that device current. Calls share the
+// array, so calls that overlap on the GPU (from several threads or streams)
+// race; the solver state is cleared at the start of every call.
+namespace
+{
+  constexpr long long NOALLOC_MAX_NODES = 1LL << 17; // 131072 nodes
+  constexpr long long NOALLOC_MAX_TILES = 4096;
+  constexpr long long NOALLOC_STATE_DOUBLES = (sizeof(CgState) + sizeof(double) - 1) / sizeof(double);
+  constexpr long long NOALLOC_DOUBLES =
+    3 * NOALLOC_MAX_NODES + 3 * NM * NOALLOC_MAX_TILES + 64 + NOALLOC_STATE_DOUBLES;
+
+  static __device__ __align__(256) double noalloc_scratch[NOALLOC_DOUBLES];
+
+  constexpr int NOALLOC_MAX_DEVICES = 64;
+  double *noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+} // namespace
+
+extern "C" int
+lbfem_gpu_mass_solve_noalloc(lbfem_gpu_ctx *ctx, double *x, const double *r)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!x || !r)
+    return fail(ctx, LBFEM_ERR_ARG, "mass_solve_noalloc: null buffer");
+  const long long N = ctx->grid.N;
+  if (N > NOALLOC_MAX_NODES)
+    return fail(ctx, LBFEM_ERR_ARG, "mass_solve_noalloc: %lld nodes exceed the fixed scratch of %lld nodes", N,
+                NOALLOC_MAX_NODES);
+  const long long tiles = with_degree(ctx->P, [&](auto PP) -> int {
+    constexpr int P = decltype(PP)::value;
+    const dim3 tg = tile_grid<P>(ctx->grid);
+    return int(tg.x * tg.y);
+  });
+  if (tiles > NOALLOC_MAX_TILES)
+    return fail(ctx, LBFEM_ERR_ARG, "mass_solve_noalloc: %lld tiles exceed the fixed scratch of %lld tiles", tiles,
+                NOALLOC_MAX_TILES);
+  if (!ctx->identity)
+    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: needs the structured DoF numbering");
+  if (ctx->prm.mass != LBFEM_MASS_CG)
+    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: the consistent mass (CG) only");
+  if (ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES)
+    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: device ordinal %d too large", ctx->device);
+  double *base = noalloc_ptr[ctx->device];
+  if (!base)
+    {
+      CK(cudaGetSymbolAddress((void **)&base, noalloc_scratch));
+      noalloc_ptr[ctx->device] = base;
+    }
+  CgScratch w{};
+  w.r = base;
+  w.p[0] = base + NOALLOC_MAX_NODES;
+  w.p[1] = base + 2 * NOALLOC_MAX_NODES;
+  w.partials = base + 3 * NOALLOC_MAX_NODES;
+  w.sums = w.partials + 3 * NM * NOALLOC_MAX_TILES;
+  w.state = reinterpret_cast<CgState *>(w.sums + 64);
+  const int solve_st = cg_run(ctx, w, r, x, nullptr, nullptr, 0, 1, nullptr);
+  if (solve_st != LBFEM_OK)
+    return solve_st;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return LBFEM_OK;
+}
