@@ -32,6 +32,18 @@ namespace lbfem_gpu
   // Reference 1-D element matrices of FE_Q(p) on [0,1] (exact Gauss integration):
   // [p-1][0] = int l_a l_b, [1] = int l_a l_b', [2] = int l_a' l_b'.
   __device__ __constant__ double c_ref[MAXPD][3][MAXPD + 1][MAXPD + 1];
+  __device__ __constant__ float c_reff[MAXPD][3][MAXPD + 1][MAXPD + 1]; // the same, rounded to FP32
+
+  // Entry (a, b) of reference matrix OP of degree P in the arithmetic type R.
+  template <typename R, int P, int OP>
+  __device__ __forceinline__ R
+  ref(int a, int b)
+  {
+    if constexpr (sizeof(R) == sizeof(float))
+      return c_reff[P - 1][OP][a][b];
+    else
+      return c_ref[P - 1][OP][a][b];
+  }
   enum
   {
     OP_M = 0,
@@ -159,6 +171,37 @@ namespace lbfem_gpu
     return c_W[a] * m.rho * (1. + 3. * eu + 4.5 * eu * eu - 1.5 * uu);
   }
 
+  // FP32 deviation form: d_a = f_a - w_a (rest state rho0 = 1). Exact in real
+  // arithmetic: rho = 1 + sum d, momentum = sum e d, and
+  // feq_a - w_a = w_a (drho + rho (3 e.u + 4.5 (e.u)^2 - 1.5 u.u)).
+  struct MomF
+  {
+    float rho, ux, uy, drho;
+  };
+
+  __device__ __forceinline__ MomF
+  moments_dev(const float (&d)[Q])
+  {
+    float drho = 0, mx = 0, my = 0;
+#pragma unroll
+    for (int a = 0; a < Q; ++a)
+      {
+        drho += d[a];
+        mx += float(c_EX[a]) * d[a];
+        my += float(c_EY[a]) * d[a];
+      }
+    const float rho = 1.f + drho;
+    return {rho, mx / rho, my / rho, drho};
+  }
+
+  __device__ __forceinline__ float
+  feqd_a(int a, const MomF &m)
+  {
+    const float uu = m.ux * m.ux + m.uy * m.uy;
+    const float eu = float(c_EX[a]) * m.ux + float(c_EY[a]) * m.uy;
+    return float(c_W[a]) * (m.drho + m.rho * (3.f * eu + 4.5f * eu * eu - 1.5f * uu));
+  }
+
   // What a node imposes on its moments (collision.h:53-72).
   __device__ __forceinline__ Mom
   impose_class(Mom m, int k, const Geo &geo)
@@ -173,6 +216,23 @@ namespace lbfem_gpu
 
   __device__ __forceinline__ Mom
   impose(Mom m, long long idx, const Geo &geo)
+  {
+    return geo.wall ? impose_class(m, geo.wall[idx], geo) : m;
+  }
+
+  __device__ __forceinline__ MomF
+  impose_class(MomF m, int k, const Geo &geo)
+  {
+    if (k)
+      {
+        m.ux = float(geo.wall_u[2 * (k - 1)]);
+        m.uy = float(geo.wall_u[2 * (k - 1) + 1]);
+      }
+    return m;
+  }
+
+  __device__ __forceinline__ MomF
+  impose(MomF m, long long idx, const Geo &geo)
   {
     return geo.wall ? impose_class(m, geo.wall[idx], geo) : m;
   }
@@ -244,19 +304,19 @@ namespace lbfem_gpu
   // Per-CTA tables of the footprint: source column and row offset of every
   // footprint column/row (-1 outside a non-periodic domain), the widths of the
   // CX+1 / CY+1 footprint cells and their inverses (0 outside the domain).
-  template <int P>
+  template <int P, typename R = double>
   struct TileMaps
   {
     int col[Tile<P>::FX];
     int rowi[Tile<P>::FY];
     long long row[Tile<P>::FY];
-    double hx[Tile<P>::CX + 1], hxi[Tile<P>::CX + 1], cx[Tile<P>::CX + 1];
-    double hy[Tile<P>::CY + 1], hyi[Tile<P>::CY + 1], cy[Tile<P>::CY + 1];
+    R hx[Tile<P>::CX + 1], hxi[Tile<P>::CX + 1], cx[Tile<P>::CX + 1];
+    R hy[Tile<P>::CY + 1], hyi[Tile<P>::CY + 1], cy[Tile<P>::CY + 1];
   };
 
-  template <int P>
+  template <int P, typename R>
   __device__ __forceinline__ void
-  build_maps(TileMaps<P> &m, const Geo &geo, int gx0, int gy0)
+  build_maps(TileMaps<P, R> &m, const Geo &geo, int gx0, int gy0)
   {
     using T = Tile<P>;
     const Grid &g = geo.g;
@@ -272,23 +332,23 @@ namespace lbfem_gpu
     for (int t = threadIdx.x; t <= T::CX; t += blockDim.x)
       {
         const int c = wrap(cx0 + t, g.px, g.ncx, g.ncx);
-        m.hx[t] = c < 0 ? 0.0 : geo.hx[c];
-        m.hxi[t] = c < 0 ? 0.0 : geo.hxi[c];
-        m.cx[t] = c < 0 ? 0.0 : 1.0;
+        m.hx[t] = R(c < 0 ? 0.0 : geo.hx[c]);
+        m.hxi[t] = R(c < 0 ? 0.0 : geo.hxi[c]);
+        m.cx[t] = R(c < 0 ? 0.0 : 1.0);
       }
     for (int t = threadIdx.x; t <= T::CY; t += blockDim.x)
       {
         const int c = wrap(cy0 + t, g.py, g.ncy, g.ncy);
-        m.hy[t] = c < 0 ? 0.0 : geo.hy[c];
-        m.hyi[t] = c < 0 ? 0.0 : geo.hyi[c];
-        m.cy[t] = c < 0 ? 0.0 : 1.0;
+        m.hy[t] = R(c < 0 ? 0.0 : geo.hy[c]);
+        m.hyi[t] = R(c < 0 ? 0.0 : geo.hyi[c]);
+        m.cy[t] = R(c < 0 ? 0.0 : 1.0);
       }
   }
 
   // s[fy*PF + fx] <- op(storage index) over the footprint (0 outside the domain).
-  template <int P, typename F>
+  template <int P, typename R, typename RM, typename F>
   __device__ __forceinline__ void
-  stage(double *s, const TileMaps<P> &m, F &&value_at)
+  stage(R *s, const TileMaps<P, RM> &m, F &&value_at)
   {
     using T = Tile<P>;
     for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
@@ -296,67 +356,67 @@ namespace lbfem_gpu
         const int fy = t / T::FX, fx = t - fy * T::FX;
         const long long r = m.row[fy];
         const int c = m.col[fx];
-        s[fy * T::PF + fx] = (r >= 0 && c >= 0) ? value_at(r + c) : 0.0;
+        s[fy * T::PF + fx] = (r >= 0 && c >= 0) ? R(value_at(r + c)) : R(0);
       }
   }
 
   // s[i*TX + j] <- src at own node (gx0 + j, gy0 + i) of the tile (0 past the grid).
-  template <int P>
+  template <int P, typename R>
   __device__ __forceinline__ void
-  stage_own(double *s, const double *__restrict__ src, const Grid &g, int gx0, int gy0)
+  stage_own(R *s, const R *__restrict__ src, const Grid &g, int gx0, int gy0)
   {
     using T = Tile<P>;
     for (int t = threadIdx.x; t < T::TY * T::TX; t += blockDim.x)
       {
         const int i = t / T::TX, j = t - i * T::TX;
         const int gx = gx0 + j, gy = gy0 + i;
-        s[t] = (gx < g.nfx && gy < g.nfy) ? src[(long long)gy * g.nfx + gx] : 0.0;
+        s[t] = (gx < g.nfx && gy < g.nfy) ? src[(long long)gy * g.nfx + gx] : R(0);
       }
   }
 
   // y[a] = sum_b R[a][b] u[b] for the reference element matrix OP.
-  template <int P, int OP>
+  template <int P, int OP, typename R>
   __device__ __forceinline__ void
-  elem(const double (&u)[P + 1], double (&y)[P + 1])
+  elem(const R (&u)[P + 1], R (&y)[P + 1])
   {
 #pragma unroll
     for (int a = 0; a <= P; ++a)
       {
-        double s = c_ref[P - 1][OP][a][0] * u[0];
+        R s = ref<R, P, OP>(a, 0) * u[0];
 #pragma unroll
         for (int b = 1; b <= P; ++b)
-          s = fma(c_ref[P - 1][OP][a][b], u[b], s);
+          s = fma(ref<R, P, OP>(a, b), u[b], s);
         y[a] = s;
       }
   }
 
   // The last row (right vertex) only.
-  template <int P, int OP>
-  __device__ __forceinline__ double
-  elem_last(const double (&u)[P + 1])
+  template <int P, int OP, typename R>
+  __device__ __forceinline__ R
+  elem_last(const R (&u)[P + 1])
   {
-    double s = c_ref[P - 1][OP][P][0] * u[0];
+    R s = ref<R, P, OP>(P, 0) * u[0];
 #pragma unroll
     for (int b = 1; b <= P; ++b)
-      s = fma(c_ref[P - 1][OP][P][b], u[b], s);
+      s = fma(ref<R, P, OP>(P, b), u[b], s);
     return s;
   }
 
   // The x pass of a mass-type operator (OP_M with the cell width as scale) on one
   // footprint row and one x segment: out[fy*PY + j] for the segment's own columns j.
-  template <int P>
+  template <int P, typename R>
   __device__ __forceinline__ void
-  mass_xpass(const double *__restrict__ s, double *__restrict__ out, const TileMaps<P> &m, int fy, int seg)
+  mass_xpass(const R *__restrict__ s, R *__restrict__ out, const TileMaps<P, R> &m, int fy, int seg)
   {
     using T = Tile<P>;
-    const double *row = s + fy * T::PF;
-    double *orow = out + fy * T::PY;
+    const R *row = s + fy * T::PF;
+    R *orow = out + fy * T::PY;
     const int q0 = seg * T::KX; // halo cell (footprint cell index)
-    double u[P + 1];
+    R u[P + 1];
 #pragma unroll
     for (int b = 0; b <= P; ++b)
       u[b] = row[q0 * P + b];
-    double pend = m.hx[q0] * elem_last<P, OP_M>(u);
+    R pend = m.hx[q0] * elem_last<P, OP_M>(u);
 #pragma unroll
     for (int q = 1; q <= T::KX; ++q)
       {
@@ -365,9 +425,9 @@ namespace lbfem_gpu
 #pragma unroll
         for (int b = 1; b <= P; ++b)
           u[b] = row[qc * P + b];
-        double y[P + 1];
+        R y[P + 1];
         elem<P, OP_M>(u, y);
-        const double sc = m.hx[qc];
+        const R sc = m.hx[qc];
         const int j0 = (qc - 1) * P;
         orow[j0] = fma(sc, y[0], pend);
 #pragma unroll
@@ -379,17 +439,17 @@ namespace lbfem_gpu
 
   // The y pass of a mass-type operator on column j and y segment seg: calls
   // emit(own row i, value) for the segment's SY own rows.
-  template <int P, typename Emit>
+  template <int P, typename R, typename Emit>
   __device__ __forceinline__ void
-  mass_ypass(const double *__restrict__ t, const TileMaps<P> &m, int j, int seg, Emit &&emit)
+  mass_ypass(const R *__restrict__ t, const TileMaps<P, R> &m, int j, int seg, Emit &&emit)
   {
     using T = Tile<P>;
     const int q0 = seg * T::KY;
-    double u[P + 1];
+    R u[P + 1];
 #pragma unroll
     for (int b = 0; b <= P; ++b)
       u[b] = t[(q0 * P + b) * T::PY + j];
-    double pend = m.hy[q0] * elem_last<P, OP_M>(u);
+    R pend = m.hy[q0] * elem_last<P, OP_M>(u);
 #pragma unroll
     for (int q = 1; q <= T::KY; ++q)
       {
@@ -398,9 +458,9 @@ namespace lbfem_gpu
 #pragma unroll
         for (int b = 1; b <= P; ++b)
           u[b] = t[(qc * P + b) * T::PY + j];
-        double y[P + 1];
+        R y[P + 1];
         elem<P, OP_M>(u, y);
-        const double sc = m.hy[qc];
+        const R sc = m.hy[qc];
         const int i0 = (qc - 1) * P;
         emit(i0, fma(sc, y[0], pend));
 #pragma unroll

@@ -50,6 +50,10 @@ struct lbfem_gpu_ctx
   int x_cur = 0, x_prev = 1, x_new = 2;
   double *d_r = nullptr, *d_p[2] = {nullptr, nullptr}, *d_v = nullptr;
   double *d_feq = nullptr, *d_stage = nullptr;
+  // mixed precision: FP32 deviations f - w and FP32 streaming / CG vectors
+  bool mixed = false;
+  float *d_fs[2] = {nullptr, nullptr}, *d_rhs_s = nullptr, *d_x_s[3] = {nullptr, nullptr, nullptr};
+  float *d_r_s = nullptr, *d_p_s[2] = {nullptr, nullptr};
   double *d_partials = nullptr, *d_sums = nullptr;
   size_t partial_cap = 0;
   CgState *d_cg = nullptr;
@@ -151,22 +155,41 @@ namespace
       }
   }
 
+  template <int P, typename R>
+  constexpr size_t
+  cg_smem(int own, bool fp64_arith = false)
+  {
+    using T = Tile<P>;
+    return (fp64_arith ? sizeof(double) : sizeof(R)) * (T::NF + T::NY) + sizeof(R) * own * T::TX * T::TY;
+  }
+
+  template <typename K>
+  int
+  set_smem(lbfem_gpu_ctx *ctx, K kernel, size_t bytes)
+  {
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    return LBFEM_OK;
+  }
+
   template <int P>
   int
   set_smem_attributes(lbfem_gpu_ctx *ctx)
   {
-    CK(cudaFuncSetAttribute(k_advection<P, ADV_TG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            int(advection_smem<P, ADV_TG>())));
-    CK(cudaFuncSetAttribute(k_advection<P, ADV_TG_COLLIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            int(advection_smem<P, ADV_TG_COLLIDE>())));
-    CK(cudaFuncSetAttribute(k_advection<P, ADV_LEELIN_FEQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            int(advection_smem<P, ADV_LEELIN_FEQ>())));
-    CK(cudaFuncSetAttribute(k_advection<P, ADV_LEELIN_FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            int(advection_smem<P, ADV_LEELIN_FUSED>())));
-    CK(cudaFuncSetAttribute(k_mass_vmult<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>())));
-    CK(cudaFuncSetAttribute(k_cg_start<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>(1))));
-    CK(cudaFuncSetAttribute(k_cg_p<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>())));
-    CK(cudaFuncSetAttribute(k_cg_update<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mass_smem<P>(2))));
+    int st;
+    if ((st = set_smem(ctx, k_advection<P, ADV_TG, double>, advection_smem<P, ADV_TG, double>())) ||
+        (st = set_smem(ctx, k_advection<P, ADV_TG_COLLIDE, double>, advection_smem<P, ADV_TG_COLLIDE, double>())) ||
+        (st = set_smem(ctx, k_advection<P, ADV_LEELIN_FEQ, double>, advection_smem<P, ADV_LEELIN_FEQ, double>())) ||
+        (st = set_smem(ctx, k_advection<P, ADV_LEELIN_FUSED, double>, advection_smem<P, ADV_LEELIN_FUSED, double>())) ||
+        (st = set_smem(ctx, k_advection<P, ADV_TG_COLLIDE, float>, advection_smem<P, ADV_TG_COLLIDE, float>())) ||
+        (st = set_smem(ctx, k_advection<P, ADV_LEELIN_FUSED, float>, advection_smem<P, ADV_LEELIN_FUSED, float>())) ||
+        (st = set_smem(ctx, k_mass_vmult<P>, cg_smem<P, double>(0))) ||
+        (st = set_smem(ctx, k_cg_start<P, double, double, double>, cg_smem<P, double>(1))) ||
+        (st = set_smem(ctx, k_cg_p<P, double>, cg_smem<P, double>(0))) ||
+        (st = set_smem(ctx, k_cg_update<P, double>, cg_smem<P, double>(2))) ||
+        (st = set_smem(ctx, k_cg_start<P, float, double, double>, cg_smem<P, float>(1, true))) ||
+        (st = set_smem(ctx, k_cg_p<P, float>, cg_smem<P, float>(0))) ||
+        (st = set_smem(ctx, k_cg_update<P, float>, cg_smem<P, float>(2))))
+      return st;
     return LBFEM_OK;
   }
 
@@ -202,9 +225,9 @@ namespace
     return e;
   }
 
+  template <typename R>
   int
-  launch_advection(lbfem_gpu_ctx *ctx, int mode, const double *f, const double *feq, double *fout, double *rhs,
-                   const AdvCoef &ac)
+  launch_advection(lbfem_gpu_ctx *ctx, int mode, const R *f, const R *feq, R *fout, R *rhs, const AdvCoef &ac)
   {
     const Geo geo = geo_of(ctx);
     return with_degree(ctx->P, [&](auto PP) -> int {
@@ -213,28 +236,31 @@ namespace
       switch (mode)
         {
           case ADV_TG:
-            k_advection<P, ADV_TG><<<grid, THREADS, advection_smem<P, ADV_TG>(), ctx->stream>>>(geo, f, feq, fout,
-                                                                                               rhs, ac);
+            if constexpr (sizeof(R) == sizeof(double))
+              k_advection<P, ADV_TG, R>
+                <<<grid, THREADS, advection_smem<P, ADV_TG, R>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
             break;
           case ADV_TG_COLLIDE:
-            k_advection<P, ADV_TG_COLLIDE>
-              <<<grid, THREADS, advection_smem<P, ADV_TG_COLLIDE>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
+            k_advection<P, ADV_TG_COLLIDE, R>
+              <<<grid, THREADS, advection_smem<P, ADV_TG_COLLIDE, R>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
             break;
           case ADV_LEELIN_FEQ:
-            k_advection<P, ADV_LEELIN_FEQ>
-              <<<grid, THREADS, advection_smem<P, ADV_LEELIN_FEQ>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
+            if constexpr (sizeof(R) == sizeof(double))
+              k_advection<P, ADV_LEELIN_FEQ, R>
+                <<<grid, THREADS, advection_smem<P, ADV_LEELIN_FEQ, R>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
             break;
           default:
-            k_advection<P, ADV_LEELIN_FUSED>
-              <<<grid, THREADS, advection_smem<P, ADV_LEELIN_FUSED>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
+            k_advection<P, ADV_LEELIN_FUSED, R>
+              <<<grid, THREADS, advection_smem<P, ADV_LEELIN_FUSED, R>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
         }
       LAUNCHED();
       return LBFEM_OK;
     });
   }
 
+  template <typename R>
   int
-  launch_wall_faces(lbfem_gpu_ctx *ctx, const double *f, double *rhs, const double *e, double dt, bool remove)
+  launch_wall_faces(lbfem_gpu_ctx *ctx, const R *f, R *rhs, const double *e, double dt, bool remove)
   {
     if (ctx->n_bnodes == 0)
       return LBFEM_OK;
@@ -258,7 +284,7 @@ namespace
     const Geo geo = geo_of(ctx);
     return with_degree(ctx->P, [&](auto PP) -> int {
       constexpr int P = decltype(PP)::value;
-      k_wall_faces<P><<<(ctx->n_bnodes + 127) / 128, 128, 0, ctx->stream>>>(geo, f, rhs, ctx->d_bnode,
+      k_wall_faces<P, R><<<(ctx->n_bnodes + 127) / 128, 128, 0, ctx->stream>>>(geo, f, rhs, ctx->d_bnode,
                                                                            ctx->n_bnodes, fc);
       LAUNCHED();
       return LBFEM_OK;
@@ -268,10 +294,13 @@ namespace
   // ------------------------------------------------------ mass solve (K2-K4)
   // The work buffers of one CG run: residual, two search directions, per-tile
   // partial sums, reduced sums and the per-system solver state.
+  template <typename R>
   struct CgScratch
   {
-    double *r, *p[2], *partials, *sums;
+    R *r, *p[2];
+    double *partials, *sums;
     CgState *state;
+    R *d; // mixed precision: the FP32 correction of a refinement round (starts at 0)
   };
 
   int
@@ -282,72 +311,107 @@ namespace
     return LBFEM_OK;
   }
 
+  // Mixed precision: each refinement round solves the FP32 correction to
+  // inner_rel times the round's true FP64 residual.
+  constexpr double MIXED_INNER_REL = 1e-4;
+  constexpr int MIXED_MAX_ROUNDS = 50;
+
   // x_new <- A^{-1} b for nsys systems (extrapolated start or the given x_new),
-  // with the work buffers w. *its_out: CG iterations summed over the systems.
+  // with the work buffers w. R = X = double: one CG run. R = float, X = double:
+  // iterative refinement -- each round computes the true residual b - A x in
+  // FP64, solves A d = r for the correction d by FP32 CG (FP64 dot products), and
+  // adds x += d in FP64, until the FP64 residual meets the tolerance.
+  // *its_out: CG iterations summed over the systems.
+  template <typename R, typename X = R>
   int
-  cg_run(lbfem_gpu_ctx *ctx, const CgScratch &w, const double *b, double *x_new, const double *x_cur,
-         const double *x_prev, int extrapolate, int nsys, int64_t *its_out)
+  cg_run(lbfem_gpu_ctx *ctx, const CgScratch<R> &w, const R *b, X *x_new, const X *x_cur, const X *x_prev,
+         int extrapolate, int nsys, int64_t *its_out)
   {
+    constexpr bool MIX = sizeof(R) == sizeof(float);
     const Geo geo = geo_of(ctx);
     const Grid &g = ctx->grid;
     const double tol = ctx->prm.cg_tolerance;
+    const double inner_rel = MIX ? MIXED_INNER_REL : 0.0;
     const int max_its = ctx->prm.cg_max_iterations;
     CK(cudaMemsetAsync(w.state, 0, sizeof(CgState), ctx->stream));
     int n_tiles = 0;
-    int st = with_degree(ctx->P, [&](auto PP) -> int {
-      constexpr int P = decltype(PP)::value;
-      dim3 grid = tile_grid<P>(g);
-      n_tiles = int(grid.x * grid.y);
-      grid.z = nsys;
-      k_cg_start<P><<<grid, THREADS, mass_smem<P>(1), ctx->stream>>>(geo, b, x_cur, x_prev, x_new, w.r, extrapolate,
-                                                                      w.partials);
-      LAUNCHED();
-      return LBFEM_OK;
-    });
-    if (st)
-      return st;
-    if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, 3 * NM)))
-      return st;
-    k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 0, tol, max_its);
-    LAUNCHED();
-    int pi = 0;
-    for (int it = 0;; ++it)
+    int st;
+    bool refined = !MIX; // mixed: a round's FP64 residual met the outer tolerance
+    for (int round = 0; round < (MIX ? MIXED_MAX_ROUNDS : 1); ++round)
       {
-        CK(cudaMemcpyAsync(ctx->h_cg, w.state, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        if (ctx->h_cg->n_active == 0)
+        st = with_degree(ctx->P, [&](auto PP) -> int {
+          constexpr int P = decltype(PP)::value;
+          dim3 grid = tile_grid<P>(g);
+          n_tiles = int(grid.x * grid.y);
+          grid.z = nsys;
+          k_cg_start<P, R, X, double><<<grid, THREADS, cg_smem<P, R>(1, true), ctx->stream>>>(
+            geo, b, x_cur, x_prev, x_new, w.r, extrapolate && round == 0, w.partials);
+          LAUNCHED();
+          return LBFEM_OK;
+        });
+        if (st)
+          return st;
+        if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, 3 * NM)))
+          return st;
+        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 0, tol, max_its, inner_rel);
+        LAUNCHED();
+        int pi = 0;
+        bool outer_done = false; // the round's true residual already meets the tolerance
+        for (int it = 0;; ++it)
+          {
+            CK(cudaMemcpyAsync(ctx->h_cg, w.state, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (ctx->h_cg->n_active == 0)
+              {
+                outer_done = it == 0;
+                break;
+              }
+            st = with_degree(ctx->P, [&](auto PP) -> int {
+              constexpr int P = decltype(PP)::value;
+              dim3 grid = tile_grid<P>(g);
+              grid.z = nsys;
+              k_cg_p<P, R><<<grid, THREADS, cg_smem<P, R>(0), ctx->stream>>>(geo, w.r, w.p[pi], w.p[1 - pi], w.state,
+                                                                              w.partials);
+              LAUNCHED();
+              return LBFEM_OK;
+            });
+            if (st)
+              return st;
+            if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, NM)))
+              return st;
+            k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 1, tol, max_its, inner_rel);
+            LAUNCHED();
+            pi = 1 - pi;
+            st = with_degree(ctx->P, [&](auto PP) -> int {
+              constexpr int P = decltype(PP)::value;
+              dim3 grid = tile_grid<P>(g);
+              grid.z = nsys;
+              R *xi;
+              if constexpr (MIX)
+                xi = w.d;
+              else
+                xi = x_new;
+              k_cg_update<P, R><<<grid, THREADS, cg_smem<P, R>(2), ctx->stream>>>(geo, xi, w.r, w.p[pi], w.state,
+                                                                                   w.partials);
+              LAUNCHED();
+              return LBFEM_OK;
+            });
+            if (st)
+              return st;
+            if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, 2 * NM)))
+              return st;
+            k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 2, tol, max_its, inner_rel);
+            LAUNCHED();
+          }
+        refined = refined || outer_done;
+        if (!MIX || ctx->h_cg->status != 0 || outer_done)
           break;
-        st = with_degree(ctx->P, [&](auto PP) -> int {
-          constexpr int P = decltype(PP)::value;
-          dim3 grid = tile_grid<P>(g);
-          grid.z = nsys;
-          k_cg_p<P><<<grid, THREADS, mass_smem<P>(), ctx->stream>>>(geo, w.r, w.p[pi], w.p[1 - pi], w.state,
-                                                                     w.partials);
-          LAUNCHED();
-          return LBFEM_OK;
-        });
-        if (st)
-          return st;
-        if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, NM)))
-          return st;
-        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 1, tol, max_its);
-        LAUNCHED();
-        pi = 1 - pi;
-        st = with_degree(ctx->P, [&](auto PP) -> int {
-          constexpr int P = decltype(PP)::value;
-          dim3 grid = tile_grid<P>(g);
-          grid.z = nsys;
-          k_cg_update<P><<<grid, THREADS, mass_smem<P>(2), ctx->stream>>>(geo, x_new, w.r, w.p[pi], w.state,
-                                                                          w.partials);
-          LAUNCHED();
-          return LBFEM_OK;
-        });
-        if (st)
-          return st;
-        if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, 2 * NM)))
-          return st;
-        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 2, tol, max_its);
-        LAUNCHED();
+        if constexpr (MIX)
+          {
+            const long long n = (long long)nsys * g.N;
+            k_refine_add<<<n_pointwise_blocks(n), THREADS, 0, ctx->stream>>>(x_new, w.d, n);
+            LAUNCHED();
+          }
       }
     if (its_out)
       *its_out = ctx->h_cg->total_its;
@@ -355,6 +419,8 @@ namespace
       return fail(ctx, LBFEM_ERR_NO_CONVERGENCE, "CG: iteration cap %d reached", max_its);
     if (ctx->h_cg->status == 3)
       return fail(ctx, LBFEM_ERR_NONFINITE, "CG: non-finite residual");
+    if (!refined)
+      return fail(ctx, LBFEM_ERR_NO_CONVERGENCE, "CG: no convergence within %d refinement rounds", MIXED_MAX_ROUNDS);
     return LBFEM_OK;
   }
 
@@ -363,9 +429,23 @@ namespace
   cg_solve(lbfem_gpu_ctx *ctx, const double *b, double *x_new, const double *x_cur, const double *x_prev,
            int extrapolate, int nsys, int64_t *its_out)
   {
-    const CgScratch w{ctx->d_r, {ctx->d_p[0], ctx->d_p[1]}, ctx->d_partials, ctx->d_sums, ctx->d_cg};
+    const CgScratch<double> w{ctx->d_r, {ctx->d_p[0], ctx->d_p[1]}, ctx->d_partials, ctx->d_sums, ctx->d_cg, nullptr};
     int64_t its = 0;
-    const int st = cg_run(ctx, w, b, x_new, x_cur, x_prev, extrapolate, nsys, &its);
+    const int st = cg_run<double, double>(ctx, w, b, x_new, x_cur, x_prev, extrapolate, nsys, &its);
+    if (its_out)
+      *its_out = its;
+    ctx->cg_its += its;
+    return st;
+  }
+
+  int
+  cg_solve_mixed(lbfem_gpu_ctx *ctx, const float *b, double *x_new, const double *x_cur, const double *x_prev,
+                 int extrapolate, int nsys, int64_t *its_out)
+  {
+    const CgScratch<float> w{ctx->d_r_s, {ctx->d_p_s[0], ctx->d_p_s[1]}, ctx->d_partials, ctx->d_sums, ctx->d_cg,
+                             ctx->d_x_s[0]};
+    int64_t its = 0;
+    const int st = cg_run<float, double>(ctx, w, b, x_new, x_cur, x_prev, extrapolate, nsys, &its);
     if (its_out)
       *its_out = its;
     ctx->cg_its += its;
@@ -378,7 +458,8 @@ namespace
   {
     if (ctx->prm.mass == LBFEM_MASS_LUMPED)
       {
-        k_lumped<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), b, x_new, nsys);
+        k_lumped<double, double><<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), b, x_new,
+                                                                                               nsys);
         LAUNCHED();
         if (its)
           *its = 0;
@@ -424,9 +505,72 @@ namespace
   }
 
   // ------------------------------------------------------------ one step
+  // Mixed precision: the same sequence on FP32 deviations d = f - w.
+  int
+  step_once_mixed(lbfem_gpu_ctx *ctx, int64_t *its)
+  {
+    const Geo geo = geo_of(ctx);
+    const double dt = ctx->dt, lam = ctx->lambda;
+    const double *e = d2q9_e();
+    const long long N = ctx->grid.N;
+    const int nb = n_pointwise_blocks(N);
+    const int rm = ctx->prm.remove_wall_mass_flux;
+    const bool cg = ctx->prm.mass == LBFEM_MASS_CG;
+    float *d = ctx->d_fs[ctx->cur];
+    double *xn = ctx->d_x[cg ? ctx->x_new : ctx->x_cur];
+    const bool bardow = ctx->prm.scheme == LBFEM_SCHEME_BARDOW;
+    float *g = ctx->d_fs[1 - ctx->cur];
+    int st;
+    if (bardow)
+      {
+        const AdvCoef ac = adv_coef(-dt, 0., -0.5 * dt * dt, e, dt / (lam + 0.5 * dt));
+        if ((st = launch_advection<float>(ctx, ADV_TG_COLLIDE, d, nullptr, g, ctx->d_rhs_s, ac)) ||
+            (st = launch_wall_faces<float>(ctx, g, ctx->d_rhs_s, e, dt, rm < 0 ? true : rm != 0)))
+          return st;
+      }
+    else
+      {
+        const double b = -0.5 * dt * dt / lam;
+        const AdvCoef ac = adv_coef(-dt - b, b, -0.5 * dt * dt, e, 0.);
+        if ((st = launch_advection<float>(ctx, ADV_LEELIN_FUSED, d, nullptr, nullptr, ctx->d_rhs_s, ac)) ||
+            (st = launch_wall_faces<float>(ctx, d, ctx->d_rhs_s, e, dt, rm < 0 ? false : rm != 0)))
+          return st;
+      }
+    if (cg)
+      {
+        if ((st = cg_solve_mixed(ctx, ctx->d_rhs_s, xn, ctx->d_x[ctx->x_cur], ctx->d_x[ctx->x_prev], 1, NM, its)))
+          return st;
+        const int old_prev = ctx->x_prev;
+        ctx->x_prev = ctx->x_cur;
+        ctx->x_cur = ctx->x_new;
+        ctx->x_new = old_prev;
+      }
+    else
+      {
+        k_lumped<float, double><<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_rhs_s, xn, NM);
+        LAUNCHED();
+        if (its)
+          *its = 0;
+      }
+    if (bardow)
+      {
+        k_add_increment_dev<<<nb, THREADS, 0, ctx->stream>>>(geo, g, ctx->d_x[ctx->x_cur]);
+        LAUNCHED();
+        ctx->cur = 1 - ctx->cur;
+      }
+    else
+      {
+        k_predictor_corrector_dev<<<nb, THREADS, 0, ctx->stream>>>(geo, d, ctx->d_x[ctx->x_cur], dt / lam);
+        LAUNCHED();
+      }
+    return LBFEM_OK;
+  }
+
   int
   step_once(lbfem_gpu_ctx *ctx, int64_t *its)
   {
+    if (ctx->mixed)
+      return step_once_mixed(ctx, its);
     const Geo geo = geo_of(ctx);
     const double dt = ctx->dt, lam = ctx->lambda;
     const double *e = d2q9_e();
@@ -441,9 +585,9 @@ namespace
         // Bardow::step (schemes.h:118-124): collide, then stream (streaming.h:88-100)
         double *g = ctx->d_f[1 - ctx->cur];
         const AdvCoef ac = adv_coef(-dt, 0., -0.5 * dt * dt, e, dt / (lam + 0.5 * dt));
-        if ((st = launch_advection(ctx, ADV_TG_COLLIDE, f, nullptr, g, ctx->d_rhs, ac)))
+        if ((st = launch_advection<double>(ctx, ADV_TG_COLLIDE, f, nullptr, g, ctx->d_rhs, ac)))
           return st;
-        if ((st = launch_wall_faces(ctx, g, ctx->d_rhs, e, dt, rm < 0 ? true : rm != 0)))
+        if ((st = launch_wall_faces<double>(ctx, g, ctx->d_rhs, e, dt, rm < 0 ? true : rm != 0)))
           return st;
         double *xn = ctx->d_x[cg ? ctx->x_new : ctx->x_cur];
         if ((st = mass_solve_dev(ctx, ctx->d_rhs, xn, ctx->d_x[ctx->x_cur], ctx->d_x[ctx->x_prev], 1, NM, its)))
@@ -455,7 +599,7 @@ namespace
             ctx->x_cur = ctx->x_new;
             ctx->x_new = old_prev;
           }
-        k_add_increment<<<nb, THREADS, 0, ctx->stream>>>(geo, g, ctx->d_x[ctx->x_cur]);
+        k_add_increment<double><<<nb, THREADS, 0, ctx->stream>>>(geo, g, ctx->d_x[ctx->x_cur]);
         LAUNCHED();
         ctx->cur = 1 - ctx->cur;
         return LBFEM_OK;
@@ -463,9 +607,9 @@ namespace
     // LeeLin::step (schemes.h:92-98): equilibria, increment, predictor-corrector
     const double b = -0.5 * dt * dt / lam;
     const AdvCoef ac = adv_coef(-dt - b, b, -0.5 * dt * dt, e, 0.);
-    if ((st = launch_advection(ctx, ADV_LEELIN_FUSED, f, nullptr, nullptr, ctx->d_rhs, ac)))
+    if ((st = launch_advection<double>(ctx, ADV_LEELIN_FUSED, f, nullptr, nullptr, ctx->d_rhs, ac)))
       return st;
-    if ((st = launch_wall_faces(ctx, f, ctx->d_rhs, e, dt, rm < 0 ? false : rm != 0)))
+    if ((st = launch_wall_faces<double>(ctx, f, ctx->d_rhs, e, dt, rm < 0 ? false : rm != 0)))
       return st;
     double *xn = ctx->d_x[cg ? ctx->x_new : ctx->x_cur];
     if ((st = mass_solve_dev(ctx, ctx->d_rhs, xn, ctx->d_x[ctx->x_cur], ctx->d_x[ctx->x_prev], 1, NM, its)))
@@ -585,7 +729,8 @@ lbfem_gpu_destroy(lbfem_gpu_ctx *ctx)
                   ctx->d_rowx, ctx->d_rowy, ctx->d_diagx, ctx->d_diagy, ctx->d_lumpx, ctx->d_lumpy, ctx->d_wall,
                   ctx->d_wall_u, ctx->d_dof, ctx->d_bnode, ctx->d_f[0], ctx->d_f[1], ctx->d_rhs, ctx->d_x[0],
                   ctx->d_x[1], ctx->d_x[2], ctx->d_r, ctx->d_p[0], ctx->d_p[1], ctx->d_v, ctx->d_feq, ctx->d_stage,
-                  ctx->d_partials, ctx->d_sums, ctx->d_cg};
+                  ctx->d_partials, ctx->d_sums, ctx->d_cg, ctx->d_fs[0], ctx->d_fs[1], ctx->d_rhs_s,
+                  ctx->d_x_s[0], ctx->d_x_s[1], ctx->d_x_s[2], ctx->d_r_s, ctx->d_p_s[0], ctx->d_p_s[1]};
   for (void *b : bufs)
     if (b)
       cudaFree(b);
@@ -618,7 +763,8 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
       return LBFEM_ERR_ARG;
   if (prm->scheme != LBFEM_SCHEME_BARDOW && prm->scheme != LBFEM_SCHEME_LEELIN)
     return LBFEM_ERR_ARG;
-  if (prm->streaming != LBFEM_STREAMING_TG2 || prm->precision != LBFEM_PRECISION_FP64 ||
+  if (prm->streaming != LBFEM_STREAMING_TG2 ||
+      (prm->precision != LBFEM_PRECISION_FP64 && prm->precision != LBFEM_PRECISION_MIXED) ||
       (prm->mass != LBFEM_MASS_CG && prm->mass != LBFEM_MASS_LUMPED))
     return LBFEM_ERR_UNSUPPORTED;
   if (!(prm->cg_tolerance >= 0) || prm->cg_max_iterations < 1)
@@ -687,6 +833,13 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
             }
       }
     CK(cudaMemcpyToSymbol(c_ref, ref, sizeof ref));
+    static float reff[MAXPD][3][MAXPD + 1][MAXPD + 1];
+    for (int q = 0; q < MAXPD; ++q)
+      for (int o = 0; o < 3; ++o)
+        for (int a = 0; a <= MAXPD; ++a)
+          for (int c = 0; c <= MAXPD; ++c)
+            reff[q][o][a][c] = float(ref[q][o][a][c]);
+    CK(cudaMemcpyToSymbol(c_reff, reff, sizeof reff));
   }
 
   // numbering: structured node -> caller DoF, and its inverse for the wall list
@@ -776,6 +929,21 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
     return st;
   if (!ctx->identity && (st = zeros(&ctx->d_stage, Q * N)))
     return st;
+  ctx->mixed = prm->precision == LBFEM_PRECISION_MIXED;
+  if (ctx->mixed)
+    {
+      auto zerosf = [&](float **d, size_t n) -> int {
+        CK(cudaMalloc(d, sizeof(float) * n));
+        CK(cudaMemset(*d, 0, sizeof(float) * n));
+        return LBFEM_OK;
+      };
+      if ((st = zerosf(&ctx->d_fs[0], Q * N)) || (st = zerosf(&ctx->d_fs[1], Q * N)) ||
+          (st = zerosf(&ctx->d_rhs_s, NM * N)) || (st = zerosf(&ctx->d_x_s[0], NM * N)) ||
+          (st = zerosf(&ctx->d_x_s[1], NM * N)) || (st = zerosf(&ctx->d_x_s[2], NM * N)) ||
+          (st = zerosf(&ctx->d_r_s, NM * N)) || (st = zerosf(&ctx->d_p_s[0], NM * N)) ||
+          (st = zerosf(&ctx->d_p_s[1], NM * N)))
+        return st;
+    }
   const long long tiles = with_degree(P, [&](auto PP) -> int {
     constexpr int Pd = decltype(PP)::value;
     const dim3 tg = tile_grid<Pd>(ctx->grid);
@@ -813,7 +981,15 @@ lbfem_gpu_set_populations(lbfem_gpu_ctx *ctx, const double *f)
     return st;
   if (!f)
     return fail(ctx, LBFEM_ERR_ARG, "set_populations: null buffer");
-  return upload(ctx, f, ctx->d_f[ctx->cur], Q);
+  if ((st = upload(ctx, f, ctx->d_f[ctx->cur], Q)))
+    return st;
+  if (ctx->mixed)
+    {
+      k_to_dev<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(ctx->d_f[ctx->cur], ctx->d_fs[ctx->cur],
+                                                                             ctx->grid.N);
+      LAUNCHED();
+    }
+  return LBFEM_OK;
 }
 
 int
@@ -824,6 +1000,12 @@ lbfem_gpu_get_populations(lbfem_gpu_ctx *ctx, double *f)
     return st;
   if (!f)
     return fail(ctx, LBFEM_ERR_ARG, "get_populations: null buffer");
+  if (ctx->mixed)
+    {
+      k_from_dev<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(ctx->d_fs[ctx->cur],
+                                                                               ctx->d_f[ctx->cur], ctx->grid.N);
+      LAUNCHED();
+    }
   return download(ctx, ctx->d_f[ctx->cur], f, Q);
 }
 
@@ -842,7 +1024,20 @@ lbfem_gpu_set_initial_populations(lbfem_gpu_ctx *ctx, const double *f)
   const long long N = ctx->grid.N;
   for (int k = 0; k < 3; ++k)
     CK(cudaMemsetAsync(ctx->d_x[k], 0, sizeof(double) * NM * N, ctx->stream));
-  if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
+  if (ctx->mixed)
+    {
+      for (int k = 0; k < 3; ++k)
+        CK(cudaMemsetAsync(ctx->d_x_s[k], 0, sizeof(float) * NM * N, ctx->stream));
+      k_to_dev<<<n_pointwise_blocks(N), THREADS, 0, ctx->stream>>>(ctx->d_f[ctx->cur], ctx->d_fs[ctx->cur], N);
+      LAUNCHED();
+      if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
+        {
+          k_bardow_transform_dev<<<n_pointwise_blocks(N), THREADS, 0, ctx->stream>>>(
+            geo_of(ctx), ctx->d_fs[ctx->cur], float(0.5 * ctx->dt / ctx->lambda));
+          LAUNCHED();
+        }
+    }
+  else if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
     {
       k_bardow_transform<<<n_pointwise_blocks(N), THREADS, 0, ctx->stream>>>(geo_of(ctx), ctx->d_f[ctx->cur],
                                                                              0.5 * ctx->dt / ctx->lambda);
@@ -925,10 +1120,10 @@ lbfem_gpu_advection(lbfem_gpu_ctx *ctx, const double *f, const double *feq, cons
     }
   else
     ac = adv_coef(-dt, 0., -0.5 * dt * dt, e, 0.);
-  if ((st = launch_advection(ctx, leelin ? ADV_LEELIN_FEQ : ADV_TG, fs, ctx->d_feq, nullptr, ctx->d_rhs, ac)))
+  if ((st = launch_advection<double>(ctx, leelin ? ADV_LEELIN_FEQ : ADV_TG, fs, ctx->d_feq, nullptr, ctx->d_rhs, ac)))
     return st;
   const bool rmv = remove < 0 ? !leelin : remove != 0;
-  if ((st = launch_wall_faces(ctx, fs, ctx->d_rhs, e, dt, rmv)))
+  if ((st = launch_wall_faces<double>(ctx, fs, ctx->d_rhs, e, dt, rmv)))
     return st;
   return download(ctx, ctx->d_rhs, rhs, NM);
 }
@@ -942,12 +1137,16 @@ lbfem_gpu_advection_resident(lbfem_gpu_ctx *ctx)
   if (!ctx->have_ts)
     return fail(ctx, LBFEM_ERR_STATE, "advection_resident needs the time step");
   const double dt = ctx->dt, lam = ctx->lambda;
-  if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
-    return launch_advection(ctx, ADV_TG_COLLIDE, ctx->d_f[ctx->cur], nullptr, ctx->d_f[1 - ctx->cur], ctx->d_rhs,
-                            adv_coef(-dt, 0., -0.5 * dt * dt, d2q9_e(), dt / (lam + 0.5 * dt)));
   const double b = -0.5 * dt * dt / lam;
-  return launch_advection(ctx, ADV_LEELIN_FUSED, ctx->d_f[ctx->cur], nullptr, nullptr, ctx->d_rhs,
-                          adv_coef(-dt - b, b, -0.5 * dt * dt, d2q9_e(), 0.));
+  const bool bardow = ctx->prm.scheme == LBFEM_SCHEME_BARDOW;
+  const AdvCoef ac = bardow ? adv_coef(-dt, 0., -0.5 * dt * dt, d2q9_e(), dt / (lam + 0.5 * dt))
+                            : adv_coef(-dt - b, b, -0.5 * dt * dt, d2q9_e(), 0.);
+  const int mode = bardow ? ADV_TG_COLLIDE : ADV_LEELIN_FUSED;
+  if (ctx->mixed)
+    return launch_advection<float>(ctx, mode, ctx->d_fs[ctx->cur], nullptr, bardow ? ctx->d_fs[1 - ctx->cur] : nullptr,
+                                   ctx->d_rhs_s, ac);
+  return launch_advection<double>(ctx, mode, ctx->d_f[ctx->cur], nullptr, bardow ? ctx->d_f[1 - ctx->cur] : nullptr,
+                                  ctx->d_rhs, ac);
 }
 
 int
@@ -1085,7 +1284,12 @@ lbfem_gpu_moments(lbfem_gpu_ctx *ctx, double *rho, double *ux, double *uy)
     return st;
   const long long N = ctx->grid.N;
   double *d = ctx->d_r; // 3 of its 8 blocks
-  k_moments<<<n_pointwise_blocks(N), THREADS, 0, ctx->stream>>>(geo_of(ctx), ctx->d_f[ctx->cur], d, d + N, d + 2 * N);
+  if (ctx->mixed)
+    k_moments_dev<<<n_pointwise_blocks(N), THREADS, 0, ctx->stream>>>(geo_of(ctx), ctx->d_fs[ctx->cur], d, d + N,
+                                                                      d + 2 * N);
+  else
+    k_moments<<<n_pointwise_blocks(N), THREADS, 0, ctx->stream>>>(geo_of(ctx), ctx->d_f[ctx->cur], d, d + N,
+                                                                  d + 2 * N);
   LAUNCHED();
   double *outs[3] = {rho, ux, uy};
   for (int k = 0; k < 3; ++k)
@@ -1103,7 +1307,10 @@ lbfem_gpu_conservation(lbfem_gpu_ctx *ctx, double out[5])
   if (!out)
     return fail(ctx, LBFEM_ERR_ARG, "conservation: null buffer");
   const int nb = n_pointwise_blocks(ctx->grid.N);
-  k_conservation<<<nb, THREADS, 0, ctx->stream>>>(geo_of(ctx), ctx->d_f[ctx->cur], ctx->d_partials);
+  if (ctx->mixed)
+    k_conservation_dev<<<nb, THREADS, 0, ctx->stream>>>(geo_of(ctx), ctx->d_fs[ctx->cur], ctx->d_partials);
+  else
+    k_conservation<<<nb, THREADS, 0, ctx->stream>>>(geo_of(ctx), ctx->d_f[ctx->cur], ctx->d_partials);
   LAUNCHED();
   if ((st = reduce(ctx, nb, 5)))
     return st;
@@ -1208,14 +1415,14 @@ lbfem_gpu_mass_solve_noalloc(lbfem_gpu_ctx *ctx, double *x, const double *r)
       CK(cudaGetSymbolAddress((void **)&base, noalloc_scratch));
       noalloc_ptr[ctx->device] = base;
     }
-  CgScratch w{};
+  CgScratch<double> w{};
   w.r = base;
   w.p[0] = base + NOALLOC_MAX_NODES;
   w.p[1] = base + 2 * NOALLOC_MAX_NODES;
   w.partials = base + 3 * NOALLOC_MAX_NODES;
   w.sums = w.partials + 3 * NM * NOALLOC_MAX_TILES;
   w.state = reinterpret_cast<CgState *>(w.sums + 64);
-  const int solve_st = cg_run(ctx, w, r, x, nullptr, nullptr, 0, 1, nullptr);
+  const int solve_st = cg_run<double, double>(ctx, w, r, x, nullptr, nullptr, 0, 1, nullptr);
   if (solve_st != LBFEM_OK)
     return solve_st;
   CK(cudaStreamSynchronize(ctx->stream));

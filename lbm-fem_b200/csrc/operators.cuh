@@ -113,9 +113,140 @@ namespace lbfem_gpu
     }
   }
 
-  // TaylorGalerkin::stream (streaming.h:94-98): f_a += x_{a-1}, a = 1..8.
+  // ----- FP32 deviation forms of the nodal maps (mixed precision) -----
+  __device__ __forceinline__ void
+  collide_node_dev(float (&d)[Q], long long idx, const Geo &geo, float omega)
+  {
+    const MomF m = moments_dev(d);
+    const MomF mt = impose(m, idx, geo);
+#pragma unroll
+    for (int a = 0; a < Q; ++a)
+      d[a] = feqd_a(a, mt) + (1.f - omega) * (d[a] - feqd_a(a, m));
+  }
+
+  // FP64 moments / equilibrium of FP32 deviations (exact forms as above).
+  __device__ __forceinline__ Mom
+  moments_dev64(const double (&d)[Q], double &drho)
+  {
+    double dr = 0, mx = 0, my = 0;
+#pragma unroll
+    for (int a = 0; a < Q; ++a)
+      {
+        dr += d[a];
+        mx += c_EX[a] * d[a];
+        my += c_EY[a] * d[a];
+      }
+    drho = dr;
+    const double rho = 1.0 + dr;
+    return {rho, mx / rho, my / rho};
+  }
+
+  __device__ __forceinline__ double
+  feqd64_a(int a, const Mom &m, double drho)
+  {
+    const double uu = m.ux * m.ux + m.uy * m.uy;
+    const double eu = c_EX[a] * m.ux + c_EY[a] * m.uy;
+    return c_W[a] * (drho + m.rho * (3. * eu + 4.5 * eu * eu - 1.5 * uu));
+  }
+
+  // predictor_corrector on FP32 deviations d = f - w with the FP64 increment x, in
+  // FP64 arithmetic (the corrector's theta (feq(fhat) - feq(f)) cancels).
   __global__ void
-  k_add_increment(const Geo geo, double *__restrict__ f, const double *__restrict__ x)
+  k_predictor_corrector_dev(const Geo geo, float *__restrict__ d, const double *__restrict__ x, double theta)
+  {
+    const long long N = geo.g.N;
+    const double inv = 1. / (1. + theta);
+    LBFEM_GRID_STRIDE(i, N)
+    {
+      double di[Q], fe[Q], fh[Q], dr;
+#pragma unroll
+      for (int a = 0; a < Q; ++a)
+        di[a] = d[a * N + i];
+      const Mom m = impose(moments_dev64(di, dr), i, geo);
+#pragma unroll
+      for (int a = 0; a < Q; ++a)
+        fe[a] = feqd64_a(a, m, dr);
+      fh[0] = inv * (di[0] + theta * fe[0]);
+#pragma unroll
+      for (int a = 1; a < Q; ++a)
+        fh[a] = inv * (di[a] + theta * fe[a] + x[(a - 1) * N + i]);
+      double drh;
+      const Mom mh = impose(moments_dev64(fh, drh), i, geo);
+#pragma unroll
+      for (int a = 0; a < Q; ++a)
+        d[a * N + i] = float(fh[a] + theta * (feqd64_a(a, mh, drh) - fe[a]));
+    }
+  }
+
+  // Bardow's stream on FP32 deviations: d_a += x_{a-1} (FP64 increment).
+  __global__ void
+  k_add_increment_dev(const Geo geo, float *__restrict__ d, const double *__restrict__ x)
+  {
+    const long long N = geo.g.N;
+    LBFEM_GRID_STRIDE(i, N)
+    {
+#pragma unroll
+      for (int a = 1; a < Q; ++a)
+        d[a * N + i] = float(double(d[a * N + i]) + x[(a - 1) * N + i]);
+    }
+  }
+
+  // One refinement step: x += d (FP64), d = 0 (the next inner solve starts from 0).
+  __global__ void
+  k_refine_add(double *__restrict__ x, float *__restrict__ d, long long n)
+  {
+    LBFEM_GRID_STRIDE(i, n)
+    {
+      x[i] += double(d[i]);
+      d[i] = 0.f;
+    }
+  }
+
+  // Bardow's initial transform on deviations: d + scale (d - (feq - w)).
+  __global__ void
+  k_bardow_transform_dev(const Geo geo, float *__restrict__ d, float scale)
+  {
+    const long long N = geo.g.N;
+    LBFEM_GRID_STRIDE(i, N)
+    {
+      float v[Q];
+#pragma unroll
+      for (int a = 0; a < Q; ++a)
+        v[a] = d[a * N + i];
+      const MomF m = moments_dev(v);
+#pragma unroll
+      for (int a = 0; a < Q; ++a)
+        d[a * N + i] = v[a] + scale * (v[a] - feqd_a(a, m));
+    }
+  }
+
+  // FP64 populations <-> FP32 deviations from the rest state.
+  __global__ void
+  k_to_dev(const double *__restrict__ f, float *__restrict__ d, long long N)
+  {
+    LBFEM_GRID_STRIDE(i, N)
+    {
+#pragma unroll
+      for (int a = 0; a < Q; ++a)
+        d[a * N + i] = float(f[a * N + i] - c_W[a]);
+    }
+  }
+
+  __global__ void
+  k_from_dev(const float *__restrict__ d, double *__restrict__ f, long long N)
+  {
+    LBFEM_GRID_STRIDE(i, N)
+    {
+#pragma unroll
+      for (int a = 0; a < Q; ++a)
+        f[a * N + i] = c_W[a] + double(d[a * N + i]);
+    }
+  }
+
+  // TaylorGalerkin::stream (streaming.h:94-98): f_a += x_{a-1}, a = 1..8.
+  template <typename R>
+  __global__ void
+  k_add_increment(const Geo geo, R *__restrict__ f, const R *__restrict__ x)
   {
     const long long N = geo.g.N;
     LBFEM_GRID_STRIDE(i, N)
@@ -127,17 +258,18 @@ namespace lbfem_gpu
   }
 
   // Lumped solve (mass.h:189-191): x = M_L^{-1} r, for nsys vectors.
+  template <typename RI, typename RO>
   __global__ void
-  k_lumped(const Geo geo, const double *__restrict__ r, double *__restrict__ x, int nsys)
+  k_lumped(const Geo geo, const RI *__restrict__ r, RO *__restrict__ x, int nsys)
   {
     const Grid &g = geo.g;
     const long long N = g.N;
     LBFEM_GRID_STRIDE(idx, N)
     {
       const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
-      const double inv = is_image(i, j, g) ? 1.0 : geo.ilx[i] * geo.ily[j];
+      const RO inv = RO(is_image(i, j, g) ? 1.0 : geo.ilx[i] * geo.ily[j]);
       for (int s = 0; s < nsys; ++s)
-        x[s * N + idx] = inv * r[s * N + idx];
+        x[s * N + idx] = inv * RO(r[s * N + idx]);
     }
   }
 
@@ -176,6 +308,68 @@ namespace lbfem_gpu
       if (uy)
         uy[idx] = m.uy;
     }
+  }
+
+  // Moments of FP32 deviations, accumulated in FP64 (images report their source).
+  __global__ void
+  k_moments_dev(const Geo geo, const float *__restrict__ d, double *__restrict__ rho, double *__restrict__ ux,
+                double *__restrict__ uy)
+  {
+    const Grid &g = geo.g;
+    const long long N = g.N;
+    LBFEM_GRID_STRIDE(idx, N)
+    {
+      const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
+      const long long src = (long long)wrap(j, g.py, g.nuy, g.nfy) * g.nfx + wrap(i, g.px, g.nux, g.nfx);
+      double dr = 0, mx = 0, my = 0;
+#pragma unroll
+      for (int a = 0; a < Q; ++a)
+        {
+          const double v = d[a * N + src];
+          dr += v;
+          mx += c_EX[a] * v;
+          my += c_EY[a] * v;
+        }
+      const double r = 1.0 + dr;
+      if (rho)
+        rho[idx] = r;
+      if (ux)
+        ux[idx] = mx / r;
+      if (uy)
+        uy[idx] = my / r;
+    }
+  }
+
+  // FP64 conservation sums over the independent nodes of FP32 deviations.
+  __global__ void __launch_bounds__(THREADS)
+    k_conservation_dev(const Geo geo, const float *__restrict__ d, double *__restrict__ partials)
+  {
+    const Grid &g = geo.g;
+    const long long N = g.N;
+    double s[5] = {0, 0, 0, 0, 0};
+    LBFEM_GRID_STRIDE(idx, N)
+    {
+      const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
+      if (is_image(i, j, g))
+        continue;
+      double dr = 0, mx = 0, my = 0;
+#pragma unroll
+      for (int a = 0; a < Q; ++a)
+        {
+          const double v = d[a * N + idx];
+          dr += v;
+          mx += c_EX[a] * v;
+          my += c_EY[a] * v;
+        }
+      const double rho = 1.0 + dr, ux = mx / rho, uy = my / rho;
+      const double w = geo.lumpx[i] * geo.lumpy[j];
+      s[0] += w;
+      s[1] += w * rho;
+      s[2] += w * mx;
+      s[3] += w * my;
+      s[4] += w * (ux * ux + uy * uy);
+    }
+    block_reduce_store<5>(s, partials, blockIdx.x, gridDim.x);
   }
 
   // FP64 conservation sums over the independent nodes (cgdbe.cc:353-368).
@@ -253,13 +447,21 @@ namespace lbfem_gpu
     return MODE == ADV_TG_COLLIDE || MODE == ADV_LEELIN_FUSED;
   }
 
-  template <int P, int MODE>
+  // Moment fields staged per footprint node: rho, ux, uy (+ drho for FP32 deviations).
+  template <typename R>
+  __host__ __device__ constexpr int
+  n_moment_fields()
+  {
+    return sizeof(R) == sizeof(float) ? 4 : 3;
+  }
+
+  template <int P, int MODE, typename R = double>
   constexpr size_t
   advection_smem()
   {
     using T = Tile<P>;
-    const int fields = (has_moments<MODE>() ? 3 : 0) + 1 + (MODE == ADV_LEELIN_FEQ ? 1 : 0);
-    return sizeof(double) * (fields * T::NF + 3 * T::NY + 2 * T::TX) +
+    const int fields = (has_moments<MODE>() ? n_moment_fields<R>() : 0) + 1 + (MODE == ADV_LEELIN_FEQ ? 1 : 0);
+    return sizeof(R) * (fields * T::NF + 3 * T::NY + 2 * T::TX) +
            (MODE == ADV_TG_COLLIDE ? size_t(T::NF + 15) / 16 * 16 : 0);
   }
 
@@ -268,41 +470,52 @@ namespace lbfem_gpu
   //   Y1 = ex Cx h + c ex^2 Kx f, Y2' = ey Mx h - 2 c ex ey Cx f + c ex ey Bx f,
   //   Y3 = c ey^2 Mx f, Y4 = c ex ey Cx f
   // (C^T = B - C, B the end-point term of the integration by parts).
+  template <typename R>
   struct AdvK
   {
-    double A, B, k1, k2, k3, k4, k5, k6;
+    R A, B, k1, k2, k3, k4, k5, k6;
   };
 
+  // The equilibrium of population a at footprint index t from the staged moments.
+  template <typename R>
+  __device__ __forceinline__ R
+  staged_feq(const R *s_m, int nf, int t, int a)
+  {
+    if constexpr (sizeof(R) == sizeof(float))
+      return feqd_a(a, MomF{s_m[t], s_m[nf + t], s_m[2 * nf + t], s_m[3 * nf + t]});
+    else
+      return feq_a(a, Mom{s_m[t], s_m[nf + t], s_m[2 * nf + t]});
+  }
+
   // Population a at footprint index t: u, and h = A u + B feq.
-  template <int HM>
+  template <int HM, typename R>
   __device__ __forceinline__ void
-  load_uh(const double *s_u, const double *s_e, const double *s_m, int nf, int t, int a, const AdvK &k, double &u,
-          double &h)
+  load_uh(const R *s_u, const R *s_e, const R *s_m, int nf, int t, int a, const AdvK<R> &k, R &u, R &h)
   {
     u = s_u[t];
     if constexpr (HM == 0)
       h = k.A * u;
     else if constexpr (HM == 1)
-      h = fma(k.B, feq_a(a, Mom{s_m[t], s_m[nf + t], s_m[2 * nf + t]}), k.A * u);
+      h = fma(k.B, staged_feq<R>(s_m, nf, t, a), k.A * u);
     else
       h = fma(k.B, s_e[t], k.A * u);
   }
 
   // x pass of K1 for one footprint row fy and one x segment. CLS: 0 e = (ex, 0), 1 e = (0, ey), 2 diagonal.
-  template <int P, int CLS, int HM>
+  template <int P, int CLS, int HM, typename R>
   __device__ __forceinline__ void
-  adv_xpass(const double *s_u, const double *s_e, const double *s_m, double *s_y, double *s_y4,
-            const TileMaps<P> &m, const AdvK &k, int a, int fy, int seg, int gx0, int y4_slot, int bx_lo, int bx_hi)
+  adv_xpass(const R *s_u, const R *s_e, const R *s_m, R *s_y, R *s_y4, const TileMaps<P, R> &m, const AdvK<R> &k,
+            int a, int fy, int seg, int gx0, int y4_slot, int bx_lo, int bx_hi)
   {
     using T = Tile<P>;
     constexpr bool XC = CLS != 1, YC = CLS != 0, DG = CLS == 2;
     const int base = fy * T::PF;
     const int q0 = seg * T::KX;
-    double u[P + 1], h[P + 1];
+    R u[P + 1], h[P + 1];
 #pragma unroll
     for (int b = 0; b <= P; ++b)
       load_uh<HM>(s_u, s_e, s_m, T::NF, base + q0 * P + b, a, k, u[b], h[b]);
-    double pCh = 0, pKu = 0, pMh = 0, pCu = 0, pMu = 0;
+    R pCh = 0, pKu = 0, pMh = 0, pCu = 0, pMu = 0;
     if constexpr (XC)
       {
         pCh = m.cx[q0] * elem_last<P, OP_C>(h);
@@ -315,7 +528,7 @@ namespace lbfem_gpu
       }
     if constexpr (DG)
       pCu = m.cx[q0] * elem_last<P, OP_C>(u);
-    double *y1 = s_y + fy * T::PY, *y2 = y1 + T::NY, *y3 = y2 + T::NY;
+    R *y1 = s_y + fy * T::PY, *y2 = y1 + T::NY, *y3 = y2 + T::NY;
 #pragma unroll
     for (int q = 1; q <= T::KX; ++q)
       {
@@ -325,7 +538,7 @@ namespace lbfem_gpu
 #pragma unroll
         for (int b = 1; b <= P; ++b)
           load_uh<HM>(s_u, s_e, s_m, T::NF, base + qc * P + b, a, k, u[b], h[b]);
-        double eCh[P + 1], eKu[P + 1], eMh[P + 1], eCu[P + 1], eMu[P + 1];
+        R eCh[P + 1], eKu[P + 1], eMh[P + 1], eCu[P + 1], eMu[P + 1];
         if constexpr (XC)
           {
             elem<P, OP_C>(h, eCh);
@@ -338,13 +551,13 @@ namespace lbfem_gpu
           }
         if constexpr (DG)
           elem<P, OP_C>(u, eCu);
-        const double sc = m.cx[qc], sh = m.hx[qc], shi = m.hxi[qc];
+        const R sc = m.cx[qc], sh = m.hx[qc], shi = m.hxi[qc];
         const int j0 = (qc - 1) * P;
 #pragma unroll
         for (int aa = 0; aa < P; ++aa)
           {
             const int j = j0 + aa;
-            double vCh = 0, vKu = 0, vMh = 0, vCu = 0, vMu = 0;
+            R vCh = 0, vKu = 0, vMh = 0, vCu = 0, vMu = 0;
             if constexpr (XC)
               {
                 vCh = sc * eCh[aa];
@@ -369,7 +582,7 @@ namespace lbfem_gpu
               y1[j] = k.k1 * vCh + k.k2 * vKu;
             if constexpr (YC)
               {
-                double y = k.k3 * vMh;
+                R y = k.k3 * vMh;
                 if constexpr (DG)
                   {
                     y = fma(k.k4, vCu, y);
@@ -406,16 +619,16 @@ namespace lbfem_gpu
   }
 
   // y pass of K1 on column j and y segment seg: emit(own row i, r).
-  template <int P, int CLS, typename Emit>
+  template <int P, int CLS, typename R, typename Emit>
   __device__ __forceinline__ void
-  adv_ypass(const double *s_y, const double *s_y4, const TileMaps<P> &m, int j, int seg, int gy0, int by_lo,
-            int by_hi, Emit &&emit)
+  adv_ypass(const R *s_y, const R *s_y4, const TileMaps<P, R> &m, int j, int seg, int gy0, int by_lo, int by_hi,
+            Emit &&emit)
   {
     using T = Tile<P>;
     constexpr bool XC = CLS != 1, YC = CLS != 0, DG = CLS == 2;
-    const double *y1 = s_y, *y2 = s_y + T::NY, *y3 = s_y + 2 * T::NY;
+    const R *y1 = s_y, *y2 = s_y + T::NY, *y3 = s_y + 2 * T::NY;
     const int q0 = seg * T::KY;
-    double v1[P + 1], v2[P + 1], v3[P + 1];
+    R v1[P + 1], v2[P + 1], v3[P + 1];
 #pragma unroll
     for (int b = 0; b <= P; ++b)
       {
@@ -428,7 +641,7 @@ namespace lbfem_gpu
             v3[b] = y3[t];
           }
       }
-    double pend = 0;
+    R pend = 0;
     if constexpr (XC)
       pend = m.hy[q0] * elem_last<P, OP_M>(v1);
     if constexpr (YC)
@@ -452,7 +665,7 @@ namespace lbfem_gpu
                 v3[b] = y3[t];
               }
           }
-        double e1[P + 1], e2[P + 1], e3[P + 1];
+        R e1[P + 1], e2[P + 1], e3[P + 1];
         if constexpr (XC)
           elem<P, OP_M>(v1, e1);
         if constexpr (YC)
@@ -460,12 +673,12 @@ namespace lbfem_gpu
             elem<P, OP_C>(v2, e2);
             elem<P, OP_K>(v3, e3);
           }
-        const double sh = m.hy[qc], sc = m.cy[qc], shi = m.hyi[qc];
+        const R sh = m.hy[qc], sc = m.cy[qc], shi = m.hyi[qc];
         const int i0 = (qc - 1) * P;
 #pragma unroll
         for (int aa = 0; aa <= P; ++aa)
           {
-            double r = 0;
+            R r = 0;
             if constexpr (XC)
               r = sh * e1[aa];
             if constexpr (YC)
@@ -494,21 +707,26 @@ namespace lbfem_gpu
   // TaylorGalerkinAdvection (advection.h:228-239) / LeeLinAdvection
   // (advection.h:275-287), in the grouped tensor-product form above. Images get
   // 0 (constrained rows, as distribute_local_to_global leaves them).
-  template <int P, int MODE>
+  // R = double: populations f; R = float: deviations f - w (the operator
+  // annihilates constants, and collide / feq are applied in deviation form).
+  template <int P, int MODE, typename R>
   __global__ void __launch_bounds__(THREADS, 2)
-    k_advection(const Geo geo, const double *__restrict__ f, const double *__restrict__ feq,
-                double *__restrict__ fout, double *__restrict__ rhs, const AdvCoef ac)
+    k_advection(const Geo geo, const R *__restrict__ f, const R *__restrict__ feq, R *__restrict__ fout,
+                R *__restrict__ rhs, const AdvCoef ac)
   {
     using T = Tile<P>;
     constexpr bool MOM = has_moments<MODE>();
+    constexpr bool DEV = sizeof(R) == sizeof(float);
+    constexpr int NMF = n_moment_fields<R>();
     constexpr int HM = MODE == ADV_LEELIN_FUSED ? 1 : MODE == ADV_LEELIN_FEQ ? 2 : 0;
-    extern __shared__ double sm[];
-    __shared__ TileMaps<P> maps;
-    double *s_m = sm;                                 // [3][NF] moments (MOM modes)
-    double *s_u = s_m + (MOM ? 3 * T::NF : 0);        // [NF] the current population
-    double *s_e = s_u + T::NF;                        // [NF] its equilibrium (ADV_LEELIN_FEQ)
-    double *s_y = s_e + (MODE == ADV_LEELIN_FEQ ? T::NF : 0); // [3][NY] x-pass outputs
-    double *s_y4 = s_y + 3 * T::NY;                   // [2][TX] Y4 on the first / last domain row
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    R *sm = reinterpret_cast<R *>(sm_raw);
+    __shared__ TileMaps<P, R> maps;
+    R *s_m = sm;                                                // [NMF][NF] moments (MOM modes)
+    R *s_u = s_m + (MOM ? NMF * T::NF : 0);                     // [NF] the current population
+    R *s_e = s_u + T::NF;                                       // [NF] its equilibrium (ADV_LEELIN_FEQ)
+    R *s_y = s_e + (MODE == ADV_LEELIN_FEQ ? T::NF : 0);        // [3][NY] x-pass outputs
+    R *s_y4 = s_y + 3 * T::NY;                                  // [2][TX] Y4 on the first / last domain row
     uint8_t *s_wall = reinterpret_cast<uint8_t *>(s_y4 + 2 * T::TX); // [NF] wall classes (ADV_TG_COLLIDE)
     const Grid &g = geo.g;
     const long long N = g.N;
@@ -525,31 +743,47 @@ namespace lbfem_gpu
             const int c = maps.col[fx];
             if (r < 0 || c < 0)
               {
-                s_m[st] = s_m[T::NF + st] = s_m[2 * T::NF + st] = 0.0;
+#pragma unroll
+                for (int q = 0; q < NMF; ++q)
+                  s_m[q * T::NF + st] = R(0);
                 if constexpr (MODE == ADV_TG_COLLIDE)
                   s_wall[st] = 0;
                 continue;
               }
             const long long idx = r + c;
-            double v[Q];
+            const int wk = geo.wall ? geo.wall[idx] : 0;
+            R v[Q];
 #pragma unroll
             for (int a = 0; a < Q; ++a)
               v[a] = f[a * N + idx];
-            Mom mo = moments(v);
-            const int wk = geo.wall ? geo.wall[idx] : 0;
-            if constexpr (MODE == ADV_LEELIN_FUSED)
-              mo = impose_class(mo, wk, geo);
+            if constexpr (DEV)
+              {
+                MomF mo = moments_dev(v);
+                if constexpr (MODE == ADV_LEELIN_FUSED)
+                  mo = impose_class(mo, wk, geo);
+                s_m[st] = mo.rho;
+                s_m[T::NF + st] = mo.ux;
+                s_m[2 * T::NF + st] = mo.uy;
+                s_m[3 * T::NF + st] = mo.drho;
+              }
             else
+              {
+                Mom mo = moments(v);
+                if constexpr (MODE == ADV_LEELIN_FUSED)
+                  mo = impose_class(mo, wk, geo);
+                s_m[st] = mo.rho;
+                s_m[T::NF + st] = mo.ux;
+                s_m[2 * T::NF + st] = mo.uy;
+              }
+            if constexpr (MODE == ADV_TG_COLLIDE)
               s_wall[st] = uint8_t(wk);
-            s_m[st] = mo.rho;
-            s_m[T::NF + st] = mo.ux;
-            s_m[2 * T::NF + st] = mo.uy;
           }
       }
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int bx_lo = g.px ? -1 : 0, bx_hi = g.px ? -1 : g.nfx - 1;
     const int by_lo = g.py ? -1 : 0, by_hi = g.py ? -1 : g.nfy - 1;
+    const R omega = R(ac.omega);
 
     for (int a = (MODE == ADV_TG_COLLIDE ? 0 : 1); a < Q; ++a)
       {
@@ -567,9 +801,19 @@ namespace lbfem_gpu
                 const int c = maps.col[fx];
                 if (r < 0 || c < 0)
                   continue;
-                const Mom mo{s_m[st], s_m[T::NF + st], s_m[2 * T::NF + st]};
-                const Mom mt = impose_class(mo, s_wall[st], geo);
-                const double gs = feq_a(a, mt) + (1. - ac.omega) * (s_u[st] - feq_a(a, mo));
+                R gs;
+                if constexpr (DEV)
+                  {
+                    const MomF mo{s_m[st], s_m[T::NF + st], s_m[2 * T::NF + st], s_m[3 * T::NF + st]};
+                    const MomF mt = impose_class(mo, s_wall[st], geo);
+                    gs = feqd_a(a, mt) + (1.f - omega) * (s_u[st] - feqd_a(a, mo));
+                  }
+                else
+                  {
+                    const Mom mo{s_m[st], s_m[T::NF + st], s_m[2 * T::NF + st]};
+                    const Mom mt = impose_class(mo, s_wall[st], geo);
+                    gs = feq_a(a, mt) + (1. - omega) * (s_u[st] - feq_a(a, mo));
+                  }
                 s_u[st] = gs;
                 const int gx = gx0 - P + fx, gy = gy0 - P + fy;
                 if (fx >= P && fx < P + T::TX && fy >= P && fy < P + T::TY && gx < g.nfx && gy < g.nfy &&
@@ -583,7 +827,14 @@ namespace lbfem_gpu
         const int al = a - 1;
         const double ex = ac.ex[al], ey = ac.ey[al];
         const int cls = ey == 0.0 ? (ex == 0.0 ? 3 : 0) : (ex == 0.0 ? 1 : 2);
-        const AdvK k{ac.a, ac.b, ex, ac.c * ex * ex, ey, -2.0 * ac.c * ex * ey, ac.c * ey * ey, ac.c * ex * ey};
+        const AdvK<R> k{R(ac.a),
+                        R(ac.b),
+                        R(ex),
+                        R(ac.c * ex * ex),
+                        R(ey),
+                        R(-2.0 * ac.c * ex * ey),
+                        R(ac.c * ey * ey),
+                        R(ac.c * ex * ey)};
         // x pass: lane = footprint row, warp = x segment
         if (warp < T::NSX && lane < T::FY)
           {
@@ -602,11 +853,11 @@ namespace lbfem_gpu
         if (j < T::TX && seg < T::NSY)
           {
             const int gx = gx0 + j;
-            double *out = rhs + (long long)al * N;
-            auto emit = [&](int i, double r) {
+            R *out = rhs + (long long)al * N;
+            auto emit = [&](int i, R r) {
               const int gy = gy0 + i;
               if (gx < g.nfx && gy < g.nfy)
-                out[(long long)gy * g.nfx + gx] = is_image(gx, gy, g) ? 0.0 : r;
+                out[(long long)gy * g.nfx + gx] = is_image(gx, gy, g) ? R(0) : r;
             };
             if (cls == 0)
               adv_ypass<P, 0>(s_y, s_y4, maps, j, seg, gy0, by_lo, by_hi, emit);
@@ -616,7 +867,7 @@ namespace lbfem_gpu
               adv_ypass<P, 2>(s_y, s_y4, maps, j, seg, gy0, by_lo, by_hi, emit);
             else
               for (int i = seg * T::SY; i < (seg + 1) * T::SY; ++i)
-                emit(i, 0.0);
+                emit(i, R(0));
           }
       }
 
@@ -630,11 +881,14 @@ namespace lbfem_gpu
             if (gx >= g.nfx || gy >= g.nfy || !is_image(gx, gy, g))
               continue;
             const long long idx = (long long)gy * g.nfx + gx;
-            double v[Q];
+            R v[Q];
 #pragma unroll
             for (int a = 0; a < Q; ++a)
               v[a] = f[a * N + idx];
-            collide_node(v, idx, geo, ac.omega);
+            if constexpr (DEV)
+              collide_node_dev(v, idx, geo, omega);
+            else
+              collide_node(v, idx, geo, omega);
 #pragma unroll
             for (int a = 0; a < Q; ++a)
               fout[a * N + idx] = v[a];
@@ -655,9 +909,9 @@ namespace lbfem_gpu
   // rhs += int_wall phi (dt^2/2)(n.e)(e.grad f) (advection.h:126-146,182-199) at the
   // boundary nodes of the non-periodic sides; one thread per boundary node
   // (bnode = (i, j, side mask: 1 bottom, 2 top, 4 left, 8 right)).
-  template <int P>
+  template <int P, typename R>
   __global__ void
-  k_wall_faces(const Geo geo, const double *__restrict__ f, double *__restrict__ rhs, const int4 *__restrict__ bnode,
+  k_wall_faces(const Geo geo, const R *__restrict__ f, R *__restrict__ rhs, const int4 *__restrict__ bnode,
                int n_bnodes, const FaceCoef fc)
   {
     constexpr int K = 2 * P + 1;
@@ -668,10 +922,10 @@ namespace lbfem_gpu
     const long long N = g.N;
     const int4 bn = bnode[t];
     const int i = bn.x, j = bn.y, sides = bn.z;
-    double R[NM];
+    double Rs[NM];
 #pragma unroll
     for (int al = 0; al < NM; ++al)
-      R[al] = 0;
+      Rs[al] = 0;
     for (int side = 0; side < 4; ++side)
       {
         if (!(sides & (1 << side)))
@@ -693,7 +947,7 @@ namespace lbfem_gpu
               continue;
             const double et = horizontal ? ex : ey;  // tangential component
             const double enn = horizontal ? ey : ex; // normal component (derivative direction)
-            const double *u = f + (long long)(al + 1) * N;
+            const R *u = f + (long long)(al + 1) * N;
             double tang = 0, norm = 0;
             for (int k = 0; k < K; ++k)
               {
@@ -715,7 +969,7 @@ namespace lbfem_gpu
                 tang += cC * u[il];
                 norm += cM * d;
               }
-            R[al] += fc.half_dt2 * en * (et * tang + enn * norm);
+            Rs[al] += fc.half_dt2 * en * (et * tang + enn * norm);
           }
       }
     if (fc.remove)
@@ -723,15 +977,15 @@ namespace lbfem_gpu
         double flux = 0;
 #pragma unroll
         for (int al = 0; al < NM; ++al)
-          flux += R[al];
+          flux += Rs[al];
 #pragma unroll
         for (int al = 0; al < NM; ++al)
-          R[al] -= (c_W[al + 1] / (1. - c_W[0])) * flux;
+          Rs[al] -= (c_W[al + 1] / (1. - c_W[0])) * flux;
       }
     const long long idx = (long long)j * g.nfx + i;
 #pragma unroll
     for (int al = 0; al < NM; ++al)
-      rhs[al * N + idx] += R[al];
+      rhs[al * N + idx] = R(double(rhs[al * N + idx]) + Rs[al]);
   }
 
   // ------------------------------------------------------ mass matrix (K2)
@@ -745,10 +999,10 @@ namespace lbfem_gpu
   }
 
   // The mass operator My (x) Mx of the staged field s_u for every own node of the
-  // tile: emit(i, j, storage index, Au, own u); images get the identity row.
-  template <int P, typename Emit>
+  // tile: emit(i, j, storage index, image, Au); images get the identity row.
+  template <int P, typename R, typename Emit>
   __device__ __forceinline__ void
-  mass_apply(const double *s_u, double *s_t, const TileMaps<P> &m, const Grid &g, int gx0, int gy0, Emit &&emit)
+  mass_apply(const R *s_u, R *s_t, const TileMaps<P, R> &m, const Grid &g, int gx0, int gy0, Emit &&emit)
   {
     using T = Tile<P>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -759,7 +1013,7 @@ namespace lbfem_gpu
     if (j < T::TX && seg < T::NSY)
       {
         const int gx = gx0 + j;
-        mass_ypass<P>(s_t, m, j, seg, [&](int i, double v) {
+        mass_ypass<P>(s_t, m, j, seg, [&](int i, R v) {
           const int gy = gy0 + i;
           if (gx < g.nfx && gy < g.nfy)
             emit(i, j, (long long)gy * g.nfx + gx, is_image(gx, gy, g), v);
@@ -774,7 +1028,7 @@ namespace lbfem_gpu
   {
     using T = Tile<P>;
     extern __shared__ double sm[];
-    __shared__ TileMaps<P> maps;
+    __shared__ TileMaps<P, double> maps;
     double *s_u = sm, *s_t = sm + T::NF;
     const Grid &g = geo.g;
     const long long N = g.N;
@@ -794,11 +1048,14 @@ namespace lbfem_gpu
   }
 
   // ------------------------------------------- Jacobi-PCG, 8 systems at once (K3)
-  // deal.II SolverCG (mass.h:204-211), one state per system.
+  // deal.II SolverCG (mass.h:204-211), one state per system. With mixed
+  // precision the vectors are FP32, the inner iterations run in FP32 with FP64
+  // dot products, and each solve restarts from a true residual computed in
+  // FP64 (iterative refinement) until the outer tolerance holds.
   struct CgState
   {
-    double tol[NM], rz[NM], rz_prev[NM], beta[NM], alpha[NM], res[NM];
-    int it[NM], active[NM];
+    double tol[NM], tol_inner[NM], rz[NM], rz_prev[NM], beta[NM], alpha[NM], res[NM];
+    int it[NM], its_total[NM], active[NM];
     int status, n_active, iter;
     unsigned long long total_its;
   };
@@ -810,17 +1067,18 @@ namespace lbfem_gpu
   }
 
   // r = b - A xg with xg = extrapolate ? 2 x_cur - x_prev (written to x_new) : x_new;
-  // partials per system: b.b, r.r, r.D^{-1}r.
-  template <int P>
+  // partials per system: b.b, r.r, r.D^{-1}r. Storage R, arithmetic A (A = double:
+  // the FP64 residual of the refinement). One system per CTA.
+  template <int P, typename R, typename X = R, typename A = R>
   __global__ void __launch_bounds__(THREADS)
-    k_cg_start(const Geo geo, const double *__restrict__ b, const double *__restrict__ x_cur,
-               const double *__restrict__ x_prev, double *__restrict__ x_new, double *__restrict__ r, int extrapolate,
-               double *__restrict__ partials)
+    k_cg_start(const Geo geo, const R *__restrict__ b, const X *__restrict__ x_cur, const X *__restrict__ x_prev,
+               X *__restrict__ x_new, R *__restrict__ r, int extrapolate, double *__restrict__ partials)
   {
     using T = Tile<P>;
-    extern __shared__ double sm[];
-    __shared__ TileMaps<P> maps;
-    double *s_u = sm, *s_t = sm + T::NF;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    A *s_u = reinterpret_cast<A *>(sm_raw), *s_t = s_u + T::NF;
+    R *s_b = reinterpret_cast<R *>(s_t + T::NY);
+    __shared__ TileMaps<P, A> maps;
     const Grid &g = geo.g;
     const long long N = g.N;
     const int s = blockIdx.z;
@@ -828,32 +1086,31 @@ namespace lbfem_gpu
     build_maps<P>(maps, geo, gx0, gy0);
     __syncthreads();
     const long long o = s * N;
-    double *s_b = s_t + T::NY;
-    stage<P>(s_u, maps, [&](long long idx) {
-      return extrapolate ? -x_prev[o + idx] + 2. * x_cur[o + idx] : x_new[o + idx];
+    stage<P>(s_u, maps, [&](long long idx) -> A {
+      return extrapolate ? -A(x_prev[o + idx]) + A(2) * A(x_cur[o + idx]) : A(x_new[o + idx]);
     });
     stage_own<P>(s_b, b + o, g, gx0, gy0);
     __syncthreads();
     double part[3] = {0, 0, 0};
-    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, long long idx, bool image, double Ax) {
+    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, long long idx, bool image, A Ax) {
       const long long id = o + idx;
-      double xg;
+      A xg;
       if (image)
         {
-          xg = extrapolate ? -x_prev[id] + 2. * x_cur[id] : x_new[id];
+          xg = extrapolate ? -A(x_prev[id]) + A(2) * A(x_cur[id]) : A(x_new[id]);
           Ax = xg;
         }
       else
         xg = s_u[(i + P) * T::PF + j + P];
       if (extrapolate)
-        x_new[id] = xg;
-      const double bb = s_b[i * T::TX + j];
-      const double rr = -Ax + bb;
-      r[id] = rr;
+        x_new[id] = X(xg);
+      const A bb = A(s_b[i * T::TX + j]);
+      const A rr = -Ax + bb;
+      r[id] = R(rr);
       const int gy = int(idx / g.nfx), gx = int(idx - (long long)gy * g.nfx);
-      part[0] += bb * bb;
-      part[1] += rr * rr;
-      part[2] += rr * (inv_jacobi_at(geo, gx, gy) * rr);
+      part[0] += double(bb) * double(bb);
+      part[1] += double(rr) * double(rr);
+      part[2] += double(rr) * (inv_jacobi_at(geo, gx, gy) * double(rr));
     });
     const int nt = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
     // partial (quantity k of system s) at [(k*NM + s) * n_tiles + tile]
@@ -861,15 +1118,15 @@ namespace lbfem_gpu
   }
 
   // p <- D^{-1} r + beta p (p <- D^{-1} r on the first iteration); partial p.Ap. One system per CTA.
-  template <int P>
+  template <int P, typename R>
   __global__ void __launch_bounds__(THREADS)
-    k_cg_p(const Geo geo, const double *__restrict__ r, const double *__restrict__ p_in, double *__restrict__ p_out,
+    k_cg_p(const Geo geo, const R *__restrict__ r, const R *__restrict__ p_in, R *__restrict__ p_out,
            const CgState *__restrict__ st, double *__restrict__ partials)
   {
     using T = Tile<P>;
-    extern __shared__ double sm[];
-    __shared__ TileMaps<P> maps;
-    double *s_u = sm, *s_t = sm + T::NF;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    R *s_u = reinterpret_cast<R *>(sm_raw), *s_t = s_u + T::NF;
+    __shared__ TileMaps<P, R> maps;
     const Grid &g = geo.g;
     const long long N = g.N;
     const int s = blockIdx.z;
@@ -879,7 +1136,7 @@ namespace lbfem_gpu
     const int gx0 = blockIdx.x * T::TX, gy0 = blockIdx.y * T::TY;
     build_maps<P>(maps, geo, gx0, gy0);
     const bool first = st->it[s] == 0;
-    const double beta = st->beta[s];
+    const R beta = R(st->beta[s]);
     const long long o = s * N;
     __syncthreads();
     for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
@@ -887,20 +1144,20 @@ namespace lbfem_gpu
         const int fy = t / T::FX, fx = t - fy * T::FX;
         const long long rw = maps.row[fy];
         const int c = maps.col[fx];
-        double v = 0;
+        R v = 0;
         if (rw >= 0 && c >= 0)
           {
             const long long id = o + rw + c;
-            const double z = inv_jacobi_at(geo, c, maps.rowi[fy]) * r[id];
+            const R z = R(inv_jacobi_at(geo, c, maps.rowi[fy])) * r[id];
             v = first ? z : fma(beta, p_in[id], z);
           }
         s_u[fy * T::PF + fx] = v;
       }
     __syncthreads();
     double part[1] = {0};
-    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, long long idx, bool image, double Ap) {
+    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, long long idx, bool image, R Ap) {
       const long long id = o + idx;
-      double pn;
+      R pn;
       if (image)
         {
           pn = first ? r[id] : fma(beta, p_in[id], r[id]);
@@ -909,21 +1166,21 @@ namespace lbfem_gpu
       else
         pn = s_u[(i + P) * T::PF + j + P];
       p_out[id] = pn;
-      part[0] += pn * Ap;
+      part[0] += double(pn) * double(Ap);
     });
     block_reduce_store<1>(part, partials + (long long)s * nt, tile, NM * nt);
   }
 
   // v = A p recomputed; x += alpha p, r -= alpha v; partials r.r, r.D^{-1}r. One system per CTA.
-  template <int P>
+  template <int P, typename R>
   __global__ void __launch_bounds__(THREADS)
-    k_cg_update(const Geo geo, double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
+    k_cg_update(const Geo geo, R *__restrict__ x, R *__restrict__ r, const R *__restrict__ p,
                 const CgState *__restrict__ st, double *__restrict__ partials)
   {
     using T = Tile<P>;
-    extern __shared__ double sm[];
-    __shared__ TileMaps<P> maps;
-    double *s_u = sm, *s_t = sm + T::NF;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    R *s_u = reinterpret_cast<R *>(sm_raw), *s_t = s_u + T::NF;
+    __shared__ TileMaps<P, R> maps;
     const Grid &g = geo.g;
     const long long N = g.N;
     const int s = blockIdx.z;
@@ -932,28 +1189,28 @@ namespace lbfem_gpu
       return;
     const int gx0 = blockIdx.x * T::TX, gy0 = blockIdx.y * T::TY;
     build_maps<P>(maps, geo, gx0, gy0);
-    const double al = st->alpha[s];
+    const R al = R(st->alpha[s]);
     const long long o = s * N;
-    const double *ps = p + o;
-    double *s_x = s_t + T::NY, *s_r = s_x + T::TX * T::TY;
+    const R *ps = p + o;
+    R *s_x = s_t + T::NY, *s_r = s_x + T::TX * T::TY;
     __syncthreads();
     stage<P>(s_u, maps, [&](long long idx) { return ps[idx]; });
     stage_own<P>(s_x, x + o, g, gx0, gy0);
     stage_own<P>(s_r, r + o, g, gx0, gy0);
     __syncthreads();
     double part[2] = {0, 0};
-    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, long long idx, bool image, double Ap) {
+    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, long long idx, bool image, R Ap) {
       const long long id = o + idx;
-      const double pv = image ? p[id] : s_u[(i + P) * T::PF + j + P];
+      const R pv = image ? p[id] : s_u[(i + P) * T::PF + j + P];
       if (image)
         Ap = pv;
       const int t = i * T::TX + j;
       x[id] = s_x[t] + al * pv;
-      const double rr = s_r[t] + -al * Ap;
+      const R rr = s_r[t] + -al * Ap;
       r[id] = rr;
       const int gy = int(idx / g.nfx), gx = int(idx - (long long)gy * g.nfx);
-      part[0] += rr * rr;
-      part[1] += rr * (inv_jacobi_at(geo, gx, gy) * rr);
+      part[0] += double(rr) * double(rr);
+      part[1] += double(rr) * (inv_jacobi_at(geo, gx, gy) * double(rr));
     });
     block_reduce_store<2>(part, partials + (long long)s * nt, tile, NM * nt);
   }
@@ -961,19 +1218,22 @@ namespace lbfem_gpu
   // The scalar work of one CG phase, one thread per system, from the reduced sums.
   // phase 0 (after start): sums = [bb, rr, rz]; phase 1 (after p): [pAp];
   // phase 2 (after update): [rr, rz].
+  // inner_rel > 0 (refinement): an inner pass stops at max(tol, inner_rel |r_true|).
   __global__ void
-  k_cg_scalars(CgState *st, const double *__restrict__ sums, int nsys, int phase, double cg_tol, int max_its)
+  k_cg_scalars(CgState *st, const double *__restrict__ sums, int nsys, int phase, double cg_tol, int max_its,
+               double inner_rel)
   {
     const int s = threadIdx.x;
     if (s < NM)
       {
         if (phase == 0)
           {
-            if (s < nsys)
+            if (s < nsys && st->status == 0 && st->its_total[s] < max_its)
               {
                 st->tol[s] = cg_tol * sqrt(sums[s]);
                 const double res = sqrt(sums[NM + s]);
                 st->res[s] = res;
+                st->tol_inner[s] = fmax(st->tol[s], inner_rel * res);
                 st->rz[s] = sums[2 * NM + s];
                 st->it[s] = 0;
                 st->beta[s] = 0;
@@ -995,7 +1255,8 @@ namespace lbfem_gpu
           }
         else if (s < nsys && st->active[s])
           {
-            const int it = ++st->it[s];
+            ++st->it[s];
+            const int it = ++st->its_total[s];
             atomicAdd(&st->total_its, 1ULL);
             const double res = sqrt(sums[s]);
             st->res[s] = res;
@@ -1004,7 +1265,7 @@ namespace lbfem_gpu
                 st->active[s] = 0;
                 atomicExch(&st->status, 3);
               }
-            else if (res <= st->tol[s])
+            else if (res <= st->tol_inner[s])
               st->active[s] = 0;
             else if (it >= max_its)
               {

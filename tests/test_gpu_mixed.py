@@ -1,0 +1,94 @@
+"""Mixed precision (FP32 deviations f - w, FP32 streaming / collision / inner
+CG, FP64 refinement residuals and FP64 sums) against the FP64 path: the
+relative L2 velocity error after a run stays within 1e-5 and the total mass
+drift stays at the FP32 rounding level."""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import rel_l2, setup_case
+from lbfem_gpu import cases, d2q9, make_params
+
+pytestmark = pytest.mark.gpu
+
+TOL_U = 1e-5
+
+
+def _gpu(mesh, params):
+    import lbfem_gpu
+
+    return lbfem_gpu.Solver(mesh, params)
+
+
+def _velocity(mesh, f):
+    ind = mesh.independent()
+    rho, ux, uy = d2q9.moments(f[:, ind])
+    return np.stack([ux, uy]), rho
+
+
+def _pair(tc, mesh, scheme, mass, dt, steps, tol=1e-12):
+    lam = tc.relaxation_time()
+    ref = setup_case(_gpu, tc, mesh, make_params(scheme, mass, cg_tolerance=tol), dt, lam)
+    mix = setup_case(_gpu, tc, mesh, make_params(scheme, mass, cg_tolerance=tol, precision="mixed"), dt, lam)
+    ref.step(steps)
+    mix.step(steps)
+    return ref, mix
+
+
+def test_mixed_population_roundtrip(gpu_lib):
+    tc = cases.TaylorGreenVortex(0.1, 1, 4)
+    tc.set_reynolds(100)
+    m = cases.build_mesh(tc, 10, 2)
+    g = _gpu(m, make_params(precision="mixed"))
+    x, y = m.nodes()
+    f = tc.initial_populations(x, y, tc.relaxation_time())
+    g.set_populations(f)
+    out = g.get_populations()
+    # FP32 deviations from the rest state: error ~ 2^-24 |f - w|
+    dev = np.abs(f - d2q9.W[:, None])
+    assert np.all(np.abs(out - f) <= 1e-7 * dev + 1e-12)
+
+
+@pytest.mark.parametrize("scheme,mass,case,p,n,steps,cfl", [
+    ("bardow", "cg", "tgv", 1, 64, 400, 0.5),
+    ("leelin", "cg", "tgv", 3, 16, 200, 0.5),
+    ("bardow", "lumped", "cavity", 2, 16, 400, 0.4),
+    ("leelin", "cg", "couette", 1, 16, 600, 0.25),
+    ("bardow", "cg", "cavity", 1, 24, 300, 0.4),
+])
+def test_mixed_matches_fp64(gpu_lib, scheme, mass, case, p, n, steps, cfl):
+    if case == "tgv":
+        tc = cases.TaylorGreenVortex(0.05 / math.sqrt(d2q9.CS2), 1, 1, shift=(0.25, 0.25), chapman_enskog=False)
+        tc.set_reynolds(100)
+    elif case == "couette":
+        tc = cases.CouetteFlow(0.05 / math.sqrt(d2q9.CS2))
+        tc.set_reynolds(50)
+    else:
+        tc = cases.LidDrivenCavity(0.1, 1.2)
+        tc.set_reynolds(400)
+    m = cases.build_mesh(tc, n, p)
+    ref, mix = _pair(tc, m, scheme, mass, m.time_step(cfl), steps)
+    fr, fm = ref.get_populations(), mix.get_populations()
+    ur, rr = _velocity(m, fr)
+    um, rm = _velocity(m, fm)
+    err_u = rel_l2(um, ur)
+    assert err_u <= TOL_U, err_u
+    assert rel_l2(rm, rr) <= 1e-6
+    cr, cm = ref.conservation(), mix.conservation()
+    assert abs(cm[1] / cm[0] - cr[1] / cr[0]) <= 1e-6  # mean density (mass drift)
+
+
+def test_mixed_against_the_oracle(gpu_lib, oracle_mod):
+    """Lee-Lin Q2 Taylor-Green, consistent mass: mixed GPU vs the FP64 oracle."""
+    tc = cases.TaylorGreenVortex(0.05 / math.sqrt(d2q9.CS2), 1, 1, shift=(0.25, 0.25), chapman_enskog=False)
+    tc.set_reynolds(100)
+    m = cases.build_mesh(tc, 12, 2)
+    dt, lam = m.time_step(0.5), tc.relaxation_time()
+    o = setup_case(oracle_mod.Oracle, tc, m, make_params("leelin", "cg", cg_tolerance=1e-12), dt, lam)
+    g = setup_case(_gpu, tc, m, make_params("leelin", "cg", cg_tolerance=1e-12, precision="mixed"), dt, lam)
+    o.step(150)
+    g.step(150)
+    uo, _ = _velocity(m, o.get_populations())
+    ug, _ = _velocity(m, g.get_populations())
+    assert rel_l2(ug, uo) <= TOL_U
