@@ -2,7 +2,8 @@
 
 Workload (default): the Taylor-Green throughput scan -- periodic unit square,
 Q3 elements on 1024 x 1024 cells (3072^2 = 9,437,184 distinct nodes), D2Q9,
-Lee-Lin predictor-corrector, consistent mass solved by Jacobi-PCG to 1e-12,
+Lee-Lin predictor-corrector, consistent mass solved by Jacobi-PCG to 1e-8 (the
+reference default; FP64 and mixed alike),
 Re 100, U0 = 0.05, CFL 0.5, u = U0 sin(2 pi x) cos(2 pi y) with the matching
 pressure, f = feq. Synthetic (analytic) input, state resident in HBM (about
 7 GB, far larger than L2, so no flush is needed between steps).
@@ -51,10 +52,10 @@ def workload(args):
     f0 = tc.initial_populations(x, y, lam)
     cfg = {
         "workload": f"taylor-green periodic, Q{args.degree} {args.cells}x{args.cells} cells, "
-                    f"{args.scheme} predictor-corrector, consistent mass (Jacobi-PCG 1e-12)",
+                    f"{args.scheme}, consistent mass (Jacobi-PCG {args.cg_tol:g})",
         "degree": args.degree, "cells": args.cells, "nodes_distinct": mesh.n_unique(), "nodes_stored": mesh.n_dofs,
-        "scheme": args.scheme, "mass": "cg", "cg_tolerance": 1e-12, "Re": 100, "U0": 0.05, "cfl": 0.5,
-        "precision": "fp64", "l2": "state > L2 (no flush needed)",
+        "scheme": args.scheme, "mass": "cg", "cg_tolerance": args.cg_tol, "Re": 100, "U0": 0.05, "cfl": 0.5,
+        "l2": "state > L2 (no flush needed)",
     }
     return tc, mesh, dt, lam, f0, cfg
 
@@ -139,7 +140,7 @@ def cpu_run(tc, mesh, dt, lam, f0, args, budget_s, max_steps):
     from lbfem_gpu import make_params
 
     threads = oracle.set_threads(os.cpu_count() or 1)
-    h = oracle.Oracle(mesh, make_params(args.scheme, "cg", cg_tolerance=1e-12))
+    h = oracle.Oracle(mesh, make_params(args.scheme, "cg", cg_tolerance=args.cg_tol))
     h.set_time_step(dt, lam)
     h.set_initial_populations(f0)
     h.step(1)
@@ -191,16 +192,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def run_ours(args):
+def run_precision(args, precision, tc, mesh, dt, lam, f0, local, pg, world):
+    """One timed run of the workload in one precision; returns its figures and final velocity."""
     import ctypes as C
 
     import lbfem_gpu
     from lbfem_gpu import make_params
 
-    world, rank, local, pg = dist_setup()
-    tc, mesh, dt, lam, f0, cfg = workload(args)
     lib = lbfem_gpu.library()
-    prm = make_params(args.scheme, "cg", cg_tolerance=1e-12, device=local)
+    prm = make_params(args.scheme, "cg", cg_tolerance=args.cg_tol, precision=precision, device=local)
     h = lbfem_gpu.Solver(mesh, prm)
     h.set_time_step(dt, lam)
     h.set_initial_populations(f0)
@@ -211,7 +211,6 @@ def run_ours(args):
         h._call("event_elapsed", ctx, a, b, C.byref(ms))
         return ms.value * 1e-3
 
-    # warm-up
     h.step(args.warmup)
     lib.lbfem_gpu_synchronize(ctx)
     barrier(pg)
@@ -225,8 +224,10 @@ def run_ours(args):
     barrier(pg)
     its, launches = C.c_double(), C.c_int64()
     h._call("last_step_stats", ctx, C.byref(its), C.byref(launches))
-    units = 9 * mesh.n_unique() * args.steps * world
-    value = units / sec
+    cons = h.conservation()
+    rho, ux, uy = (np.empty(mesh.n_dofs) for _ in range(3))
+    P = C.POINTER(C.c_double)
+    h._call("moments", ctx, rho.ctypes.data_as(P), ux.ctypes.data_as(P), uy.ctypes.data_as(P))
 
     # roofline of the streaming kernel (K1), timed alone on the context's stream
     reps = 10
@@ -237,13 +238,44 @@ def run_ours(args):
         h._call("advection_resident", ctx)
     h._call("event_record", ctx, 3)
     k1 = elapsed(2, 3) / reps
-    n_reads = 9
-    n_writes = 8 if args.scheme == "leelin" else 17
-    alg_bytes = 8 * mesh.n_dofs * (n_reads + n_writes)
+    real = 4 if precision == "mixed" else 8
+    n_writes = 8 if args.scheme == "leelin" else 17  # Bardow also writes the collided populations
+    alg_bytes = real * mesh.n_dofs * (9 + n_writes)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / k1 / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "kernel": f"k_advection<{args.degree}, {args.scheme} fused, "
+                                       f"{'float' if precision == 'mixed' else 'double'}>",
+            "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": 1e3 * k1,
+            "peak_kind": f"{peak_kind} HBM copy bandwidth (burst)"}
+    out = {"sec": sec, "its": its.value, "launches": int(launches.value), "roofline": roof,
+           "clocks": clocks.summary(), "mass": cons[1] / cons[0], "u": np.stack([ux, uy]), "handle": h}
+    return out
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import lbfem_gpu
+
+    world, rank, local, pg = dist_setup()
+    tc, mesh, dt, lam, f0, cfg = workload(args)
+    lib = lbfem_gpu.library()
+    ind = mesh.independent()
+    runs = {}
+    for precision in ("fp64", "mixed"):
+        r = run_precision(args, precision, tc, mesh, dt, lam, f0, local, pg, world)
+        if precision == "fp64":
+            r.pop("handle").close()
+        runs[precision] = r
+    mix, f64 = runs["mixed"], runs["fp64"]
+    h = mix.pop("handle")
+    du = mix["u"][:, ind] - f64["u"][:, ind]
+    rel_u = float(np.linalg.norm(du) / np.linalg.norm(f64["u"][:, ind]))
+    units = 9 * mesh.n_unique() * args.steps * world
 
     # end to end through the host-buffer C ABI call: upload f, one step, download f
+    ctx = h.h
     n_e2e = max(1, min(args.steps, 5))
     fbuf_ptr = lib.lbfem_gpu_host_alloc(9 * mesh.n_dofs * 8)
     fbuf = np.ctypeslib.as_array((C.c_double * (9 * mesh.n_dofs)).from_address(fbuf_ptr))
@@ -257,6 +289,7 @@ def run_ours(args):
     e2e_sec = allreduce_max(pg, time.perf_counter() - t0)
     e2e_value = 9 * mesh.n_unique() * n_e2e * world / e2e_sec
     lib.lbfem_gpu_host_free(fbuf_ptr)
+    h.close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -265,25 +298,30 @@ def run_ours(args):
         cpu = {"value": cval, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{cn} step(s) of the full mesh after 1 warm-up step ({csec:.1f} s), CPU FP64 oracle port, "
                          f"{threads} OpenMP threads, {cpu_model()}"}
-    h.close()
     if rank != 0:
         return 0
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Taylor-Green initial state)",
-        "config": dict(cfg, parallelism=f"replicas x{world}" if world > 1 else "single GPU",
-                       cg_iterations_per_solve=its.value),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": f"k_advection<{args.degree}, {args.scheme} fused>",
-                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": 1e3 * k1,
-                     "peak_kind": f"{peak_kind} copy bandwidth (burst)"},
+        "metric": METRIC, "value": units / mix["sec"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * mix["sec"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 mixed (FP32 deviations, FP32 streaming/collision/inner CG; FP64 refinement residuals, "
+                 "CG dot products and conservation sums)",
+        "data": "synthetic (analytic Taylor-Green initial state)",
+        "config": dict(cfg, precision="mixed (headline) and fp64", parallelism=f"replicas x{world}" if world > 1
+                       else "single GPU", cg_iterations_per_solve={"mixed": mix["its"], "fp64": f64["its"]}),
+        "fp64": {"value": units / f64["sec"], "ms_per_step": 1e3 * f64["sec"] / args.steps,
+                 "roofline": f64["roofline"], "gpu_launches": f64["launches"]},
+        "accuracy": {"rel_l2_u_mixed_vs_fp64": rel_u, "target": 1e-5, "mean_density_fp64": f64["mass"],
+                     "mean_density_mixed": mix["mass"],
+                     "note": f"after {args.warmup + args.steps} steps of both runs from the same initial state"},
+        "mixed_vs_fp64_speedup": f64["sec"] / mix["sec"],
+        "roofline": mix["roofline"],
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 9 * 8 * mesh.n_dofs,
                 "d2h_bytes_per_step": 9 * 8 * mesh.n_dofs, "steps": n_e2e,
-                "call": "lbfem_gpu_step_host (pinned host populations in, one step, populations out)"},
-        "clocks": clocks.summary(),
-        "gpu_launches": int(launches.value),
+                "call": "lbfem_gpu_step_host on the mixed context (FP64 host populations in, one step, out)"},
+        "clocks": mix["clocks"],
+        "gpu_launches": mix["launches"],
     }
     print(json.dumps(line))
     return 0
@@ -299,6 +337,8 @@ def main():
     ap.add_argument("--degree", type=int, default=3)
     ap.add_argument("--scheme", default="leelin", choices=["leelin", "bardow"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cg-tol", type=float, default=1e-8,
+                    help="relative CG tolerance of both precisions (MassSettings default 1e-8, mass.h:33)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -312,6 +312,7 @@ namespace lbfem_gpu
     long long row[Tile<P>::FY];
     R hx[Tile<P>::CX + 1], hxi[Tile<P>::CX + 1], cx[Tile<P>::CX + 1];
     R hy[Tile<P>::CY + 1], hyi[Tile<P>::CY + 1], cy[Tile<P>::CY + 1];
+    double ijx[Tile<P>::FX], ijy[Tile<P>::FY]; // inverse Jacobi diagonal factors of the footprint's storage nodes
   };
 
   template <int P, typename R>
@@ -321,12 +322,17 @@ namespace lbfem_gpu
     using T = Tile<P>;
     const Grid &g = geo.g;
     for (int t = threadIdx.x; t < T::FX; t += blockDim.x)
-      m.col[t] = wrap(gx0 - P + t, g.px, g.nux, g.nfx);
+      {
+        const int c = wrap(gx0 - P + t, g.px, g.nux, g.nfx);
+        m.col[t] = c;
+        m.ijx[t] = c < 0 ? 0.0 : geo.ijx[c];
+      }
     for (int t = threadIdx.x; t < T::FY; t += blockDim.x)
       {
         const int r = wrap(gy0 - P + t, g.py, g.nuy, g.nfy);
         m.rowi[t] = r;
         m.row[t] = r < 0 ? -1 : (long long)r * g.nfx;
+        m.ijy[t] = r < 0 ? 0.0 : geo.ijy[r];
       }
     const int cx0 = gx0 / P - 1, cy0 = gy0 / P - 1;
     for (int t = threadIdx.x; t <= T::CX; t += blockDim.x)
@@ -351,12 +357,66 @@ namespace lbfem_gpu
   stage(R *s, const TileMaps<P, RM> &m, F &&value_at)
   {
     using T = Tile<P>;
-    for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
+    // all loads of a thread are issued before its first shared store (memory-level parallelism)
+    constexpr int NT = T::FY * T::FX, IT = (NT + THREADS - 1) / THREADS;
+    R v[IT];
+#pragma unroll
+    for (int k = 0; k < IT; ++k)
       {
-        const int fy = t / T::FX, fx = t - fy * T::FX;
-        const long long r = m.row[fy];
-        const int c = m.col[fx];
-        s[fy * T::PF + fx] = (r >= 0 && c >= 0) ? R(value_at(r + c)) : R(0);
+        const int t = threadIdx.x + k * THREADS;
+        v[k] = R(0);
+        if (t < NT)
+          {
+            const int fy = t / T::FX, fx = t - fy * T::FX;
+            const long long r = m.row[fy];
+            const int c = m.col[fx];
+            if (r >= 0 && c >= 0)
+              v[k] = R(value_at(r + c));
+          }
+      }
+#pragma unroll
+    for (int k = 0; k < IT; ++k)
+      {
+        const int t = threadIdx.x + k * THREADS;
+        if (t < NT)
+          {
+            const int fy = t / T::FX, fx = t - fy * T::FX;
+            s[fy * T::PF + fx] = v[k];
+          }
+      }
+  }
+
+  // The same with the storage coordinates: value_at(storage index, column, row).
+  template <int P, typename R, typename RM, typename F>
+  __device__ __forceinline__ void
+  stage_ij(R *s, const TileMaps<P, RM> &m, F &&value_at)
+  {
+    using T = Tile<P>;
+    constexpr int NT = T::FY * T::FX, IT = (NT + THREADS - 1) / THREADS;
+    R v[IT];
+#pragma unroll
+    for (int k = 0; k < IT; ++k)
+      {
+        const int t = threadIdx.x + k * THREADS;
+        v[k] = R(0);
+        if (t < NT)
+          {
+            const int fy = t / T::FX, fx = t - fy * T::FX;
+            const long long r = m.row[fy];
+            const int c = m.col[fx];
+            if (r >= 0 && c >= 0)
+              v[k] = R(value_at(r + c, c, m.rowi[fy]));
+          }
+      }
+#pragma unroll
+    for (int k = 0; k < IT; ++k)
+      {
+        const int t = threadIdx.x + k * THREADS;
+        if (t < NT)
+          {
+            const int fy = t / T::FX, fx = t - fy * T::FX;
+            s[fy * T::PF + fx] = v[k];
+          }
       }
   }
 
@@ -366,11 +426,22 @@ namespace lbfem_gpu
   stage_own(R *s, const R *__restrict__ src, const Grid &g, int gx0, int gy0)
   {
     using T = Tile<P>;
-    for (int t = threadIdx.x; t < T::TY * T::TX; t += blockDim.x)
+    constexpr int NT = T::TY * T::TX, IT = (NT + THREADS - 1) / THREADS;
+    R v[IT];
+#pragma unroll
+    for (int k = 0; k < IT; ++k)
       {
+        const int t = threadIdx.x + k * THREADS;
         const int i = t / T::TX, j = t - i * T::TX;
         const int gx = gx0 + j, gy = gy0 + i;
-        s[t] = (gx < g.nfx && gy < g.nfy) ? src[(long long)gy * g.nfx + gx] : R(0);
+        v[k] = (t < NT && gx < g.nfx && gy < g.nfy) ? src[(long long)gy * g.nfx + gx] : R(0);
+      }
+#pragma unroll
+    for (int k = 0; k < IT; ++k)
+      {
+        const int t = threadIdx.x + k * THREADS;
+        if (t < NT)
+          s[t] = v[k];
       }
   }
 

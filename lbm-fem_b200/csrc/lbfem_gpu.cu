@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -63,6 +64,7 @@ struct lbfem_gpu_ctx
   int64_t cg_its = 0;
   double last_its_per_solve = 0;
   int64_t launches = 0, last_launches = 0;
+  bool trace = false; // LBFEM_TRACE set: the CG rounds print their residuals to stderr
   std::string err;
 };
 
@@ -312,8 +314,11 @@ namespace
   }
 
   // Mixed precision: each refinement round solves the FP32 correction to
-  // inner_rel times the round's true FP64 residual.
+  // inner_rel times the round's true FP64 residual. The right-hand side comes
+  // from the FP32 streaming kernel and is resolved to about 1e-7 of its norm, so
+  // the outer tolerance is at least MIXED_TOL_FLOOR.
   constexpr double MIXED_INNER_REL = 1e-4;
+  constexpr double MIXED_TOL_FLOOR = 1e-7;
   constexpr int MIXED_MAX_ROUNDS = 50;
 
   // x_new <- A^{-1} b for nsys systems (extrapolated start or the given x_new),
@@ -330,7 +335,7 @@ namespace
     constexpr bool MIX = sizeof(R) == sizeof(float);
     const Geo geo = geo_of(ctx);
     const Grid &g = ctx->grid;
-    const double tol = ctx->prm.cg_tolerance;
+    const double tol = MIX ? std::max(ctx->prm.cg_tolerance, MIXED_TOL_FLOOR) : ctx->prm.cg_tolerance;
     const double inner_rel = MIX ? MIXED_INNER_REL : 0.0;
     const int max_its = ctx->prm.cg_max_iterations;
     CK(cudaMemsetAsync(w.state, 0, sizeof(CgState), ctx->stream));
@@ -361,6 +366,14 @@ namespace
           {
             CK(cudaMemcpyAsync(ctx->h_cg, w.state, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaStreamSynchronize(ctx->stream));
+            if (ctx->trace)
+              {
+                double worst = 0;
+                for (int q = 0; q < nsys; ++q)
+                  worst = std::max(worst, ctx->h_cg->tol[q] > 0 ? ctx->h_cg->res[q] / ctx->h_cg->tol[q] : 0.0);
+                std::fprintf(stderr, "lbfem cg: round %d it %d active %d max res/tol %.3e\n", round, it,
+                             ctx->h_cg->n_active, worst);
+              }
             if (ctx->h_cg->n_active == 0)
               {
                 outer_done = it == 0;
@@ -783,6 +796,7 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
   std::unique_ptr<lbfem_gpu_ctx, int (*)(lbfem_gpu_ctx *)> guard(ctx, lbfem_gpu_destroy);
   ctx->device = prm->device;
   ctx->prm = *prm;
+  ctx->trace = std::getenv("LBFEM_TRACE") != nullptr;
   ctx->P = P;
   ctx->n_dofs = m->n_dofs;
   ctx->identity = m->dof_index == nullptr;

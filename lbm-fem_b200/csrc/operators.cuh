@@ -736,47 +736,71 @@ namespace lbfem_gpu
 
     if constexpr (MOM)
       {
-        for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
+        // two footprint nodes per iteration: 18 loads in flight per thread
+        constexpr int NT = T::FY * T::FX;
+        for (int t0 = threadIdx.x; t0 < NT; t0 += 2 * THREADS)
           {
-            const int fy = t / T::FX, fx = t - fy * T::FX, st = fy * T::PF + fx;
-            const long long r = maps.row[fy];
-            const int c = maps.col[fx];
-            if (r < 0 || c < 0)
-              {
+            R v[2][Q];
+            long long idx[2];
+            int wk[2];
 #pragma unroll
-                for (int q = 0; q < NMF; ++q)
-                  s_m[q * T::NF + st] = R(0);
+            for (int h = 0; h < 2; ++h)
+              {
+                const int t = t0 + h * THREADS;
+                idx[h] = -1;
+                wk[h] = 0;
+                if (t < NT)
+                  {
+                    const int fy = t / T::FX, fx = t - fy * T::FX;
+                    const long long r = maps.row[fy];
+                    const int c = maps.col[fx];
+                    if (r >= 0 && c >= 0)
+                      idx[h] = r + c;
+                  }
+#pragma unroll
+                for (int a = 0; a < Q; ++a)
+                  v[h][a] = idx[h] >= 0 ? f[a * N + idx[h]] : R(0);
+                if (idx[h] >= 0 && geo.wall)
+                  wk[h] = geo.wall[idx[h]];
+              }
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+              {
+                const int t = t0 + h * THREADS;
+                if (t >= NT)
+                  continue;
+                const int fy = t / T::FX, fx = t - fy * T::FX, st = fy * T::PF + fx;
+                if (idx[h] < 0)
+                  {
+#pragma unroll
+                    for (int q = 0; q < NMF; ++q)
+                      s_m[q * T::NF + st] = R(0);
+                    if constexpr (MODE == ADV_TG_COLLIDE)
+                      s_wall[st] = 0;
+                    continue;
+                  }
+                if constexpr (DEV)
+                  {
+                    MomF mo = moments_dev(v[h]);
+                    if constexpr (MODE == ADV_LEELIN_FUSED)
+                      mo = impose_class(mo, wk[h], geo);
+                    s_m[st] = mo.rho;
+                    s_m[T::NF + st] = mo.ux;
+                    s_m[2 * T::NF + st] = mo.uy;
+                    s_m[3 * T::NF + st] = mo.drho;
+                  }
+                else
+                  {
+                    Mom mo = moments(v[h]);
+                    if constexpr (MODE == ADV_LEELIN_FUSED)
+                      mo = impose_class(mo, wk[h], geo);
+                    s_m[st] = mo.rho;
+                    s_m[T::NF + st] = mo.ux;
+                    s_m[2 * T::NF + st] = mo.uy;
+                  }
                 if constexpr (MODE == ADV_TG_COLLIDE)
-                  s_wall[st] = 0;
-                continue;
+                  s_wall[st] = uint8_t(wk[h]);
               }
-            const long long idx = r + c;
-            const int wk = geo.wall ? geo.wall[idx] : 0;
-            R v[Q];
-#pragma unroll
-            for (int a = 0; a < Q; ++a)
-              v[a] = f[a * N + idx];
-            if constexpr (DEV)
-              {
-                MomF mo = moments_dev(v);
-                if constexpr (MODE == ADV_LEELIN_FUSED)
-                  mo = impose_class(mo, wk, geo);
-                s_m[st] = mo.rho;
-                s_m[T::NF + st] = mo.ux;
-                s_m[2 * T::NF + st] = mo.uy;
-                s_m[3 * T::NF + st] = mo.drho;
-              }
-            else
-              {
-                Mom mo = moments(v);
-                if constexpr (MODE == ADV_LEELIN_FUSED)
-                  mo = impose_class(mo, wk, geo);
-                s_m[st] = mo.rho;
-                s_m[T::NF + st] = mo.ux;
-                s_m[2 * T::NF + st] = mo.uy;
-              }
-            if constexpr (MODE == ADV_TG_COLLIDE)
-              s_wall[st] = uint8_t(wk);
           }
       }
 
@@ -999,7 +1023,8 @@ namespace lbfem_gpu
   }
 
   // The mass operator My (x) Mx of the staged field s_u for every own node of the
-  // tile: emit(i, j, storage index, image, Au); images get the identity row.
+  // tile: emit(i, j, storage index, image, Au); images get the identity row. The
+  // storage index is 32-bit: a population array holds fewer than 2^31 nodes.
   template <int P, typename R, typename Emit>
   __device__ __forceinline__ void
   mass_apply(const R *s_u, R *s_t, const TileMaps<P, R> &m, const Grid &g, int gx0, int gy0, Emit &&emit)
@@ -1016,7 +1041,7 @@ namespace lbfem_gpu
         mass_ypass<P>(s_t, m, j, seg, [&](int i, R v) {
           const int gy = gy0 + i;
           if (gx < g.nfx && gy < g.nfy)
-            emit(i, j, (long long)gy * g.nfx + gx, is_image(gx, gy, g), v);
+            emit(i, j, gy * g.nfx + gx, is_image(gx, gy, g), v);
         });
       }
   }
@@ -1040,7 +1065,7 @@ namespace lbfem_gpu
         const double *xs = x + s * N;
         stage<P>(s_u, maps, [&](long long idx) { return xs[idx]; });
         __syncthreads();
-        mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int, int, long long idx, bool image, double v) {
+        mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int, int, int idx, bool image, double v) {
           y[s * N + idx] = image ? xs[idx] : v;
         });
         __syncthreads();
@@ -1064,6 +1089,14 @@ namespace lbfem_gpu
   inv_jacobi_at(const Geo &geo, int i, int j)
   {
     return is_image(i, j, geo.g) ? 1.0 : geo.ijx[i] * geo.ijy[j];
+  }
+
+  // The inverse Jacobi diagonal at own node (i, j) of a tile, from its maps.
+  template <int P, typename RM>
+  __device__ __forceinline__ double
+  own_inv_jacobi(const TileMaps<P, RM> &m, int i, int j, bool image)
+  {
+    return image ? 1.0 : m.ijx[j + P] * m.ijy[i + P];
   }
 
   // r = b - A xg with xg = extrapolate ? 2 x_cur - x_prev (written to x_new) : x_new;
@@ -1092,7 +1125,8 @@ namespace lbfem_gpu
     stage_own<P>(s_b, b + o, g, gx0, gy0);
     __syncthreads();
     double part[3] = {0, 0, 0};
-    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, long long idx, bool image, A Ax) {
+    R *rs = r + o;
+    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, int idx, bool image, A Ax) {
       const long long id = o + idx;
       A xg;
       if (image)
@@ -1106,11 +1140,10 @@ namespace lbfem_gpu
         x_new[id] = X(xg);
       const A bb = A(s_b[i * T::TX + j]);
       const A rr = -Ax + bb;
-      r[id] = R(rr);
-      const int gy = int(idx / g.nfx), gx = int(idx - (long long)gy * g.nfx);
+      rs[idx] = R(rr);
       part[0] += double(bb) * double(bb);
       part[1] += double(rr) * double(rr);
-      part[2] += double(rr) * (inv_jacobi_at(geo, gx, gy) * double(rr));
+      part[2] += double(rr) * (own_inv_jacobi(maps, i, j, image) * double(rr));
     });
     const int nt = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
     // partial (quantity k of system s) at [(k*NM + s) * n_tiles + tile]
@@ -1139,33 +1172,24 @@ namespace lbfem_gpu
     const R beta = R(st->beta[s]);
     const long long o = s * N;
     __syncthreads();
-    for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
-      {
-        const int fy = t / T::FX, fx = t - fy * T::FX;
-        const long long rw = maps.row[fy];
-        const int c = maps.col[fx];
-        R v = 0;
-        if (rw >= 0 && c >= 0)
-          {
-            const long long id = o + rw + c;
-            const R z = R(inv_jacobi_at(geo, c, maps.rowi[fy])) * r[id];
-            v = first ? z : fma(beta, p_in[id], z);
-          }
-        s_u[fy * T::PF + fx] = v;
-      }
+    const R *rsys = r + o, *psys = p_in + o;
+    stage_ij<P>(s_u, maps, [&](long long idx, int c, int rw) -> R {
+      const R z = R(geo.ijx[c] * geo.ijy[rw]) * rsys[idx];
+      return first ? z : fma(beta, psys[idx], z);
+    });
     __syncthreads();
     double part[1] = {0};
-    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, long long idx, bool image, R Ap) {
-      const long long id = o + idx;
+    R *posys = p_out + o;
+    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, int idx, bool image, R Ap) {
       R pn;
       if (image)
         {
-          pn = first ? r[id] : fma(beta, p_in[id], r[id]);
+          pn = first ? rsys[idx] : fma(beta, psys[idx], rsys[idx]);
           Ap = pn;
         }
       else
         pn = s_u[(i + P) * T::PF + j + P];
-      p_out[id] = pn;
+      posys[idx] = pn;
       part[0] += double(pn) * double(Ap);
     });
     block_reduce_store<1>(part, partials + (long long)s * nt, tile, NM * nt);
@@ -1199,18 +1223,17 @@ namespace lbfem_gpu
     stage_own<P>(s_r, r + o, g, gx0, gy0);
     __syncthreads();
     double part[2] = {0, 0};
-    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, long long idx, bool image, R Ap) {
-      const long long id = o + idx;
-      const R pv = image ? p[id] : s_u[(i + P) * T::PF + j + P];
+    R *xs = x + o, *rs = r + o;
+    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, int idx, bool image, R Ap) {
+      const R pv = image ? ps[idx] : s_u[(i + P) * T::PF + j + P];
       if (image)
         Ap = pv;
       const int t = i * T::TX + j;
-      x[id] = s_x[t] + al * pv;
+      xs[idx] = s_x[t] + al * pv;
       const R rr = s_r[t] + -al * Ap;
-      r[id] = rr;
-      const int gy = int(idx / g.nfx), gx = int(idx - (long long)gy * g.nfx);
+      rs[idx] = rr;
       part[0] += double(rr) * double(rr);
-      part[1] += double(rr) * (inv_jacobi_at(geo, gx, gy) * double(rr));
+      part[1] += double(rr) * (own_inv_jacobi(maps, i, j, image) * double(rr));
     });
     block_reduce_store<2>(part, partials + (long long)s * nt, tile, NM * nt);
   }
