@@ -98,7 +98,19 @@ typedef struct lbfem_params {
   double cg_tolerance;           /* relative to |r|, reference default 1e-8 */
   int32_t remove_wall_mass_flux; /* -1: scheme default (Bardow 1, Lee-Lin 0), advection.h:182-199 */
   int32_t device;                /* CUDA device ordinal */
+  /*
+   * LBFEM_PRECISION_MIXED only: the relative CG tolerance of the mass solve is
+   * max(cg_tolerance, mixed_tolerance); 0 selects LBFEM_MIXED_TOLERANCE. The
+   * right-hand side of the mixed path comes from FP32 arithmetic, so it is
+   * resolved to about 1e-7 of its norm on coarse meshes and to about
+   * 1e-7 / (2 pi h) on node spacing h; a tolerance far below that solves
+   * rounding noise. No counterpart in the reference (FP64 only).
+   */
+  double mixed_tolerance;
 } lbfem_params;
+
+/* Default relative CG tolerance of the mixed-precision mass solve. */
+#define LBFEM_MIXED_TOLERANCE 1e-6
 
 typedef struct lbfem_gpu_ctx lbfem_gpu_ctx;
 

@@ -184,4 +184,83 @@ namespace lbfem_gpu
       }
     return ax;
   }
+
+  std::vector<float>
+  window_ldl(const Axis &ax, int T, int W, int n_tiles)
+  {
+    const int p = ax.p, K = 2 * p + 1, n = T + 2 * W;
+    std::vector<float> out(size_t(n_tiles) * n * (p + 1), 0.f);
+    std::vector<long double> a(size_t(n) * K), d(n), l(size_t(n) * (p + 1));
+    auto row = [&](int q) { return &a[size_t(q) * K]; };  // band of row q: [k] couples q to q + k - p
+    auto lo = [&](int q, int k) -> long double & { return l[size_t(q) * (p + 1) + k]; }; // l_{q, q-k}
+    for (int t = 0; t < n_tiles; ++t)
+      {
+        // the window's band
+        for (int q = 0; q < n; ++q)
+          {
+            long double *r = row(q);
+            for (int k = 0; k < K; ++k)
+              r[k] = 0;
+            int c = t * T - W + q;
+            bool valid = true;
+            if (ax.periodic)
+              {
+                c %= ax.n_unique;
+                if (c < 0)
+                  c += ax.n_unique;
+              }
+            else
+              valid = c >= 0 && c < ax.n_nodes;
+            if (!valid)
+              {
+                r[p] = 1; // identity row outside the axis
+                continue;
+              }
+            for (int k = 0; k < K; ++k)
+              {
+                const int q2 = q + k - p;
+                if (q2 < 0 || q2 >= n)
+                  continue;
+                if (!ax.periodic)
+                  {
+                    const int c2 = t * T - W + q2;
+                    if (c2 < 0 || c2 >= ax.n_nodes)
+                      continue;
+                  }
+                r[k] = ax.rows[(size_t(0) * ax.n_nodes + c) * K + k];
+              }
+          }
+        // banded LDL^T (no pivoting: the window matrix is symmetric positive definite)
+        for (int q = 0; q < n; ++q)
+          {
+            for (int k = p; k >= 1; --k) // columns j = q - k in increasing order
+              {
+                const int j = q - k; // l_{q,j} = (a_{q,j} - sum_{m<j} l_{q,m} l_{j,m} d_m) / d_j
+                if (j < 0)
+                  {
+                    lo(q, k) = 0;
+                    continue;
+                  }
+                long double s = row(q)[p - k];
+                for (int m = 1; m <= p - k; ++m)
+                  if (j - m >= 0)
+                    s -= lo(q, k + m) * lo(j, m) * d[j - m];
+                lo(q, k) = s / d[j];
+              }
+            long double s = row(q)[p];
+            for (int k = 1; k <= p; ++k)
+              if (q - k >= 0)
+                s -= lo(q, k) * lo(q, k) * d[q - k];
+            d[q] = s;
+          }
+        float *o = &out[size_t(t) * n * (p + 1)];
+        for (int q = 0; q < n; ++q)
+          {
+            for (int k = 1; k <= p; ++k)
+              o[q * (p + 1) + k - 1] = float(lo(q, k));
+            o[q * (p + 1) + p] = float(1.0L / d[q]);
+          }
+      }
+    return out;
+  }
 } // namespace lbfem_gpu

@@ -300,6 +300,23 @@ namespace lbfem_gpu
       }
   }
 
+  // ------------------------------------------------------ asynchronous copies
+  // A 4-byte global -> shared copy that does not hold a register until it
+  // lands (cp.async, sm_80+); valid = false writes zero and reads nothing.
+  __device__ __forceinline__ void
+  cp_async4(void *smem, const void *gmem, bool valid)
+  {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 4 : 0)
+                 : "memory");
+  }
+
+  __device__ __forceinline__ void
+  cp_async_wait_all()
+  {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+  }
+
   // ------------------------------------------------------------ tile staging
   // Per-CTA tables of the footprint: source column and row offset of every
   // footprint column/row (-1 outside a non-periodic domain), the widths of the

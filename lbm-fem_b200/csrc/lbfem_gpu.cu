@@ -55,6 +55,7 @@ struct lbfem_gpu_ctx
   bool mixed = false;
   float *d_fs[2] = {nullptr, nullptr}, *d_rhs_s = nullptr, *d_x_s[3] = {nullptr, nullptr, nullptr};
   float *d_r_s = nullptr, *d_p_s[2] = {nullptr, nullptr};
+  float *d_winx = nullptr, *d_winy = nullptr; // window LDL^T factors of Mx, My (mixed consistent mass)
   double *d_partials = nullptr, *d_sums = nullptr;
   size_t partial_cap = 0;
   CgState *d_cg = nullptr;
@@ -188,9 +189,8 @@ namespace
         (st = set_smem(ctx, k_cg_start<P, double, double, double>, cg_smem<P, double>(1))) ||
         (st = set_smem(ctx, k_cg_p<P, double>, cg_smem<P, double>(0))) ||
         (st = set_smem(ctx, k_cg_update<P, double>, cg_smem<P, double>(2))) ||
-        (st = set_smem(ctx, k_cg_start<P, float, double, double>, cg_smem<P, float>(1, true))) ||
-        (st = set_smem(ctx, k_cg_p<P, float>, cg_smem<P, float>(0))) ||
-        (st = set_smem(ctx, k_cg_update<P, float>, cg_smem<P, float>(2))))
+        (st = set_smem(ctx, k_cg_start<P, float, float, double>, cg_smem<P, float>(1, true))) ||
+        (st = set_smem(ctx, k_window_correct<P>, window_smem<P>())))
       return st;
     return LBFEM_OK;
   }
@@ -302,7 +302,6 @@ namespace
     R *r, *p[2];
     double *partials, *sums;
     CgState *state;
-    R *d; // mixed precision: the FP32 correction of a refinement round (starts at 0)
   };
 
   int
@@ -313,118 +312,88 @@ namespace
     return LBFEM_OK;
   }
 
-  // Mixed precision: each refinement round solves the FP32 correction to
-  // inner_rel times the round's true FP64 residual. The right-hand side comes
-  // from the FP32 streaming kernel and is resolved to about 1e-7 of its norm, so
-  // the outer tolerance is at least MIXED_TOL_FLOOR.
-  constexpr double MIXED_INNER_REL = 1e-4;
-  constexpr double MIXED_TOL_FLOOR = 1e-7;
-  constexpr int MIXED_MAX_ROUNDS = 50;
-
-  // x_new <- A^{-1} b for nsys systems (extrapolated start or the given x_new),
-  // with the work buffers w. R = X = double: one CG run. R = float, X = double:
-  // iterative refinement -- each round computes the true residual b - A x in
-  // FP64, solves A d = r for the correction d by FP32 CG (FP64 dot products), and
-  // adds x += d in FP64, until the FP64 residual meets the tolerance.
-  // *its_out: CG iterations summed over the systems.
-  template <typename R, typename X = R>
-  int
-  cg_run(lbfem_gpu_ctx *ctx, const CgScratch<R> &w, const R *b, X *x_new, const X *x_cur, const X *x_prev,
-         int extrapolate, int nsys, int64_t *its_out)
+  // The relative tolerance of the mixed-precision mass solve.
+  double
+  mixed_tolerance(const lbfem_params &p)
   {
-    constexpr bool MIX = sizeof(R) == sizeof(float);
+    return std::max(p.cg_tolerance, p.mixed_tolerance > 0 ? p.mixed_tolerance : LBFEM_MIXED_TOLERANCE);
+  }
+
+  // x_new <- A^{-1} b for nsys systems by Jacobi-PCG in the order of updates of
+  // deal.II SolverCG (mass.h:204-211), from the extrapolated start 2 x_cur -
+  // x_prev or from the given x_new, with the work buffers w. *its_out: CG
+  // iterations summed over the systems.
+  int
+  cg_run(lbfem_gpu_ctx *ctx, const CgScratch<double> &w, const double *b, double *x_new, const double *x_cur,
+         const double *x_prev, int extrapolate, int nsys, int64_t *its_out)
+  {
     const Geo geo = geo_of(ctx);
     const Grid &g = ctx->grid;
-    const double tol = MIX ? std::max(ctx->prm.cg_tolerance, MIXED_TOL_FLOOR) : ctx->prm.cg_tolerance;
-    const double inner_rel = MIX ? MIXED_INNER_REL : 0.0;
+    const double tol = ctx->prm.cg_tolerance;
     const int max_its = ctx->prm.cg_max_iterations;
     CK(cudaMemsetAsync(w.state, 0, sizeof(CgState), ctx->stream));
     int n_tiles = 0;
-    int st;
-    bool refined = !MIX; // mixed: a round's FP64 residual met the outer tolerance
-    for (int round = 0; round < (MIX ? MIXED_MAX_ROUNDS : 1); ++round)
+    int st = with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      dim3 grid = tile_grid<P>(g);
+      n_tiles = int(grid.x * grid.y);
+      grid.z = nsys;
+      k_cg_start<P, double, double, double><<<grid, THREADS, cg_smem<P, double>(1, true), ctx->stream>>>(
+        geo, b, x_cur, x_prev, x_new, w.r, extrapolate, w.partials);
+      LAUNCHED();
+      return LBFEM_OK;
+    });
+    if (st)
+      return st;
+    if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, 3 * NM)))
+      return st;
+    k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 0, tol, max_its);
+    LAUNCHED();
+    int pi = 0;
+    for (int it = 0;; ++it)
       {
+        CK(cudaMemcpyAsync(ctx->h_cg, w.state, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (ctx->trace)
+          {
+            double worst = 0;
+            for (int q = 0; q < nsys; ++q)
+              worst = std::max(worst, ctx->h_cg->tol[q] > 0 ? ctx->h_cg->res[q] / ctx->h_cg->tol[q] : 0.0);
+            std::fprintf(stderr, "lbfem cg: it %d active %d max res/tol %.3e\n", it, ctx->h_cg->n_active, worst);
+          }
+        if (ctx->h_cg->n_active == 0)
+          break;
         st = with_degree(ctx->P, [&](auto PP) -> int {
           constexpr int P = decltype(PP)::value;
           dim3 grid = tile_grid<P>(g);
-          n_tiles = int(grid.x * grid.y);
           grid.z = nsys;
-          k_cg_start<P, R, X, double><<<grid, THREADS, cg_smem<P, R>(1, true), ctx->stream>>>(
-            geo, b, x_cur, x_prev, x_new, w.r, extrapolate && round == 0, w.partials);
+          k_cg_p<P, double><<<grid, THREADS, cg_smem<P, double>(0), ctx->stream>>>(geo, w.r, w.p[pi], w.p[1 - pi],
+                                                                                    w.state, w.partials);
           LAUNCHED();
           return LBFEM_OK;
         });
         if (st)
           return st;
-        if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, 3 * NM)))
+        if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, NM)))
           return st;
-        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 0, tol, max_its, inner_rel);
+        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 1, tol, max_its);
         LAUNCHED();
-        int pi = 0;
-        bool outer_done = false; // the round's true residual already meets the tolerance
-        for (int it = 0;; ++it)
-          {
-            CK(cudaMemcpyAsync(ctx->h_cg, w.state, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
-            if (ctx->trace)
-              {
-                double worst = 0;
-                for (int q = 0; q < nsys; ++q)
-                  worst = std::max(worst, ctx->h_cg->tol[q] > 0 ? ctx->h_cg->res[q] / ctx->h_cg->tol[q] : 0.0);
-                std::fprintf(stderr, "lbfem cg: round %d it %d active %d max res/tol %.3e\n", round, it,
-                             ctx->h_cg->n_active, worst);
-              }
-            if (ctx->h_cg->n_active == 0)
-              {
-                outer_done = it == 0;
-                break;
-              }
-            st = with_degree(ctx->P, [&](auto PP) -> int {
-              constexpr int P = decltype(PP)::value;
-              dim3 grid = tile_grid<P>(g);
-              grid.z = nsys;
-              k_cg_p<P, R><<<grid, THREADS, cg_smem<P, R>(0), ctx->stream>>>(geo, w.r, w.p[pi], w.p[1 - pi], w.state,
-                                                                              w.partials);
-              LAUNCHED();
-              return LBFEM_OK;
-            });
-            if (st)
-              return st;
-            if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, NM)))
-              return st;
-            k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 1, tol, max_its, inner_rel);
-            LAUNCHED();
-            pi = 1 - pi;
-            st = with_degree(ctx->P, [&](auto PP) -> int {
-              constexpr int P = decltype(PP)::value;
-              dim3 grid = tile_grid<P>(g);
-              grid.z = nsys;
-              R *xi;
-              if constexpr (MIX)
-                xi = w.d;
-              else
-                xi = x_new;
-              k_cg_update<P, R><<<grid, THREADS, cg_smem<P, R>(2), ctx->stream>>>(geo, xi, w.r, w.p[pi], w.state,
-                                                                                   w.partials);
-              LAUNCHED();
-              return LBFEM_OK;
-            });
-            if (st)
-              return st;
-            if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, 2 * NM)))
-              return st;
-            k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 2, tol, max_its, inner_rel);
-            LAUNCHED();
-          }
-        refined = refined || outer_done;
-        if (!MIX || ctx->h_cg->status != 0 || outer_done)
-          break;
-        if constexpr (MIX)
-          {
-            const long long n = (long long)nsys * g.N;
-            k_refine_add<<<n_pointwise_blocks(n), THREADS, 0, ctx->stream>>>(x_new, w.d, n);
-            LAUNCHED();
-          }
+        pi = 1 - pi;
+        st = with_degree(ctx->P, [&](auto PP) -> int {
+          constexpr int P = decltype(PP)::value;
+          dim3 grid = tile_grid<P>(g);
+          grid.z = nsys;
+          k_cg_update<P, double><<<grid, THREADS, cg_smem<P, double>(2), ctx->stream>>>(geo, x_new, w.r, w.p[pi],
+                                                                                         w.state, w.partials);
+          LAUNCHED();
+          return LBFEM_OK;
+        });
+        if (st)
+          return st;
+        if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, 2 * NM)))
+          return st;
+        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 2, tol, max_its);
+        LAUNCHED();
       }
     if (its_out)
       *its_out = ctx->h_cg->total_its;
@@ -432,8 +401,6 @@ namespace
       return fail(ctx, LBFEM_ERR_NO_CONVERGENCE, "CG: iteration cap %d reached", max_its);
     if (ctx->h_cg->status == 3)
       return fail(ctx, LBFEM_ERR_NONFINITE, "CG: non-finite residual");
-    if (!refined)
-      return fail(ctx, LBFEM_ERR_NO_CONVERGENCE, "CG: no convergence within %d refinement rounds", MIXED_MAX_ROUNDS);
     return LBFEM_OK;
   }
 
@@ -442,27 +409,88 @@ namespace
   cg_solve(lbfem_gpu_ctx *ctx, const double *b, double *x_new, const double *x_cur, const double *x_prev,
            int extrapolate, int nsys, int64_t *its_out)
   {
-    const CgScratch<double> w{ctx->d_r, {ctx->d_p[0], ctx->d_p[1]}, ctx->d_partials, ctx->d_sums, ctx->d_cg, nullptr};
+    const CgScratch<double> w{ctx->d_r, {ctx->d_p[0], ctx->d_p[1]}, ctx->d_partials, ctx->d_sums, ctx->d_cg};
     int64_t its = 0;
-    const int st = cg_run<double, double>(ctx, w, b, x_new, x_cur, x_prev, extrapolate, nsys, &its);
+    const int st = cg_run(ctx, w, b, x_new, x_cur, x_prev, extrapolate, nsys, &its);
     if (its_out)
       *its_out = its;
     ctx->cg_its += its;
     return st;
   }
 
+  // The mixed-precision mass solve of the 8 moving populations: FP64 iterative
+  // refinement around the tensor-product window solve. Each round computes the
+  // true residual r = b - A x in FP64 arithmetic (from the FP32-stored x and b),
+  // stops the systems whose residual meets the tolerance, and adds the FP32
+  // correction M^{-1} r (window solves) to the others. The first round starts
+  // from the extrapolation 2 x_cur - x_prev. A correction reduces the residual
+  // to a few 1e-8 of itself, so one correction is the rule; the tolerance floor
+  // is the FP32 rounding of x (about 1e-7 relative). *its_out: corrections,
+  // summed over the systems.
   int
-  cg_solve_mixed(lbfem_gpu_ctx *ctx, const float *b, double *x_new, const double *x_cur, const double *x_prev,
-                 int extrapolate, int nsys, int64_t *its_out)
+  mixed_solve(lbfem_gpu_ctx *ctx, const float *b, float *x_new, const float *x_cur, const float *x_prev,
+              int nsys, int64_t *its_out)
   {
-    const CgScratch<float> w{ctx->d_r_s, {ctx->d_p_s[0], ctx->d_p_s[1]}, ctx->d_partials, ctx->d_sums, ctx->d_cg,
-                             ctx->d_x_s[0]};
-    int64_t its = 0;
-    const int st = cg_run<float, double>(ctx, w, b, x_new, x_cur, x_prev, extrapolate, nsys, &its);
+    const Geo geo = geo_of(ctx);
+    const Grid &g = ctx->grid;
+    const double tol = mixed_tolerance(ctx->prm);
+    const int max_rounds = ctx->prm.cg_max_iterations;
+    CK(cudaMemsetAsync(ctx->d_cg, 0, sizeof(CgState), ctx->stream));
+    int64_t corrections = 0;
+    int st;
+    for (int round = 0;; ++round)
+      {
+        int n_tiles = 0;
+        st = with_degree(ctx->P, [&](auto PP) -> int {
+          constexpr int P = decltype(PP)::value;
+          dim3 grid = tile_grid<P>(g);
+          n_tiles = int(grid.x * grid.y);
+          grid.z = nsys;
+          k_cg_start<P, float, float, double><<<grid, THREADS, cg_smem<P, float>(1, true), ctx->stream>>>(
+            geo, b, x_cur, x_prev, x_new, ctx->d_r_s, round == 0, ctx->d_partials);
+          LAUNCHED();
+          return LBFEM_OK;
+        });
+        if (st)
+          return st;
+        if ((st = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, 3 * NM)))
+          return st;
+        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nsys, 0, tol, max_rounds + 1);
+        LAUNCHED();
+        CK(cudaMemcpyAsync(ctx->h_cg, ctx->d_cg, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (ctx->trace)
+          {
+            double worst = 0;
+            for (int q = 0; q < nsys; ++q)
+              worst = std::max(worst, ctx->h_cg->tol[q] > 0 ? ctx->h_cg->res[q] / ctx->h_cg->tol[q] : 0.0);
+            std::fprintf(stderr, "lbfem mixed solve: round %d active %d max res/tol %.3e\n", round,
+                         ctx->h_cg->n_active, worst);
+          }
+        if (ctx->h_cg->status == 3)
+          return fail(ctx, LBFEM_ERR_NONFINITE, "mixed mass solve: non-finite residual");
+        if (ctx->h_cg->n_active == 0)
+          break;
+        if (round >= max_rounds)
+          return fail(ctx, LBFEM_ERR_NO_CONVERGENCE, "mixed mass solve: no convergence within %d corrections",
+                      max_rounds);
+        corrections += ctx->h_cg->n_active;
+        st = with_degree(ctx->P, [&](auto PP) -> int {
+          constexpr int P = decltype(PP)::value;
+          using S = WinShape<P>;
+          const dim3 grid((g.nfx + S::TX - 1) / S::TX, (g.nfy + S::TY - 1) / S::TY, nsys);
+          k_window_correct<P><<<grid, S::THREADS, window_smem<P>(), ctx->stream>>>(geo, ctx->d_winx, ctx->d_winy,
+                                                                                  ctx->d_r_s, x_new, ctx->d_cg);
+          LAUNCHED();
+          return LBFEM_OK;
+        });
+        if (st)
+          return st;
+      }
     if (its_out)
-      *its_out = its;
-    ctx->cg_its += its;
-    return st;
+      *its_out = corrections;
+    ctx->cg_its += corrections;
+    return LBFEM_OK;
   }
 
   int
@@ -530,7 +558,7 @@ namespace
     const int rm = ctx->prm.remove_wall_mass_flux;
     const bool cg = ctx->prm.mass == LBFEM_MASS_CG;
     float *d = ctx->d_fs[ctx->cur];
-    double *xn = ctx->d_x[cg ? ctx->x_new : ctx->x_cur];
+    float *xn = ctx->d_x_s[cg ? ctx->x_new : ctx->x_cur];
     const bool bardow = ctx->prm.scheme == LBFEM_SCHEME_BARDOW;
     float *g = ctx->d_fs[1 - ctx->cur];
     int st;
@@ -551,7 +579,7 @@ namespace
       }
     if (cg)
       {
-        if ((st = cg_solve_mixed(ctx, ctx->d_rhs_s, xn, ctx->d_x[ctx->x_cur], ctx->d_x[ctx->x_prev], 1, NM, its)))
+        if ((st = mixed_solve(ctx, ctx->d_rhs_s, xn, ctx->d_x_s[ctx->x_cur], ctx->d_x_s[ctx->x_prev], NM, its)))
           return st;
         const int old_prev = ctx->x_prev;
         ctx->x_prev = ctx->x_cur;
@@ -560,20 +588,20 @@ namespace
       }
     else
       {
-        k_lumped<float, double><<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_rhs_s, xn, NM);
+        k_lumped<float, float><<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_rhs_s, xn, NM);
         LAUNCHED();
         if (its)
           *its = 0;
       }
     if (bardow)
       {
-        k_add_increment_dev<<<nb, THREADS, 0, ctx->stream>>>(geo, g, ctx->d_x[ctx->x_cur]);
+        k_add_increment<float><<<nb, THREADS, 0, ctx->stream>>>(geo, g, ctx->d_x_s[ctx->x_cur]);
         LAUNCHED();
         ctx->cur = 1 - ctx->cur;
       }
     else
       {
-        k_predictor_corrector_dev<<<nb, THREADS, 0, ctx->stream>>>(geo, d, ctx->d_x[ctx->x_cur], dt / lam);
+        k_predictor_corrector_dev<<<nb, THREADS, 0, ctx->stream>>>(geo, d, ctx->d_x_s[ctx->x_cur], dt / lam);
         LAUNCHED();
       }
     return LBFEM_OK;
@@ -665,6 +693,7 @@ lbfem_gpu_default_params(lbfem_params *p)
   p->cg_tolerance = 1e-8;
   p->remove_wall_mass_flux = -1;
   p->device = 0;
+  p->mixed_tolerance = 0.0;
 }
 
 const char *
@@ -743,7 +772,8 @@ lbfem_gpu_destroy(lbfem_gpu_ctx *ctx)
                   ctx->d_wall_u, ctx->d_dof, ctx->d_bnode, ctx->d_f[0], ctx->d_f[1], ctx->d_rhs, ctx->d_x[0],
                   ctx->d_x[1], ctx->d_x[2], ctx->d_r, ctx->d_p[0], ctx->d_p[1], ctx->d_v, ctx->d_feq, ctx->d_stage,
                   ctx->d_partials, ctx->d_sums, ctx->d_cg, ctx->d_fs[0], ctx->d_fs[1], ctx->d_rhs_s,
-                  ctx->d_x_s[0], ctx->d_x_s[1], ctx->d_x_s[2], ctx->d_r_s, ctx->d_p_s[0], ctx->d_p_s[1]};
+                  ctx->d_x_s[0], ctx->d_x_s[1], ctx->d_x_s[2], ctx->d_r_s, ctx->d_p_s[0], ctx->d_p_s[1],
+                  ctx->d_winx, ctx->d_winy};
   for (void *b : bufs)
     if (b)
       cudaFree(b);
@@ -780,7 +810,7 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
       (prm->precision != LBFEM_PRECISION_FP64 && prm->precision != LBFEM_PRECISION_MIXED) ||
       (prm->mass != LBFEM_MASS_CG && prm->mass != LBFEM_MASS_LUMPED))
     return LBFEM_ERR_UNSUPPORTED;
-  if (!(prm->cg_tolerance >= 0) || prm->cg_max_iterations < 1)
+  if (!(prm->cg_tolerance >= 0) || prm->cg_max_iterations < 1 || !(prm->mixed_tolerance >= 0))
     return LBFEM_ERR_ARG;
   const int P = m->degree;
   const int nfx = P * m->n_cells_x + 1, nfy = P * m->n_cells_y + 1;
@@ -957,6 +987,23 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
           (st = zerosf(&ctx->d_r_s, NM * N)) || (st = zerosf(&ctx->d_p_s[0], NM * N)) ||
           (st = zerosf(&ctx->d_p_s[1], NM * N)))
         return st;
+      if (prm->mass == LBFEM_MASS_CG)
+        {
+          // the window factors of the mixed-precision mass solve
+          st = with_degree(P, [&](auto PP) -> int {
+            using S = WinShape<decltype(PP)::value>;
+            const int ntx = (nfx + S::TX - 1) / S::TX, nty = (nfy + S::TY - 1) / S::TY;
+            const std::vector<float> wx = window_ldl(ctx->ax, S::TX, S::W, ntx);
+            const std::vector<float> wy = window_ldl(ctx->ay, S::TY, S::W, nty);
+            CK(cudaMalloc(&ctx->d_winx, sizeof(float) * wx.size()));
+            CK(cudaMalloc(&ctx->d_winy, sizeof(float) * wy.size()));
+            CK(cudaMemcpy(ctx->d_winx, wx.data(), sizeof(float) * wx.size(), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ctx->d_winy, wy.data(), sizeof(float) * wy.size(), cudaMemcpyHostToDevice));
+            return LBFEM_OK;
+          });
+          if (st)
+            return st;
+        }
     }
   const long long tiles = with_degree(P, [&](auto PP) -> int {
     constexpr int Pd = decltype(PP)::value;
@@ -1436,7 +1483,7 @@ lbfem_gpu_mass_solve_noalloc(lbfem_gpu_ctx *ctx, double *x, const double *r)
   w.partials = base + 3 * NOALLOC_MAX_NODES;
   w.sums = w.partials + 3 * NM * NOALLOC_MAX_TILES;
   w.state = reinterpret_cast<CgState *>(w.sums + 64);
-  const int solve_st = cg_run<double, double>(ctx, w, r, x, nullptr, nullptr, 0, 1, nullptr);
+  const int solve_st = cg_run(ctx, w, r, x, nullptr, nullptr, 0, 1, nullptr);
   if (solve_st != LBFEM_OK)
     return solve_st;
   CK(cudaStreamSynchronize(ctx->stream));

@@ -149,10 +149,10 @@ namespace lbfem_gpu
     return c_W[a] * (drho + m.rho * (3. * eu + 4.5 * eu * eu - 1.5 * uu));
   }
 
-  // predictor_corrector on FP32 deviations d = f - w with the FP64 increment x, in
+  // predictor_corrector on FP32 deviations d = f - w with the FP32 increment x, in
   // FP64 arithmetic (the corrector's theta (feq(fhat) - feq(f)) cancels).
   __global__ void
-  k_predictor_corrector_dev(const Geo geo, float *__restrict__ d, const double *__restrict__ x, double theta)
+  k_predictor_corrector_dev(const Geo geo, float *__restrict__ d, const float *__restrict__ x, double theta)
   {
     const long long N = geo.g.N;
     const double inv = 1. / (1. + theta);
@@ -175,30 +175,6 @@ namespace lbfem_gpu
 #pragma unroll
       for (int a = 0; a < Q; ++a)
         d[a * N + i] = float(fh[a] + theta * (feqd64_a(a, mh, drh) - fe[a]));
-    }
-  }
-
-  // Bardow's stream on FP32 deviations: d_a += x_{a-1} (FP64 increment).
-  __global__ void
-  k_add_increment_dev(const Geo geo, float *__restrict__ d, const double *__restrict__ x)
-  {
-    const long long N = geo.g.N;
-    LBFEM_GRID_STRIDE(i, N)
-    {
-#pragma unroll
-      for (int a = 1; a < Q; ++a)
-        d[a * N + i] = float(double(d[a * N + i]) + x[(a - 1) * N + i]);
-    }
-  }
-
-  // One refinement step: x += d (FP64), d = 0 (the next inner solve starts from 0).
-  __global__ void
-  k_refine_add(double *__restrict__ x, float *__restrict__ d, long long n)
-  {
-    LBFEM_GRID_STRIDE(i, n)
-    {
-      x[i] += double(d[i]);
-      d[i] = 0.f;
     }
   }
 
@@ -1079,7 +1055,7 @@ namespace lbfem_gpu
   // FP64 (iterative refinement) until the outer tolerance holds.
   struct CgState
   {
-    double tol[NM], tol_inner[NM], rz[NM], rz_prev[NM], beta[NM], alpha[NM], res[NM];
+    double tol[NM], rz[NM], rz_prev[NM], beta[NM], alpha[NM], res[NM];
     int it[NM], its_total[NM], active[NM];
     int status, n_active, iter;
     unsigned long long total_its;
@@ -1119,8 +1095,9 @@ namespace lbfem_gpu
     build_maps<P>(maps, geo, gx0, gy0);
     __syncthreads();
     const long long o = s * N;
+    // the start as stored (rounded to X), so that r is the residual of the stored x
     stage<P>(s_u, maps, [&](long long idx) -> A {
-      return extrapolate ? -A(x_prev[o + idx]) + A(2) * A(x_cur[o + idx]) : A(x_new[o + idx]);
+      return extrapolate ? A(X(-A(x_prev[o + idx]) + A(2) * A(x_cur[o + idx]))) : A(x_new[o + idx]);
     });
     stage_own<P>(s_b, b + o, g, gx0, gy0);
     __syncthreads();
@@ -1131,7 +1108,7 @@ namespace lbfem_gpu
       A xg;
       if (image)
         {
-          xg = extrapolate ? -A(x_prev[id]) + A(2) * A(x_cur[id]) : A(x_new[id]);
+          xg = extrapolate ? A(X(-A(x_prev[id]) + A(2) * A(x_cur[id]))) : A(x_new[id]);
           Ax = xg;
         }
       else
@@ -1238,13 +1215,189 @@ namespace lbfem_gpu
     block_reduce_store<2>(part, partials + (long long)s * nt, tile, NM * nt);
   }
 
+  // --------------------------- tensor-product window solve (mixed precision)
+  // On an axis-parallel tensor-product mesh the consistent mass matrix is
+  // M = My (x) Mx, so M^{-1} = My^{-1} (x) Mx^{-1}. The rows of the 1-D inverses
+  // decay exponentially, so M^{-1} r at the own nodes of a tile follows from
+  // banded LDL^T solves on a window of W nodes around the tile in each direction
+  // (factors from window_ldl on the host), to a few 1e-8 of |r|.
+  template <int P>
+  struct WinShape
+  {
+    static constexpr int W = P == 1 ? 12 : P == 2 ? 20 : P == 3 ? 24 : 28;
+    static constexpr int TX = 128, TY = 64;                // own nodes
+    static constexpr int FX = TX + 2 * W, FY = TY + 2 * W; // window
+    static constexpr int PF = FX | 1;                      // odd pitch: conflict-free row and column sweeps
+    static constexpr int NC = P + 1;                       // factor entries per window position
+    static constexpr int THREADS = 128;
+    static_assert(FY <= THREADS && TX == THREADS, "one thread per window row and per own column");
+    static_assert(FX % 4 == 0 && FY % 4 == 0 && (FX - W) % 4 == 0 && (FY - W) % 4 == 0, "whole chunks");
+  };
+
+  template <int P>
+  constexpr size_t
+  window_smem()
+  {
+    using S = WinShape<P>;
+    return sizeof(float) * size_t(S::PF) * S::FY;
+  }
+
+  // Forward and backward substitution of one banded LDL^T system of n
+  // unknowns stored at line[q * stride] (in place), with the factors
+  // c[q * (P+1) + k-1] = l_{q,q-k} and c[q * (P+1) + P] = 1/d_q; the backward
+  // sweep stops at position stop. Chunks of four positions: the loads of a
+  // chunk are issued before its dependent chain.
+  template <int P, int n, int stride, int stop>
+  __device__ __forceinline__ void
+  ldl_solve(float *line, const float *c)
+  {
+    constexpr int NC = P + 1, CH = 4;
+    float y[P];
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+      y[k] = 0.f; // y[k]: the value k + 1 positions back
+#pragma unroll 2
+    for (int q0 = 0; q0 < n; q0 += CH)
+      {
+        float v[CH], l[CH][NC];
+#pragma unroll
+        for (int u = 0; u < CH; ++u)
+          {
+            v[u] = line[(q0 + u) * stride];
+#pragma unroll
+            for (int k = 0; k < NC; ++k)
+              l[u][k] = c[(q0 + u) * NC + k];
+          }
+#pragma unroll
+        for (int u = 0; u < CH; ++u)
+          {
+            float t = v[u];
+#pragma unroll
+            for (int k = P; k >= 1; --k)
+              t = fmaf(-l[u][k - 1], y[k - 1], t);
+#pragma unroll
+            for (int k = P - 1; k >= 1; --k)
+              y[k] = y[k - 1];
+            y[0] = t;
+            v[u] = t * l[u][P];
+          }
+#pragma unroll
+        for (int u = 0; u < CH; ++u)
+          line[(q0 + u) * stride] = v[u];
+      }
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+      y[k] = 0.f; // y[k]: the value k + 1 positions ahead
+#pragma unroll 2
+    for (int q0 = n - CH; q0 >= stop; q0 -= CH)
+      {
+        float v[CH], l[CH + P][P];
+#pragma unroll
+        for (int u = 0; u < CH; ++u)
+          v[u] = line[(q0 + u) * stride];
+#pragma unroll
+        for (int u = 0; u < CH + P; ++u)
+#pragma unroll
+          for (int k = 0; k < P; ++k)
+            l[u][k] = q0 + u < n ? c[(q0 + u) * NC + k] : 0.f;
+#pragma unroll
+        for (int u = CH - 1; u >= 0; --u)
+          {
+            float t = v[u];
+#pragma unroll
+            for (int k = P; k >= 1; --k)
+              t = fmaf(-l[u + k][k - 1], y[k - 1], t);
+#pragma unroll
+            for (int k = P - 1; k >= 1; --k)
+              y[k] = y[k - 1];
+            y[0] = t;
+            v[u] = t;
+          }
+#pragma unroll
+        for (int u = 0; u < CH; ++u)
+          line[(q0 + u) * stride] = v[u];
+      }
+  }
+
+  // x <- x + M^{-1} r for the active systems (FP32: the correction of one
+  // refinement round). lx / ly: window factors of the x / y tile partitions.
+  // Periodic images have identity rows: x += r there.
+  template <int P>
+  __global__ void __launch_bounds__(WinShape<P>::THREADS)
+    k_window_correct(const Geo geo, const float *__restrict__ lx, const float *__restrict__ ly,
+                     const float *__restrict__ r, float *__restrict__ x, const CgState *__restrict__ st)
+  {
+    using S = WinShape<P>;
+    constexpr int W = S::W, FX = S::FX, FY = S::FY, PF = S::PF, NC = S::NC;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    float *s_w = reinterpret_cast<float *>(sm_raw); // [FY][PF] the window
+    __shared__ float s_lx[FX * NC], s_ly[FY * NC];  // factors (apart from the window: no aliasing)
+    __shared__ int s_col[FX], s_row[FY];            // storage column / row, -1 outside the grid
+    const int s = blockIdx.z;
+    if (!st->active[s])
+      return;
+    const Grid &g = geo.g;
+    const long long N = g.N;
+    const int gx0 = blockIdx.x * S::TX, gy0 = blockIdx.y * S::TY;
+    const int tid = threadIdx.x;
+    const float *lxt = lx + (size_t)blockIdx.x * FX * NC, *lyt = ly + (size_t)blockIdx.y * FY * NC;
+    for (int t = tid; t < FX * NC; t += S::THREADS)
+      s_lx[t] = lxt[t];
+    for (int t = tid; t < FY * NC; t += S::THREADS)
+      s_ly[t] = lyt[t];
+    for (int t = tid; t < FX; t += S::THREADS)
+      s_col[t] = wrap(gx0 - W + t, g.px, g.nux, g.nfx);
+    for (int t = tid; t < FY; t += S::THREADS)
+      s_row[t] = wrap(gy0 - W + t, g.py, g.nuy, g.nfy);
+    __syncthreads();
+    const float *rs = r + (long long)s * N;
+    // the window by asynchronous copies (all in flight at once), and this
+    // thread's own column of x into registers meanwhile
+    for (int t = tid; t < FX * FY; t += S::THREADS)
+      {
+        const int q = t / FX, c = t - q * FX;
+        const int row = s_row[q], col = s_col[c];
+        const bool ok = row >= 0 && col >= 0;
+        cp_async4(&s_w[q * PF + c], ok ? rs + ((long long)row * g.nfx + col) : rs, ok);
+      }
+    const int gx = gx0 + tid;
+    float *xs = x + (long long)s * N;
+    float xo[S::TY];
+#pragma unroll
+    for (int i = 0; i < S::TY; ++i)
+      {
+        const int gy = gy0 + i;
+        xo[i] = (gx < g.nfx && gy < g.nfy) ? xs[(long long)gy * g.nfx + gx] : 0.f;
+      }
+    cp_async_wait_all();
+    __syncthreads();
+    // x solves: one thread per window row (the y solves read the own columns only)
+    if (tid < FY)
+      ldl_solve<P, FX, 1, W>(s_w + tid * PF, s_lx);
+    __syncthreads();
+    // y solves: one thread per own column, then the own nodes of that column
+    ldl_solve<P, FY, PF, W>(s_w + W + tid, s_ly);
+    if (gx < g.nfx)
+      {
+#pragma unroll
+        for (int i = 0; i < S::TY; ++i)
+          {
+            const int gy = gy0 + i;
+            if (gy < g.nfy)
+              {
+                const long long idx = (long long)gy * g.nfx + gx;
+                const float z = is_image(gx, gy, g) ? rs[idx] : s_w[(W + i) * PF + W + tid];
+                xs[idx] = xo[i] + z;
+              }
+          }
+      }
+  }
+
   // The scalar work of one CG phase, one thread per system, from the reduced sums.
   // phase 0 (after start): sums = [bb, rr, rz]; phase 1 (after p): [pAp];
   // phase 2 (after update): [rr, rz].
-  // inner_rel > 0 (refinement): an inner pass stops at max(tol, inner_rel |r_true|).
   __global__ void
-  k_cg_scalars(CgState *st, const double *__restrict__ sums, int nsys, int phase, double cg_tol, int max_its,
-               double inner_rel)
+  k_cg_scalars(CgState *st, const double *__restrict__ sums, int nsys, int phase, double cg_tol, int max_its)
   {
     const int s = threadIdx.x;
     if (s < NM)
@@ -1256,7 +1409,6 @@ namespace lbfem_gpu
                 st->tol[s] = cg_tol * sqrt(sums[s]);
                 const double res = sqrt(sums[NM + s]);
                 st->res[s] = res;
-                st->tol_inner[s] = fmax(st->tol[s], inner_rel * res);
                 st->rz[s] = sums[2 * NM + s];
                 st->it[s] = 0;
                 st->beta[s] = 0;
@@ -1288,7 +1440,7 @@ namespace lbfem_gpu
                 st->active[s] = 0;
                 atomicExch(&st->status, 3);
               }
-            else if (res <= st->tol_inner[s])
+            else if (res <= st->tol[s])
               st->active[s] = 0;
             else if (it >= max_its)
               {

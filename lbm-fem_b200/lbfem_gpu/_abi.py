@@ -53,14 +53,14 @@ class Params(C.Structure):
     _fields_ = [
         ("scheme", C.c_int32), ("mass", C.c_int32), ("richardson", C.c_int32), ("streaming", C.c_int32),
         ("precision", C.c_int32), ("cg_max_iterations", C.c_int32), ("cg_tolerance", C.c_double),
-        ("remove_wall_mass_flux", C.c_int32), ("device", C.c_int32),
+        ("remove_wall_mass_flux", C.c_int32), ("device", C.c_int32), ("mixed_tolerance", C.c_double),
     ]
 
 
 def make_params(scheme="bardow", mass="cg", cg_tolerance=1e-8, cg_max_iterations=200, precision="fp64",
-                richardson=2, remove_wall_mass_flux=-1, device=0):
+                richardson=2, remove_wall_mass_flux=-1, device=0, mixed_tolerance=0.0):
     return Params(SCHEME[scheme], MASS[mass], richardson, 0, PRECISION[precision], cg_max_iterations,
-                  cg_tolerance, remove_wall_mass_flux, device)
+                  cg_tolerance, remove_wall_mass_flux, device, mixed_tolerance)
 
 
 def _dptr(a):
