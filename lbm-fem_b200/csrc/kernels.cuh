@@ -317,6 +317,20 @@ namespace lbfem_gpu
     asm volatile("cp.async.wait_all;\n" ::: "memory");
   }
 
+  __device__ __forceinline__ void
+  cp_async_commit()
+  {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
+
+  // Waits until at most N committed groups of this thread are still in flight.
+  template <int N>
+  __device__ __forceinline__ void
+  cp_async_wait_group()
+  {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+  }
+
   // ------------------------------------------------------------ tile staging
   // Per-CTA tables of the footprint: source column and row offset of every
   // footprint column/row (-1 outside a non-periodic domain), the widths of the
@@ -381,7 +395,7 @@ namespace lbfem_gpu
     for (int k = 0; k < IT; ++k)
       {
         const int t = threadIdx.x + k * THREADS;
-        v[k] = R(0);
+        v[k] = R{};
         if (t < NT)
           {
             const int fy = t / T::FX, fx = t - fy * T::FX;
@@ -415,7 +429,7 @@ namespace lbfem_gpu
     for (int k = 0; k < IT; ++k)
       {
         const int t = threadIdx.x + k * THREADS;
-        v[k] = R(0);
+        v[k] = R{};
         if (t < NT)
           {
             const int fy = t / T::FX, fx = t - fy * T::FX;

@@ -5,6 +5,7 @@
 
 #include "geometry.h"
 #include "operators.cuh"
+#include "stream_pair.cuh"
 
 #include <cuda_runtime.h>
 
@@ -183,8 +184,8 @@ namespace
         (st = set_smem(ctx, k_advection<P, ADV_TG_COLLIDE, double>, advection_smem<P, ADV_TG_COLLIDE, double>())) ||
         (st = set_smem(ctx, k_advection<P, ADV_LEELIN_FEQ, double>, advection_smem<P, ADV_LEELIN_FEQ, double>())) ||
         (st = set_smem(ctx, k_advection<P, ADV_LEELIN_FUSED, double>, advection_smem<P, ADV_LEELIN_FUSED, double>())) ||
-        (st = set_smem(ctx, k_advection<P, ADV_TG_COLLIDE, float>, advection_smem<P, ADV_TG_COLLIDE, float>())) ||
-        (st = set_smem(ctx, k_advection<P, ADV_LEELIN_FUSED, float>, advection_smem<P, ADV_LEELIN_FUSED, float>())) ||
+        (st = set_smem(ctx, k_stream_pair<P, PAIR_LEELIN>, pair_smem<P, PAIR_LEELIN>())) ||
+        (st = set_smem(ctx, k_stream_pair<P, PAIR_BARDOW>, pair_smem<P, PAIR_BARDOW>())) ||
         (st = set_smem(ctx, k_mass_vmult<P>, cg_smem<P, double>(0))) ||
         (st = set_smem(ctx, k_cg_start<P, double, double, double>, cg_smem<P, double>(1))) ||
         (st = set_smem(ctx, k_cg_p<P, double>, cg_smem<P, double>(0))) ||
@@ -255,6 +256,25 @@ namespace
             k_advection<P, ADV_LEELIN_FUSED, R>
               <<<grid, THREADS, advection_smem<P, ADV_LEELIN_FUSED, R>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
         }
+      LAUNCHED();
+      return LBFEM_OK;
+    });
+  }
+
+  // The FP32 streaming kernel of the mixed-precision step (pairs of opposite populations).
+  int
+  launch_pair(lbfem_gpu_ctx *ctx, int mode, const float *d, float *dout, float *rhs, const AdvCoef &ac)
+  {
+    const Geo geo = geo_of(ctx);
+    return with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      const dim3 grid = tile_grid<P>(ctx->grid);
+      if (mode == PAIR_BARDOW)
+        k_stream_pair<P, PAIR_BARDOW><<<grid, THREADS, pair_smem<P, PAIR_BARDOW>(), ctx->stream>>>(geo, d, dout, rhs,
+                                                                                                 ac);
+      else
+        k_stream_pair<P, PAIR_LEELIN><<<grid, THREADS, pair_smem<P, PAIR_LEELIN>(), ctx->stream>>>(geo, d, dout, rhs,
+                                                                                                 ac);
       LAUNCHED();
       return LBFEM_OK;
     });
@@ -356,10 +376,10 @@ namespace
         CK(cudaStreamSynchronize(ctx->stream));
         if (ctx->trace)
           {
-            double worst = 0;
+            std::fprintf(stderr, "lbfem cg: it %d active %d res/tol", it, ctx->h_cg->n_active);
             for (int q = 0; q < nsys; ++q)
-              worst = std::max(worst, ctx->h_cg->tol[q] > 0 ? ctx->h_cg->res[q] / ctx->h_cg->tol[q] : 0.0);
-            std::fprintf(stderr, "lbfem cg: it %d active %d max res/tol %.3e\n", it, ctx->h_cg->n_active, worst);
+              std::fprintf(stderr, " %.2e", ctx->h_cg->tol[q] > 0 ? ctx->h_cg->res[q] / ctx->h_cg->tol[q] : 0.0);
+            std::fprintf(stderr, "\n");
           }
         if (ctx->h_cg->n_active == 0)
           break;
@@ -420,13 +440,17 @@ namespace
 
   // The mixed-precision mass solve of the 8 moving populations: FP64 iterative
   // refinement around the tensor-product window solve. Each round computes the
-  // true residual r = b - A x in FP64 arithmetic (from the FP32-stored x and b),
-  // stops the systems whose residual meets the tolerance, and adds the FP32
-  // correction M^{-1} r (window solves) to the others. The first round starts
-  // from the extrapolation 2 x_cur - x_prev. A correction reduces the residual
-  // to a few 1e-8 of itself, so one correction is the rule; the tolerance floor
-  // is the FP32 rounding of x (about 1e-7 relative). *its_out: corrections,
-  // summed over the systems.
+  // true residual r = b - A x in FP64 arithmetic (from the FP32-stored x and b)
+  // and adds the FP32 correction M^{-1} r (window solves) to every system whose
+  // residual misses the tolerance. The first round starts from the
+  // extrapolation 2 x_cur - x_prev and corrects every system: accepting the
+  // extrapolation itself whenever it meets the tolerance would march on
+  // extrapolated increments, whose errors accumulate from step to step (on a
+  // coarse mesh the FP32 right-hand side is resolved to about the tolerance, so
+  // that happens often). A correction reduces the residual to a few 1e-8 of
+  // itself, so one correction is the rule; the tolerance floor is the FP32
+  // rounding of x (about 1e-7 relative). *its_out: corrections, summed over the
+  // systems.
   int
   mixed_solve(lbfem_gpu_ctx *ctx, const float *b, float *x_new, const float *x_cur, const float *x_prev,
               int nsys, int64_t *its_out)
@@ -437,6 +461,7 @@ namespace
     const int max_rounds = ctx->prm.cg_max_iterations;
     CK(cudaMemsetAsync(ctx->d_cg, 0, sizeof(CgState), ctx->stream));
     int64_t corrections = 0;
+    double prev_res[NM];
     int st;
     for (int round = 0;; ++round)
       {
@@ -461,26 +486,41 @@ namespace
         CK(cudaStreamSynchronize(ctx->stream));
         if (ctx->trace)
           {
-            double worst = 0;
+            std::fprintf(stderr, "lbfem mixed solve: round %d active %d res/tol", round, ctx->h_cg->n_active);
             for (int q = 0; q < nsys; ++q)
-              worst = std::max(worst, ctx->h_cg->tol[q] > 0 ? ctx->h_cg->res[q] / ctx->h_cg->tol[q] : 0.0);
-            std::fprintf(stderr, "lbfem mixed solve: round %d active %d max res/tol %.3e\n", round,
-                         ctx->h_cg->n_active, worst);
+              std::fprintf(stderr, " %.2e", ctx->h_cg->tol[q] > 0 ? ctx->h_cg->res[q] / ctx->h_cg->tol[q] : 0.0);
+            std::fprintf(stderr, "\n");
           }
         if (ctx->h_cg->status == 3)
           return fail(ctx, LBFEM_ERR_NONFINITE, "mixed mass solve: non-finite residual");
-        if (ctx->h_cg->n_active == 0)
+        if (ctx->h_cg->n_active == 0 && round > 0)
           break;
         if (round >= max_rounds)
           return fail(ctx, LBFEM_ERR_NO_CONVERGENCE, "mixed mass solve: no convergence within %d corrections",
                       max_rounds);
-        corrections += ctx->h_cg->n_active;
+        if (round > 0)
+          {
+            // a correction reduces the residual by orders of magnitude; one that does not
+            // halve it has reached the FP32 resolution of x, which lies above the tolerance
+            bool progress = false;
+            for (int q = 0; q < nsys; ++q)
+              progress = progress || (ctx->h_cg->active[q] && ctx->h_cg->res[q] <= 0.5 * prev_res[q]);
+            if (!progress)
+              return fail(ctx, LBFEM_ERR_NO_CONVERGENCE,
+                          "mixed mass solve: the residual stagnates at %.3e of the tolerance (the tolerance %.1e is "
+                          "below the FP32 resolution of the solution)",
+                          ctx->h_cg->res[0] / std::max(ctx->h_cg->tol[0], 1e-300), tol);
+          }
+        for (int q = 0; q < nsys; ++q)
+          prev_res[q] = ctx->h_cg->res[q];
+        corrections += round == 0 ? nsys : ctx->h_cg->n_active;
         st = with_degree(ctx->P, [&](auto PP) -> int {
           constexpr int P = decltype(PP)::value;
           using S = WinShape<P>;
           const dim3 grid((g.nfx + S::TX - 1) / S::TX, (g.nfy + S::TY - 1) / S::TY, nsys);
           k_window_correct<P><<<grid, S::THREADS, window_smem<P>(), ctx->stream>>>(geo, ctx->d_winx, ctx->d_winy,
-                                                                                  ctx->d_r_s, x_new, ctx->d_cg);
+                                                                                  ctx->d_r_s, x_new, ctx->d_cg,
+                                                                                  round == 0);
           LAUNCHED();
           return LBFEM_OK;
         });
@@ -565,7 +605,7 @@ namespace
     if (bardow)
       {
         const AdvCoef ac = adv_coef(-dt, 0., -0.5 * dt * dt, e, dt / (lam + 0.5 * dt));
-        if ((st = launch_advection<float>(ctx, ADV_TG_COLLIDE, d, nullptr, g, ctx->d_rhs_s, ac)) ||
+        if ((st = launch_pair(ctx, PAIR_BARDOW, d, g, ctx->d_rhs_s, ac)) ||
             (st = launch_wall_faces<float>(ctx, g, ctx->d_rhs_s, e, dt, rm < 0 ? true : rm != 0)))
           return st;
       }
@@ -573,7 +613,7 @@ namespace
       {
         const double b = -0.5 * dt * dt / lam;
         const AdvCoef ac = adv_coef(-dt - b, b, -0.5 * dt * dt, e, 0.);
-        if ((st = launch_advection<float>(ctx, ADV_LEELIN_FUSED, d, nullptr, nullptr, ctx->d_rhs_s, ac)) ||
+        if ((st = launch_pair(ctx, PAIR_LEELIN, d, nullptr, ctx->d_rhs_s, ac)) ||
             (st = launch_wall_faces<float>(ctx, d, ctx->d_rhs_s, e, dt, rm < 0 ? false : rm != 0)))
           return st;
       }
@@ -884,6 +924,13 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
           for (int c = 0; c <= MAXPD; ++c)
             reff[q][o][a][c] = float(ref[q][o][a][c]);
     CK(cudaMemcpyToSymbol(c_reff, reff, sizeof reff));
+    static float2 ref2[MAXPD][3][MAXPD + 1][MAXPD + 1];
+    for (int q = 0; q < MAXPD; ++q)
+      for (int o = 0; o < 3; ++o)
+        for (int a = 0; a <= MAXPD; ++a)
+          for (int c = 0; c <= MAXPD; ++c)
+            ref2[q][o][a][c] = make_float2(reff[q][o][a][c], reff[q][o][a][c]);
+    CK(cudaMemcpyToSymbol(c_ref2, ref2, sizeof ref2));
   }
 
   // numbering: structured node -> caller DoF, and its inverse for the wall list
@@ -1204,8 +1251,8 @@ lbfem_gpu_advection_resident(lbfem_gpu_ctx *ctx)
                             : adv_coef(-dt - b, b, -0.5 * dt * dt, d2q9_e(), 0.);
   const int mode = bardow ? ADV_TG_COLLIDE : ADV_LEELIN_FUSED;
   if (ctx->mixed)
-    return launch_advection<float>(ctx, mode, ctx->d_fs[ctx->cur], nullptr, bardow ? ctx->d_fs[1 - ctx->cur] : nullptr,
-                                   ctx->d_rhs_s, ac);
+    return launch_pair(ctx, bardow ? PAIR_BARDOW : PAIR_LEELIN, ctx->d_fs[ctx->cur],
+                       bardow ? ctx->d_fs[1 - ctx->cur] : nullptr, ctx->d_rhs_s, ac);
   return launch_advection<double>(ctx, mode, ctx->d_f[ctx->cur], nullptr, bardow ? ctx->d_f[1 - ctx->cur] : nullptr,
                                   ctx->d_rhs, ac);
 }

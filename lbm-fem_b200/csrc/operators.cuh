@@ -1319,13 +1319,13 @@ namespace lbfem_gpu
       }
   }
 
-  // x <- x + M^{-1} r for the active systems (FP32: the correction of one
-  // refinement round). lx / ly: window factors of the x / y tile partitions.
-  // Periodic images have identity rows: x += r there.
+  // x <- x + M^{-1} r for the active systems, or for all systems when all is
+  // set (FP32: the correction of one refinement round). lx / ly: window factors
+  // of the x / y tile partitions. Periodic images have identity rows: x += r there.
   template <int P>
   __global__ void __launch_bounds__(WinShape<P>::THREADS)
     k_window_correct(const Geo geo, const float *__restrict__ lx, const float *__restrict__ ly,
-                     const float *__restrict__ r, float *__restrict__ x, const CgState *__restrict__ st)
+                     const float *__restrict__ r, float *__restrict__ x, const CgState *__restrict__ st, int all)
   {
     using S = WinShape<P>;
     constexpr int W = S::W, FX = S::FX, FY = S::FY, PF = S::PF, NC = S::NC;
@@ -1334,7 +1334,7 @@ namespace lbfem_gpu
     __shared__ float s_lx[FX * NC], s_ly[FY * NC];  // factors (apart from the window: no aliasing)
     __shared__ int s_col[FX], s_row[FY];            // storage column / row, -1 outside the grid
     const int s = blockIdx.z;
-    if (!st->active[s])
+    if (!all && !st->active[s])
       return;
     const Grid &g = geo.g;
     const long long N = g.N;

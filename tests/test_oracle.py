@@ -196,3 +196,40 @@ def test_bardow_cavity_conserves_mass(oracle_mod):
     c1 = o.conservation()
     assert abs(c1[1] / c1[0] - c0[1] / c0[0]) < 1e-13
     assert c1[4] > 0  # the lid has set the fluid in motion
+
+
+def _checkerboard_amplitude(mesh, f):
+    """Amplitude of the (pi, pi) mode of population 1 on the distinct nodes."""
+    n = mesh.degree * mesh.n_cells_x
+    e = f[1, mesh.independent()].reshape(n, n)
+    sign = (-1.0) ** np.add.outer(np.arange(n), np.arange(n))
+    return abs(np.mean(e * sign))
+
+
+@pytest.mark.parametrize("cfl,grows", [(0.5, True), (0.45, False)])
+def test_leelin_q1_checkerboard_stability_limit(oracle_mod, cfl, grows):
+    """Lee-Lin with the consistent mass on Q1 (TGV 64^2, Re 100) is linearly
+    unstable at CFL 0.5 for the checkerboard mode and stable at 0.45. From
+    symmetric initial data the mode stays at round-off in FP64, so an unseeded
+    run survives; a 1e-7 seed (the size of FP32 rounding) grows by about 1.08
+    per step. The reference's own algorithm (CG to 1e-8, schemes.h:92-98) is
+    the oracle here."""
+    tc = cases.TaylorGreenVortex(0.05 / math.sqrt(d2q9.CS2), 1, 1, shift=(0.25, 0.25), chapman_enskog=False)
+    tc.set_reynolds(100)
+    m = cases.build_mesh(tc, 64, 1)
+    dt, lam = m.time_step(cfl), tc.relaxation_time()
+    x, y = m.nodes()
+    nfx = m.n_cells_x + 1
+    k = np.arange(m.n_dofs)
+    f0 = tc.initial_populations(x, y, lam) + 1e-7 * ((-1.0) ** (k % nfx + k // nfx))[None, :]
+    o = oracle_mod.Oracle(m, make_params("leelin", "cg", cg_tolerance=1e-8))
+    o.set_time_step(dt, lam)
+    o.set_initial_populations(f0)
+    o.step(100)
+    a100 = _checkerboard_amplitude(m, o.get_populations())
+    o.step(100)
+    a200 = _checkerboard_amplitude(m, o.get_populations())
+    if grows:
+        assert a200 > 100 * a100 > 0, (a100, a200)
+    else:
+        assert a200 < a100 < 1e-9, (a100, a200)  # decays from the 1e-7 seed
