@@ -186,10 +186,10 @@ namespace lbfem_gpu
   }
 
   std::vector<float>
-  window_ldl(const Axis &ax, int T, int W, int n_tiles)
+  window_ldl(const Axis &ax, int T, int W, int n_tiles, int stride)
   {
     const int p = ax.p, K = 2 * p + 1, n = T + 2 * W;
-    std::vector<float> out(size_t(n_tiles) * n * (p + 1), 0.f);
+    std::vector<float> out(size_t(n_tiles) * n * stride, 0.f);
     std::vector<long double> a(size_t(n) * K), d(n), l(size_t(n) * (p + 1));
     auto row = [&](int q) { return &a[size_t(q) * K]; };  // band of row q: [k] couples q to q + k - p
     auto lo = [&](int q, int k) -> long double & { return l[size_t(q) * (p + 1) + k]; }; // l_{q, q-k}
@@ -253,12 +253,12 @@ namespace lbfem_gpu
                 s -= lo(q, k) * lo(q, k) * d[q - k];
             d[q] = s;
           }
-        float *o = &out[size_t(t) * n * (p + 1)];
+        float *o = &out[size_t(t) * n * stride];
         for (int q = 0; q < n; ++q)
           {
             for (int k = 1; k <= p; ++k)
-              o[q * (p + 1) + k - 1] = float(lo(q, k));
-            o[q * (p + 1) + p] = float(1.0L / d[q]);
+              o[q * stride + k - 1] = float(lo(q, k));
+            o[q * stride + p] = float(1.0L / d[q]);
           }
       }
     return out;

@@ -237,6 +237,31 @@ namespace lbfem_gpu
     return geo.wall ? impose_class(m, geo.wall[idx], geo) : m;
   }
 
+  // Counters that outlive one solve: the first failure of any solve (sticky:
+  // a CgState status, 4 = stagnation), CG iterations / mixed corrections summed
+  // over systems and solves, loop-body runs of graph-launched solves, and the
+  // steps completed.
+  struct DevStats
+  {
+    int sticky;
+    int pad;
+    unsigned long long its, bodies, steps_done;
+  };
+
+  // The nodal update that completes a step: skipped after a failure (the
+  // populations stay those before the failing step); block 0 counts the step.
+  __device__ __forceinline__ bool
+  step_skipped(DevStats *ds)
+  {
+    if (!ds)
+      return false;
+    if (ds->sticky)
+      return true;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+      atomicAdd(&ds->steps_done, 1ULL);
+    return false;
+  }
+
   // ---------------------------------------------------- fixed-order reductions
   // Sums v[0..NQ) over the CTA (warp shuffles, then warp 0) and stores the CTA
   // totals at partials[q * n_blocks + block].
@@ -263,6 +288,41 @@ namespace lbfem_gpu
         for (int q = 0; q < NQ; ++q)
           {
             double s = lane < THREADS / 32 ? warp_sum[q][lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+              s += __shfl_down_sync(0xffffffffu, s, o);
+            if (lane == 0)
+              partials[(long long)q * n_blocks + block] = s;
+          }
+      }
+    __syncthreads();
+  }
+
+  // The same for a CTA of NT threads (NT a multiple of 32, at most 1024).
+  template <int NQ, int NT>
+  __device__ __forceinline__ void
+  block_reduce_store_n(double (&v)[NQ], double *partials, int block, int n_blocks)
+  {
+    static_assert(NT % 32 == 0 && NT <= 1024, "whole warps");
+    __shared__ double warp_sum[NQ][NT / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+      {
+        double s = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+          s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0)
+          warp_sum[q][warp] = s;
+      }
+    __syncthreads();
+    if (warp == 0)
+      {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+          {
+            double s = lane < NT / 32 ? warp_sum[q][lane] : 0.0;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1)
               s += __shfl_down_sync(0xffffffffu, s, o);

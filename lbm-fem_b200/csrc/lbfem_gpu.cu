@@ -66,7 +66,16 @@ struct lbfem_gpu_ctx
   int64_t cg_its = 0;
   double last_its_per_solve = 0;
   int64_t launches = 0, last_launches = 0;
-  bool trace = false; // LBFEM_TRACE set: the CG rounds print their residuals to stderr
+  bool trace = false; // LBFEM_TRACE set: host-driven steps whose CG rounds print their residuals to stderr
+  // graph-launched steps: one instantiated graph per state of the buffer rotation
+  struct StepGraph
+  {
+    cudaGraphExec_t exec = nullptr;
+    int64_t fixed = 0, body = 0; // kernels outside the solver loop, kernels per loop body
+  };
+  std::map<int, StepGraph> graphs;
+  cudaStream_t cap = nullptr;     // captures the loop bodies
+  DevStats *d_stats = nullptr, *h_stats = nullptr;
   std::string err;
 };
 
@@ -190,7 +199,7 @@ namespace
         (st = set_smem(ctx, k_cg_start<P, double, double, double>, cg_smem<P, double>(1))) ||
         (st = set_smem(ctx, k_cg_p<P, double>, cg_smem<P, double>(0))) ||
         (st = set_smem(ctx, k_cg_update<P, double>, cg_smem<P, double>(2))) ||
-        (st = set_smem(ctx, k_cg_start<P, float, float, double>, cg_smem<P, float>(1, true))) ||
+        (st = set_smem(ctx, k_cg_start<P, float, float, float>, cg_smem<P, float>(1))) ||
         (st = set_smem(ctx, k_window_correct<P>, window_smem<P>())))
       return st;
     return LBFEM_OK;
@@ -228,9 +237,11 @@ namespace
     return e;
   }
 
+  // ds: the step counters of a step (its kernel does nothing after a failure), null otherwise.
   template <typename R>
   int
-  launch_advection(lbfem_gpu_ctx *ctx, int mode, const R *f, const R *feq, R *fout, R *rhs, const AdvCoef &ac)
+  launch_advection(lbfem_gpu_ctx *ctx, int mode, const R *f, const R *feq, R *fout, R *rhs, const AdvCoef &ac,
+                   const DevStats *ds = nullptr)
   {
     const Geo geo = geo_of(ctx);
     return with_degree(ctx->P, [&](auto PP) -> int {
@@ -241,20 +252,20 @@ namespace
           case ADV_TG:
             if constexpr (sizeof(R) == sizeof(double))
               k_advection<P, ADV_TG, R>
-                <<<grid, THREADS, advection_smem<P, ADV_TG, R>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
+                <<<grid, THREADS, advection_smem<P, ADV_TG, R>(), ctx->stream>>>(geo, ds, f, feq, fout, rhs, ac);
             break;
           case ADV_TG_COLLIDE:
             k_advection<P, ADV_TG_COLLIDE, R>
-              <<<grid, THREADS, advection_smem<P, ADV_TG_COLLIDE, R>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
+              <<<grid, THREADS, advection_smem<P, ADV_TG_COLLIDE, R>(), ctx->stream>>>(geo, ds, f, feq, fout, rhs, ac);
             break;
           case ADV_LEELIN_FEQ:
             if constexpr (sizeof(R) == sizeof(double))
               k_advection<P, ADV_LEELIN_FEQ, R>
-                <<<grid, THREADS, advection_smem<P, ADV_LEELIN_FEQ, R>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
+                <<<grid, THREADS, advection_smem<P, ADV_LEELIN_FEQ, R>(), ctx->stream>>>(geo, ds, f, feq, fout, rhs, ac);
             break;
           default:
             k_advection<P, ADV_LEELIN_FUSED, R>
-              <<<grid, THREADS, advection_smem<P, ADV_LEELIN_FUSED, R>(), ctx->stream>>>(geo, f, feq, fout, rhs, ac);
+              <<<grid, THREADS, advection_smem<P, ADV_LEELIN_FUSED, R>(), ctx->stream>>>(geo, ds, f, feq, fout, rhs, ac);
         }
       LAUNCHED();
       return LBFEM_OK;
@@ -263,17 +274,18 @@ namespace
 
   // The FP32 streaming kernel of the mixed-precision step (pairs of opposite populations).
   int
-  launch_pair(lbfem_gpu_ctx *ctx, int mode, const float *d, float *dout, float *rhs, const AdvCoef &ac)
+  launch_pair(lbfem_gpu_ctx *ctx, int mode, const float *d, float *dout, float *rhs, const AdvCoef &ac,
+              const DevStats *ds = nullptr)
   {
     const Geo geo = geo_of(ctx);
     return with_degree(ctx->P, [&](auto PP) -> int {
       constexpr int P = decltype(PP)::value;
       const dim3 grid = tile_grid<P>(ctx->grid);
       if (mode == PAIR_BARDOW)
-        k_stream_pair<P, PAIR_BARDOW><<<grid, THREADS, pair_smem<P, PAIR_BARDOW>(), ctx->stream>>>(geo, d, dout, rhs,
+        k_stream_pair<P, PAIR_BARDOW><<<grid, THREADS, pair_smem<P, PAIR_BARDOW>(), ctx->stream>>>(geo, ds, d, dout, rhs,
                                                                                                  ac);
       else
-        k_stream_pair<P, PAIR_LEELIN><<<grid, THREADS, pair_smem<P, PAIR_LEELIN>(), ctx->stream>>>(geo, d, dout, rhs,
+        k_stream_pair<P, PAIR_LEELIN><<<grid, THREADS, pair_smem<P, PAIR_LEELIN>(), ctx->stream>>>(geo, ds, d, dout, rhs,
                                                                                                  ac);
       LAUNCHED();
       return LBFEM_OK;
@@ -438,98 +450,108 @@ namespace
     return st;
   }
 
-  // The mixed-precision mass solve of the 8 moving populations: FP64 iterative
-  // refinement around the tensor-product window solve. Each round computes the
-  // true residual r = b - A x in FP64 arithmetic (from the FP32-stored x and b)
-  // and adds the FP32 correction M^{-1} r (window solves) to every system whose
-  // residual misses the tolerance. The first round starts from the
-  // extrapolation 2 x_cur - x_prev and corrects every system: accepting the
-  // extrapolation itself whenever it meets the tolerance would march on
-  // extrapolated increments, whose errors accumulate from step to step (on a
-  // coarse mesh the FP32 right-hand side is resolved to about the tolerance, so
-  // that happens often). A correction reduces the residual to a few 1e-8 of
-  // itself, so one correction is the rule; the tolerance floor is the FP32
-  // rounding of x (about 1e-7 relative). *its_out: corrections, summed over the
-  // systems.
+  // The status code of a failed mixed-precision solve (CgState status, 0: none).
   int
-  mixed_solve(lbfem_gpu_ctx *ctx, const float *b, float *x_new, const float *x_cur, const float *x_prev,
-              int nsys, int64_t *its_out)
+  mixed_status(lbfem_gpu_ctx *ctx, int status, double tol)
+  {
+    switch (status)
+      {
+        case 0:
+          return LBFEM_OK;
+        case 3:
+          return fail(ctx, LBFEM_ERR_NONFINITE, "mixed mass solve: non-finite residual");
+        case 4:
+          return fail(ctx, LBFEM_ERR_NO_CONVERGENCE,
+                      "mixed mass solve: a correction no longer halves the residual (the tolerance %.1e is below the "
+                      "FP32 resolution of the solution)",
+                      tol);
+        default:
+          return fail(ctx, LBFEM_ERR_NO_CONVERGENCE, "mixed mass solve: no convergence within %d corrections",
+                      ctx->prm.cg_max_iterations);
+      }
+  }
+
+  // The mixed-precision mass solve of the 8 moving populations: FP64 iterative
+  // refinement around the tensor-product window solve, on the FP32 solution
+  // history of the context. The start is the extrapolation x0 = 2 x_cur - x_prev
+  // with its residual r0 = b - A x0 (FP32 arithmetic: it only feeds the first
+  // correction). Each round then adds the FP32 correction
+  // M^{-1} r (window solves) and forms the new residual b - A x in FP64
+  // arithmetic, in one kernel; the systems whose residual meets the tolerance
+  // stop. The first round corrects every system: accepting the extrapolation
+  // whenever it meets the tolerance would march on extrapolated increments,
+  // whose errors accumulate from step to step. A correction reduces the
+  // residual to a few 1e-8 of itself, so one round is the rule; the tolerance
+  // floor is the FP32 rounding of x (about 1e-7 relative). On return x_cur holds
+  // the solution and the history has moved on by one step. *its_out:
+  // corrections, summed over the systems.
+  int
+  mixed_solve(lbfem_gpu_ctx *ctx, const float *b, int nsys, int64_t *its_out)
   {
     const Geo geo = geo_of(ctx);
     const Grid &g = ctx->grid;
     const double tol = mixed_tolerance(ctx->prm);
     const int max_rounds = ctx->prm.cg_max_iterations;
+    const int ic = ctx->x_cur, ip = ctx->x_prev, in = ctx->x_new;
     CK(cudaMemsetAsync(ctx->d_cg, 0, sizeof(CgState), ctx->stream));
-    int64_t corrections = 0;
-    double prev_res[NM];
-    int st;
+    int st = with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      dim3 grid = tile_grid<P>(g);
+      grid.z = nsys;
+      // FP32 arithmetic: r0 only feeds the FP32 correction (the rounds form the FP64 residuals)
+      k_cg_start<P, float, float, float><<<grid, THREADS, cg_smem<P, float>(1), ctx->stream>>>(
+        geo, b, ctx->d_x_s[ic], ctx->d_x_s[ip], ctx->d_x_s[in], ctx->d_r_s, 1, ctx->d_partials);
+      LAUNCHED();
+      return LBFEM_OK;
+    });
+    if (st)
+      return st;
+    // the rounds alternate between x_new and x_prev's buffer (free once the start has read it)
+    int xi = in, xo = ip;
+    float *r_in = ctx->d_r_s, *r_out = ctx->d_p_s[0];
     for (int round = 0;; ++round)
       {
         int n_tiles = 0;
         st = with_degree(ctx->P, [&](auto PP) -> int {
           constexpr int P = decltype(PP)::value;
-          dim3 grid = tile_grid<P>(g);
+          using S = WinShape<P>;
+          const dim3 grid((g.nfx + S::TX - 1) / S::TX, (g.nfy + S::TY - 1) / S::TY, nsys);
           n_tiles = int(grid.x * grid.y);
-          grid.z = nsys;
-          k_cg_start<P, float, float, double><<<grid, THREADS, cg_smem<P, float>(1, true), ctx->stream>>>(
-            geo, b, x_cur, x_prev, x_new, ctx->d_r_s, round == 0, ctx->d_partials);
+          k_window_correct<P><<<grid, S::THREADS, window_smem<P>(), ctx->stream>>>(
+            geo, ctx->d_winx, ctx->d_winy, r_in, ctx->d_x_s[xi], b, ctx->d_x_s[xo], r_out, ctx->d_cg, round == 0,
+            ctx->d_partials);
           LAUNCHED();
           return LBFEM_OK;
         });
         if (st)
           return st;
+        std::swap(xi, xo);
+        std::swap(r_in, r_out);
         if ((st = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, 3 * NM)))
           return st;
-        k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nsys, 0, tol, max_rounds + 1);
+        k_mixed_round<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nullptr, nsys, tol, max_rounds, 0, 0);
         LAUNCHED();
         CK(cudaMemcpyAsync(ctx->h_cg, ctx->d_cg, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
         if (ctx->trace)
           {
-            std::fprintf(stderr, "lbfem mixed solve: round %d active %d res/tol", round, ctx->h_cg->n_active);
+            std::fprintf(stderr, "lbfem mixed solve: round %d still active %d res/tol", round, ctx->h_cg->n_active);
             for (int q = 0; q < nsys; ++q)
               std::fprintf(stderr, " %.2e", ctx->h_cg->tol[q] > 0 ? ctx->h_cg->res[q] / ctx->h_cg->tol[q] : 0.0);
             std::fprintf(stderr, "\n");
           }
-        if (ctx->h_cg->status == 3)
-          return fail(ctx, LBFEM_ERR_NONFINITE, "mixed mass solve: non-finite residual");
-        if (ctx->h_cg->n_active == 0 && round > 0)
-          break;
-        if (round >= max_rounds)
-          return fail(ctx, LBFEM_ERR_NO_CONVERGENCE, "mixed mass solve: no convergence within %d corrections",
-                      max_rounds);
-        if (round > 0)
-          {
-            // a correction reduces the residual by orders of magnitude; one that does not
-            // halve it has reached the FP32 resolution of x, which lies above the tolerance
-            bool progress = false;
-            for (int q = 0; q < nsys; ++q)
-              progress = progress || (ctx->h_cg->active[q] && ctx->h_cg->res[q] <= 0.5 * prev_res[q]);
-            if (!progress)
-              return fail(ctx, LBFEM_ERR_NO_CONVERGENCE,
-                          "mixed mass solve: the residual stagnates at %.3e of the tolerance (the tolerance %.1e is "
-                          "below the FP32 resolution of the solution)",
-                          ctx->h_cg->res[0] / std::max(ctx->h_cg->tol[0], 1e-300), tol);
-          }
-        for (int q = 0; q < nsys; ++q)
-          prev_res[q] = ctx->h_cg->res[q];
-        corrections += round == 0 ? nsys : ctx->h_cg->n_active;
-        st = with_degree(ctx->P, [&](auto PP) -> int {
-          constexpr int P = decltype(PP)::value;
-          using S = WinShape<P>;
-          const dim3 grid((g.nfx + S::TX - 1) / S::TX, (g.nfy + S::TY - 1) / S::TY, nsys);
-          k_window_correct<P><<<grid, S::THREADS, window_smem<P>(), ctx->stream>>>(geo, ctx->d_winx, ctx->d_winy,
-                                                                                  ctx->d_r_s, x_new, ctx->d_cg,
-                                                                                  round == 0);
-          LAUNCHED();
-          return LBFEM_OK;
-        });
-        if (st)
+        if ((st = mixed_status(ctx, ctx->h_cg->status, tol)))
           return st;
+        if (ctx->h_cg->n_active == 0)
+          break;
       }
+    // the solution is in buffer xi
+    ctx->x_prev = ic;
+    ctx->x_cur = xi;
+    ctx->x_new = xi == in ? ip : in;
     if (its_out)
-      *its_out = corrections;
-    ctx->cg_its += corrections;
+      *its_out = int64_t(ctx->h_cg->total_its);
+    ctx->cg_its += int64_t(ctx->h_cg->total_its);
     return LBFEM_OK;
   }
 
@@ -586,124 +608,422 @@ namespace
   }
 
   // ------------------------------------------------------------ one step
-  // Mixed precision: the same sequence on FP32 deviations d = f - w.
+  // A step is front (streaming right-hand side, wall faces), solve (the mass
+  // solve of the 8 increments) and back (the nodal update that completes it).
+  // LeeLin::step is schemes.h:92-98, Bardow::step schemes.h:118-124 (collide,
+  // then stream, streaming.h:88-100). The mixed-precision step runs the same
+  // sequence on FP32 deviations d = f - w.
   int
-  step_once_mixed(lbfem_gpu_ctx *ctx, int64_t *its)
+  step_front(lbfem_gpu_ctx *ctx)
   {
-    const Geo geo = geo_of(ctx);
     const double dt = ctx->dt, lam = ctx->lambda;
     const double *e = d2q9_e();
-    const long long N = ctx->grid.N;
-    const int nb = n_pointwise_blocks(N);
     const int rm = ctx->prm.remove_wall_mass_flux;
-    const bool cg = ctx->prm.mass == LBFEM_MASS_CG;
-    float *d = ctx->d_fs[ctx->cur];
-    float *xn = ctx->d_x_s[cg ? ctx->x_new : ctx->x_cur];
     const bool bardow = ctx->prm.scheme == LBFEM_SCHEME_BARDOW;
-    float *g = ctx->d_fs[1 - ctx->cur];
+    const double b = -0.5 * dt * dt / lam;
+    const AdvCoef ac = bardow ? adv_coef(-dt, 0., -0.5 * dt * dt, e, dt / (lam + 0.5 * dt))
+                              : adv_coef(-dt - b, b, -0.5 * dt * dt, e, 0.);
+    const bool remove = rm < 0 ? bardow : rm != 0;
     int st;
-    if (bardow)
+    if (ctx->mixed)
       {
-        const AdvCoef ac = adv_coef(-dt, 0., -0.5 * dt * dt, e, dt / (lam + 0.5 * dt));
-        if ((st = launch_pair(ctx, PAIR_BARDOW, d, g, ctx->d_rhs_s, ac)) ||
-            (st = launch_wall_faces<float>(ctx, g, ctx->d_rhs_s, e, dt, rm < 0 ? true : rm != 0)))
+        float *d = ctx->d_fs[ctx->cur], *g = ctx->d_fs[1 - ctx->cur];
+        if ((st = launch_pair(ctx, bardow ? PAIR_BARDOW : PAIR_LEELIN, d, bardow ? g : nullptr, ctx->d_rhs_s, ac,
+                              ctx->d_stats)))
           return st;
+        return launch_wall_faces<float>(ctx, bardow ? g : d, ctx->d_rhs_s, e, dt, remove);
       }
-    else
+    double *f = ctx->d_f[ctx->cur], *g = ctx->d_f[1 - ctx->cur];
+    if ((st = launch_advection<double>(ctx, bardow ? ADV_TG_COLLIDE : ADV_LEELIN_FUSED, f, nullptr,
+                                       bardow ? g : nullptr, ctx->d_rhs, ac, ctx->d_stats)))
+      return st;
+    return launch_wall_faces<double>(ctx, bardow ? g : f, ctx->d_rhs, e, dt, remove);
+  }
+
+  // The nodal update with the increment in x_cur (Bardow: f = g* + x, which
+  // flips the population buffers; Lee-Lin: the predictor-corrector).
+  int
+  step_back(lbfem_gpu_ctx *ctx)
+  {
+    const Geo geo = geo_of(ctx);
+    const int nb = n_pointwise_blocks(ctx->grid.N);
+    const double theta = ctx->dt / ctx->lambda;
+    if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
       {
-        const double b = -0.5 * dt * dt / lam;
-        const AdvCoef ac = adv_coef(-dt - b, b, -0.5 * dt * dt, e, 0.);
-        if ((st = launch_pair(ctx, PAIR_LEELIN, d, nullptr, ctx->d_rhs_s, ac)) ||
-            (st = launch_wall_faces<float>(ctx, d, ctx->d_rhs_s, e, dt, rm < 0 ? false : rm != 0)))
-          return st;
-      }
-    if (cg)
-      {
-        if ((st = mixed_solve(ctx, ctx->d_rhs_s, xn, ctx->d_x_s[ctx->x_cur], ctx->d_x_s[ctx->x_prev], NM, its)))
-          return st;
-        const int old_prev = ctx->x_prev;
-        ctx->x_prev = ctx->x_cur;
-        ctx->x_cur = ctx->x_new;
-        ctx->x_new = old_prev;
-      }
-    else
-      {
-        k_lumped<float, float><<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_rhs_s, xn, NM);
-        LAUNCHED();
-        if (its)
-          *its = 0;
-      }
-    if (bardow)
-      {
-        k_add_increment<float><<<nb, THREADS, 0, ctx->stream>>>(geo, g, ctx->d_x_s[ctx->x_cur]);
+        if (ctx->mixed)
+          k_add_increment<float><<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_stats, ctx->d_fs[1 - ctx->cur],
+                                                                  ctx->d_x_s[ctx->x_cur]);
+        else
+          k_add_increment<double><<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_stats, ctx->d_f[1 - ctx->cur],
+                                                                   ctx->d_x[ctx->x_cur]);
         LAUNCHED();
         ctx->cur = 1 - ctx->cur;
+        return LBFEM_OK;
       }
+    if (ctx->mixed)
+      k_predictor_corrector_dev<<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_stats, ctx->d_fs[ctx->cur],
+                                                                 ctx->d_x_s[ctx->x_cur], theta);
     else
-      {
-        k_predictor_corrector_dev<<<nb, THREADS, 0, ctx->stream>>>(geo, d, ctx->d_x_s[ctx->x_cur], dt / lam);
-        LAUNCHED();
-      }
+      k_predictor_corrector<<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_stats, ctx->d_f[ctx->cur], nullptr,
+                                                             ctx->d_x[ctx->x_cur], theta);
+    LAUNCHED();
     return LBFEM_OK;
   }
 
+  // The lumped solve x_cur = M_L^{-1} rhs (no history).
+  int
+  lumped_solve(lbfem_gpu_ctx *ctx)
+  {
+    const Geo geo = geo_of(ctx);
+    const int nb = n_pointwise_blocks(ctx->grid.N);
+    if (ctx->mixed)
+      k_lumped<float, float><<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_rhs_s, ctx->d_x_s[ctx->x_cur], NM);
+    else
+      k_lumped<double, double><<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_rhs, ctx->d_x[ctx->x_cur], NM);
+    LAUNCHED();
+    return LBFEM_OK;
+  }
+
+  // One host-driven step: the solver loops read their state back after every
+  // iteration (the path of LBFEM_TRACE).
   int
   step_once(lbfem_gpu_ctx *ctx, int64_t *its)
   {
-    if (ctx->mixed)
-      return step_once_mixed(ctx, its);
-    const Geo geo = geo_of(ctx);
-    const double dt = ctx->dt, lam = ctx->lambda;
-    const double *e = d2q9_e();
-    const long long N = ctx->grid.N;
-    const int nb = n_pointwise_blocks(N);
-    const int rm = ctx->prm.remove_wall_mass_flux;
-    const bool cg = ctx->prm.mass == LBFEM_MASS_CG;
-    double *f = ctx->d_f[ctx->cur];
     int st;
-    if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
+    if ((st = step_front(ctx)))
+      return st;
+    if (its)
+      *its = 0;
+    if (ctx->prm.mass != LBFEM_MASS_CG)
+      st = lumped_solve(ctx);
+    else if (ctx->mixed)
+      st = mixed_solve(ctx, ctx->d_rhs_s, NM, its);
+    else
       {
-        // Bardow::step (schemes.h:118-124): collide, then stream (streaming.h:88-100)
-        double *g = ctx->d_f[1 - ctx->cur];
-        const AdvCoef ac = adv_coef(-dt, 0., -0.5 * dt * dt, e, dt / (lam + 0.5 * dt));
-        if ((st = launch_advection<double>(ctx, ADV_TG_COLLIDE, f, nullptr, g, ctx->d_rhs, ac)))
-          return st;
-        if ((st = launch_wall_faces<double>(ctx, g, ctx->d_rhs, e, dt, rm < 0 ? true : rm != 0)))
-          return st;
-        double *xn = ctx->d_x[cg ? ctx->x_new : ctx->x_cur];
-        if ((st = mass_solve_dev(ctx, ctx->d_rhs, xn, ctx->d_x[ctx->x_cur], ctx->d_x[ctx->x_prev], 1, NM, its)))
-          return st;
-        if (cg)
+        st = cg_solve(ctx, ctx->d_rhs, ctx->d_x[ctx->x_new], ctx->d_x[ctx->x_cur], ctx->d_x[ctx->x_prev], 1, NM, its);
+        if (!st)
           {
             const int old_prev = ctx->x_prev;
             ctx->x_prev = ctx->x_cur;
             ctx->x_cur = ctx->x_new;
             ctx->x_new = old_prev;
           }
-        k_add_increment<double><<<nb, THREADS, 0, ctx->stream>>>(geo, g, ctx->d_x[ctx->x_cur]);
-        LAUNCHED();
-        ctx->cur = 1 - ctx->cur;
-        return LBFEM_OK;
       }
-    // LeeLin::step (schemes.h:92-98): equilibria, increment, predictor-corrector
-    const double b = -0.5 * dt * dt / lam;
-    const AdvCoef ac = adv_coef(-dt - b, b, -0.5 * dt * dt, e, 0.);
-    if ((st = launch_advection<double>(ctx, ADV_LEELIN_FUSED, f, nullptr, nullptr, ctx->d_rhs, ac)))
+    if (st)
       return st;
-    if ((st = launch_wall_faces<double>(ctx, f, ctx->d_rhs, e, dt, rm < 0 ? false : rm != 0)))
+    return step_back(ctx);
+  }
+
+  // ------------------------------------------------------- graph-launched steps
+  // A whole step as one CUDA graph: the solver loops become conditional WHILE
+  // nodes whose bodies end in a control kernel that sets the condition on the
+  // device (no host round trip per iteration). Failures are recorded in the
+  // sticky status of DevStats; the step-completing kernels then do nothing, so
+  // the populations stay those before the failing step.
+
+  // Appends a WHILE node after the work captured so far on ctx->stream and
+  // captures body() into it on ctx->cap; *body_kernels: the kernels of one body.
+  template <typename Body>
+  int
+  capture_while(lbfem_gpu_ctx *ctx, cudaGraphConditionalHandle h, Body &&body, int64_t *body_kernels)
+  {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo_v3(ctx->stream, &cs, nullptr, &g, &deps, nullptr, &nd));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nd, &np));
+    CK(cudaStreamBeginCaptureToGraph(ctx->cap, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    const int64_t l0 = ctx->launches;
+    std::swap(ctx->stream, ctx->cap);
+    const int st = body();
+    std::swap(ctx->stream, ctx->cap);
+    cudaGraph_t bg = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->cap, &bg);
+    if (st)
       return st;
-    double *xn = ctx->d_x[cg ? ctx->x_new : ctx->x_cur];
-    if ((st = mass_solve_dev(ctx, ctx->d_rhs, xn, ctx->d_x[ctx->x_cur], ctx->d_x[ctx->x_prev], 1, NM, its)))
+    if (e != cudaSuccess)
+      return fail(ctx, LBFEM_ERR_CUDA, "loop body capture: %s", cudaGetErrorString(e));
+    *body_kernels = ctx->launches - l0;
+    CK(cudaStreamUpdateCaptureDependencies_v2(ctx->stream, &node, nullptr, 1, cudaStreamSetCaptureDependencies));
+    return LBFEM_OK;
+  }
+
+  // Jacobi-PCG of the FP64 step (the order of cg_run), with the loop on the
+  // device. One loop body is two iterations: the search directions alternate
+  // between two buffers, and an iteration of a converged system does nothing.
+  int
+  cg_graph(lbfem_gpu_ctx *ctx, int64_t *body_kernels)
+  {
+    const Geo geo = geo_of(ctx);
+    const Grid &g = ctx->grid;
+    const double tol = ctx->prm.cg_tolerance;
+    const int max_its = ctx->prm.cg_max_iterations;
+    const double *b = ctx->d_rhs;
+    double *x_new = ctx->d_x[ctx->x_new];
+    const double *x_cur = ctx->d_x[ctx->x_cur], *x_prev = ctx->d_x[ctx->x_prev];
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamGetCaptureInfo_v3(ctx->stream, &cs, nullptr, &graph, nullptr, nullptr, nullptr));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
+    CK(cudaMemsetAsync(ctx->d_cg, 0, sizeof(CgState), ctx->stream));
+    int n_tiles = 0;
+    int st = with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      dim3 grid = tile_grid<P>(g);
+      n_tiles = int(grid.x * grid.y);
+      grid.z = NM;
+      k_cg_start<P, double, double, double><<<grid, THREADS, cg_smem<P, double>(1, true), ctx->stream>>>(
+        geo, b, x_cur, x_prev, x_new, ctx->d_r, 1, ctx->d_partials);
+      LAUNCHED();
+      return LBFEM_OK;
+    });
+    if (st || (st = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, 3 * NM)))
       return st;
-    if (cg)
-      {
-        const int old_prev = ctx->x_prev;
-        ctx->x_prev = ctx->x_cur;
-        ctx->x_cur = ctx->x_new;
-        ctx->x_new = old_prev;
-      }
-    k_predictor_corrector<<<nb, THREADS, 0, ctx->stream>>>(geo, f, nullptr, ctx->d_x[ctx->x_cur], dt / lam);
+    k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, NM, 0, tol, max_its);
     LAUNCHED();
+    k_cg_control<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_stats, h, 0);
+    LAUNCHED();
+    auto iteration = [&](int pi) -> int {
+      int s2 = with_degree(ctx->P, [&](auto PP) -> int {
+        constexpr int P = decltype(PP)::value;
+        dim3 grid = tile_grid<P>(g);
+        grid.z = NM;
+        k_cg_p<P, double><<<grid, THREADS, cg_smem<P, double>(0), ctx->stream>>>(geo, ctx->d_r, ctx->d_p[pi],
+                                                                                  ctx->d_p[1 - pi], ctx->d_cg,
+                                                                                  ctx->d_partials);
+        LAUNCHED();
+        return LBFEM_OK;
+      });
+      if (s2 || (s2 = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, NM)))
+        return s2;
+      k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, NM, 1, tol, max_its);
+      LAUNCHED();
+      s2 = with_degree(ctx->P, [&](auto PP) -> int {
+        constexpr int P = decltype(PP)::value;
+        dim3 grid = tile_grid<P>(g);
+        grid.z = NM;
+        k_cg_update<P, double><<<grid, THREADS, cg_smem<P, double>(2), ctx->stream>>>(
+          geo, x_new, ctx->d_r, ctx->d_p[1 - pi], ctx->d_cg, ctx->d_partials);
+        LAUNCHED();
+        return LBFEM_OK;
+      });
+      if (s2 || (s2 = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, 2 * NM)))
+        return s2;
+      k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, NM, 2, tol, max_its);
+      LAUNCHED();
+      return LBFEM_OK;
+    };
+    return capture_while(
+      ctx, h,
+      [&]() -> int {
+        int s2;
+        if ((s2 = iteration(0)) || (s2 = iteration(1)))
+          return s2;
+        k_cg_control<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_stats, h, 1);
+        LAUNCHED();
+        return LBFEM_OK;
+      },
+      body_kernels);
+  }
+
+  // The mixed-precision solve of mixed_solve with the rounds on the device. One
+  // loop body is two rounds, x_prev's buffer -> x_new's -> x_prev's; a round of a
+  // converged system copies, so the solution always ends in x_prev's buffer.
+  int
+  mixed_graph(lbfem_gpu_ctx *ctx, int64_t *body_kernels)
+  {
+    const Geo geo = geo_of(ctx);
+    const Grid &g = ctx->grid;
+    const double tol = mixed_tolerance(ctx->prm);
+    const int max_rounds = ctx->prm.cg_max_iterations;
+    const float *b = ctx->d_rhs_s;
+    float *xn = ctx->d_x_s[ctx->x_new], *xp = ctx->d_x_s[ctx->x_prev];
+    const float *xc = ctx->d_x_s[ctx->x_cur];
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamGetCaptureInfo_v3(ctx->stream, &cs, nullptr, &graph, nullptr, nullptr, nullptr));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
+    CK(cudaMemsetAsync(ctx->d_cg, 0, sizeof(CgState), ctx->stream));
+    int st = with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      dim3 grid = tile_grid<P>(g);
+      grid.z = NM;
+      k_cg_start<P, float, float, float><<<grid, THREADS, cg_smem<P, float>(1), ctx->stream>>>(
+        geo, b, xc, xp, xn, ctx->d_r_s, 1, ctx->d_partials);
+      LAUNCHED();
+      return LBFEM_OK;
+    });
+    if (st)
+      return st;
+    auto round = [&](const float *r_in, const float *x_in, float *x_out, float *r_out, int all, int set) -> int {
+      int n_tiles = 0;
+      int s2 = with_degree(ctx->P, [&](auto PP) -> int {
+        constexpr int P = decltype(PP)::value;
+        using S = WinShape<P>;
+        const dim3 grid((g.nfx + S::TX - 1) / S::TX, (g.nfy + S::TY - 1) / S::TY, NM);
+        n_tiles = int(grid.x * grid.y);
+        k_window_correct<P><<<grid, S::THREADS, window_smem<P>(), ctx->stream>>>(
+          geo, ctx->d_winx, ctx->d_winy, r_in, x_in, b, x_out, r_out, ctx->d_cg, all, ctx->d_partials);
+        LAUNCHED();
+        return LBFEM_OK;
+      });
+      if (s2 || (s2 = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, 3 * NM)))
+        return s2;
+      k_mixed_round<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, ctx->d_stats, NM, tol, max_rounds, h, set);
+      LAUNCHED();
+      return LBFEM_OK;
+    };
+    float *r0 = ctx->d_r_s, *r1 = ctx->d_p_s[0];
+    if ((st = round(r0, xn, xp, r1, 1, 1)))
+      return st;
+    return capture_while(
+      ctx, h,
+      [&]() -> int {
+        int s2;
+        if ((s2 = round(r1, xp, xn, r0, 0, 0)) || (s2 = round(r0, xn, xp, r1, 0, 1)))
+          return s2;
+        return LBFEM_OK;
+      },
+      body_kernels);
+  }
+
+  // The buffer rotation a graph-launched step applies (host bookkeeping).
+  void
+  rotate_after_step(lbfem_gpu_ctx *ctx)
+  {
+    if (ctx->prm.mass == LBFEM_MASS_CG)
+      {
+        const int c = ctx->x_cur, p = ctx->x_prev, n = ctx->x_new;
+        if (ctx->mixed)
+          {
+            ctx->x_cur = p; // the rounds end in x_prev's buffer
+            ctx->x_prev = c;
+            ctx->x_new = n;
+          }
+        else
+          {
+            ctx->x_cur = n;
+            ctx->x_prev = c;
+            ctx->x_new = p;
+          }
+      }
+    if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
+      ctx->cur = 1 - ctx->cur;
+  }
+
+  int
+  graph_key(const lbfem_gpu_ctx *ctx)
+  {
+    return ctx->cur * 9 + ctx->x_cur * 3 + ctx->x_prev;
+  }
+
+  // Captures and instantiates the step graph of the current buffer state.
+  int
+  capture_step(lbfem_gpu_ctx *ctx, lbfem_gpu_ctx::StepGraph &sg)
+  {
+    const int cur0 = ctx->cur, c0 = ctx->x_cur, p0 = ctx->x_prev, n0 = ctx->x_new;
+    const int64_t l0 = ctx->launches;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int64_t body = 0;
+    int st = step_front(ctx);
+    if (!st)
+      {
+        if (ctx->prm.mass != LBFEM_MASS_CG)
+          st = lumped_solve(ctx);
+        else
+          st = ctx->mixed ? mixed_graph(ctx, &body) : cg_graph(ctx, &body);
+      }
+    if (!st)
+      {
+        rotate_after_step(ctx);
+        if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
+          ctx->cur = 1 - ctx->cur; // step_back flips it again
+        st = step_back(ctx);
+      }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    const int64_t total = ctx->launches - l0;
+    ctx->cur = cur0;
+    ctx->x_cur = c0;
+    ctx->x_prev = p0;
+    ctx->x_new = n0;
+    ctx->launches = l0;
+    if (st || e != cudaSuccess)
+      {
+        if (graph)
+          cudaGraphDestroy(graph);
+        return st ? st : fail(ctx, LBFEM_ERR_CUDA, "step capture: %s", cudaGetErrorString(e));
+      }
+    const cudaError_t ei = cudaGraphInstantiate(&sg.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess)
+      return fail(ctx, LBFEM_ERR_CUDA, "step graph instantiation: %s", cudaGetErrorString(ei));
+    sg.fixed = total - body;
+    sg.body = body;
+    return LBFEM_OK;
+  }
+
+  // n steps as graph launches, with one synchronisation at the end.
+  int
+  step_graphs(lbfem_gpu_ctx *ctx, int n, int64_t *its_total, int64_t *launches)
+  {
+    CK(cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const DevStats before = *ctx->h_stats;
+    const int cur0 = ctx->cur, c0 = ctx->x_cur, p0 = ctx->x_prev, n0 = ctx->x_new;
+    int64_t fixed = 0, body = 0;
+    for (int k = 0; k < n; ++k)
+      {
+        auto &sg = ctx->graphs[graph_key(ctx)];
+        int st;
+        if (!sg.exec && (st = capture_step(ctx, sg)))
+          return st;
+        CK(cudaGraphLaunch(sg.exec, ctx->stream));
+        fixed += sg.fixed;
+        body = sg.body;
+        rotate_after_step(ctx);
+      }
+    CK(cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const DevStats after = *ctx->h_stats;
+    *its_total = int64_t(after.its - before.its);
+    *launches = fixed + int64_t(after.bodies - before.bodies) * body;
+    if (after.sticky)
+      {
+        // the steps after the failing one did nothing: put the buffer state back to
+        // the completed steps, restart the extrapolation history, clear the failure
+        ctx->cur = cur0;
+        ctx->x_cur = c0;
+        ctx->x_prev = p0;
+        ctx->x_new = n0;
+        for (unsigned long long k = 0; k < after.steps_done - before.steps_done; ++k)
+          rotate_after_step(ctx);
+        const long long N = ctx->grid.N;
+        for (int k = 0; k < 3; ++k)
+          {
+            CK(cudaMemsetAsync(ctx->d_x[k], 0, sizeof(double) * NM * N, ctx->stream));
+            if (ctx->mixed)
+              CK(cudaMemsetAsync(ctx->d_x_s[k], 0, sizeof(float) * NM * N, ctx->stream));
+          }
+        CK(cudaMemsetAsync(&ctx->d_stats->sticky, 0, sizeof(int), ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        const double tol = ctx->mixed ? mixed_tolerance(ctx->prm) : ctx->prm.cg_tolerance;
+        if (ctx->mixed)
+          return mixed_status(ctx, after.sticky, tol);
+        if (after.sticky == 3)
+          return fail(ctx, LBFEM_ERR_NONFINITE, "CG: non-finite residual");
+        return fail(ctx, LBFEM_ERR_NO_CONVERGENCE, "CG: iteration cap %d reached", ctx->prm.cg_max_iterations);
+      }
     return LBFEM_OK;
   }
 
@@ -819,6 +1139,15 @@ lbfem_gpu_destroy(lbfem_gpu_ctx *ctx)
       cudaFree(b);
   if (ctx->h_cg)
     cudaFreeHost(ctx->h_cg);
+  for (auto &kv : ctx->graphs)
+    if (kv.second.exec)
+      cudaGraphExecDestroy(kv.second.exec);
+  if (ctx->d_stats)
+    cudaFree(ctx->d_stats);
+  if (ctx->h_stats)
+    cudaFreeHost(ctx->h_stats);
+  if (ctx->cap)
+    cudaStreamDestroy(ctx->cap);
   for (auto &e : ctx->ev)
     if (e)
       cudaEventDestroy(e);
@@ -1040,8 +1369,8 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
           st = with_degree(P, [&](auto PP) -> int {
             using S = WinShape<decltype(PP)::value>;
             const int ntx = (nfx + S::TX - 1) / S::TX, nty = (nfy + S::TY - 1) / S::TY;
-            const std::vector<float> wx = window_ldl(ctx->ax, S::TX, S::W, ntx);
-            const std::vector<float> wy = window_ldl(ctx->ay, S::TY, S::W, nty);
+            const std::vector<float> wx = window_ldl(ctx->ax, S::TX, S::W, ntx, S::NC);
+            const std::vector<float> wy = window_ldl(ctx->ay, S::TY, S::W, nty, S::NC);
             CK(cudaMalloc(&ctx->d_winx, sizeof(float) * wx.size()));
             CK(cudaMalloc(&ctx->d_winy, sizeof(float) * wy.size()));
             CK(cudaMemcpy(ctx->d_winx, wx.data(), sizeof(float) * wx.size(), cudaMemcpyHostToDevice));
@@ -1062,6 +1391,10 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
     return st;
   CK(cudaMalloc(&ctx->d_cg, sizeof(CgState)));
   CK(cudaHostAlloc(&ctx->h_cg, sizeof(CgState), cudaHostAllocDefault));
+  CK(cudaMalloc(&ctx->d_stats, sizeof(DevStats)));
+  CK(cudaMemset(ctx->d_stats, 0, sizeof(DevStats)));
+  CK(cudaHostAlloc(&ctx->h_stats, sizeof(DevStats), cudaHostAllocDefault));
+  CK(cudaStreamCreateWithFlags(&ctx->cap, cudaStreamNonBlocking));
   if ((st = with_degree(P, [&](auto PP) -> int { return set_smem_attributes<decltype(PP)::value>(ctx); })))
     return st;
   *out = guard.release();
@@ -1078,6 +1411,12 @@ lbfem_gpu_set_time_step(lbfem_gpu_ctx *ctx, double dt, double lambda)
   ctx->dt = dt;
   ctx->lambda = lambda;
   ctx->have_ts = true;
+  // the step graphs hold the coefficients of the old time step
+  cudaSetDevice(ctx->device);
+  for (auto &kv : ctx->graphs)
+    if (kv.second.exec)
+      cudaGraphExecDestroy(kv.second.exec);
+  ctx->graphs.clear();
   return LBFEM_OK;
 }
 
@@ -1167,14 +1506,27 @@ lbfem_gpu_step(lbfem_gpu_ctx *ctx, int32_t n_steps)
     return fail(ctx, LBFEM_ERR_STATE, "step needs the time step");
   const int64_t launches0 = ctx->launches;
   int64_t its_total = 0;
-  for (int s = 0; s < n_steps; ++s)
+  if (ctx->trace)
     {
-      int64_t its = 0;
-      if ((st = step_once(ctx, &its)))
-        return st;
-      its_total += its;
+      // host-driven steps (the solver rounds print their residuals)
+      for (int s = 0; s < n_steps; ++s)
+        {
+          int64_t its = 0;
+          if ((st = step_once(ctx, &its)))
+            return st;
+          its_total += its;
+        }
+      CK(cudaStreamSynchronize(ctx->stream));
     }
-  CK(cudaStreamSynchronize(ctx->stream));
+  else
+    {
+      int64_t launched = 0;
+      st = step_graphs(ctx, n_steps, &its_total, &launched);
+      ctx->launches += launched;
+      ctx->cg_its += its_total;
+      if (st)
+        return st;
+    }
   ctx->last_launches = ctx->launches - launches0;
   ctx->last_its_per_solve = n_steps > 0 ? double(its_total) / (double(n_steps) * NM) : 0.0;
   return LBFEM_OK;
@@ -1352,8 +1704,8 @@ lbfem_gpu_predictor_corrector(lbfem_gpu_ctx *ctx, double *f, const double *feq, 
   double *d = ctx->d_f[1 - ctx->cur];
   if ((st = upload(ctx, f, d, Q)) || (st = upload(ctx, feq, ctx->d_feq, Q)) || (st = upload(ctx, incr, ctx->d_r, NM)))
     return st;
-  k_predictor_corrector<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), d, ctx->d_feq,
-                                                                                      ctx->d_r, theta);
+  k_predictor_corrector<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), nullptr, d,
+                                                                                      ctx->d_feq, ctx->d_r, theta);
   LAUNCHED();
   return download(ctx, d, f, Q);
 }

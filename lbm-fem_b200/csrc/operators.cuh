@@ -60,9 +60,11 @@ namespace lbfem_gpu
   // predictor_corrector (collision.h:119-145); feq == nullptr: the equilibria of
   // f^n are recomputed here (the fused Lee-Lin step never stores them).
   __global__ void
-  k_predictor_corrector(const Geo geo, double *__restrict__ f, const double *__restrict__ feq,
+  k_predictor_corrector(const Geo geo, DevStats *__restrict__ ds, double *__restrict__ f, const double *__restrict__ feq,
                         const double *__restrict__ x, double theta)
   {
+    if (step_skipped(ds))
+      return;
     const long long N = geo.g.N;
     const double inv = 1. / (1. + theta);
     LBFEM_GRID_STRIDE(i, N)
@@ -152,8 +154,11 @@ namespace lbfem_gpu
   // predictor_corrector on FP32 deviations d = f - w with the FP32 increment x, in
   // FP64 arithmetic (the corrector's theta (feq(fhat) - feq(f)) cancels).
   __global__ void
-  k_predictor_corrector_dev(const Geo geo, float *__restrict__ d, const float *__restrict__ x, double theta)
+  k_predictor_corrector_dev(const Geo geo, DevStats *__restrict__ ds, float *__restrict__ d,
+                            const float *__restrict__ x, double theta)
   {
+    if (step_skipped(ds))
+      return;
     const long long N = geo.g.N;
     const double inv = 1. / (1. + theta);
     LBFEM_GRID_STRIDE(i, N)
@@ -222,8 +227,10 @@ namespace lbfem_gpu
   // TaylorGalerkin::stream (streaming.h:94-98): f_a += x_{a-1}, a = 1..8.
   template <typename R>
   __global__ void
-  k_add_increment(const Geo geo, R *__restrict__ f, const R *__restrict__ x)
+  k_add_increment(const Geo geo, DevStats *__restrict__ ds, R *__restrict__ f, const R *__restrict__ x)
   {
+    if (step_skipped(ds))
+      return;
     const long long N = geo.g.N;
     LBFEM_GRID_STRIDE(i, N)
     {
@@ -687,9 +694,11 @@ namespace lbfem_gpu
   // annihilates constants, and collide / feq are applied in deviation form).
   template <int P, int MODE, typename R>
   __global__ void __launch_bounds__(THREADS, 2)
-    k_advection(const Geo geo, const R *__restrict__ f, const R *__restrict__ feq, R *__restrict__ fout,
-                R *__restrict__ rhs, const AdvCoef ac)
+    k_advection(const Geo geo, const DevStats *__restrict__ ds, const R *__restrict__ f, const R *__restrict__ feq,
+                R *__restrict__ fout, R *__restrict__ rhs, const AdvCoef ac)
   {
+    if (ds && ds->sticky)
+      return; // a step after a failed solve: the populations must stay as they are
     using T = Tile<P>;
     constexpr bool MOM = has_moments<MODE>();
     constexpr bool DEV = sizeof(R) == sizeof(float);
@@ -1227,11 +1236,15 @@ namespace lbfem_gpu
     static constexpr int W = P == 1 ? 12 : P == 2 ? 20 : P == 3 ? 24 : 28;
     static constexpr int TX = 128, TY = 64;                // own nodes
     static constexpr int FX = TX + 2 * W, FY = TY + 2 * W; // window
-    static constexpr int PF = FX | 1;                      // odd pitch: conflict-free row and column sweeps
-    static constexpr int NC = P + 1;                       // factor entries per window position
-    static constexpr int THREADS = 128;
-    static_assert(FY <= THREADS && TX == THREADS, "one thread per window row and per own column");
-    static_assert(FX % 4 == 0 && FY % 4 == 0 && (FX - W) % 4 == 0 && (FY - W) % 4 == 0, "whole chunks");
+    // pitch = 4 (mod 8): rows are 16-byte aligned, and eight lanes on eight rows hit
+    // distinct bank groups with 16-byte accesses (row sweeps) as with 4-byte ones
+    // on consecutive columns (column sweeps)
+    static constexpr int PF = FX + 4;
+    static constexpr int NC = P == 1 ? 2 : P <= 3 ? 4 : 8; // factor floats per window position (padded)
+    static constexpr int K = 2 * P + 1;                    // entries of an assembled 1-D row
+    static constexpr int THREADS = 160;
+    static_assert(FY <= THREADS && TX + 2 * P <= THREADS, "one thread per window row and per own-plus-halo column");
+    static_assert(FX % 8 == 0 && FY % 4 == 0 && W - P >= 3, "whole chunks; the backward sweeps stop at W - P");
   };
 
   template <int P>
@@ -1239,19 +1252,76 @@ namespace lbfem_gpu
   window_smem()
   {
     using S = WinShape<P>;
-    return sizeof(float) * size_t(S::PF) * S::FY;
+    return sizeof(float) * size_t(S::PF) * S::FY + sizeof(double) * S::TY * S::K;
+  }
+
+  // The factor row of window position q: l[k-1] = l_{q,q-k}, l[P] = 1/d_q (one
+  // or two vector loads from rows of NC floats, 16-byte aligned).
+  template <int P, int NC>
+  __device__ __forceinline__ void
+  ldl_row(const float *c, int q, float (&l)[P + 1])
+  {
+    if constexpr (NC == 2)
+      {
+        const float2 v = *reinterpret_cast<const float2 *>(c + q * NC);
+        l[0] = v.x;
+        l[1] = v.y;
+      }
+    else
+      {
+        float tmp[NC];
+#pragma unroll
+        for (int h = 0; h < NC; h += 4)
+          {
+            const float4 v = *reinterpret_cast<const float4 *>(c + q * NC + h);
+            tmp[h] = v.x;
+            tmp[h + 1] = v.y;
+            tmp[h + 2] = v.z;
+            tmp[h + 3] = v.w;
+          }
+#pragma unroll
+        for (int k = 0; k <= P; ++k)
+          l[k] = tmp[k];
+      }
   }
 
   // Forward and backward substitution of one banded LDL^T system of n
-  // unknowns stored at line[q * stride] (in place), with the factors
-  // c[q * (P+1) + k-1] = l_{q,q-k} and c[q * (P+1) + P] = 1/d_q; the backward
-  // sweep stops at position stop. Chunks of four positions: the loads of a
-  // chunk are issued before its dependent chain.
-  template <int P, int n, int stride, int stop>
+  // unknowns stored at line[q * stride] (in place), with the factor rows of
+  // ldl_row; the backward sweep stops at the chunk holding position stop.
+  // Chunks of four positions: the loads of a chunk are issued before its
+  // dependent chain; with stride 1 a chunk is one 16-byte access.
+  template <int P, int NC, int n, int stride, int stop>
   __device__ __forceinline__ void
   ldl_solve(float *line, const float *c)
   {
-    constexpr int NC = P + 1, CH = 4;
+    static_assert(n % 4 == 0, "whole chunks");
+    constexpr int CH = 4;
+    auto load4 = [&](int q0, float (&v)[CH]) {
+      if constexpr (stride == 1)
+        {
+          const float4 t = *reinterpret_cast<const float4 *>(line + q0);
+          v[0] = t.x;
+          v[1] = t.y;
+          v[2] = t.z;
+          v[3] = t.w;
+        }
+      else
+        {
+#pragma unroll
+          for (int u = 0; u < CH; ++u)
+            v[u] = line[(q0 + u) * stride];
+        }
+    };
+    auto store4 = [&](int q0, const float (&v)[CH]) {
+      if constexpr (stride == 1)
+        *reinterpret_cast<float4 *>(line + q0) = make_float4(v[0], v[1], v[2], v[3]);
+      else
+        {
+#pragma unroll
+          for (int u = 0; u < CH; ++u)
+            line[(q0 + u) * stride] = v[u];
+        }
+    };
     float y[P];
 #pragma unroll
     for (int k = 0; k < P; ++k)
@@ -1259,15 +1329,11 @@ namespace lbfem_gpu
 #pragma unroll 2
     for (int q0 = 0; q0 < n; q0 += CH)
       {
-        float v[CH], l[CH][NC];
+        float v[CH], l[CH][P + 1];
+        load4(q0, v);
 #pragma unroll
         for (int u = 0; u < CH; ++u)
-          {
-            v[u] = line[(q0 + u) * stride];
-#pragma unroll
-            for (int k = 0; k < NC; ++k)
-              l[u][k] = c[(q0 + u) * NC + k];
-          }
+          ldl_row<P, NC>(c, q0 + u, l[u]);
 #pragma unroll
         for (int u = 0; u < CH; ++u)
           {
@@ -1281,25 +1347,26 @@ namespace lbfem_gpu
             y[0] = t;
             v[u] = t * l[u][P];
           }
-#pragma unroll
-        for (int u = 0; u < CH; ++u)
-          line[(q0 + u) * stride] = v[u];
+        store4(q0, v);
       }
 #pragma unroll
     for (int k = 0; k < P; ++k)
       y[k] = 0.f; // y[k]: the value k + 1 positions ahead
 #pragma unroll 2
-    for (int q0 = n - CH; q0 >= stop; q0 -= CH)
+    for (int q0 = n - CH; q0 + CH > stop; q0 -= CH) // the last chunk may reach below stop
       {
-        float v[CH], l[CH + P][P];
-#pragma unroll
-        for (int u = 0; u < CH; ++u)
-          v[u] = line[(q0 + u) * stride];
+        float v[CH], l[CH + P][P + 1];
+        load4(q0, v);
 #pragma unroll
         for (int u = 0; u < CH + P; ++u)
+          {
+            if (q0 + u < n)
+              ldl_row<P, NC>(c, q0 + u, l[u]);
+            else
 #pragma unroll
-          for (int k = 0; k < P; ++k)
-            l[u][k] = q0 + u < n ? c[(q0 + u) * NC + k] : 0.f;
+              for (int k = 0; k <= P; ++k)
+                l[u][k] = 0.f;
+          }
 #pragma unroll
         for (int u = CH - 1; u >= 0; --u)
           {
@@ -1313,84 +1380,210 @@ namespace lbfem_gpu
             y[0] = t;
             v[u] = t;
           }
-#pragma unroll
-        for (int u = 0; u < CH; ++u)
-          line[(q0 + u) * stride] = v[u];
+        store4(q0, v);
       }
   }
 
-  // x <- x + M^{-1} r for the active systems, or for all systems when all is
-  // set (FP32: the correction of one refinement round). lx / ly: window factors
-  // of the x / y tile partitions. Periodic images have identity rows: x += r there.
+  // One refinement round of the mixed-precision mass solve, for the active
+  // systems (all of them when all is set):
+  //   x_out = x_in + M^{-1} r_in   (FP32 window solves),
+  //   r_out = b - A x_out           (FP64 arithmetic on the FP32 values),
+  // with the partial sums b.b, r.r and r.D^{-1}r of each system. The window
+  // solves give the correction on the own nodes and on a halo of P nodes, so
+  // that A x_out follows without another pass; the halo's correction is the
+  // window solve's own, within a few 1e-8 of the neighbouring tile's. An
+  // inactive system is copied (x_out = x_in, r_out = r_in): all systems end a
+  // round in the same buffers. x and r are never updated in place (the halos
+  // read the inputs). Periodic images have identity rows.
   template <int P>
-  __global__ void __launch_bounds__(WinShape<P>::THREADS)
+  __global__ void __launch_bounds__(WinShape<P>::THREADS, 2)
     k_window_correct(const Geo geo, const float *__restrict__ lx, const float *__restrict__ ly,
-                     const float *__restrict__ r, float *__restrict__ x, const CgState *__restrict__ st, int all)
+                     const float *__restrict__ r_in, const float *__restrict__ x_in, const float *__restrict__ b,
+                     float *__restrict__ x_out, float *__restrict__ r_out, const CgState *__restrict__ st, int all,
+                     double *__restrict__ partials)
   {
     using S = WinShape<P>;
-    constexpr int W = S::W, FX = S::FX, FY = S::FY, PF = S::PF, NC = S::NC;
+    constexpr int W = S::W, FX = S::FX, FY = S::FY, PF = S::PF, NC = S::NC, K = S::K, NT = S::THREADS;
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    float *s_w = reinterpret_cast<float *>(sm_raw); // [FY][PF] the window
-    __shared__ float s_lx[FX * NC], s_ly[FY * NC];  // factors (apart from the window: no aliasing)
-    __shared__ int s_col[FX], s_row[FY];            // storage column / row, -1 outside the grid
+    float *s_w = reinterpret_cast<float *>(sm_raw);                  // [FY][PF] the window
+    double *s_my = reinterpret_cast<double *>(s_w + PF * FY);       // [TY][K] My rows of the own rows
+    __shared__ __align__(16) float s_lx[FX * NC], s_ly[FY * NC];     // factors (apart from the window: no aliasing)
+    __shared__ int s_col[FX], s_row[FY];                             // storage column / row, -1 outside the grid
+    __shared__ double s_ijy[S::TY];                                  // inverse Jacobi factors of the own rows
     const int s = blockIdx.z;
-    if (!all && !st->active[s])
-      return;
     const Grid &g = geo.g;
     const long long N = g.N;
     const int gx0 = blockIdx.x * S::TX, gy0 = blockIdx.y * S::TY;
     const int tid = threadIdx.x;
+    const int n_tiles = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
+    const float *rs = r_in + (long long)s * N, *xs = x_in + (long long)s * N, *bs = b + (long long)s * N;
+    float *xo = x_out + (long long)s * N, *ro = r_out + (long long)s * N;
+    double part[3] = {0, 0, 0};
+    if (!all && !st->active[s])
+      {
+        // converged: carried over to the output buffers
+        for (int t = tid; t < S::TX * S::TY; t += NT)
+          {
+            const int i = t / S::TX, j = t - i * S::TX;
+            const int gx = gx0 + j, gy = gy0 + i;
+            if (gx < g.nfx && gy < g.nfy)
+              {
+                const long long idx = (long long)gy * g.nfx + gx;
+                xo[idx] = xs[idx];
+                ro[idx] = rs[idx];
+              }
+          }
+        block_reduce_store_n<3, NT>(part, partials + (long long)s * n_tiles, tile, NM * n_tiles);
+        return;
+      }
     const float *lxt = lx + (size_t)blockIdx.x * FX * NC, *lyt = ly + (size_t)blockIdx.y * FY * NC;
-    for (int t = tid; t < FX * NC; t += S::THREADS)
+    for (int t = tid; t < FX * NC; t += NT)
       s_lx[t] = lxt[t];
-    for (int t = tid; t < FY * NC; t += S::THREADS)
+    for (int t = tid; t < FY * NC; t += NT)
       s_ly[t] = lyt[t];
-    for (int t = tid; t < FX; t += S::THREADS)
+    for (int t = tid; t < FX; t += NT)
       s_col[t] = wrap(gx0 - W + t, g.px, g.nux, g.nfx);
-    for (int t = tid; t < FY; t += S::THREADS)
+    for (int t = tid; t < FY; t += NT)
       s_row[t] = wrap(gy0 - W + t, g.py, g.nuy, g.nfy);
+    for (int t = tid; t < S::TY * K; t += NT)
+      {
+        const int i = t / K, k = t - i * K, gy = gy0 + i;
+        s_my[t] = (gy < g.nfy && !(g.py && gy == g.nuy)) ? geo.rowy[(long long)gy * K + k] : 0.0;
+      }
+    for (int t = tid; t < S::TY; t += NT)
+      s_ijy[t] = gy0 + t < g.nfy ? geo.ijy[gy0 + t] : 0.0;
     __syncthreads();
-    const float *rs = r + (long long)s * N;
-    // the window by asynchronous copies (all in flight at once), and this
-    // thread's own column of x into registers meanwhile
-    for (int t = tid; t < FX * FY; t += S::THREADS)
+    // the window of r_in by asynchronous copies, all in flight at once; meanwhile
+    // this thread's column of x_in (own rows and a halo of P) and of b into registers
+    for (int t = tid; t < FX * FY; t += NT)
       {
         const int q = t / FX, c = t - q * FX;
         const int row = s_row[q], col = s_col[c];
         const bool ok = row >= 0 && col >= 0;
         cp_async4(&s_w[q * PF + c], ok ? rs + ((long long)row * g.nfx + col) : rs, ok);
       }
-    const int gx = gx0 + tid;
-    float *xs = x + (long long)s * N;
-    float xo[S::TY];
+    const int cw = W - P + tid; // window column of this thread's y solve
+    float xr[S::TY + 2 * P];
+    {
+      const int col = tid < S::TX + 2 * P ? s_col[cw] : -1;
 #pragma unroll
-    for (int i = 0; i < S::TY; ++i)
-      {
-        const int gy = gy0 + i;
-        xo[i] = (gx < g.nfx && gy < g.nfy) ? xs[(long long)gy * g.nfx + gx] : 0.f;
-      }
+      for (int q = 0; q < S::TY + 2 * P; ++q)
+        {
+          const int row = s_row[W - P + q];
+          xr[q] = (row >= 0 && col >= 0) ? xs[(long long)row * g.nfx + col] : 0.f;
+        }
+    }
     cp_async_wait_all();
     __syncthreads();
-    // x solves: one thread per window row (the y solves read the own columns only)
+    // x solves: one thread per window row (the y solves read the own columns and a halo of P)
     if (tid < FY)
-      ldl_solve<P, FX, 1, W>(s_w + tid * PF, s_lx);
+      ldl_solve<P, NC, FX, 1, W - P>(s_w + tid * PF, s_lx);
     __syncthreads();
-    // y solves: one thread per own column, then the own nodes of that column
-    ldl_solve<P, FY, PF, W>(s_w + W + tid, s_ly);
-    if (gx < g.nfx)
+    // y solves: one thread per own-or-halo column, then x_out = x_in + z on the
+    // own rows and a halo of P rows of that column (kept in the window)
+    if (tid < S::TX + 2 * P)
       {
+        ldl_solve<P, NC, FY, PF, W - P>(s_w + cw, s_ly);
+        const int col = s_col[cw];
 #pragma unroll
-        for (int i = 0; i < S::TY; ++i)
+        for (int q = 0; q < S::TY + 2 * P; ++q)
           {
-            const int gy = gy0 + i;
-            if (gy < g.nfy)
-              {
-                const long long idx = (long long)gy * g.nfx + gx;
-                const float z = is_image(gx, gy, g) ? rs[idx] : s_w[(W + i) * PF + W + tid];
-                xs[idx] = xo[i] + z;
-              }
+            const int row = s_row[W - P + q];
+            float *w = &s_w[(W - P + q) * PF + cw];
+            *w = (row >= 0 && col >= 0) ? xr[q] + *w : 0.f;
           }
       }
+    __syncthreads();
+    // own columns: write x_out, form r_out = b - A x_out in FP64
+    if (tid < S::TX)
+      {
+        const int j = tid, gx = gx0 + j, c = W + j;
+        const bool col_ok = gx < g.nfx;
+        const bool img_col = g.px && gx == g.nux;
+        double mx[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          mx[k] = (col_ok && !img_col) ? geo.rowx[(long long)gx * K + k] : 0.0;
+        const double ijx = col_ok ? geo.ijx[gx] : 0.0;
+        // this column of b in batches of BR rows, the next batch in flight while one is used
+        constexpr int BR = 16;
+        static_assert(S::TY % BR == 0, "whole batches");
+        float bn[BR];
+        auto load_b = [&](int i0) {
+#pragma unroll
+          for (int u = 0; u < BR; ++u)
+            bn[u] = (col_ok && gy0 + i0 + u < g.nfy) ? bs[(long long)(gy0 + i0 + u) * g.nfx + gx] : 0.f;
+        };
+        load_b(0);
+        // t[k] = (Mx x)(row i - P + k) of this column, a sliding window of 2P + 1 rows;
+        // each row's sum in two independent halves (shorter FP64 dependency chains)
+        double t[K];
+        auto xrow = [&](int q) -> double {
+          const float *w = &s_w[q * PF + c - P];
+          double v0 = mx[0] * double(w[0]), v1 = mx[1] * double(w[1]);
+#pragma unroll
+          for (int l = 2; l < K; l += 2)
+            {
+              v0 = fma(mx[l], double(w[l]), v0);
+              if (l + 1 < K)
+                v1 = fma(mx[l + 1], double(w[l + 1]), v1);
+            }
+          return v0 + v1;
+        };
+#pragma unroll
+        for (int k = 1; k < K; ++k)
+          t[k] = xrow(W - P + k - 1);
+#pragma unroll 1
+        for (int i0 = 0; i0 < S::TY; i0 += BR)
+        {
+        float bc[BR];
+#pragma unroll
+        for (int u = 0; u < BR; ++u)
+          bc[u] = bn[u];
+        if (i0 + BR < S::TY)
+          load_b(i0 + BR);
+#pragma unroll
+        for (int u = 0; u < BR; ++u)
+          {
+            const int i = i0 + u;
+#pragma unroll
+            for (int k = 0; k < K - 1; ++k)
+              t[k] = t[k + 1];
+            t[K - 1] = xrow(W + i + P);
+            const int gy = gy0 + i;
+            if (!col_ok || gy >= g.nfy)
+              continue;
+            const long long idx = (long long)gy * g.nfx + gx;
+            const bool image = img_col || (g.py && gy == g.nuy);
+            double xv, ax;
+            if (image)
+              {
+                xv = double(xs[idx]) + double(rs[idx]); // identity rows
+                ax = xv;
+              }
+            else
+              {
+                xv = s_w[(W + i) * PF + c];
+                double a0 = s_my[i * K] * t[0], a1 = s_my[i * K + 1] * t[1];
+#pragma unroll
+                for (int k = 2; k < K; k += 2)
+                  {
+                    a0 = fma(s_my[i * K + k], t[k], a0);
+                    if (k + 1 < K)
+                      a1 = fma(s_my[i * K + k + 1], t[k + 1], a1);
+                  }
+                ax = a0 + a1;
+              }
+            const double bb = bc[u], rr = bb - ax;
+            xo[idx] = float(xv);
+            ro[idx] = float(rr);
+            part[0] += bb * bb;
+            part[1] += rr * rr;
+            part[2] += rr * ((image ? 1.0 : ijx * s_ijy[i]) * rr);
+          }
+        }
+      }
+    block_reduce_store_n<3, NT>(part, partials + (long long)s * n_tiles, tile, NM * n_tiles);
   }
 
   // The scalar work of one CG phase, one thread per system, from the reduced sums.
@@ -1464,6 +1657,93 @@ namespace lbfem_gpu
         st->n_active = n;
         if (phase == 2)
           ++st->iter;
+      }
+  }
+
+  // ------------------------------------------------- device-side step control
+  // Graph control after a CG phase: the loop goes on while a system is active
+  // and no failure occurred; on exit the solve is folded into the counters.
+  __global__ void
+  k_cg_control(const CgState *__restrict__ st, DevStats *__restrict__ ds, cudaGraphConditionalHandle h, int in_body)
+  {
+    if (threadIdx.x != 0)
+      return;
+    const bool go = st->n_active > 0 && st->status == 0;
+    if (in_body)
+      ++ds->bodies;
+    if (!go)
+      {
+        ds->its += st->total_its;
+        if (st->status != 0 && ds->sticky == 0)
+          ds->sticky = st->status;
+      }
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+  }
+
+  // The bookkeeping of one round of the mixed-precision mass solve, after the
+  // round's correction kernel and the reduction of its sums [bb, rr, rz]: a
+  // corrected system whose residual meets tol stops; a round that halves no
+  // active residual means the tolerance lies below the FP32 resolution of the
+  // solution (status 4); round max_rounds is the cap (status 2). Corrections
+  // are counted; use_h: sets the graph loop condition.
+  __global__ void
+  k_mixed_round(CgState *__restrict__ st, const double *__restrict__ sums, DevStats *__restrict__ ds, int nsys,
+                double tol, int max_rounds, cudaGraphConditionalHandle h, int use_h)
+  {
+    __shared__ int corrected[NM], progress[NM];
+    const int s = threadIdx.x;
+    const int round = st->iter;
+    if (s < NM)
+      {
+        corrected[s] = s < nsys && (round == 0 || st->active[s]);
+        progress[s] = 0;
+        if (corrected[s] && st->status == 0)
+          {
+            const double res = sqrt(sums[NM + s]), tv = tol * sqrt(sums[s]);
+            st->tol[s] = tv;
+            if (isnan(res))
+              {
+                st->active[s] = 0;
+                atomicExch(&st->status, 3); // LBFEM_ERR_NONFINITE
+              }
+            else
+              {
+                st->active[s] = res > tv ? 1 : 0;
+                progress[s] = st->active[s] && (round == 0 || res <= 0.5 * st->res[s]);
+              }
+            st->res[s] = res;
+          }
+        else if (!corrected[s])
+          st->active[s] = 0;
+      }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      {
+        int n = 0, nc = 0, np = 0;
+        for (int k = 0; k < NM; ++k)
+          {
+            n += st->active[k];
+            nc += corrected[k];
+            np += progress[k];
+          }
+        st->total_its += nc;
+        if (ds)
+          ds->its += nc;
+        ++st->iter;
+        if (st->status == 0 && n > 0 && np == 0)
+          st->status = 4; // stagnation
+        else if (st->status == 0 && n > 0 && st->iter >= max_rounds)
+          st->status = 2; // LBFEM_ERR_NO_CONVERGENCE
+        st->n_active = st->status ? 0 : n;
+        if (ds)
+          {
+            if (round > 0 && nc > 0)
+              ++ds->bodies;
+            if (st->status != 0 && ds->sticky == 0)
+              ds->sticky = st->status;
+          }
+        if (use_h)
+          cudaGraphSetConditional(h, st->n_active > 0 ? 1u : 0u);
       }
   }
 } // namespace lbfem_gpu

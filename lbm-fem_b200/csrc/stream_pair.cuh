@@ -8,10 +8,11 @@
 //   k1 = ex, k3 = ey flip sign; c ex^2, -2 c ex ey, c ey^2, c ex ey do not.
 // The kernel stages each pair as float2 {u_a, u_abar} and runs the x and y
 // passes with packed FP32 arithmetic (fma.rn.f32x2, sm_100): one instruction,
-// one shared-memory access and one barrier serve two populations. The
-// equilibria of a pair share their even part:
+// one shared-memory access and one barrier serve two populations. In the
+// Lee-Lin right-hand side the equilibria of a pair share their even part:
 //   feq_a - w = E + O, feq_abar - w = E - O,
-//   E = w (drho + rho (4.5 (e.u)^2 - 1.5 u.u)), O = 3 w rho e.u.
+//   E = w (drho + rho (4.5 (e.u)^2 - 1.5 u.u)), O = 3 w rho e.u;
+// the Bardow collision, which writes the state, takes each population's own.
 // Storage is the FP32 deviation d = f - w (advection annihilates constants).
 #pragma once
 
@@ -373,9 +374,11 @@ namespace lbfem_gpu
   // Images get r = 0 (constrained rows).
   template <int P, int MODE>
   __global__ void __launch_bounds__(THREADS, 2)
-    k_stream_pair(const Geo geo, const float *__restrict__ d, float *__restrict__ dout, float *__restrict__ rhs,
-                  const AdvCoef ac)
+    k_stream_pair(const Geo geo, const DevStats *__restrict__ ds, const float *__restrict__ d,
+                  float *__restrict__ dout, float *__restrict__ rhs, const AdvCoef ac)
   {
+    if (ds && ds->sticky)
+      return; // a step after a failed solve: the populations must stay as they are
     using T = Tile<P>;
     constexpr bool BARDOW = MODE == PAIR_BARDOW;
     extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -542,16 +545,10 @@ namespace lbfem_gpu
                     const float2 gv = s_u[st];
                     const MomF mo{s_m[st], s_m[T::NF + st], s_m[2 * T::NF + st], s_m[3 * T::NF + st]};
                     const MomF mt = impose_class(mo, s_wall[st], geo);
-                    auto even_odd = [&](const MomF &m, float &E, float &O) {
-                      const float eu = fmaf(ey, m.uy, ex * m.ux), reu = m.rho * eu;
-                      E = w * fmaf(4.5f * reu, eu, m.drho - 1.5f * m.rho * (m.ux * m.ux + m.uy * m.uy));
-                      O = 3.f * w * reu;
-                    };
-                    float E, O, Et, Ot;
-                    even_odd(mo, E, O);
-                    even_odd(mt, Et, Ot);
-                    gs = fma2(bc(1.f - omega), add2(gv, make_float2(-(E + O), -(E - O))),
-                              make_float2(Et + Ot, Et - Ot));
+                    // each population's own equilibrium: the collision writes the state, and the
+                    // rounding of the even +- odd form accumulates there from step to step
+                    gs.x = feqd_a(a, mt) + (1.f - omega) * (gv.x - feqd_a(a, mo));
+                    gs.y = feqd_a(ab, mt) + (1.f - omega) * (gv.y - feqd_a(ab, mo));
                     const int gx = gx0 - P + fx, gy = gy0 - P + fy;
                     if (fx >= P && fx < P + T::TX && fy >= P && fy < P + T::TY && gx < g.nfx && gy < g.nfy &&
                         !is_image(gx, gy, g))

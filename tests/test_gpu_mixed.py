@@ -51,7 +51,7 @@ def test_mixed_population_roundtrip(gpu_lib):
 
 
 @pytest.mark.parametrize("scheme,mass,case,p,n,steps,cfl", [
-    ("bardow", "cg", "tgv", 2, 32, 400, 0.4),
+    ("bardow", "cg", "cavity", 2, 32, 400, 0.4),
     ("leelin", "cg", "tgv", 3, 16, 200, 0.5),
     ("bardow", "lumped", "cavity", 2, 16, 400, 0.4),
     ("leelin", "cg", "couette", 1, 16, 600, 0.25),

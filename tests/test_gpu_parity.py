@@ -194,3 +194,40 @@ def test_dof_permutation(gpu_lib):
     g.step(20)
     out = g.get_populations()
     assert np.array_equal(out[:, perm], ref.get_populations())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_step_failure_leaves_the_populations(gpu_lib, precision):
+    """A solver failure inside graph-launched steps: step raises NoConvergence
+    (the reference's SolverControl::NoConvergence out of Scheme::step), and the
+    populations are those before the failing step."""
+    tc = cases.TaylorGreenVortex(0.05 / math.sqrt(d2q9.CS2), 1, 1, shift=(0.25, 0.25), chapman_enskog=False)
+    tc.set_reynolds(100)
+    m = cases.build_mesh(tc, 16, 1)
+    dt, lam = m.time_step(0.4), tc.relaxation_time()
+    if precision == "fp64":
+        prm = make_params("bardow", "cg", cg_tolerance=1e-14, cg_max_iterations=1)
+    else:  # a tolerance below the FP32 resolution of the solution: the rounds stagnate
+        prm = make_params("bardow", "cg", precision="mixed", mixed_tolerance=1e-12)
+    g = setup_case(_gpu, tc, m, prm, dt, lam)
+    before = g.get_populations()
+    with pytest.raises(_abi.NoConvergence):
+        g.step(3)
+    assert np.array_equal(g.get_populations(), before)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_steps_match_host_driven_steps(gpu_lib, precision, monkeypatch):
+    """The graph-launched steps (device-side solver loops) and the host-driven
+    steps (LBFEM_TRACE) run the same kernels in the same order: bitwise equal."""
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    tc.set_reynolds(400)
+    m = cases.build_mesh(tc, 12, 2)
+    dt, lam = m.time_step(0.4), tc.relaxation_time()
+    prm = make_params("leelin", "cg", cg_tolerance=1e-10, precision=precision)
+    g = setup_case(_gpu, tc, m, prm, dt, lam)
+    monkeypatch.setenv("LBFEM_TRACE", "1")
+    h = setup_case(_gpu, tc, m, prm, dt, lam)
+    g.step(7)
+    h.step(7)
+    assert np.array_equal(g.get_populations(), h.get_populations())
