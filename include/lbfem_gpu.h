@@ -243,6 +243,25 @@ int lbfem_gpu_advection_resident(lbfem_gpu_ctx *ctx);
 int lbfem_gpu_last_step_stats(const lbfem_gpu_ctx *ctx, double *cg_iterations_per_solve, int64_t *kernel_launches);
 
 /*
+ * Batched stepping of independent instances (contexts of any mesh, degree,
+ * scheme and precision on one device). lbfem_gpu_batch_step advances every
+ * instance by n_steps steps; each step of all instances is one CUDA graph
+ * launch, whose independent branches are the instances' own step graphs, so
+ * small instances run side by side on the GPU. Results are those of
+ * lbfem_gpu_step on each context. A solver failure in any instance is returned
+ * (the lowest instance index, its message in lbfem_gpu_batch_last_error); that
+ * instance stays as before its failing step, the others complete all steps.
+ * The contexts must have their time step set and must not be stepped through
+ * another call while a batch call runs. No counterpart in the reference (one
+ * instance per run, cgdbe.cc).
+ */
+typedef struct lbfem_gpu_batch lbfem_gpu_batch;
+int lbfem_gpu_batch_create(lbfem_gpu_ctx *const *ctxs, int32_t n_ctxs, lbfem_gpu_batch **batch);
+int lbfem_gpu_batch_step(lbfem_gpu_batch *batch, int32_t n_steps);
+const char *lbfem_gpu_batch_last_error(const lbfem_gpu_batch *batch);
+int lbfem_gpu_batch_destroy(lbfem_gpu_batch *batch);
+
+/*
  * The mass solve of lbfem_gpu_mass_solve (consistent mass, Jacobi-PCG) for
  * callers that cannot allocate device memory at the time of the call: for
  * example code that runs while a CUDA stream is being captured, or a host

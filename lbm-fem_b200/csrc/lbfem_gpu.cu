@@ -74,6 +74,7 @@ struct lbfem_gpu_ctx
     int64_t fixed = 0, body = 0; // kernels outside the solver loop, kernels per loop body
   };
   std::map<int, StepGraph> graphs;
+  int64_t graph_epoch = 0; // counts the invalidations of the step graphs (batch graphs embed them)
   cudaStream_t cap = nullptr;     // captures the loop bodies
   DevStats *d_stats = nullptr, *h_stats = nullptr;
   std::string err;
@@ -773,7 +774,7 @@ namespace
     cudaGraph_t graph = nullptr;
     CK(cudaStreamGetCaptureInfo_v3(ctx->stream, &cs, nullptr, &graph, nullptr, nullptr, nullptr));
     cudaGraphConditionalHandle h;
-    CK(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
+    CK(cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault)); // 0 at every launch
     CK(cudaMemsetAsync(ctx->d_cg, 0, sizeof(CgState), ctx->stream));
     int n_tiles = 0;
     int st = with_degree(ctx->P, [&](auto PP) -> int {
@@ -852,7 +853,7 @@ namespace
     cudaGraph_t graph = nullptr;
     CK(cudaStreamGetCaptureInfo_v3(ctx->stream, &cs, nullptr, &graph, nullptr, nullptr, nullptr));
     cudaGraphConditionalHandle h;
-    CK(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
+    CK(cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault)); // 0 at every launch
     CK(cudaMemsetAsync(ctx->d_cg, 0, sizeof(CgState), ctx->stream));
     int st = with_degree(ctx->P, [&](auto PP) -> int {
       constexpr int P = decltype(PP)::value;
@@ -927,21 +928,23 @@ namespace
     return ctx->cur * 9 + ctx->x_cur * 3 + ctx->x_prev;
   }
 
-  // Captures and instantiates the step graph of the current buffer state.
+  // Records one step of the current buffer state on ctx->stream, which is being
+  // captured (into a step graph of its own or into a batch graph); the buffer
+  // state is left as it was. *fixed: the kernels outside the solver loop; *body:
+  // the kernels of one loop body.
   int
-  capture_step(lbfem_gpu_ctx *ctx, lbfem_gpu_ctx::StepGraph &sg)
+  record_step(lbfem_gpu_ctx *ctx, int64_t *fixed, int64_t *body)
   {
     const int cur0 = ctx->cur, c0 = ctx->x_cur, p0 = ctx->x_prev, n0 = ctx->x_new;
     const int64_t l0 = ctx->launches;
-    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    int64_t body = 0;
+    *body = 0;
     int st = step_front(ctx);
     if (!st)
       {
         if (ctx->prm.mass != LBFEM_MASS_CG)
           st = lumped_solve(ctx);
         else
-          st = ctx->mixed ? mixed_graph(ctx, &body) : cg_graph(ctx, &body);
+          st = ctx->mixed ? mixed_graph(ctx, body) : cg_graph(ctx, body);
       }
     if (!st)
       {
@@ -950,14 +953,24 @@ namespace
           ctx->cur = 1 - ctx->cur; // step_back flips it again
         st = step_back(ctx);
       }
-    cudaGraph_t graph = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
-    const int64_t total = ctx->launches - l0;
+    *fixed = ctx->launches - l0 - *body;
     ctx->cur = cur0;
     ctx->x_cur = c0;
     ctx->x_prev = p0;
     ctx->x_new = n0;
     ctx->launches = l0;
+    return st;
+  }
+
+  // Captures and instantiates the step graph of the current buffer state.
+  int
+  capture_step(lbfem_gpu_ctx *ctx, lbfem_gpu_ctx::StepGraph &sg)
+  {
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int64_t fixed = 0, body = 0;
+    const int st = record_step(ctx, &fixed, &body);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
     if (st || e != cudaSuccess)
       {
         if (graph)
@@ -968,10 +981,45 @@ namespace
     cudaGraphDestroy(graph);
     if (ei != cudaSuccess)
       return fail(ctx, LBFEM_ERR_CUDA, "step graph instantiation: %s", cudaGetErrorString(ei));
-    sg.fixed = total - body;
+    sg.fixed = fixed;
     sg.body = body;
     return LBFEM_OK;
   }
+
+  // The buffer state and counters of a context before a run of graph-launched steps.
+  struct RunStart
+  {
+    DevStats stats;
+    int cur, x_cur, x_prev, x_new;
+    int64_t fixed = 0, body = 0; // kernels of the launched steps outside the loops; per loop body
+  };
+
+  RunStart
+  run_start(const lbfem_gpu_ctx *ctx, const DevStats &stats)
+  {
+    RunStart r{};
+    r.stats = stats;
+    r.cur = ctx->cur;
+    r.x_cur = ctx->x_cur;
+    r.x_prev = ctx->x_prev;
+    r.x_new = ctx->x_new;
+    return r;
+  }
+
+  // The step graph of the current buffer state (captured on first use).
+  int
+  current_step_graph(lbfem_gpu_ctx *ctx, lbfem_gpu_ctx::StepGraph **out)
+  {
+    auto &sg = ctx->graphs[graph_key(ctx)];
+    int st;
+    if (!sg.exec && (st = capture_step(ctx, sg)))
+      return st;
+    *out = &sg;
+    return LBFEM_OK;
+  }
+
+  int finish_run(lbfem_gpu_ctx *ctx, const RunStart &r0, const DevStats &after, int64_t *its_total,
+                 int64_t *launches);
 
   // n steps as graph launches, with one synchronisation at the end.
   int
@@ -979,25 +1027,32 @@ namespace
   {
     CK(cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    const DevStats before = *ctx->h_stats;
-    const int cur0 = ctx->cur, c0 = ctx->x_cur, p0 = ctx->x_prev, n0 = ctx->x_new;
-    int64_t fixed = 0, body = 0;
+    RunStart r0 = run_start(ctx, *ctx->h_stats);
     for (int k = 0; k < n; ++k)
       {
-        auto &sg = ctx->graphs[graph_key(ctx)];
+        lbfem_gpu_ctx::StepGraph *sg;
         int st;
-        if (!sg.exec && (st = capture_step(ctx, sg)))
+        if ((st = current_step_graph(ctx, &sg)))
           return st;
-        CK(cudaGraphLaunch(sg.exec, ctx->stream));
-        fixed += sg.fixed;
-        body = sg.body;
+        CK(cudaGraphLaunch(sg->exec, ctx->stream));
+        r0.fixed += sg->fixed;
+        r0.body = sg->body;
         rotate_after_step(ctx);
       }
     CK(cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    const DevStats after = *ctx->h_stats;
+    return finish_run(ctx, r0, *ctx->h_stats, its_total, launches);
+  }
+
+  // After a run: the counters, and on a failure the buffer state of the completed steps, a
+  // restarted extrapolation history and the failure's status.
+  int
+  finish_run(lbfem_gpu_ctx *ctx, const RunStart &r0, const DevStats &after, int64_t *its_total, int64_t *launches)
+  {
+    const DevStats &before = r0.stats;
+    const int cur0 = r0.cur, c0 = r0.x_cur, p0 = r0.x_prev, n0 = r0.x_new;
     *its_total = int64_t(after.its - before.its);
-    *launches = fixed + int64_t(after.bodies - before.bodies) * body;
+    *launches = r0.fixed + int64_t(after.bodies - before.bodies) * r0.body;
     if (after.sticky)
       {
         // the steps after the failing one did nothing: put the buffer state back to
@@ -1417,6 +1472,7 @@ lbfem_gpu_set_time_step(lbfem_gpu_ctx *ctx, double dt, double lambda)
     if (kv.second.exec)
       cudaGraphExecDestroy(kv.second.exec);
   ctx->graphs.clear();
+  ++ctx->graph_epoch;
   return LBFEM_OK;
 }
 
@@ -1814,6 +1870,239 @@ lbfem_gpu_last_step_stats(const lbfem_gpu_ctx *ctx, double *its, int64_t *launch
   if (launches)
     *launches = ctx->last_launches;
   return LBFEM_OK;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched stepping: one graph launch per step of all instances, whose steps are
+// independent branches of the graph (no edges between them).
+struct lbfem_gpu_batch
+{
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  std::vector<lbfem_gpu_ctx *> ctxs;
+  struct Entry
+  {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int64_t> epochs;      // the time-step epochs of the instances it was recorded with
+    std::vector<int64_t> fixed, body; // per instance: kernels outside the loops, per loop body
+  };
+  std::map<std::vector<int>, Entry> graphs; // by the buffer states of the instances
+  DevStats *h_stats = nullptr;              // pinned, one per instance
+  std::string err;
+};
+
+namespace
+{
+  int
+  batch_fail(lbfem_gpu_batch *b, int status, const char *fmt, ...)
+  {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    b->err = buf;
+    return status;
+  }
+
+#define BCK(call)                                                                                         \
+  do                                                                                                      \
+    {                                                                                                     \
+      const cudaError_t e_ = (call);                                                                      \
+      if (e_ != cudaSuccess)                                                                              \
+        return batch_fail(b, LBFEM_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    }                                                                                                     \
+  while (0)
+
+  // The batch graph of the instances' current buffer states: one capture in
+  // which every instance's step is recorded on its own stream, forked from and
+  // joined to the batch stream, so the instances are independent branches
+  // (recorded on first use, again when an instance's time step changed).
+  int
+  batch_graph(lbfem_gpu_batch *b, lbfem_gpu_batch::Entry **out)
+  {
+    std::vector<int> key;
+    std::vector<int64_t> epochs;
+    for (auto *c : b->ctxs)
+      {
+        key.push_back(graph_key(c));
+        epochs.push_back(c->graph_epoch);
+      }
+    auto &e = b->graphs[key];
+    if (e.exec && e.epochs == epochs)
+      {
+        *out = &e;
+        return LBFEM_OK;
+      }
+    if (e.exec)
+      {
+        cudaGraphExecDestroy(e.exec);
+        e.exec = nullptr;
+      }
+    e.fixed.assign(b->ctxs.size(), 0);
+    e.body.assign(b->ctxs.size(), 0);
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int st = LBFEM_OK;
+    cudaError_t ce = cudaEventRecord(b->fork, b->stream);
+    for (size_t k = 0; k < b->ctxs.size() && !st && ce == cudaSuccess; ++k)
+      {
+        lbfem_gpu_ctx *c = b->ctxs[k];
+        ce = cudaStreamWaitEvent(c->stream, b->fork, 0);
+        if (ce != cudaSuccess)
+          break;
+        if ((st = record_step(c, &e.fixed[k], &e.body[k])))
+          {
+            batch_fail(b, st, "instance %zu: %s", k, c->err.c_str());
+            break;
+          }
+        if ((ce = cudaEventRecord(b->join, c->stream)) == cudaSuccess)
+          ce = cudaStreamWaitEvent(b->stream, b->join, 0);
+      }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(b->stream, &graph);
+    if (st || ce != cudaSuccess || ee != cudaSuccess)
+      {
+        if (graph)
+          cudaGraphDestroy(graph);
+        if (st)
+          return st;
+        return batch_fail(b, LBFEM_ERR_CUDA, "batch capture: %s",
+                          cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+      }
+    const cudaError_t ei = cudaGraphInstantiate(&e.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess)
+      {
+        e.exec = nullptr;
+        return batch_fail(b, LBFEM_ERR_CUDA, "batch graph instantiation: %s", cudaGetErrorString(ei));
+      }
+    e.epochs = epochs;
+    *out = &e;
+    return LBFEM_OK;
+  }
+} // namespace
+
+extern "C" {
+
+int
+lbfem_gpu_batch_create(lbfem_gpu_ctx *const *ctxs, int32_t n, lbfem_gpu_batch **out)
+{
+  if (!ctxs || n < 1 || !out)
+    return LBFEM_ERR_ARG;
+  *out = nullptr;
+  for (int k = 0; k < n; ++k)
+    {
+      if (!ctxs[k])
+        return LBFEM_ERR_ARG;
+      if (ctxs[k]->device != ctxs[0]->device)
+        return LBFEM_ERR_UNSUPPORTED;
+      for (int j = 0; j < k; ++j)
+        if (ctxs[j] == ctxs[k])
+          return LBFEM_ERR_ARG;
+    }
+  auto b = std::make_unique<lbfem_gpu_batch>();
+  b->device = ctxs[0]->device;
+  b->ctxs.assign(ctxs, ctxs + n);
+  if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess ||
+      cudaHostAlloc(&b->h_stats, sizeof(DevStats) * n, cudaHostAllocDefault) != cudaSuccess)
+    {
+      cudaGetLastError();
+      lbfem_gpu_batch_destroy(b.release());
+      return LBFEM_ERR_CUDA;
+    }
+  *out = b.release();
+  return LBFEM_OK;
+}
+
+const char *
+lbfem_gpu_batch_last_error(const lbfem_gpu_batch *b)
+{
+  return b ? b->err.c_str() : "";
+}
+
+int
+lbfem_gpu_batch_destroy(lbfem_gpu_batch *b)
+{
+  if (!b)
+    return LBFEM_OK;
+  cudaSetDevice(b->device);
+  if (b->stream)
+    cudaStreamSynchronize(b->stream);
+  for (auto &kv : b->graphs)
+    if (kv.second.exec)
+      cudaGraphExecDestroy(kv.second.exec);
+  if (b->h_stats)
+    cudaFreeHost(b->h_stats);
+  if (b->fork)
+    cudaEventDestroy(b->fork);
+  if (b->join)
+    cudaEventDestroy(b->join);
+  if (b->stream)
+    cudaStreamDestroy(b->stream);
+  delete b;
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_batch_step(lbfem_gpu_batch *b, int32_t n_steps)
+{
+  if (!b)
+    return LBFEM_ERR_ARG;
+  if (n_steps < 0)
+    return batch_fail(b, LBFEM_ERR_ARG, "batch_step: negative count");
+  BCK(cudaSetDevice(b->device));
+  const size_t n = b->ctxs.size();
+  for (size_t k = 0; k < n; ++k)
+    {
+      lbfem_gpu_ctx *c = b->ctxs[k];
+      if (!c->have_ts)
+        return batch_fail(b, LBFEM_ERR_STATE, "instance %zu: step needs the time step", k);
+      // the instance's own queued work first, then its counters
+      BCK(cudaStreamSynchronize(c->stream));
+      BCK(cudaMemcpy(&b->h_stats[k], c->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost));
+    }
+  std::vector<RunStart> r0;
+  for (size_t k = 0; k < n; ++k)
+    r0.push_back(run_start(b->ctxs[k], b->h_stats[k]));
+  for (int s = 0; s < n_steps; ++s)
+    {
+      lbfem_gpu_batch::Entry *e;
+      int st;
+      if ((st = batch_graph(b, &e)))
+        return st;
+      BCK(cudaGraphLaunch(e->exec, b->stream));
+      for (size_t k = 0; k < n; ++k)
+        {
+          r0[k].fixed += e->fixed[k];
+          r0[k].body = e->body[k];
+          rotate_after_step(b->ctxs[k]);
+        }
+    }
+  for (size_t k = 0; k < n; ++k)
+    BCK(cudaMemcpyAsync(&b->h_stats[k], b->ctxs[k]->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  int first = LBFEM_OK;
+  for (size_t k = 0; k < n; ++k)
+    {
+      lbfem_gpu_ctx *c = b->ctxs[k];
+      int64_t its = 0, launched = 0;
+      const int st = finish_run(c, r0[k], b->h_stats[k], &its, &launched);
+      c->cg_its += its;
+      c->launches += launched;
+      c->last_launches = launched;
+      c->last_its_per_solve = n_steps > 0 ? double(its) / (double(n_steps) * NM) : 0.0;
+      if (st && first == LBFEM_OK)
+        {
+          first = st;
+          batch_fail(b, st, "instance %zu: %s", k, c->err.c_str());
+        }
+    }
+  return first;
 }
 
 } // extern "C"

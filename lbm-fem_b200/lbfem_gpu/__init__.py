@@ -64,4 +64,50 @@ class Solver:
         return Handle(library(), "lbfem_gpu_", mesh, params, dof_index=dof_index)
 
 
-__all__ = ["Solver", "cases", "d2q9", "make_params", "LbfemError", "NoConvergence", "library", "device_count"]
+class Batch:
+    """Independent instances (Solver handles on one device) stepped together:
+    each step of all of them is one graph launch (lbfem_gpu_batch_step). The
+    handles stay usable on their own; keep them alive while the batch is."""
+
+    def __init__(self, solvers):
+        from ._abi import LbfemError
+
+        self.lib = library()
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s.h.value for s in self.solvers])
+        fn = self.lib.lbfem_gpu_batch_create
+        fn.restype, fn.argtypes = C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]
+        h = C.c_void_p()
+        st = fn(arr, len(self.solvers), C.byref(h))
+        if st != 0:
+            raise LbfemError(st, "lbfem_gpu_batch_create")
+        self.h = h
+        self.lib.lbfem_gpu_batch_last_error.restype = C.c_char_p
+        self.lib.lbfem_gpu_batch_last_error.argtypes = [C.c_void_p]
+
+    def step(self, n=1):
+        from ._abi import LBFEM_ERR_NO_CONVERGENCE, LbfemError, NoConvergence
+
+        fn = self.lib.lbfem_gpu_batch_step
+        fn.restype, fn.argtypes = C.c_int, [C.c_void_p, C.c_int32]
+        st = fn(self.h, int(n))
+        if st != 0:
+            msg = self.lib.lbfem_gpu_batch_last_error(self.h).decode()
+            raise (NoConvergence if st == LBFEM_ERR_NO_CONVERGENCE else LbfemError)(st, f"lbfem_gpu_batch_step: {msg}")
+
+    def close(self):
+        if getattr(self, "h", None) is not None:
+            fn = self.lib.lbfem_gpu_batch_destroy
+            fn.restype, fn.argtypes = C.c_int, [C.c_void_p]
+            fn(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+__all__ = ["Solver", "Batch", "cases", "d2q9", "make_params", "LbfemError", "NoConvergence", "library",
+           "device_count"]

@@ -1,0 +1,67 @@
+"""Batched stepping of independent instances (lbfem_gpu_batch_step): every
+instance ends where lbfem_gpu_step alone takes it, bitwise; a failing instance
+is reported and left as before its failing step while the others finish."""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import setup_case
+from lbfem_gpu import cases, d2q9, make_params
+
+pytestmark = pytest.mark.gpu
+
+
+def _instances():
+    """Uneven instances: cavities and Taylor-Green vortices, p = 1, 2, both schemes and precisions."""
+    out = []
+    table = [("cavity", 12, 2, "bardow", "fp64"), ("tgv", 16, 1, "leelin", "mixed"), ("cavity", 20, 1, "leelin", "fp64"),
+             ("tgv", 10, 2, "bardow", "mixed"), ("cavity", 8, 2, "bardow", "mixed"), ("tgv", 24, 1, "bardow", "fp64")]
+    for case, n, p, scheme, precision in table:
+        if case == "tgv":
+            tc = cases.TaylorGreenVortex(0.05 / math.sqrt(d2q9.CS2), 1, 1, shift=(0.25, 0.25), chapman_enskog=False)
+            tc.set_reynolds(100)
+        else:
+            tc = cases.LidDrivenCavity(0.1, 1.2)
+            tc.set_reynolds(400)
+        m = cases.build_mesh(tc, n, p)
+        out.append((tc, m, make_params(scheme, "cg", cg_tolerance=1e-10, precision=precision), m.time_step(0.4)))
+    return out
+
+
+def test_batch_matches_single_instances(gpu_lib):
+    import lbfem_gpu
+
+    batch_handles, single_handles = [], []
+    for tc, m, prm, dt in _instances():
+        batch_handles.append(setup_case(lbfem_gpu.Solver, tc, m, prm, dt, tc.relaxation_time()))
+        single_handles.append(setup_case(lbfem_gpu.Solver, tc, m, prm, dt, tc.relaxation_time()))
+    b = lbfem_gpu.Batch(batch_handles)
+    b.step(5)
+    b.step(4)  # a second call continues (the buffer states differ per instance)
+    for h in single_handles:
+        h.step(9)
+    for hb, hs in zip(batch_handles, single_handles):
+        assert np.array_equal(hb.get_populations(), hs.get_populations())
+    b.close()
+
+
+def test_batch_failure_of_one_instance(gpu_lib):
+    import lbfem_gpu
+
+    inst = _instances()[:3]
+    handles = []
+    for k, (tc, m, prm, dt) in enumerate(inst):
+        if k == 1:  # an iteration cap of one in an FP64 solve at 1e-14: fails at its first step
+            prm = make_params("bardow", "cg", cg_tolerance=1e-14, cg_max_iterations=1)
+        handles.append(setup_case(lbfem_gpu.Solver, tc, m, prm, dt, tc.relaxation_time()))
+    before = handles[1].get_populations()
+    ref = setup_case(lbfem_gpu.Solver, inst[2][0], inst[2][1], inst[2][2], inst[2][3], inst[2][0].relaxation_time())
+    ref.step(3)
+    b = lbfem_gpu.Batch(handles)
+    with pytest.raises(lbfem_gpu.NoConvergence) as ei:
+        b.step(3)
+    assert "instance 1" in str(ei.value)
+    assert np.array_equal(handles[1].get_populations(), before)
+    assert np.array_equal(handles[2].get_populations(), ref.get_populations())
+    b.close()
