@@ -91,7 +91,7 @@ typedef struct lbfem_mesh_desc {
 typedef struct lbfem_params {
   int32_t scheme;                /* LBFEM_SCHEME_* */
   int32_t mass;                  /* LBFEM_MASS_* */
-  int32_t richardson;            /* passes of LBFEM_MASS_RICHARDSON (reference default 2) */
+  int32_t richardson;            /* passes of LBFEM_MASS_RICHARDSON after the lumped start (reference default 2) */
   int32_t streaming;             /* LBFEM_STREAMING_* (TG2 implemented) */
   int32_t precision;             /* LBFEM_PRECISION_* */
   int32_t cg_max_iterations;     /* reference default 200 */
@@ -177,8 +177,9 @@ int lbfem_gpu_advection(lbfem_gpu_ctx *ctx, const double *f, const double *feq, 
  * MassSolver::solve (mass.h:185-213): x <- A^{-1} r with A = M (+ tg3 K_e(e),
  * not implemented: tg3_coefficient must be 0). One block of n_dofs values.
  * CG starts from x (input) and stops at |r - A x| <= cg_tolerance |r|;
- * lumped and Richardson overwrite x. Returns LBFEM_ERR_NO_CONVERGENCE when the
- * iteration cap is hit (x then holds the last iterate). Host buffers.
+ * lumped and Richardson (x = M_L^{-1} r, then `richardson` passes
+ * x += M_L^{-1} (r - M x)) overwrite x. Returns LBFEM_ERR_NO_CONVERGENCE when
+ * the iteration cap is hit (x then holds the last iterate). Host buffers.
  */
 int lbfem_gpu_mass_solve(lbfem_gpu_ctx *ctx, double *x, const double *r, const double *e, double tg3_coefficient);
 

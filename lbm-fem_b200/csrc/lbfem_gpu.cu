@@ -201,7 +201,9 @@ namespace
         (st = set_smem(ctx, k_cg_p<P, double>, cg_smem<P, double>(0))) ||
         (st = set_smem(ctx, k_cg_update<P, double>, cg_smem<P, double>(2))) ||
         (st = set_smem(ctx, k_cg_start<P, float, float, float>, cg_smem<P, float>(1))) ||
-        (st = set_smem(ctx, k_window_correct<P>, window_smem<P>())))
+        (st = set_smem(ctx, k_window_correct<P>, window_smem<P>())) ||
+        (st = set_smem(ctx, k_richardson_pass<P, double>, cg_smem<P, double>(0))) ||
+        (st = set_smem(ctx, k_richardson_pass<P, float>, cg_smem<P, float>(0))))
       return st;
     return LBFEM_OK;
   }
@@ -556,6 +558,37 @@ namespace
     return LBFEM_OK;
   }
 
+  // The iterated lumping of MassSolver::solve (mass.h:193-202): x = M_L^{-1} b, then
+  // prm.richardson passes x += M_L^{-1} (b - M x). The passes alternate between
+  // out and scratch; the result is in out (an odd count ends with a copy-free
+  // swap of the roles: the first pass reads out and writes scratch).
+  template <typename R>
+  int
+  richardson_passes(lbfem_gpu_ctx *ctx, const R *b, R *out, R *scratch, int nsys)
+  {
+    const Geo geo = geo_of(ctx);
+    const int k = ctx->prm.richardson;
+    R *first = (k % 2) ? scratch : out; // the lumped start, so that the last pass writes out
+    k_lumped<R, R><<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo, b, first, nsys);
+    LAUNCHED();
+    R *in = first, *to = first == out ? scratch : out;
+    for (int j = 0; j < k; ++j)
+      {
+        const int st = with_degree(ctx->P, [&](auto PP) -> int {
+          constexpr int P = decltype(PP)::value;
+          dim3 grid = tile_grid<P>(ctx->grid);
+          grid.z = nsys;
+          k_richardson_pass<P, R><<<grid, THREADS, cg_smem<P, R>(0), ctx->stream>>>(geo, b, in, to);
+          LAUNCHED();
+          return LBFEM_OK;
+        });
+        if (st)
+          return st;
+        std::swap(in, to);
+      }
+    return LBFEM_OK;
+  }
+
   int
   mass_solve_dev(lbfem_gpu_ctx *ctx, const double *b, double *x_new, const double *x_cur, const double *x_prev,
                  int extrapolate, int nsys, int64_t *its)
@@ -569,8 +602,14 @@ namespace
           *its = 0;
         return LBFEM_OK;
       }
-    if (ctx->prm.mass != LBFEM_MASS_CG)
-      return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass solve: only cg and lumped are implemented");
+    if (ctx->prm.mass == LBFEM_MASS_RICHARDSON)
+      {
+        // x_new <- the passes (the start in x_new is not used, as in the reference)
+        int st = richardson_passes<double>(ctx, b, x_new, ctx->d_v, nsys);
+        if (its)
+          *its = 0;
+        return st;
+      }
     return cg_solve(ctx, b, x_new, x_cur, x_prev, extrapolate, nsys, its);
   }
 
@@ -671,12 +710,17 @@ namespace
     return LBFEM_OK;
   }
 
-  // The lumped solve x_cur = M_L^{-1} rhs (no history).
+  // The lumped solve x_cur = M_L^{-1} rhs, or the iterated lumping into x_cur with
+  // x_new's buffer as scratch (no history either way).
   int
   lumped_solve(lbfem_gpu_ctx *ctx)
   {
     const Geo geo = geo_of(ctx);
     const int nb = n_pointwise_blocks(ctx->grid.N);
+    if (ctx->prm.mass == LBFEM_MASS_RICHARDSON)
+      return ctx->mixed ? richardson_passes<float>(ctx, ctx->d_rhs_s, ctx->d_x_s[ctx->x_cur],
+                                                   ctx->d_x_s[ctx->x_new], NM)
+                        : richardson_passes<double>(ctx, ctx->d_rhs, ctx->d_x[ctx->x_cur], ctx->d_x[ctx->x_new], NM);
     if (ctx->mixed)
       k_lumped<float, float><<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_rhs_s, ctx->d_x_s[ctx->x_cur], NM);
     else
@@ -1232,8 +1276,10 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
     return LBFEM_ERR_ARG;
   if (prm->streaming != LBFEM_STREAMING_TG2 ||
       (prm->precision != LBFEM_PRECISION_FP64 && prm->precision != LBFEM_PRECISION_MIXED) ||
-      (prm->mass != LBFEM_MASS_CG && prm->mass != LBFEM_MASS_LUMPED))
+      (prm->mass != LBFEM_MASS_CG && prm->mass != LBFEM_MASS_LUMPED && prm->mass != LBFEM_MASS_RICHARDSON))
     return LBFEM_ERR_UNSUPPORTED;
+  if (prm->mass == LBFEM_MASS_RICHARDSON && prm->richardson < 0)
+    return LBFEM_ERR_ARG;
   if (!(prm->cg_tolerance >= 0) || prm->cg_max_iterations < 1 || !(prm->mixed_tolerance >= 0))
     return LBFEM_ERR_ARG;
   const int P = m->degree;

@@ -1057,6 +1057,37 @@ namespace lbfem_gpu
       }
   }
 
+  // ---------------------------------------- iterated lumping (Richardson)
+  // One Richardson pass of MassSolver::solve with Mass::richardson (mass.h:193-202):
+  // x_out = x_in + M_L^{-1} (b - M x_in) for nsys systems (grid.z), constrained
+  // rows the identity. x_in is read with a halo, so x_out is another buffer.
+  template <int P, typename R>
+  __global__ void __launch_bounds__(THREADS)
+    k_richardson_pass(const Geo geo, const R *__restrict__ b, const R *__restrict__ x_in, R *__restrict__ x_out)
+  {
+    using T = Tile<P>;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    R *s_u = reinterpret_cast<R *>(sm_raw), *s_t = s_u + T::NF;
+    __shared__ TileMaps<P, R> maps;
+    const Grid &g = geo.g;
+    const long long o = (long long)blockIdx.z * g.N;
+    const int gx0 = blockIdx.x * T::TX, gy0 = blockIdx.y * T::TY;
+    build_maps<P>(maps, geo, gx0, gy0);
+    __syncthreads();
+    const R *xs = x_in + o, *bs = b + o;
+    R *xo = x_out + o;
+    stage<P>(s_u, maps, [&](long long idx) { return xs[idx]; });
+    __syncthreads();
+    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, int idx, bool image, R Ax) {
+      const R xv = image ? xs[idx] : s_u[(i + P) * T::PF + j + P];
+      if (image)
+        Ax = xv;
+      const int gx = gx0 + j, gy = gy0 + i;
+      const R inv = R(image ? 1.0 : geo.ilx[gx] * geo.ily[gy]);
+      xo[idx] = xv + inv * (bs[idx] - Ax);
+    });
+  }
+
   // ------------------------------------------- Jacobi-PCG, 8 systems at once (K3)
   // deal.II SolverCG (mass.h:204-211), one state per system. With mixed
   // precision the vectors are FP32, the inner iterations run in FP32 with FP64

@@ -54,6 +54,7 @@ def test_mixed_population_roundtrip(gpu_lib):
     ("bardow", "cg", "cavity", 2, 32, 400, 0.4),
     ("leelin", "cg", "tgv", 3, 16, 200, 0.5),
     ("bardow", "lumped", "cavity", 2, 16, 400, 0.4),
+    ("bardow", "richardson", "cavity", 2, 16, 400, 0.4),
     ("leelin", "cg", "couette", 1, 16, 600, 0.25),
     ("bardow", "cg", "cavity", 1, 24, 300, 0.4),
 ])

@@ -80,7 +80,7 @@ def test_mass_operator(gpu_lib, oracle_mod, name, tc, _p, n, p):
 
 @pytest.mark.parametrize("name,tc,_p,n", MESHES, ids=[m[0] for m in MESHES])
 @pytest.mark.parametrize("p", [1, 2])
-@pytest.mark.parametrize("mass", ["cg", "lumped"])
+@pytest.mark.parametrize("mass", ["cg", "lumped", "richardson"])
 def test_mass_solve(gpu_lib, oracle_mod, name, tc, _p, n, p, mass):
     m = cases.build_mesh(tc, n, p)
     prm = make_params(mass=mass, cg_tolerance=1e-13)
@@ -132,6 +132,8 @@ def _run_pair(oracle_mod, tc, m, prm, dt, steps, lam=None):
     ("bardow", "cg", "cavity", 1, 12, 60),
     ("leelin", "lumped", "cavity", 3, 5, 40),
     ("bardow", "cg", "couette", 3, 4, 40),
+    ("bardow", "richardson", "cavity", 2, 10, 60),
+    ("leelin", "richardson", "tgv", 1, 16, 50),
 ])
 def test_step(gpu_lib, oracle_mod, scheme, mass, case, p, n, steps):
     if case == "tgv":
@@ -231,3 +233,15 @@ def test_graph_steps_match_host_driven_steps(gpu_lib, precision, monkeypatch):
     g.step(7)
     h.step(7)
     assert np.array_equal(g.get_populations(), h.get_populations())
+
+
+@pytest.mark.parametrize("passes", [0, 1, 2, 3])
+def test_richardson_passes(gpu_lib, oracle_mod, passes):
+    """--mass richardson[k] (mass.h:193-202): k = 0 is the lumped solve; odd and even k
+    end in the same buffer; each agrees with the oracle."""
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    tc.set_reynolds(400)
+    m = cases.build_mesh(tc, 8, 2)
+    prm = make_params("bardow", "richardson", richardson=passes)
+    g, o = _run_pair(oracle_mod, tc, m, prm, m.time_step(0.3), 30)
+    assert rel_l2(g.get_populations(), o.get_populations()) <= 1e-12
