@@ -149,6 +149,17 @@ int lbfem_gpu_set_initial_populations(lbfem_gpu_ctx *ctx, const double *f);
 int lbfem_gpu_set_populations(lbfem_gpu_ctx *ctx, const double *f);
 int lbfem_gpu_get_populations(lbfem_gpu_ctx *ctx, double *f);
 
+/*
+ * Raw checkpoints of Scheme::f in the reference's format (io.h:137-165,
+ * write_checkpoint / read_checkpoint): the file name.rank holds the 9 blocks
+ * of n_dofs FP64 values one after the other, in the caller's DoF numbering. It
+ * is written to name.rank.tmp and renamed, never leaving a torn file. A file
+ * of another size is rejected (LBFEM_ERR_ARG). Valid for the same mesh and
+ * numbering; Bardow's transformed populations also assume the same dt.
+ */
+int lbfem_gpu_write_checkpoint(lbfem_gpu_ctx *ctx, const char *name, int32_t rank);
+int lbfem_gpu_read_checkpoint(lbfem_gpu_ctx *ctx, const char *name, int32_t rank);
+
 /* Scheme::step (LeeLin schemes.h:92-98, Bardow schemes.h:118-124), n_steps times, device-resident. */
 int lbfem_gpu_step(lbfem_gpu_ctx *ctx, int32_t n_steps);
 

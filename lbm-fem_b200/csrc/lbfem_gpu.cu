@@ -1136,6 +1136,46 @@ namespace
   }
 } // namespace
 
+
+namespace
+{
+  // The raw population checkpoint shared by write and read (io.h:137-165).
+  std::string
+  checkpoint_path(const char *name, int32_t rank)
+  {
+    return std::string(name) + "." + std::to_string(rank);
+  }
+
+  int
+  write_raw(const std::string &file, const std::vector<double> &f)
+  {
+    const std::string tmp = file + ".tmp";
+    FILE *out = std::fopen(tmp.c_str(), "wb");
+    if (!out)
+      return LBFEM_ERR_ARG;
+    const size_t n = std::fwrite(f.data(), sizeof(double), f.size(), out);
+    const int closed = std::fclose(out);
+    if (n != f.size() || closed != 0 || std::rename(tmp.c_str(), file.c_str()) != 0)
+      {
+        std::remove(tmp.c_str());
+        return LBFEM_ERR_ARG;
+      }
+    return LBFEM_OK;
+  }
+
+  int
+  read_raw(const std::string &file, std::vector<double> &f)
+  {
+    FILE *in = std::fopen(file.c_str(), "rb");
+    if (!in)
+      return LBFEM_ERR_ARG;
+    const size_t n = std::fread(f.data(), sizeof(double), f.size(), in);
+    const bool more = std::fgetc(in) != EOF;
+    std::fclose(in);
+    return n == f.size() && !more ? LBFEM_OK : LBFEM_ERR_ARG;
+  }
+} // namespace
+
 extern "C" {
 
 void
@@ -1556,6 +1596,39 @@ lbfem_gpu_get_populations(lbfem_gpu_ctx *ctx, double *f)
       LAUNCHED();
     }
   return download(ctx, ctx->d_f[ctx->cur], f, Q);
+}
+
+int
+lbfem_gpu_write_checkpoint(lbfem_gpu_ctx *ctx, const char *name, int32_t rank)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!name || rank < 0)
+    return fail(ctx, LBFEM_ERR_ARG, "write_checkpoint: bad argument");
+  std::vector<double> f(size_t(Q) * ctx->n_dofs);
+  if ((st = lbfem_gpu_get_populations(ctx, f.data())))
+    return st;
+  const std::string file = checkpoint_path(name, rank);
+  if ((st = write_raw(file, f)))
+    return fail(ctx, st, "write_checkpoint: cannot write %s", file.c_str());
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_read_checkpoint(lbfem_gpu_ctx *ctx, const char *name, int32_t rank)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!name || rank < 0)
+    return fail(ctx, LBFEM_ERR_ARG, "read_checkpoint: bad argument");
+  std::vector<double> f(size_t(Q) * ctx->n_dofs);
+  const std::string file = checkpoint_path(name, rank);
+  if ((st = read_raw(file, f)))
+    return fail(ctx, st, "cannot read checkpoint %s (9 x %lld doubles expected)", file.c_str(),
+                (long long)ctx->n_dofs);
+  return lbfem_gpu_set_populations(ctx, f.data());
 }
 
 int

@@ -143,6 +143,14 @@ class Handle:
         self._call("get_populations", self.h, _dptr(out))
         return out
 
+    def write_checkpoint(self, name, rank=0):
+        """write_checkpoint (io.h:144-154): the raw populations to name.rank."""
+        self._call("write_checkpoint", self.h, str(name).encode(), C.c_int32(rank))
+
+    def read_checkpoint(self, name, rank=0):
+        """read_checkpoint (io.h:156-165)."""
+        self._call("read_checkpoint", self.h, str(name).encode(), C.c_int32(rank))
+
     def step(self, n=1):
         self._call("step", self.h, C.c_int32(n))
 
@@ -222,6 +230,7 @@ def declare(lib, prefix):
         "moments": [vp, dp, dp, dp], "event_record": [vp, i32],
         "event_elapsed": [vp, i32, i32, C.POINTER(C.c_float)], "advection_resident": [vp],
         "last_step_stats": [vp, dp, C.POINTER(i64)],
+        "write_checkpoint": [vp, C.c_char_p, i32], "read_checkpoint": [vp, C.c_char_p, i32],
     }
     for name, args in sig.items():
         fn = getattr(lib, prefix + name, None)

@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -969,6 +970,41 @@ lbfem_oracle_get_populations(lbfem_oracle *h, double *f)
   if (!h || !f)
     return LBFEM_ERR_ARG;
   std::copy(h->f.begin(), h->f.end(), f);
+  return LBFEM_OK;
+}
+
+// write_checkpoint / read_checkpoint (io.h:137-165): name.rank holds the blocks of
+// Scheme::f one after the other (raw FP64), written through name.rank.tmp.
+int
+lbfem_oracle_write_checkpoint(lbfem_oracle *h, const char *name, int32_t rank)
+{
+  if (!h || !name || rank < 0)
+    return LBFEM_ERR_ARG;
+  const std::string file = std::string(name) + "." + std::to_string(rank), tmp = file + ".tmp";
+  FILE *out = std::fopen(tmp.c_str(), "wb");
+  if (!out)
+    return LBFEM_ERR_ARG;
+  const bool ok = std::fwrite(h->f.data(), sizeof(double), h->f.size(), out) == h->f.size();
+  if (std::fclose(out) != 0 || !ok || std::rename(tmp.c_str(), file.c_str()) != 0)
+    return LBFEM_ERR_ARG;
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_read_checkpoint(lbfem_oracle *h, const char *name, int32_t rank)
+{
+  if (!h || !name || rank < 0)
+    return LBFEM_ERR_ARG;
+  const std::string file = std::string(name) + "." + std::to_string(rank);
+  FILE *in = std::fopen(file.c_str(), "rb");
+  if (!in)
+    return LBFEM_ERR_ARG;
+  std::vector<double> f(h->f.size());
+  const bool ok = std::fread(f.data(), sizeof(double), f.size(), in) == f.size() && std::fgetc(in) == EOF;
+  std::fclose(in);
+  if (!ok)
+    return LBFEM_ERR_ARG;
+  h->f = f;
   return LBFEM_OK;
 }
 

@@ -35,6 +35,8 @@ int lbfem_oracle_set_time_step(lbfem_oracle *h, double dt, double lambda);
 int lbfem_oracle_set_initial_populations(lbfem_oracle *h, const double *f);
 int lbfem_oracle_set_populations(lbfem_oracle *h, const double *f);
 int lbfem_oracle_get_populations(lbfem_oracle *h, double *f);
+int lbfem_oracle_write_checkpoint(lbfem_oracle *h, const char *name, int32_t rank);
+int lbfem_oracle_read_checkpoint(lbfem_oracle *h, const char *name, int32_t rank);
 int lbfem_oracle_step(lbfem_oracle *h, int32_t n_steps);
 int lbfem_oracle_advection(lbfem_oracle *h, const double *f, const double *feq, const double *e, double dt,
                            double lambda, int32_t kind, int32_t remove_wall_mass_flux, double *rhs);

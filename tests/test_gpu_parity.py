@@ -245,3 +245,30 @@ def test_richardson_passes(gpu_lib, oracle_mod, passes):
     prm = make_params("bardow", "richardson", richardson=passes)
     g, o = _run_pair(oracle_mod, tc, m, prm, m.time_step(0.3), 30)
     assert rel_l2(g.get_populations(), o.get_populations()) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_checkpoint_restart(gpu_lib, oracle_mod, tmp_path, precision):
+    """write_checkpoint / read_checkpoint (io.h:137-165): a restarted context holds
+    the same populations, and continues to the solver tolerance (the checkpoint,
+    like the reference's, holds f only: the CG start history restarts). The file
+    is the oracle's format."""
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    tc.set_reynolds(400)
+    m = cases.build_mesh(tc, 12, 2)
+    dt, lam = m.time_step(0.4), tc.relaxation_time()
+    prm = make_params("bardow", "cg", cg_tolerance=1e-12, precision=precision)
+    a = setup_case(_gpu, tc, m, prm, dt, lam)
+    a.step(10)
+    name = str(tmp_path / "cavity")
+    a.write_checkpoint(name)
+    b = _gpu(m, prm)
+    b.set_time_step(dt, lam)
+    b.read_checkpoint(name)
+    assert np.array_equal(b.get_populations(), a.get_populations())
+    o = oracle_mod.Oracle(m, make_params("bardow", "cg", cg_tolerance=1e-12))
+    o.read_checkpoint(name)
+    assert np.array_equal(o.get_populations(), a.get_populations())
+    a.step(10)
+    b.step(10)
+    assert rel_l2(b.get_populations(), a.get_populations()) <= (1e-10 if precision == "fp64" else 1e-6)

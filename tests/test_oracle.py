@@ -233,3 +233,23 @@ def test_leelin_q1_checkerboard_stability_limit(oracle_mod, cfl, grows):
         assert a200 > 100 * a100 > 0, (a100, a200)
     else:
         assert a200 < a100 < 1e-9, (a100, a200)  # decays from the 1e-7 seed
+
+
+def test_checkpoint_format(oracle_mod, tmp_path):
+    """write_checkpoint / read_checkpoint (io.h:137-165): name.rank holds the nine
+    blocks of Scheme::f one after the other, raw FP64; a torn or foreign file is refused."""
+    tc, m = tgv(6, p=2)
+    o = setup_case(oracle_mod.Oracle, tc, m, make_params("bardow", "cg"), m.time_step(0.3), tc.relaxation_time())
+    o.step(3)
+    f = o.get_populations()
+    name = str(tmp_path / "state")
+    o.write_checkpoint(name, rank=3)
+    raw = np.fromfile(name + ".3", dtype=np.float64)
+    assert raw.size == 9 * m.n_dofs and np.array_equal(raw.reshape(9, -1), f)
+    assert not os.path.exists(name + ".3.tmp")
+    (2 * f).tofile(name + ".4")
+    o.read_checkpoint(name, rank=4)
+    assert np.array_equal(o.get_populations(), 2 * f)
+    f[:, :5].tofile(name + ".5")
+    with pytest.raises(_abi.LbfemError):
+        o.read_checkpoint(name, rank=5)
