@@ -185,6 +185,13 @@ def run_reference(args):
     return 0
 
 
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the default
+# workload's kernels, from ncu captures on the Q3 512^2 case scaled by the stored nodes
+# (x 3.997); the profiles/ summaries give the commands.
+STREAMING_TRAFFIC = {"fp64": 1147e6, "mixed": 482e6}
+WINDOW_TRAFFIC = 1349e6
+
+
 def mixed_tol(cg_tol):
     """The relative tolerance of the mixed-precision mass solve (LBFEM_MIXED_TOLERANCE = 1e-6)."""
     return max(cg_tol, 1e-6)
@@ -236,27 +243,42 @@ def run_precision(args, precision, tc, mesh, dt, lam, f0, local, pg, world):
     P = C.POINTER(C.c_double)
     h._call("moments", ctx, rho.ctypes.data_as(P), ux.ctypes.data_as(P), uy.ctypes.data_as(P))
 
-    # roofline of the streaming kernel (K1), timed alone on the context's stream
+    # rooflines, each kernel timed alone on the context's stream (CUDA events, 10 launches)
     reps = 10
-    h._call("advection_resident", ctx)
-    lib.lbfem_gpu_synchronize(ctx)
-    h._call("event_record", ctx, 2)
-    for _ in range(reps):
-        h._call("advection_resident", ctx)
-    h._call("event_record", ctx, 3)
-    k1 = elapsed(2, 3) / reps
-    real = 4 if precision == "mixed" else 8
-    n_writes = 8 if args.scheme == "leelin" else 17  # Bardow also writes the collided populations
-    alg_bytes = real * mesh.n_dofs * (9 + n_writes)
     peak, peak_kind = measured_peaks()
-    achieved = alg_bytes / k1 / 1e9
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None,
-            "kernel": (f"k_stream_pair<{args.degree}, {args.scheme}> (FP32, population pairs)" if precision == "mixed"
-                       else f"k_advection<{args.degree}, {args.scheme} fused, double>"),
-            "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": 1e3 * k1,
-            "peak_kind": f"{peak_kind} HBM copy bandwidth (burst)"}
-    out = {"sec": sec, "its": its.value, "launches": int(launches.value), "roofline": roof,
+
+    def timed(entry):
+        h._call(entry, ctx)
+        lib.lbfem_gpu_synchronize(ctx)
+        h._call("event_record", ctx, 2)
+        for _ in range(reps):
+            h._call(entry, ctx)
+        h._call("event_record", ctx, 3)
+        return elapsed(2, 3) / reps
+
+    def roofline(kernel, alg_bytes, t, traffic):
+        achieved = alg_bytes / t / 1e9
+        return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": kernel, "algorithmic_bytes_per_launch": alg_bytes,
+                "launch_ms": 1e3 * t, "peak_kind": f"{peak_kind} HBM copy bandwidth (burst)"}
+
+    # the streaming kernel (K1): reads f (9 arrays), writes r (8; Bardow also the 9 collided populations)
+    real = 4 if precision == "mixed" else 8
+    n_writes = 8 if args.scheme == "leelin" else 17
+    default_workload = args.cells == 1024 and args.degree == 3 and args.scheme == "leelin"
+    k1 = roofline(f"k_stream_pair<{args.degree}, {args.scheme}> (FP32, population pairs)" if precision == "mixed"
+                  else f"k_advection<{args.degree}, {args.scheme} fused, double>",
+                  real * mesh.n_dofs * (9 + n_writes), timed("advection_resident"),
+                  (STREAMING_TRAFFIC[precision] if default_workload else None))
+    if precision == "mixed":
+        # the dominant kernel of the mixed step: one round of the mixed solve, 8 systems, reading r, x, b and
+        # writing x, r (FP32)
+        roof = roofline(f"k_window_correct<{args.degree}> (window solve + FP64 residual, 8 systems)",
+                        5 * 4 * 8 * mesh.n_dofs, timed("solve_round_resident"),
+                        WINDOW_TRAFFIC if default_workload else None)
+    else:
+        roof = k1
+    out = {"sec": sec, "its": its.value, "launches": int(launches.value), "roofline": roof, "streaming": k1,
            "clocks": clocks.summary(), "mass": cons[1] / cons[0], "u": np.stack([ux, uy]), "handle": h}
     return out
 
@@ -321,6 +343,7 @@ def run_ours(args):
                                                     "fp64 (Jacobi-PCG)": f64["its"]}),
         "fp64": {"value": units / f64["sec"], "ms_per_step": 1e3 * f64["sec"] / args.steps,
                  "roofline": f64["roofline"], "gpu_launches": f64["launches"]},
+        "streaming_kernel": mix["streaming"],
         "accuracy": {"rel_l2_u_mixed_vs_fp64": rel_u, "target": 1e-5, "mean_density_fp64": f64["mass"],
                      "mean_density_mixed": mix["mass"],
                      "note": f"after {args.warmup + args.steps} steps of both runs from the same initial state"},

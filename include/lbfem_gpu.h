@@ -251,6 +251,15 @@ int lbfem_gpu_event_elapsed(lbfem_gpu_ctx *ctx, int32_t a, int32_t b, float *ms)
  */
 int lbfem_gpu_advection_resident(lbfem_gpu_ctx *ctx);
 
+/*
+ * One refinement round of the mixed-precision mass solve (the window
+ * correction with its FP64 residual, k_window_correct) for all 8 systems, on the
+ * resident right-hand side and solution, into scratch buffers (the solution
+ * history is not touched). For timing and profiling of that kernel; mixed
+ * precision with consistent mass only.
+ */
+int lbfem_gpu_solve_round_resident(lbfem_gpu_ctx *ctx);
+
 /* Statistics of the last lbfem_gpu_step call: CG iterations per solve (mean) and kernel launches. */
 int lbfem_gpu_last_step_stats(const lbfem_gpu_ctx *ctx, double *cg_iterations_per_solve, int64_t *kernel_launches);
 

@@ -59,7 +59,7 @@ namespace lbfem_gpu
   // periodic line, unrolled), an identity row outside a non-periodic axis.
   // Because the rows of M^{-1} decay exponentially, the window solve gives
   // M^{-1} r at the own nodes to about the decay over W nodes (a few 1e-8
-  // relative for W = 12, 18, 24, 28 at p = 1..4).
+  // relative for W = 12, 20, 24, 28 at p = 1..4, a few 1e-6 for W = 8, 12, 16, 20).
   // Layout [tile][q][stride]: l_{q,q-k} for k = 1..p, then 1 / d_q, then zeros
   // up to stride >= p + 1 (a whole vector load per position).
   std::vector<float> window_ldl(const Axis &ax, int T, int W, int n_tiles, int stride);

@@ -1785,6 +1785,28 @@ lbfem_gpu_advection_resident(lbfem_gpu_ctx *ctx)
 }
 
 int
+lbfem_gpu_solve_round_resident(lbfem_gpu_ctx *ctx)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!ctx->mixed || ctx->prm.mass != LBFEM_MASS_CG)
+    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "solve_round_resident: mixed precision with consistent mass only");
+  const Geo geo = geo_of(ctx);
+  const Grid &g = ctx->grid;
+  return with_degree(ctx->P, [&](auto PP) -> int {
+    constexpr int P = decltype(PP)::value;
+    using S = WinShape<P>;
+    const dim3 grid((g.nfx + S::TX - 1) / S::TX, (g.nfy + S::TY - 1) / S::TY, NM);
+    k_window_correct<P><<<grid, S::THREADS, window_smem<P>(), ctx->stream>>>(
+      geo, ctx->d_winx, ctx->d_winy, ctx->d_r_s, ctx->d_x_s[ctx->x_cur], ctx->d_rhs_s, ctx->d_p_s[1], ctx->d_p_s[0],
+      ctx->d_cg, 1, ctx->d_partials);
+    LAUNCHED();
+    return LBFEM_OK;
+  });
+}
+
+int
 lbfem_gpu_mass_solve(lbfem_gpu_ctx *ctx, double *x, const double *r, const double *, double tg3)
 {
   int st;

@@ -1260,11 +1260,13 @@ namespace lbfem_gpu
   // M = My (x) Mx, so M^{-1} = My^{-1} (x) Mx^{-1}. The rows of the 1-D inverses
   // decay exponentially, so M^{-1} r at the own nodes of a tile follows from
   // banded LDL^T solves on a window of W nodes around the tile in each direction
-  // (factors from window_ldl on the host), to a few 1e-8 of |r|.
+  // (factors from window_ldl on the host), to a few 1e-6 of |r|.
   template <int P>
   struct WinShape
   {
-    static constexpr int W = P == 1 ? 12 : P == 2 ? 20 : P == 3 ? 24 : 28;
+    // window halo: the 1-D inverses decay to a few 1e-6 over W nodes; one round's FP64
+    // check then finds the residual at about 1e-5 of the round's start residual
+    static constexpr int W = P == 1 ? 8 : P == 2 ? 12 : P == 3 ? 16 : 20;
     static constexpr int TX = 128, TY = 64;                // own nodes
     static constexpr int FX = TX + 2 * W, FY = TY + 2 * W; // window
     // pitch = 4 (mod 8): rows are 16-byte aligned, and eight lanes on eight rows hit

@@ -229,6 +229,7 @@ def declare(lib, prefix):
         "node_weight": [vp, dp], "jacobi_diagonal": [vp, dp], "conservation": [vp, dp],
         "moments": [vp, dp, dp, dp], "event_record": [vp, i32],
         "event_elapsed": [vp, i32, i32, C.POINTER(C.c_float)], "advection_resident": [vp],
+        "solve_round_resident": [vp],
         "last_step_stats": [vp, dp, C.POINTER(i64)],
         "write_checkpoint": [vp, C.c_char_p, i32], "read_checkpoint": [vp, C.c_char_p, i32],
     }
