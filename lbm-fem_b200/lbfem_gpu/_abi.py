@@ -22,6 +22,7 @@ SCHEME = {"leelin": 0, "bardow": 1}
 MASS = {"cg": 0, "lumped": 1, "richardson": 2}
 PRECISION = {"fp64": 0, "mixed": 1}
 ADVECTION = {"taylor_galerkin": 0, "leelin": 1}
+STREAMING = {"tg2": 0, "tg3": 1, "tg3-split": 2}
 
 _STATUS = {
     0: "ok", 1: "bad argument", 2: "CG did not converge", 3: "non-finite value",
@@ -58,9 +59,9 @@ class Params(C.Structure):
 
 
 def make_params(scheme="bardow", mass="cg", cg_tolerance=1e-8, cg_max_iterations=200, precision="fp64",
-                richardson=2, remove_wall_mass_flux=-1, device=0, mixed_tolerance=0.0):
-    return Params(SCHEME[scheme], MASS[mass], richardson, 0, PRECISION[precision], cg_max_iterations,
-                  cg_tolerance, remove_wall_mass_flux, device, mixed_tolerance)
+                richardson=2, remove_wall_mass_flux=-1, device=0, mixed_tolerance=0.0, streaming="tg2"):
+    return Params(SCHEME[scheme], MASS[mass], richardson, STREAMING[streaming], PRECISION[precision],
+                  cg_max_iterations, cg_tolerance, remove_wall_mass_flux, device, mixed_tolerance)
 
 
 def _dptr(a):

@@ -25,7 +25,8 @@
 //     predictor_corrector (collision.h:105-168).
 //   * TaylorGalerkin::increment / stream with the extrapolated CG start
 //     2 x^n - x^{n-1} (streaming.h:66-100) and the two schemes
-//     (schemes.h:92-98,118-141).
+//     (schemes.h:92-98,118-141); TG3 (A = M + dt^2/6 K_e, StreamingMatrix,
+//     mass.h:57-129) and its x / y split sweeps (streaming.h:41-60,102-121).
 //
 // Cells are processed in four colours (no two cells of a colour share a node)
 // so that the OpenMP scatter-add is race-free; dot products use a fixed chunking
@@ -608,9 +609,92 @@ namespace
         dst[i] = src[i];
   }
 
+  // dst = (M + c K_e) src over the cells, K_e = int (e.grad N)(e.grad N^T):
+  // StreamingMatrix::cell_integral (mass.h:107-129) with coef != 0 -- value
+  // submitted as is, gradient flux c e (e.grad u). Evaluated point by point
+  // (no sum factorisation): the oracle runs it on small meshes only.
+  template <int P>
+  void
+  streaming_cells(const lbfem_oracle &o, const double *src, double *dst, double ex, double ey, double c)
+  {
+    constexpr int n = P + 1;
+    const Basis &B = *o.basis;
+    std::fill(dst, dst + o.N, 0.);
+    for_cells_coloured(o, [&](int cx, int cy) {
+      const double hx = o.vx[cx + 1] - o.vx[cx], hy = o.vy[cy + 1] - o.vy[cy];
+      int64_t idx[n][n];
+      double u[n][n];
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+          {
+            idx[j][i] = o.master(cx * P + i, cy * P + j);
+            u[j][i] = src[idx[j][i]];
+          }
+      double out[n][n] = {};
+      for (int q2 = 0; q2 < n; ++q2)
+        for (int q1 = 0; q1 < n; ++q1)
+          {
+            double v = 0, gx = 0, gy = 0;
+            for (int bb = 0; bb < n; ++bb)
+              for (int aa = 0; aa < n; ++aa)
+                {
+                  v += B.S[q2][bb] * B.S[q1][aa] * u[bb][aa];
+                  gx += B.S[q2][bb] * B.D[q1][aa] * u[bb][aa];
+                  gy += B.D[q2][bb] * B.S[q1][aa] * u[bb][aa];
+                }
+            gx /= hx;
+            gy /= hy;
+            const double JxW = B.qw[q1] * B.qw[q2] * hx * hy;
+            const double eg = ex * gx + ey * gy;
+            const double sv = v * JxW, fx = (c * ex) * eg * JxW, fy = (c * ey) * eg * JxW;
+            for (int bb = 0; bb < n; ++bb)
+              for (int aa = 0; aa < n; ++aa)
+                out[bb][aa] += B.S[q2][bb] * B.S[q1][aa] * sv + B.S[q2][bb] * (B.D[q1][aa] / hx) * fx +
+                               (B.D[q2][bb] / hy) * B.S[q1][aa] * fy;
+          }
+      for (int bb = 0; bb < n; ++bb)
+        for (int aa = 0; aa < n; ++aa)
+          dst[idx[bb][aa]] += out[bb][aa];
+    });
+  }
+
+  // The matrix of the streaming step, A = M + c K_e (MassSolver::with_matrix,
+  // mass.h:219-231): the mass operator for c = 0; constrained rows identity.
+  struct StreamOp
+  {
+    double ex = 0, ey = 0, c = 0;
+  };
+
+  void
+  op_vmult(const lbfem_oracle &o, const StreamOp &A, double *dst, const double *src)
+  {
+    if (A.c == 0.)
+      {
+        mass_vmult(o, dst, src);
+        return;
+      }
+    switch (o.p)
+      {
+        case 1:
+          streaming_cells<1>(o, src, dst, A.ex, A.ey, A.c);
+          break;
+        case 2:
+          streaming_cells<2>(o, src, dst, A.ex, A.ey, A.c);
+          break;
+        case 3:
+          streaming_cells<3>(o, src, dst, A.ex, A.ey, A.c);
+          break;
+        default:
+          streaming_cells<4>(o, src, dst, A.ex, A.ey, A.c);
+      }
+    for (int64_t i = 0; i < o.N; ++i)
+      if (o.constrained[i])
+        dst[i] = src[i];
+  }
+
   // deal.II SolverCG with the Jacobi preconditioner, in its order of updates.
   int
-  cg_solve(lbfem_oracle &o, double *x, const double *b, int64_t *its)
+  cg_solve(lbfem_oracle &o, const StreamOp &A, double *x, const double *b, int64_t *its)
   {
     const int64_t N = o.N;
     double *r = o.cg_r.data(), *p = o.cg_p.data(), *v = o.cg_v.data(), *z = o.cg_z.data();
@@ -620,7 +704,7 @@ namespace
       zero = x[i] == 0.;
     if (!zero)
       {
-        mass_vmult(o, r, x);
+        op_vmult(o, A, r, x);
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < N; ++i)
           r[i] = -r[i] + b[i];
@@ -653,7 +737,7 @@ namespace
           }
         else
           std::copy(z, z + N, p);
-        mass_vmult(o, v, p);
+        op_vmult(o, A, v, p);
         const double pAp = dot(p, v, N);
         const double alpha = rz / pAp;
 #pragma omp parallel for schedule(static)
@@ -674,7 +758,7 @@ namespace
   }
 
   int
-  mass_solve(lbfem_oracle &o, double *x, const double *r)
+  mass_solve(lbfem_oracle &o, double *x, const double *r, const StreamOp &A = {})
   {
     if (o.prm.mass == LBFEM_MASS_LUMPED)
       {
@@ -692,14 +776,14 @@ namespace
           x[i] = inv[i] * r[i];
         for (int k = 0; k < o.prm.richardson; ++k)
           {
-            mass_vmult(o, o.cg_v.data(), x);
+            op_vmult(o, A, o.cg_v.data(), x);
             for (int64_t i = 0; i < o.N; ++i)
               x[i] += inv[i] * (r[i] - o.cg_v[i]);
           }
         return LBFEM_OK;
       }
     int64_t its = 0;
-    const int st = cg_solve(o, x, r, &its);
+    const int st = cg_solve(o, A, x, r, &its);
     o.cg_its += its;
     return st;
   }
@@ -771,21 +855,42 @@ namespace
     });
   }
 
-  int
-  increment(lbfem_oracle &o, const double *f, const double *feq, double a, double b, double c, bool remove_flux)
+  // The directions of the populations in sweep s of the step: D2Q9::e, or
+  // for the split TG3 sweeps D2Q9::e with the other component zeroed
+  // (TaylorGalerkin::axis, streaming.h:107-115).
+  void
+  sweep_directions(const lbfem_oracle &o, int s, double *e)
   {
-    double e[2 * Q];
+    const bool split = o.prm.streaming == LBFEM_STREAMING_TG3_SPLIT;
     for (int k = 0; k < Q; ++k)
       {
-        e[2 * k] = EX[k];
-        e[2 * k + 1] = EY[k];
+        e[2 * k] = split && s == 1 ? 0. : EX[k];
+        e[2 * k + 1] = split && s == 0 ? 0. : EY[k];
       }
+  }
+
+  // TaylorGalerkin::increment (streaming.h:66-85): the right-hand side along
+  // the directions of sweep s, then x_a <- A^{-1} r_a for the populations that
+  // move in the sweep, A = M + tg3 dt^2 K_e(e_a). The CG start is the
+  // extrapolation 2 x^n - x^{n-1} (x0 and x1) unless the step is split, where
+  // each sweep starts from its own previous increment (x0: sweep 0, x1: sweep 1).
+  int
+  increment(lbfem_oracle &o, int s, const double *f, const double *feq, double a, double b, double c,
+            bool remove_flux)
+  {
+    double e[2 * Q];
+    sweep_directions(o, s, e);
     advection(o, f, feq, e, a, b, c, o.dt, remove_flux, o.rhs.data());
-    const bool extrapolate = o.prm.mass == LBFEM_MASS_CG;
+    const bool split = o.prm.streaming == LBFEM_STREAMING_TG3_SPLIT;
+    const bool extrapolate = o.prm.mass == LBFEM_MASS_CG && !split;
+    const double tg3 = o.prm.streaming == LBFEM_STREAMING_TG2 ? 0. : 1. / 6.;
     const int64_t N = o.N;
     for (int al = 0; al < NM; ++al)
       {
-        double *xa = o.x0.data() + al * N, *xb = o.x1.data() + al * N;
+        const double ex = e[2 * (al + 1)], ey = e[2 * (al + 1) + 1];
+        if (ex == 0. && ey == 0.)
+          continue;
+        double *xa = (s == 0 ? o.x0.data() : o.x1.data()) + al * N, *xb = o.x1.data() + al * N;
         if (extrapolate)
           {
             // x[1].block(a).sadd(-1., 2., xa); xa.swap(x[1].block(a)) (streaming.h:76-80)
@@ -793,7 +898,7 @@ namespace
               xb[i] = -xb[i] + 2. * xa[i];
             std::swap_ranges(xa, xa + N, xb);
           }
-        const int st = mass_solve(o, xa, o.rhs.data() + al * N);
+        const int st = mass_solve(o, xa, o.rhs.data() + al * N, StreamOp{ex, ey, tg3 * o.dt * o.dt});
         if (st != LBFEM_OK)
           return st;
       }
@@ -808,18 +913,28 @@ namespace
     const int rm = o.prm.remove_wall_mass_flux;
     if (bardow)
       {
-        // Bardow::step, schemes.h:118-124
+        // Bardow::step, schemes.h:118-124, and TaylorGalerkin::stream,
+        // streaming.h:88-100: f_a += x_a sweep by sweep.
         collide_bgk(o, o.f.data(), o.dt / (o.lambda + 0.5 * o.dt));
-        const int st = increment(o, o.f.data(), nullptr, -o.dt, 0., -0.5 * o.dt * o.dt, rm < 0 ? true : rm != 0);
-        if (st != LBFEM_OK)
-          return st;
-        for (int al = 0; al < NM; ++al)
+        const int n_sweeps = o.prm.streaming == LBFEM_STREAMING_TG3_SPLIT ? 2 : 1;
+        for (int s = 0; s < n_sweeps; ++s)
           {
-            double *fa = o.f.data() + (al + 1) * N;
-            const double *xa = o.x0.data() + al * N;
+            const int st =
+              increment(o, s, o.f.data(), nullptr, -o.dt, 0., -0.5 * o.dt * o.dt, rm < 0 ? true : rm != 0);
+            if (st != LBFEM_OK)
+              return st;
+            double e[2 * Q];
+            sweep_directions(o, s, e);
+            for (int al = 0; al < NM; ++al)
+              {
+                if (e[2 * (al + 1)] == 0. && e[2 * (al + 1) + 1] == 0.)
+                  continue;
+                double *fa = o.f.data() + (al + 1) * N;
+                const double *xa = (s == 0 ? o.x0.data() : o.x1.data()) + al * N;
 #pragma omp parallel for schedule(static)
-            for (int64_t i = 0; i < N; ++i)
-              fa[i] += xa[i];
+                for (int64_t i = 0; i < N; ++i)
+                  fa[i] += xa[i];
+              }
           }
         return LBFEM_OK;
       }
@@ -827,7 +942,7 @@ namespace
     compute_equilibrium(o, o.f.data(), o.feq.data());
     const double bb = -0.5 * o.dt * o.dt / o.lambda;
     const int st =
-      increment(o, o.f.data(), o.feq.data(), -o.dt - bb, bb, -0.5 * o.dt * o.dt, rm < 0 ? false : rm != 0);
+      increment(o, 0, o.f.data(), o.feq.data(), -o.dt - bb, bb, -0.5 * o.dt * o.dt, rm < 0 ? false : rm != 0);
     if (st != LBFEM_OK)
       return st;
     predictor_corrector(o, o.f.data(), o.feq.data(), o.x0.data(), o.dt / o.lambda);
@@ -876,6 +991,11 @@ lbfem_oracle_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_ora
   if (m->degree < 1 || m->degree > MAXP || m->n_cells_x < 1 || m->n_cells_y < 1 || m->dof_index)
     return LBFEM_ERR_ARG;
   if ((m->periodic_x && m->n_cells_x < 2) || (m->periodic_y && m->n_cells_y < 2))
+    return LBFEM_ERR_ARG;
+  // TG3 needs the consistent mass (streaming.h:51-52); Lee-Lin streams with TG2 only (schemes.h:87).
+  if (prm->streaming < LBFEM_STREAMING_TG2 || prm->streaming > LBFEM_STREAMING_TG3_SPLIT)
+    return LBFEM_ERR_ARG;
+  if (prm->streaming != LBFEM_STREAMING_TG2 && (prm->mass != LBFEM_MASS_CG || prm->scheme != LBFEM_SCHEME_BARDOW))
     return LBFEM_ERR_ARG;
   auto o = std::make_unique<lbfem_oracle>();
   o->p = m->degree;
@@ -1073,13 +1193,13 @@ lbfem_oracle_advection(lbfem_oracle *h, const double *f, const double *feq, cons
 }
 
 int
-lbfem_oracle_mass_solve(lbfem_oracle *h, double *x, const double *r, const double *, double tg3)
+lbfem_oracle_mass_solve(lbfem_oracle *h, double *x, const double *r, const double *e, double tg3)
 {
   if (!h || !x || !r)
     return LBFEM_ERR_ARG;
-  if (tg3 != 0.)
-    return LBFEM_ERR_UNSUPPORTED;
-  return mass_solve(*h, x, r);
+  if (tg3 != 0. && !e)
+    return LBFEM_ERR_ARG;
+  return mass_solve(*h, x, r, tg3 != 0. ? StreamOp{e[0], e[1], tg3} : StreamOp{});
 }
 
 int

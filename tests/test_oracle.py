@@ -12,6 +12,7 @@ import pytest
 from conftest import GOLDEN
 from helpers import directions, rel_l2, setup_case, tgv, unit_mesh
 from lbfem_gpu import _abi, cases, d2q9, make_params
+from lbfem_gpu._abi import LbfemError
 
 
 # ------------------------------------------------------------- lattice KATs
@@ -150,6 +151,74 @@ def test_tgv_error_table(oracle_mod, N, scheme, mass, p, expected):
     """docs/results.md:54-59 (modes (1,4), Re 100, CFL 0.25, t = t_ref/4, Ma 0.05), to the printed digits."""
     err = _tgv_error(oracle_mod, N, scheme, mass, p)
     assert float(f"{err:.1e}") == expected, err
+
+
+@pytest.mark.parametrize("N,streaming,cfl,mach,expected,its", [
+    (24, "tg3", 0.25, 0.05, 1.49e-1, None),
+    (32, "tg3", 0.25, 0.05, 6.16e-2, None),
+    (24, "tg3", 1.0, 0.05, 1.04e-1, 5.1),
+    (32, "tg3", 1.0, 0.05, 5.00e-2, 4.9),
+    (24, "tg3-split", 1.0, 0.05, 3.26e-2, None),
+    (32, "tg3-split", 1.0, 0.05, 2.15e-2, None),
+    (48, "tg3-split", 1.0, 0.05, 5.75e-3, None),
+    (24, "tg3-split", 1.0, 1.6 / 24, 5.38e-2, None),
+])
+def test_tg3_error_table(oracle_mod, N, streaming, cfl, mach, expected, its):
+    """docs/results.md:97-107 (TG3 at CFL 0.25 and 1, with the mean CG iterations
+    per solve at CFL 1) and :143-149 (split TG3 at CFL 1, Ma 0.05 and 1.6/N):
+    bardow, consistent mass, modes (1,4), Re 100, t = t_ref/4, to the printed digits."""
+    tc, m = tgv(N, mach=mach)
+    dt, n = cases.run_length(tc, m, cfl, 0.25)
+    o = setup_case(oracle_mod.Oracle, tc, m, make_params("bardow", "cg", streaming=streaming), dt,
+                   tc.relaxation_time())
+    o.step(n)
+    err = cases.diagnostics(tc, m, o.node_weight(), o.get_populations(), n * dt)["rel_l2_u"]
+    assert float(f"{err:.2e}") == expected, err
+    if its is not None:
+        solves = n * (12 if streaming == "tg3-split" else 8)
+        assert round(o.cg_iterations() / solves, 1) == its
+
+
+def test_tg3_operator(oracle_mod):
+    """A = M + c K_e (mass.h:57-129): symmetric, K_e annihilates functions constant
+    along e, and on a uniform periodic Q1 grid at c = h^2/6 along x the x sweep
+    operator is I_x (x) M_y (the 1-D matrix (M_x + K_x/6) of a unit CFL is the
+    identity times h), so A u = h (I (x) M_y) u."""
+    n, h = 8, 1.0 / 8
+    m = unit_mesh(n, 1, h=h)
+    tc, _ = tgv(n)
+    o = setup_case(oracle_mod.Oracle, tc, m, make_params("bardow", "cg", streaming="tg3"), 0.1 * h, 1.0)
+    rng = np.random.default_rng(3)
+    ind = m.master()
+    x, y = m.nodes()
+    # symmetry through the solve: r -> x = A^{-1} r with A symmetric => <A^{-1} r1, r2> = <r1, A^{-1} r2>
+    e = np.array([1.0, -1.0])
+    r1, r2 = rng.standard_normal(m.n_dofs)[ind], rng.standard_normal(m.n_dofs)[ind]
+    x1 = o.mass_solve(r1, e=e, tg3_coefficient=0.3 * h * h)
+    x2 = o.mass_solve(r2, e=e, tg3_coefficient=0.3 * h * h)
+    indep = m.independent()
+    assert abs(x1[indep] @ r2[indep] - r1[indep] @ x2[indep]) < 1e-6 * abs(x1[indep] @ r2[indep])  # CG to 1e-8 of |r|
+    # unit-CFL x sweep: A u = h (I (x) M_y) u  =>  A^{-1} (h (I (x) M_y) u) = u
+    u = np.sin(2 * np.pi * x) * np.cos(4 * np.pi * y) + 0.1 * rng.standard_normal(m.n_dofs)
+    u = u[ind]
+    nfx = m.nfx
+    U = u.reshape(m.nfy, nfx)[:-1, :-1]
+    # (I (x) M_y) u on the periodic grid, M_y = h/6 [1 4 1]
+    myU = h / 6 * (np.roll(U, 1, 0) + 4 * U + np.roll(U, -1, 0))
+    b = np.zeros((m.nfy, nfx))
+    b[:-1, :-1] = h * myU
+    b[-1, :] = b[0, :]
+    b[:, -1] = b[:, 0]
+    got = o.mass_solve(b.ravel(), e=np.array([1.0, 0.0]), tg3_coefficient=h * h / 6)
+    assert np.max(np.abs(got[indep] - u[indep])) < 1e-6 * np.max(np.abs(u))
+
+
+def test_tg3_needs_bardow_and_consistent_mass(oracle_mod):
+    """streaming.h:51-52 (TG3 needs Mass::cg) and schemes.h:87 (Lee-Lin streams with TG2 only)."""
+    tc, m = tgv(8)
+    for scheme, mass in (("bardow", "lumped"), ("bardow", "richardson"), ("leelin", "cg")):
+        with pytest.raises(LbfemError):
+            oracle_mod.Oracle(m, make_params(scheme, mass, streaming="tg3-split"))
 
 
 def test_couette_steady_profile(oracle_mod):
