@@ -92,7 +92,7 @@ typedef struct lbfem_params {
   int32_t scheme;                /* LBFEM_SCHEME_* */
   int32_t mass;                  /* LBFEM_MASS_* */
   int32_t richardson;            /* passes of LBFEM_MASS_RICHARDSON after the lumped start (reference default 2) */
-  int32_t streaming;             /* LBFEM_STREAMING_* (TG2 implemented) */
+  int32_t streaming;             /* LBFEM_STREAMING_*; TG3 and TG3_SPLIT need Bardow, CG and FP64 */
   int32_t precision;             /* LBFEM_PRECISION_* */
   int32_t cg_max_iterations;     /* reference default 200 */
   double cg_tolerance;           /* relative to |r|, reference default 1e-8 */
@@ -185,8 +185,10 @@ int lbfem_gpu_advection(lbfem_gpu_ctx *ctx, const double *f, const double *feq, 
                         double lambda, int32_t kind, int32_t remove_wall_mass_flux, double *rhs);
 
 /*
- * MassSolver::solve (mass.h:185-213): x <- A^{-1} r with A = M (+ tg3 K_e(e),
- * not implemented: tg3_coefficient must be 0). One block of n_dofs values.
+ * MassSolver::solve (mass.h:185-213): x <- A^{-1} r with A = M + tg3 K_e(e),
+ * K_e = int (e.grad N)(e.grad N^T) (StreamingMatrix, mass.h:57-129; e: 2 values,
+ * needed when tg3_coefficient != 0, which CG supports and iterated lumping does
+ * not: LBFEM_ERR_UNSUPPORTED). One block of n_dofs values.
  * CG starts from x (input) and stops at |r - A x| <= cg_tolerance |r|;
  * lumped and Richardson (x = M_L^{-1} r, then `richardson` passes
  * x += M_L^{-1} (r - M x)) overwrite x. Returns LBFEM_ERR_NO_CONVERGENCE when

@@ -248,16 +248,17 @@ namespace lbfem_gpu
     unsigned long long its, bodies, steps_done;
   };
 
-  // The nodal update that completes a step: skipped after a failure (the
-  // populations stay those before the failing step); block 0 counts the step.
+  // The nodal update that completes a step (or a sweep of it): skipped after a
+  // failure (the populations stay those before the failing step); with count,
+  // block 0 counts the step.
   __device__ __forceinline__ bool
-  step_skipped(DevStats *ds)
+  step_skipped(DevStats *ds, bool count = true)
   {
     if (!ds)
       return false;
     if (ds->sticky)
       return true;
-    if (blockIdx.x == 0 && threadIdx.x == 0)
+    if (count && blockIdx.x == 0 && threadIdx.x == 0)
       atomicAdd(&ds->steps_done, 1ULL);
     return false;
   }

@@ -169,12 +169,13 @@ namespace
       }
   }
 
-  template <int P, typename R>
+  template <int P, typename R, bool TG3 = false>
   constexpr size_t
   cg_smem(int own, bool fp64_arith = false)
   {
     using T = Tile<P>;
-    return (fp64_arith ? sizeof(double) : sizeof(R)) * (T::NF + T::NY) + sizeof(R) * own * T::TX * T::TY;
+    return (fp64_arith ? sizeof(double) : sizeof(R)) * (T::NF + op_scratch<P, TG3>()) +
+           sizeof(R) * own * T::TX * T::TY;
   }
 
   template <typename K>
@@ -200,6 +201,9 @@ namespace
         (st = set_smem(ctx, k_cg_start<P, double, double, double>, cg_smem<P, double>(1))) ||
         (st = set_smem(ctx, k_cg_p<P, double>, cg_smem<P, double>(0))) ||
         (st = set_smem(ctx, k_cg_update<P, double>, cg_smem<P, double>(2))) ||
+        (st = set_smem(ctx, k_cg_start<P, double, double, double, true>, cg_smem<P, double, true>(1))) ||
+        (st = set_smem(ctx, k_cg_p<P, double, true>, cg_smem<P, double, true>(0))) ||
+        (st = set_smem(ctx, k_cg_update<P, double, true>, cg_smem<P, double, true>(2))) ||
         (st = set_smem(ctx, k_cg_start<P, float, float, float>, cg_smem<P, float>(1))) ||
         (st = set_smem(ctx, k_window_correct<P>, window_smem<P>())) ||
         (st = set_smem(ctx, k_richardson_pass<P, double>, cg_smem<P, double>(0))) ||
@@ -354,33 +358,98 @@ namespace
     return std::max(p.cg_tolerance, p.mixed_tolerance > 0 ? p.mixed_tolerance : LBFEM_MIXED_TOLERANCE);
   }
 
-  // x_new <- A^{-1} b for nsys systems by Jacobi-PCG in the order of updates of
-  // deal.II SolverCG (mass.h:204-211), from the extrapolated start 2 x_cur -
-  // x_prev or from the given x_new, with the work buffers w. *its_out: CG
-  // iterations summed over the systems.
+  // One FP64 CG solve: x_new <- A^{-1} b for nsys systems, from the extrapolated
+  // start 2 x_cur - x_prev or from the given x_new. A is the mass matrix, or with
+  // tg3 the streaming matrix M + c K_e of each system (sc); the systems of skip
+  // are left alone (populations at rest in a split TG3 sweep).
+  struct CgCall
+  {
+    const double *b = nullptr;
+    double *x_new = nullptr;
+    const double *x_cur = nullptr, *x_prev = nullptr;
+    int extrapolate = 0, nsys = NM;
+    bool tg3 = false;
+    StreamCoef sc{};
+    int skip = 0;
+  };
+
+  template <typename F>
   int
-  cg_run(lbfem_gpu_ctx *ctx, const CgScratch<double> &w, const double *b, double *x_new, const double *x_cur,
-         const double *x_prev, int extrapolate, int nsys, int64_t *its_out)
+  with_op(bool tg3, F &&f)
+  {
+    return tg3 ? f(std::true_type()) : f(std::false_type());
+  }
+
+  // r = b - A x_start and the start sums; *n_tiles: the tiles of one system.
+  int
+  cg_launch_start(lbfem_gpu_ctx *ctx, const CgScratch<double> &w, const CgCall &c, int *n_tiles)
   {
     const Geo geo = geo_of(ctx);
-    const Grid &g = ctx->grid;
+    return with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      dim3 grid = tile_grid<P>(ctx->grid);
+      *n_tiles = int(grid.x * grid.y);
+      grid.z = c.nsys;
+      return with_op(c.tg3, [&](auto TT) -> int {
+        constexpr bool TG3 = decltype(TT)::value;
+        k_cg_start<P, double, double, double, TG3><<<grid, THREADS, cg_smem<P, double, TG3>(1, true), ctx->stream>>>(
+          geo, c.b, c.x_cur, c.x_prev, c.x_new, w.r, c.extrapolate, w.partials, c.sc, c.skip);
+        LAUNCHED();
+        return LBFEM_OK;
+      });
+    });
+  }
+
+  // p[1-pi] <- D^{-1} r + beta p[pi] and the sums p.Ap.
+  int
+  cg_launch_p(lbfem_gpu_ctx *ctx, const CgScratch<double> &w, const CgCall &c, int pi)
+  {
+    const Geo geo = geo_of(ctx);
+    return with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      dim3 grid = tile_grid<P>(ctx->grid);
+      grid.z = c.nsys;
+      return with_op(c.tg3, [&](auto TT) -> int {
+        constexpr bool TG3 = decltype(TT)::value;
+        k_cg_p<P, double, TG3><<<grid, THREADS, cg_smem<P, double, TG3>(0), ctx->stream>>>(
+          geo, w.r, w.p[pi], w.p[1 - pi], w.state, w.partials, c.sc);
+        LAUNCHED();
+        return LBFEM_OK;
+      });
+    });
+  }
+
+  // x += alpha p, r -= alpha A p with p = p[pi], and the sums r.r, r.D^{-1}r.
+  int
+  cg_launch_update(lbfem_gpu_ctx *ctx, const CgScratch<double> &w, const CgCall &c, int pi)
+  {
+    const Geo geo = geo_of(ctx);
+    return with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      dim3 grid = tile_grid<P>(ctx->grid);
+      grid.z = c.nsys;
+      return with_op(c.tg3, [&](auto TT) -> int {
+        constexpr bool TG3 = decltype(TT)::value;
+        k_cg_update<P, double, TG3><<<grid, THREADS, cg_smem<P, double, TG3>(2), ctx->stream>>>(
+          geo, c.x_new, w.r, w.p[pi], w.state, w.partials, c.sc);
+        LAUNCHED();
+        return LBFEM_OK;
+      });
+    });
+  }
+
+  // Jacobi-PCG in the order of updates of deal.II SolverCG (mass.h:204-211),
+  // host-driven, with the work buffers w. *its_out: CG iterations summed over
+  // the systems.
+  int
+  cg_run(lbfem_gpu_ctx *ctx, const CgScratch<double> &w, const CgCall &c, int64_t *its_out)
+  {
     const double tol = ctx->prm.cg_tolerance;
     const int max_its = ctx->prm.cg_max_iterations;
+    const int nsys = c.nsys;
     CK(cudaMemsetAsync(w.state, 0, sizeof(CgState), ctx->stream));
-    int n_tiles = 0;
-    int st = with_degree(ctx->P, [&](auto PP) -> int {
-      constexpr int P = decltype(PP)::value;
-      dim3 grid = tile_grid<P>(g);
-      n_tiles = int(grid.x * grid.y);
-      grid.z = nsys;
-      k_cg_start<P, double, double, double><<<grid, THREADS, cg_smem<P, double>(1, true), ctx->stream>>>(
-        geo, b, x_cur, x_prev, x_new, w.r, extrapolate, w.partials);
-      LAUNCHED();
-      return LBFEM_OK;
-    });
-    if (st)
-      return st;
-    if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, 3 * NM)))
+    int n_tiles = 0, st;
+    if ((st = cg_launch_start(ctx, w, c, &n_tiles)) || (st = reduce_into(ctx, w.partials, w.sums, n_tiles, 3 * NM)))
       return st;
     k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 0, tol, max_its);
     LAUNCHED();
@@ -398,34 +467,12 @@ namespace
           }
         if (ctx->h_cg->n_active == 0)
           break;
-        st = with_degree(ctx->P, [&](auto PP) -> int {
-          constexpr int P = decltype(PP)::value;
-          dim3 grid = tile_grid<P>(g);
-          grid.z = nsys;
-          k_cg_p<P, double><<<grid, THREADS, cg_smem<P, double>(0), ctx->stream>>>(geo, w.r, w.p[pi], w.p[1 - pi],
-                                                                                    w.state, w.partials);
-          LAUNCHED();
-          return LBFEM_OK;
-        });
-        if (st)
-          return st;
-        if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, NM)))
+        if ((st = cg_launch_p(ctx, w, c, pi)) || (st = reduce_into(ctx, w.partials, w.sums, n_tiles, NM)))
           return st;
         k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 1, tol, max_its);
         LAUNCHED();
         pi = 1 - pi;
-        st = with_degree(ctx->P, [&](auto PP) -> int {
-          constexpr int P = decltype(PP)::value;
-          dim3 grid = tile_grid<P>(g);
-          grid.z = nsys;
-          k_cg_update<P, double><<<grid, THREADS, cg_smem<P, double>(2), ctx->stream>>>(geo, x_new, w.r, w.p[pi],
-                                                                                         w.state, w.partials);
-          LAUNCHED();
-          return LBFEM_OK;
-        });
-        if (st)
-          return st;
-        if ((st = reduce_into(ctx, w.partials, w.sums, n_tiles, 2 * NM)))
+        if ((st = cg_launch_update(ctx, w, c, pi)) || (st = reduce_into(ctx, w.partials, w.sums, n_tiles, 2 * NM)))
           return st;
         k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 2, tol, max_its);
         LAUNCHED();
@@ -439,18 +486,48 @@ namespace
     return LBFEM_OK;
   }
 
+  CgScratch<double>
+  ctx_scratch(lbfem_gpu_ctx *ctx)
+  {
+    return CgScratch<double>{ctx->d_r, {ctx->d_p[0], ctx->d_p[1]}, ctx->d_partials, ctx->d_sums, ctx->d_cg};
+  }
+
   // The context's own work buffers.
   int
-  cg_solve(lbfem_gpu_ctx *ctx, const double *b, double *x_new, const double *x_cur, const double *x_prev,
-           int extrapolate, int nsys, int64_t *its_out)
+  cg_solve(lbfem_gpu_ctx *ctx, const CgCall &c, int64_t *its_out)
   {
-    const CgScratch<double> w{ctx->d_r, {ctx->d_p[0], ctx->d_p[1]}, ctx->d_partials, ctx->d_sums, ctx->d_cg};
     int64_t its = 0;
-    const int st = cg_run(ctx, w, b, x_new, x_cur, x_prev, extrapolate, nsys, &its);
+    const int st = cg_run(ctx, ctx_scratch(ctx), c, &its);
     if (its_out)
       *its_out = its;
     ctx->cg_its += its;
     return st;
+  }
+
+  // The streaming matrix coefficients of the directions e (2 Q values) and the dt^2 coefficient c.
+  StreamCoef
+  stream_coef(const double *e, double c)
+  {
+    StreamCoef sc{};
+    for (int al = 0; al < NM; ++al)
+      {
+        const double ex = e[2 * (al + 1)], ey = e[2 * (al + 1) + 1];
+        sc.kxx[al] = c * ex * ex;
+        sc.kyy[al] = c * ey * ey;
+        sc.kxy[al] = c * ex * ey;
+      }
+    return sc;
+  }
+
+  // The moving populations at rest in the directions e, as a system mask.
+  int
+  resting(const double *e)
+  {
+    int m = 0;
+    for (int al = 0; al < NM; ++al)
+      if (e[2 * (al + 1)] == 0. && e[2 * (al + 1) + 1] == 0.)
+        m |= 1 << al;
+    return m;
   }
 
   // The status code of a failed mixed-precision solve (CgState status, 0: none).
@@ -503,7 +580,7 @@ namespace
       grid.z = nsys;
       // FP32 arithmetic: r0 only feeds the FP32 correction (the rounds form the FP64 residuals)
       k_cg_start<P, float, float, float><<<grid, THREADS, cg_smem<P, float>(1), ctx->stream>>>(
-        geo, b, ctx->d_x_s[ic], ctx->d_x_s[ip], ctx->d_x_s[in], ctx->d_r_s, 1, ctx->d_partials);
+        geo, b, ctx->d_x_s[ic], ctx->d_x_s[ip], ctx->d_x_s[in], ctx->d_r_s, 1, ctx->d_partials, StreamCoef{}, 0);
       LAUNCHED();
       return LBFEM_OK;
     });
@@ -589,10 +666,12 @@ namespace
     return LBFEM_OK;
   }
 
+  // One system of MassSolver::solve (mass.h:185-213) on device buffers: x_new <-
+  // A^{-1} b, CG from the start in x_new; sc / tg3: the TG3 matrix of system 0.
   int
-  mass_solve_dev(lbfem_gpu_ctx *ctx, const double *b, double *x_new, const double *x_cur, const double *x_prev,
-                 int extrapolate, int nsys, int64_t *its)
+  mass_solve_dev(lbfem_gpu_ctx *ctx, const double *b, double *x_new, bool tg3, const StreamCoef &sc, int64_t *its)
   {
+    const int nsys = 1;
     if (ctx->prm.mass == LBFEM_MASS_LUMPED)
       {
         k_lumped<double, double><<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), b, x_new,
@@ -610,7 +689,13 @@ namespace
           *its = 0;
         return st;
       }
-    return cg_solve(ctx, b, x_new, x_cur, x_prev, extrapolate, nsys, its);
+    CgCall c;
+    c.b = b;
+    c.x_new = x_new;
+    c.nsys = nsys;
+    c.tg3 = tg3;
+    c.sc = sc;
+    return cg_solve(ctx, c, its);
   }
 
   // ------------------------------------------------------- host <-> device
@@ -653,11 +738,67 @@ namespace
   // LeeLin::step is schemes.h:92-98, Bardow::step schemes.h:118-124 (collide,
   // then stream, streaming.h:88-100). The mixed-precision step runs the same
   // sequence on FP32 deviations d = f - w.
+  // The number of sweeps of a step: 2 for split TG3 (x, then y), else 1.
   int
-  step_front(lbfem_gpu_ctx *ctx)
+  n_sweeps(const lbfem_gpu_ctx *ctx)
+  {
+    return ctx->prm.streaming == LBFEM_STREAMING_TG3_SPLIT ? 2 : 1;
+  }
+
+  // The directions of the populations in sweep s: D2Q9::e, or for the split TG3
+  // sweeps D2Q9::e with the other component zeroed (TaylorGalerkin::axis,
+  // streaming.h:107-115).
+  void
+  sweep_directions(const lbfem_gpu_ctx *ctx, int s, double *e)
+  {
+    const double *e0 = d2q9_e();
+    const bool split = n_sweeps(ctx) == 2;
+    for (int k = 0; k < Q; ++k)
+      {
+        e[2 * k] = split && s == 1 ? 0. : e0[2 * k];
+        e[2 * k + 1] = split && s == 0 ? 0. : e0[2 * k + 1];
+      }
+  }
+
+  // The CG solve of sweep s of an FP64 step (TaylorGalerkin::increment,
+  // streaming.h:66-85): TG2 / TG3 start from the extrapolation of the two
+  // previous increments into x_new; a split sweep starts from its own previous
+  // increment in d_x[s] and skips the populations at rest in the sweep.
+  CgCall
+  step_cg_call(const lbfem_gpu_ctx *ctx, int s)
+  {
+    double e[2 * Q];
+    sweep_directions(ctx, s, e);
+    CgCall c;
+    c.b = ctx->d_rhs;
+    c.nsys = NM;
+    c.tg3 = ctx->prm.streaming != LBFEM_STREAMING_TG2;
+    c.sc = stream_coef(e, c.tg3 ? ctx->dt * ctx->dt / 6. : 0.);
+    if (n_sweeps(ctx) == 2)
+      {
+        c.x_new = ctx->d_x[s];
+        c.extrapolate = 0;
+        c.skip = resting(e);
+      }
+    else
+      {
+        c.x_new = ctx->d_x[ctx->x_new];
+        c.x_cur = ctx->d_x[ctx->x_cur];
+        c.x_prev = ctx->d_x[ctx->x_prev];
+        c.extrapolate = 1;
+      }
+    return c;
+  }
+
+  // Sweep s of the front of a step: the streaming right-hand side of the sweep's
+  // directions. The first sweep of Bardow collides on the fly into the other
+  // population buffer; the second split sweep streams that buffer as it stands.
+  int
+  step_front(lbfem_gpu_ctx *ctx, int sweep = 0)
   {
     const double dt = ctx->dt, lam = ctx->lambda;
-    const double *e = d2q9_e();
+    double e[2 * Q];
+    sweep_directions(ctx, sweep, e);
     const int rm = ctx->prm.remove_wall_mass_flux;
     const bool bardow = ctx->prm.scheme == LBFEM_SCHEME_BARDOW;
     const double b = -0.5 * dt * dt / lam;
@@ -674,30 +815,39 @@ namespace
         return launch_wall_faces<float>(ctx, bardow ? g : d, ctx->d_rhs_s, e, dt, remove);
       }
     double *f = ctx->d_f[ctx->cur], *g = ctx->d_f[1 - ctx->cur];
-    if ((st = launch_advection<double>(ctx, bardow ? ADV_TG_COLLIDE : ADV_LEELIN_FUSED, f, nullptr,
-                                       bardow ? g : nullptr, ctx->d_rhs, ac, ctx->d_stats)))
+    if (sweep > 0)
+      st = launch_advection<double>(ctx, ADV_TG, g, nullptr, nullptr, ctx->d_rhs, ac, ctx->d_stats);
+    else
+      st = launch_advection<double>(ctx, bardow ? ADV_TG_COLLIDE : ADV_LEELIN_FUSED, f, nullptr, bardow ? g : nullptr,
+                                    ctx->d_rhs, ac, ctx->d_stats);
+    if (st)
       return st;
     return launch_wall_faces<double>(ctx, bardow ? g : f, ctx->d_rhs, e, dt, remove);
   }
 
-  // The nodal update with the increment in x_cur (Bardow: f = g* + x, which
-  // flips the population buffers; Lee-Lin: the predictor-corrector).
+  // The nodal update of sweep s with its increment (x_cur, or d_x[s] for a split
+  // sweep). Bardow: f = g* + x (TaylorGalerkin::stream, streaming.h:88-100),
+  // which flips the population buffers after the last sweep; Lee-Lin: the
+  // predictor-corrector.
   int
-  step_back(lbfem_gpu_ctx *ctx)
+  step_back(lbfem_gpu_ctx *ctx, int sweep = 0)
   {
     const Geo geo = geo_of(ctx);
     const int nb = n_pointwise_blocks(ctx->grid.N);
     const double theta = ctx->dt / ctx->lambda;
     if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
       {
+        const bool last = sweep == n_sweeps(ctx) - 1;
         if (ctx->mixed)
           k_add_increment<float><<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_stats, ctx->d_fs[1 - ctx->cur],
-                                                                  ctx->d_x_s[ctx->x_cur]);
+                                                                  ctx->d_x_s[ctx->x_cur], 1);
         else
-          k_add_increment<double><<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_stats, ctx->d_f[1 - ctx->cur],
-                                                                   ctx->d_x[ctx->x_cur]);
+          k_add_increment<double><<<nb, THREADS, 0, ctx->stream>>>(
+            geo, ctx->d_stats, ctx->d_f[1 - ctx->cur], n_sweeps(ctx) == 2 ? ctx->d_x[sweep] : ctx->d_x[ctx->x_cur],
+            last ? 1 : 0);
         LAUNCHED();
-        ctx->cur = 1 - ctx->cur;
+        if (last)
+          ctx->cur = 1 - ctx->cur;
         return LBFEM_OK;
       }
     if (ctx->mixed)
@@ -735,28 +885,34 @@ namespace
   step_once(lbfem_gpu_ctx *ctx, int64_t *its)
   {
     int st;
-    if ((st = step_front(ctx)))
-      return st;
     if (its)
       *its = 0;
-    if (ctx->prm.mass != LBFEM_MASS_CG)
-      st = lumped_solve(ctx);
-    else if (ctx->mixed)
-      st = mixed_solve(ctx, ctx->d_rhs_s, NM, its);
-    else
+    for (int s = 0; s < n_sweeps(ctx); ++s)
       {
-        st = cg_solve(ctx, ctx->d_rhs, ctx->d_x[ctx->x_new], ctx->d_x[ctx->x_cur], ctx->d_x[ctx->x_prev], 1, NM, its);
-        if (!st)
+        if ((st = step_front(ctx, s)))
+          return st;
+        int64_t sweep_its = 0;
+        if (ctx->prm.mass != LBFEM_MASS_CG)
+          st = lumped_solve(ctx);
+        else if (ctx->mixed)
+          st = mixed_solve(ctx, ctx->d_rhs_s, NM, &sweep_its);
+        else
           {
-            const int old_prev = ctx->x_prev;
-            ctx->x_prev = ctx->x_cur;
-            ctx->x_cur = ctx->x_new;
-            ctx->x_new = old_prev;
+            st = cg_solve(ctx, step_cg_call(ctx, s), &sweep_its);
+            if (!st && n_sweeps(ctx) == 1)
+              {
+                const int old_prev = ctx->x_prev;
+                ctx->x_prev = ctx->x_cur;
+                ctx->x_cur = ctx->x_new;
+                ctx->x_new = old_prev;
+              }
           }
+        if (its)
+          *its += sweep_its;
+        if (st || (st = step_back(ctx, s)))
+          return st;
       }
-    if (st)
-      return st;
-    return step_back(ctx);
+    return LBFEM_OK;
   }
 
   // ------------------------------------------------------- graph-launched steps
@@ -805,65 +961,33 @@ namespace
   // device. One loop body is two iterations: the search directions alternate
   // between two buffers, and an iteration of a converged system does nothing.
   int
-  cg_graph(lbfem_gpu_ctx *ctx, int64_t *body_kernels)
+  cg_graph(lbfem_gpu_ctx *ctx, const CgCall &c, int64_t *body_kernels)
   {
-    const Geo geo = geo_of(ctx);
-    const Grid &g = ctx->grid;
     const double tol = ctx->prm.cg_tolerance;
     const int max_its = ctx->prm.cg_max_iterations;
-    const double *b = ctx->d_rhs;
-    double *x_new = ctx->d_x[ctx->x_new];
-    const double *x_cur = ctx->d_x[ctx->x_cur], *x_prev = ctx->d_x[ctx->x_prev];
+    const CgScratch<double> w = ctx_scratch(ctx);
     cudaStreamCaptureStatus cs;
     cudaGraph_t graph = nullptr;
     CK(cudaStreamGetCaptureInfo_v3(ctx->stream, &cs, nullptr, &graph, nullptr, nullptr, nullptr));
     cudaGraphConditionalHandle h;
     CK(cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault)); // 0 at every launch
-    CK(cudaMemsetAsync(ctx->d_cg, 0, sizeof(CgState), ctx->stream));
-    int n_tiles = 0;
-    int st = with_degree(ctx->P, [&](auto PP) -> int {
-      constexpr int P = decltype(PP)::value;
-      dim3 grid = tile_grid<P>(g);
-      n_tiles = int(grid.x * grid.y);
-      grid.z = NM;
-      k_cg_start<P, double, double, double><<<grid, THREADS, cg_smem<P, double>(1, true), ctx->stream>>>(
-        geo, b, x_cur, x_prev, x_new, ctx->d_r, 1, ctx->d_partials);
-      LAUNCHED();
-      return LBFEM_OK;
-    });
-    if (st || (st = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, 3 * NM)))
+    CK(cudaMemsetAsync(w.state, 0, sizeof(CgState), ctx->stream));
+    int n_tiles = 0, st;
+    if ((st = cg_launch_start(ctx, w, c, &n_tiles)) || (st = reduce_into(ctx, w.partials, w.sums, n_tiles, 3 * NM)))
       return st;
-    k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, NM, 0, tol, max_its);
+    k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, c.nsys, 0, tol, max_its);
     LAUNCHED();
-    k_cg_control<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_stats, h, 0);
+    k_cg_control<<<1, 32, 0, ctx->stream>>>(w.state, ctx->d_stats, h, 0);
     LAUNCHED();
     auto iteration = [&](int pi) -> int {
-      int s2 = with_degree(ctx->P, [&](auto PP) -> int {
-        constexpr int P = decltype(PP)::value;
-        dim3 grid = tile_grid<P>(g);
-        grid.z = NM;
-        k_cg_p<P, double><<<grid, THREADS, cg_smem<P, double>(0), ctx->stream>>>(geo, ctx->d_r, ctx->d_p[pi],
-                                                                                  ctx->d_p[1 - pi], ctx->d_cg,
-                                                                                  ctx->d_partials);
-        LAUNCHED();
-        return LBFEM_OK;
-      });
-      if (s2 || (s2 = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, NM)))
+      int s2;
+      if ((s2 = cg_launch_p(ctx, w, c, pi)) || (s2 = reduce_into(ctx, w.partials, w.sums, n_tiles, NM)))
         return s2;
-      k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, NM, 1, tol, max_its);
+      k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, c.nsys, 1, tol, max_its);
       LAUNCHED();
-      s2 = with_degree(ctx->P, [&](auto PP) -> int {
-        constexpr int P = decltype(PP)::value;
-        dim3 grid = tile_grid<P>(g);
-        grid.z = NM;
-        k_cg_update<P, double><<<grid, THREADS, cg_smem<P, double>(2), ctx->stream>>>(
-          geo, x_new, ctx->d_r, ctx->d_p[1 - pi], ctx->d_cg, ctx->d_partials);
-        LAUNCHED();
-        return LBFEM_OK;
-      });
-      if (s2 || (s2 = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, 2 * NM)))
+      if ((s2 = cg_launch_update(ctx, w, c, 1 - pi)) || (s2 = reduce_into(ctx, w.partials, w.sums, n_tiles, 2 * NM)))
         return s2;
-      k_cg_scalars<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, NM, 2, tol, max_its);
+      k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, c.nsys, 2, tol, max_its);
       LAUNCHED();
       return LBFEM_OK;
     };
@@ -873,7 +997,7 @@ namespace
         int s2;
         if ((s2 = iteration(0)) || (s2 = iteration(1)))
           return s2;
-        k_cg_control<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_stats, h, 1);
+        k_cg_control<<<1, 32, 0, ctx->stream>>>(w.state, ctx->d_stats, h, 1);
         LAUNCHED();
         return LBFEM_OK;
       },
@@ -904,7 +1028,7 @@ namespace
       dim3 grid = tile_grid<P>(g);
       grid.z = NM;
       k_cg_start<P, float, float, float><<<grid, THREADS, cg_smem<P, float>(1), ctx->stream>>>(
-        geo, b, xc, xp, xn, ctx->d_r_s, 1, ctx->d_partials);
+        geo, b, xc, xp, xn, ctx->d_r_s, 1, ctx->d_partials, StreamCoef{}, 0);
       LAUNCHED();
       return LBFEM_OK;
     });
@@ -946,7 +1070,7 @@ namespace
   void
   rotate_after_step(lbfem_gpu_ctx *ctx)
   {
-    if (ctx->prm.mass == LBFEM_MASS_CG)
+    if (ctx->prm.mass == LBFEM_MASS_CG && n_sweeps(ctx) == 1)
       {
         const int c = ctx->x_cur, p = ctx->x_prev, n = ctx->x_new;
         if (ctx->mixed)
@@ -982,22 +1106,33 @@ namespace
     const int cur0 = ctx->cur, c0 = ctx->x_cur, p0 = ctx->x_prev, n0 = ctx->x_new;
     const int64_t l0 = ctx->launches;
     *body = 0;
-    int st = step_front(ctx);
-    if (!st)
+    int64_t bodies = 0; // kernels of the loop bodies of all sweeps (the same in each)
+    int st = LBFEM_OK;
+    const int ns = n_sweeps(ctx);
+    for (int s = 0; s < ns && !st; ++s)
       {
-        if (ctx->prm.mass != LBFEM_MASS_CG)
+        st = step_front(ctx, s);
+        if (!st && ctx->prm.mass == LBFEM_MASS_CG)
+          {
+            int64_t b = 0;
+            st = ctx->mixed ? mixed_graph(ctx, &b) : cg_graph(ctx, step_cg_call(ctx, s), &b);
+            *body = b;
+            bodies += b;
+          }
+        else if (!st)
           st = lumped_solve(ctx);
-        else
-          st = ctx->mixed ? mixed_graph(ctx, body) : cg_graph(ctx, body);
+        if (!st)
+          {
+            if (s == ns - 1)
+              {
+                rotate_after_step(ctx);
+                if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
+                  ctx->cur = 1 - ctx->cur; // step_back flips it again
+              }
+            st = step_back(ctx, s);
+          }
       }
-    if (!st)
-      {
-        rotate_after_step(ctx);
-        if (ctx->prm.scheme == LBFEM_SCHEME_BARDOW)
-          ctx->cur = 1 - ctx->cur; // step_back flips it again
-        st = step_back(ctx);
-      }
-    *fixed = ctx->launches - l0 - *body;
+    *fixed = ctx->launches - l0 - bodies;
     ctx->cur = cur0;
     ctx->x_cur = c0;
     ctx->x_prev = p0;
@@ -1314,10 +1449,16 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
       return LBFEM_ERR_ARG;
   if (prm->scheme != LBFEM_SCHEME_BARDOW && prm->scheme != LBFEM_SCHEME_LEELIN)
     return LBFEM_ERR_ARG;
-  if (prm->streaming != LBFEM_STREAMING_TG2 ||
-      (prm->precision != LBFEM_PRECISION_FP64 && prm->precision != LBFEM_PRECISION_MIXED) ||
+  if (prm->streaming < LBFEM_STREAMING_TG2 || prm->streaming > LBFEM_STREAMING_TG3_SPLIT)
+    return LBFEM_ERR_ARG;
+  // TG3 needs the consistent mass (streaming.h:51-52); Lee-Lin streams with TG2 only (schemes.h:87)
+  if (prm->streaming != LBFEM_STREAMING_TG2 && (prm->mass != LBFEM_MASS_CG || prm->scheme != LBFEM_SCHEME_BARDOW))
+    return LBFEM_ERR_ARG;
+  if ((prm->precision != LBFEM_PRECISION_FP64 && prm->precision != LBFEM_PRECISION_MIXED) ||
       (prm->mass != LBFEM_MASS_CG && prm->mass != LBFEM_MASS_LUMPED && prm->mass != LBFEM_MASS_RICHARDSON))
     return LBFEM_ERR_UNSUPPORTED;
+  if (prm->streaming != LBFEM_STREAMING_TG2 && prm->precision == LBFEM_PRECISION_MIXED)
+    return LBFEM_ERR_UNSUPPORTED; // TG3 runs in FP64
   if (prm->mass == LBFEM_MASS_RICHARDSON && prm->richardson < 0)
     return LBFEM_ERR_ARG;
   if (!(prm->cg_tolerance >= 0) || prm->cg_max_iterations < 1 || !(prm->mixed_tolerance >= 0))
@@ -1807,19 +1948,28 @@ lbfem_gpu_solve_round_resident(lbfem_gpu_ctx *ctx)
 }
 
 int
-lbfem_gpu_mass_solve(lbfem_gpu_ctx *ctx, double *x, const double *r, const double *, double tg3)
+lbfem_gpu_mass_solve(lbfem_gpu_ctx *ctx, double *x, const double *r, const double *e, double tg3)
 {
   int st;
   if ((st = check_ctx(ctx)))
     return st;
   if (!x || !r)
     return fail(ctx, LBFEM_ERR_ARG, "mass_solve: null buffer");
+  if (tg3 != 0. && !e)
+    return fail(ctx, LBFEM_ERR_ARG, "mass_solve: the TG3 matrix needs the direction e");
+  if (tg3 != 0. && ctx->prm.mass == LBFEM_MASS_RICHARDSON)
+    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve: the TG3 matrix with iterated lumping is not implemented");
+  StreamCoef sc{};
   if (tg3 != 0.)
-    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve: the TG3 left-hand side is not implemented");
+    {
+      sc.kxx[0] = tg3 * e[0] * e[0];
+      sc.kyy[0] = tg3 * e[1] * e[1];
+      sc.kxy[0] = tg3 * e[0] * e[1];
+    }
   double *xn = ctx->d_x[ctx->x_new];
   if ((st = upload(ctx, r, ctx->d_rhs, 1)) || (st = upload(ctx, x, xn, 1)))
     return st;
-  const int solve_st = mass_solve_dev(ctx, ctx->d_rhs, xn, nullptr, nullptr, 0, 1, nullptr);
+  const int solve_st = mass_solve_dev(ctx, ctx->d_rhs, xn, tg3 != 0., sc, nullptr);
   if (solve_st != LBFEM_OK && solve_st != LBFEM_ERR_NO_CONVERGENCE && solve_st != LBFEM_ERR_NONFINITE)
     return solve_st;
   if ((st = download(ctx, xn, x, 1)))
@@ -2312,7 +2462,11 @@ lbfem_gpu_mass_solve_noalloc(lbfem_gpu_ctx *ctx, double *x, const double *r)
   w.partials = base + 3 * NOALLOC_MAX_NODES;
   w.sums = w.partials + 3 * NM * NOALLOC_MAX_TILES;
   w.state = reinterpret_cast<CgState *>(w.sums + 64);
-  const int solve_st = cg_run(ctx, w, r, x, nullptr, nullptr, 0, 1, nullptr);
+  CgCall c;
+  c.b = r;
+  c.x_new = x;
+  c.nsys = 1;
+  const int solve_st = cg_run(ctx, w, c, nullptr);
   if (solve_st != LBFEM_OK)
     return solve_st;
   CK(cudaStreamSynchronize(ctx->stream));

@@ -227,9 +227,10 @@ namespace lbfem_gpu
   // TaylorGalerkin::stream (streaming.h:94-98): f_a += x_{a-1}, a = 1..8.
   template <typename R>
   __global__ void
-  k_add_increment(const Geo geo, DevStats *__restrict__ ds, R *__restrict__ f, const R *__restrict__ x)
+  k_add_increment(const Geo geo, DevStats *__restrict__ ds, R *__restrict__ f, const R *__restrict__ x,
+                  int count_step)
   {
-    if (step_skipped(ds))
+    if (step_skipped(ds, count_step != 0))
       return;
     const long long N = geo.g.N;
     LBFEM_GRID_STRIDE(i, N)
@@ -1057,6 +1058,285 @@ namespace lbfem_gpu
       }
   }
 
+  // ------------------------------------------ TG3 streaming matrix (K2, TG3)
+  // The matrix of a TG3 streaming solve, A = M + c K_e with
+  // K_e = int (e.grad N)(e.grad N^T) (StreamingMatrix, mass.h:57-129), per
+  // system: kxx = c ex^2, kyy = c ey^2, kxy = c ex ey (all 0: A = M). In the
+  // grouped tensor-product form of the flux term of the advection operator,
+  //   A = My (x) Z1 + Cy (x) Z2 + Ky (x) Z3 + By (x) Z4,
+  //   Z1 = Mx + kxx Kx, Z2 = kxy (Bx - 2 Cx), Z3 = kyy Mx, Z4 = kxy Cx
+  // (C^T = B - C, B the end-point term). An axis-parallel e (kxy = 0, one of
+  // kxx, kyy 0) makes it the product (My + kyy Ky) (x) (Mx + kxx Kx).
+  struct StreamCoef
+  {
+    double kxx[NM], kyy[NM], kxy[NM];
+  };
+
+  // Scratch of the TG3 apply beyond the staged field: three x-pass output
+  // arrays and Z4 on the first / last domain row (elements of R).
+  template <int P>
+  __host__ __device__ constexpr int
+  tg3_scratch()
+  {
+    return 3 * Tile<P>::NY + 2 * Tile<P>::TX;
+  }
+
+  // x pass of the product form: out = (Mx + kxx Kx) s on one footprint row / x segment.
+  template <int P, typename R>
+  __device__ __forceinline__ void
+  sep_xpass(const R *__restrict__ s, R *__restrict__ out, const TileMaps<P, R> &m, int fy, int seg, R kxx)
+  {
+    using T = Tile<P>;
+    const R *row = s + fy * T::PF;
+    R *orow = out + fy * T::PY;
+    const int q0 = seg * T::KX;
+    R u[P + 1];
+#pragma unroll
+    for (int b = 0; b <= P; ++b)
+      u[b] = row[q0 * P + b];
+    R pend = fma(kxx * m.hxi[q0], elem_last<P, OP_K>(u), m.hx[q0] * elem_last<P, OP_M>(u));
+#pragma unroll
+    for (int q = 1; q <= T::KX; ++q)
+      {
+        const int qc = q0 + q;
+        u[0] = u[P];
+#pragma unroll
+        for (int b = 1; b <= P; ++b)
+          u[b] = row[qc * P + b];
+        R yM[P + 1], yK[P + 1];
+        elem<P, OP_M>(u, yM);
+        elem<P, OP_K>(u, yK);
+        const R sm = m.hx[qc], sk = kxx * m.hxi[qc];
+        const int j0 = (qc - 1) * P;
+        orow[j0] = fma(sk, yK[0], fma(sm, yM[0], pend));
+#pragma unroll
+        for (int a = 1; a < P; ++a)
+          orow[j0 + a] = fma(sk, yK[a], sm * yM[a]);
+        pend = fma(sk, yK[P], sm * yM[P]);
+      }
+  }
+
+  // y pass of the product form: (My + kyy Ky) t on column j / y segment seg, emit(own row i, value).
+  template <int P, typename R, typename Emit>
+  __device__ __forceinline__ void
+  sep_ypass(const R *__restrict__ t, const TileMaps<P, R> &m, int j, int seg, R kyy, Emit &&emit)
+  {
+    using T = Tile<P>;
+    const int q0 = seg * T::KY;
+    R u[P + 1];
+#pragma unroll
+    for (int b = 0; b <= P; ++b)
+      u[b] = t[(q0 * P + b) * T::PY + j];
+    R pend = fma(kyy * m.hyi[q0], elem_last<P, OP_K>(u), m.hy[q0] * elem_last<P, OP_M>(u));
+#pragma unroll
+    for (int q = 1; q <= T::KY; ++q)
+      {
+        const int qc = q0 + q;
+        u[0] = u[P];
+#pragma unroll
+        for (int b = 1; b <= P; ++b)
+          u[b] = t[(qc * P + b) * T::PY + j];
+        R yM[P + 1], yK[P + 1];
+        elem<P, OP_M>(u, yM);
+        elem<P, OP_K>(u, yK);
+        const R sm = m.hy[qc], sk = kyy * m.hyi[qc];
+        const int i0 = (qc - 1) * P;
+        emit(i0, fma(sk, yK[0], fma(sm, yM[0], pend)));
+#pragma unroll
+        for (int a = 1; a < P; ++a)
+          emit(i0 + a, fma(sk, yK[a], sm * yM[a]));
+        pend = fma(sk, yK[P], sm * yM[P]);
+      }
+  }
+
+  // x pass of the general form on one footprint row / x segment: Z1, Z2, Z3 into
+  // s_y (three arrays of NY), Z4 into s_y4[slot] when the row is the first
+  // (slot 0) or last (slot 1) row of a non-periodic y axis.
+  template <int P, typename R>
+  __device__ __forceinline__ void
+  full_xpass(const R *__restrict__ s, R *__restrict__ s_y, R *__restrict__ s_y4, const TileMaps<P, R> &m, int fy,
+             int seg, R kxx, R kyy, R kxy, int gx0, int y4_slot, int bx_lo, int bx_hi)
+  {
+    using T = Tile<P>;
+    const R *row = s + fy * T::PF;
+    R *y1 = s_y + fy * T::PY, *y2 = y1 + T::NY, *y3 = y2 + T::NY;
+    const int q0 = seg * T::KX;
+    R u[P + 1];
+#pragma unroll
+    for (int b = 0; b <= P; ++b)
+      u[b] = row[q0 * P + b];
+    R pM = m.hx[q0] * elem_last<P, OP_M>(u), pK = m.hxi[q0] * elem_last<P, OP_K>(u),
+      pC = m.cx[q0] * elem_last<P, OP_C>(u);
+#pragma unroll
+    for (int q = 1; q <= T::KX; ++q)
+      {
+        const int qc = q0 + q;
+        u[0] = u[P];
+#pragma unroll
+        for (int b = 1; b <= P; ++b)
+          u[b] = row[qc * P + b];
+        R eM[P + 1], eK[P + 1], eC[P + 1];
+        elem<P, OP_M>(u, eM);
+        elem<P, OP_K>(u, eK);
+        elem<P, OP_C>(u, eC);
+        const R sh = m.hx[qc], shi = m.hxi[qc], sc = m.cx[qc];
+        const int j0 = (qc - 1) * P;
+#pragma unroll
+        for (int aa = 0; aa < P; ++aa)
+          {
+            const int j = j0 + aa;
+            R vM = sh * eM[aa], vK = shi * eK[aa], vC = sc * eC[aa];
+            if (aa == 0)
+              {
+                vM += pM;
+                vK += pK;
+                vC += pC;
+              }
+            R z2 = R(-2) * kxy * vC;
+            if (aa == 0)
+              {
+                // Bx u = -u at the first node, +u at the last node of a non-periodic x axis
+                const int gx = gx0 + j;
+                if (gx == bx_lo)
+                  z2 = fma(-kxy, u[0], z2);
+                else if (gx == bx_hi)
+                  z2 = fma(kxy, u[0], z2);
+              }
+            y1[j] = fma(kxx, vK, vM);
+            y2[j] = z2;
+            y3[j] = kyy * vM;
+            if (y4_slot >= 0)
+              s_y4[y4_slot * T::TX + j] = kxy * vC;
+          }
+        pM = sh * eM[P];
+        pK = shi * eK[P];
+        pC = sc * eC[P];
+      }
+  }
+
+  // y pass of the general form on column j / y segment seg: emit(own row i, value).
+  template <int P, typename R, typename Emit>
+  __device__ __forceinline__ void
+  full_ypass(const R *__restrict__ s_y, const R *__restrict__ s_y4, const TileMaps<P, R> &m, int j, int seg, int gy0,
+             int by_lo, int by_hi, Emit &&emit)
+  {
+    using T = Tile<P>;
+    const R *y1 = s_y, *y2 = s_y + T::NY, *y3 = s_y + 2 * T::NY;
+    const int q0 = seg * T::KY;
+    R v1[P + 1], v2[P + 1], v3[P + 1];
+#pragma unroll
+    for (int b = 0; b <= P; ++b)
+      {
+        const int t = (q0 * P + b) * T::PY + j;
+        v1[b] = y1[t];
+        v2[b] = y2[t];
+        v3[b] = y3[t];
+      }
+    R pend = m.hy[q0] * elem_last<P, OP_M>(v1) + m.cy[q0] * elem_last<P, OP_C>(v2) +
+             m.hyi[q0] * elem_last<P, OP_K>(v3);
+#pragma unroll
+    for (int q = 1; q <= T::KY; ++q)
+      {
+        const int qc = q0 + q;
+        v1[0] = v1[P];
+        v2[0] = v2[P];
+        v3[0] = v3[P];
+#pragma unroll
+        for (int b = 1; b <= P; ++b)
+          {
+            const int t = (qc * P + b) * T::PY + j;
+            v1[b] = y1[t];
+            v2[b] = y2[t];
+            v3[b] = y3[t];
+          }
+        R e1[P + 1], e2[P + 1], e3[P + 1];
+        elem<P, OP_M>(v1, e1);
+        elem<P, OP_C>(v2, e2);
+        elem<P, OP_K>(v3, e3);
+        const R sh = m.hy[qc], sc = m.cy[qc], shi = m.hyi[qc];
+        const int i0 = (qc - 1) * P;
+#pragma unroll
+        for (int aa = 0; aa <= P; ++aa)
+          {
+            R r = sh * e1[aa] + sc * e2[aa] + shi * e3[aa];
+            if (aa == P)
+              {
+                pend = r;
+                break;
+              }
+            if (aa == 0)
+              r += pend;
+            const int gy = gy0 + i0 + aa;
+            if (gy == by_lo)
+              r -= s_y4[j];
+            else if (gy == by_hi)
+              r += s_y4[T::TX + j];
+            emit(i0 + aa, r);
+          }
+      }
+  }
+
+  // A u for every own node of the tile, u staged in s_u; s_t holds tg3_scratch<P>()
+  // elements. emit(i, j, storage index, image, Au) as mass_apply (images: identity row).
+  template <int P, typename R, typename Emit>
+  __device__ __forceinline__ void
+  tg3_apply(const R *s_u, R *s_t, const TileMaps<P, R> &m, const Grid &g, int gx0, int gy0, R kxx, R kyy, R kxy,
+            Emit &&emit)
+  {
+    using T = Tile<P>;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool sep = kxy == R(0);
+    R *s_y4 = s_t + 3 * T::NY;
+    if (warp < T::NSX && lane < T::FY)
+      {
+        if (sep)
+          sep_xpass<P>(s_u, s_t, m, lane, warp, kxx);
+        else
+          {
+            const int gy = gy0 - P + lane;
+            const int y4_slot = g.py ? -1 : gy == 0 ? 0 : gy == g.nfy - 1 ? 1 : -1;
+            full_xpass<P>(s_u, s_t, s_y4, m, lane, warp, kxx, kyy, kxy, gx0, y4_slot, g.px ? -1 : 0,
+                          g.px ? -1 : g.nfx - 1);
+          }
+      }
+    __syncthreads();
+    const int j = threadIdx.x % T::YL, seg = threadIdx.x / T::YL;
+    if (j < T::TX && seg < T::NSY)
+      {
+        const int gx = gx0 + j;
+        auto out = [&](int i, R v) {
+          const int gy = gy0 + i;
+          if (gx < g.nfx && gy < g.nfy)
+            emit(i, j, gy * g.nfx + gx, is_image(gx, gy, g), v);
+        };
+        if (sep)
+          sep_ypass<P>(s_t, m, j, seg, kyy, out);
+        else
+          full_ypass<P>(s_t, s_y4, m, j, seg, gy0, g.py ? -1 : 0, g.py ? -1 : g.nfy - 1, out);
+      }
+  }
+
+  // The operator of a CG kernel: the mass matrix, or with TG3 the streaming
+  // matrix of system s.
+  template <int P, bool TG3, typename R, typename Emit>
+  __device__ __forceinline__ void
+  op_apply(const R *s_u, R *s_t, const TileMaps<P, R> &m, const Grid &g, int gx0, int gy0, const StreamCoef &sc,
+           int s, Emit &&emit)
+  {
+    if constexpr (TG3)
+      tg3_apply<P>(s_u, s_t, m, g, gx0, gy0, R(sc.kxx[s]), R(sc.kyy[s]), R(sc.kxy[s]), emit);
+    else
+      mass_apply<P>(s_u, s_t, m, g, gx0, gy0, emit);
+  }
+
+  // Elements of the x-pass scratch of a CG kernel.
+  template <int P, bool TG3>
+  __host__ __device__ constexpr int
+  op_scratch()
+  {
+    return TG3 ? tg3_scratch<P>() : Tile<P>::NY;
+  }
+
   // ---------------------------------------- iterated lumping (Richardson)
   // One Richardson pass of MassSolver::solve with Mass::richardson (mass.h:193-202):
   // x_out = x_in + M_L^{-1} (b - M x_in) for nsys systems (grid.z), constrained
@@ -1118,19 +1398,32 @@ namespace lbfem_gpu
   // r = b - A xg with xg = extrapolate ? 2 x_cur - x_prev (written to x_new) : x_new;
   // partials per system: b.b, r.r, r.D^{-1}r. Storage R, arithmetic A (A = double:
   // the FP64 residual of the refinement). One system per CTA.
-  template <int P, typename R, typename X = R, typename A = R>
+  // TG3: A is the streaming matrix of sc; systems whose bit is set in skip are
+  // not solved (zero sums: converged at the start, x untouched).
+  template <int P, typename R, typename X = R, typename A = R, bool TG3 = false>
   __global__ void __launch_bounds__(THREADS)
     k_cg_start(const Geo geo, const R *__restrict__ b, const X *__restrict__ x_cur, const X *__restrict__ x_prev,
-               X *__restrict__ x_new, R *__restrict__ r, int extrapolate, double *__restrict__ partials)
+               X *__restrict__ x_new, R *__restrict__ r, int extrapolate, double *__restrict__ partials,
+               const StreamCoef sc, int skip)
   {
     using T = Tile<P>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     A *s_u = reinterpret_cast<A *>(sm_raw), *s_t = s_u + T::NF;
-    R *s_b = reinterpret_cast<R *>(s_t + T::NY);
+    R *s_b = reinterpret_cast<R *>(s_t + op_scratch<P, TG3>());
     __shared__ TileMaps<P, A> maps;
     const Grid &g = geo.g;
     const long long N = g.N;
     const int s = blockIdx.z;
+    if ((skip >> s) & 1)
+      {
+        if (threadIdx.x == 0)
+          {
+            const int nt = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
+            for (int q = 0; q < 3; ++q)
+              partials[(long long)(q * NM + s) * nt + tile] = 0.0;
+          }
+        return;
+      }
     const int gx0 = blockIdx.x * T::TX, gy0 = blockIdx.y * T::TY;
     build_maps<P>(maps, geo, gx0, gy0);
     __syncthreads();
@@ -1143,7 +1436,7 @@ namespace lbfem_gpu
     __syncthreads();
     double part[3] = {0, 0, 0};
     R *rs = r + o;
-    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, int idx, bool image, A Ax) {
+    op_apply<P, TG3>(s_u, s_t, maps, g, gx0, gy0, sc, s, [&](int i, int j, int idx, bool image, A Ax) {
       const long long id = o + idx;
       A xg;
       if (image)
@@ -1168,10 +1461,10 @@ namespace lbfem_gpu
   }
 
   // p <- D^{-1} r + beta p (p <- D^{-1} r on the first iteration); partial p.Ap. One system per CTA.
-  template <int P, typename R>
+  template <int P, typename R, bool TG3 = false>
   __global__ void __launch_bounds__(THREADS)
     k_cg_p(const Geo geo, const R *__restrict__ r, const R *__restrict__ p_in, R *__restrict__ p_out,
-           const CgState *__restrict__ st, double *__restrict__ partials)
+           const CgState *__restrict__ st, double *__restrict__ partials, const StreamCoef sc)
   {
     using T = Tile<P>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -1197,7 +1490,7 @@ namespace lbfem_gpu
     __syncthreads();
     double part[1] = {0};
     R *posys = p_out + o;
-    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, int idx, bool image, R Ap) {
+    op_apply<P, TG3>(s_u, s_t, maps, g, gx0, gy0, sc, s, [&](int i, int j, int idx, bool image, R Ap) {
       R pn;
       if (image)
         {
@@ -1213,10 +1506,10 @@ namespace lbfem_gpu
   }
 
   // v = A p recomputed; x += alpha p, r -= alpha v; partials r.r, r.D^{-1}r. One system per CTA.
-  template <int P, typename R>
+  template <int P, typename R, bool TG3 = false>
   __global__ void __launch_bounds__(THREADS)
     k_cg_update(const Geo geo, R *__restrict__ x, R *__restrict__ r, const R *__restrict__ p,
-                const CgState *__restrict__ st, double *__restrict__ partials)
+                const CgState *__restrict__ st, double *__restrict__ partials, const StreamCoef sc)
   {
     using T = Tile<P>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -1233,7 +1526,7 @@ namespace lbfem_gpu
     const R al = R(st->alpha[s]);
     const long long o = s * N;
     const R *ps = p + o;
-    R *s_x = s_t + T::NY, *s_r = s_x + T::TX * T::TY;
+    R *s_x = s_t + op_scratch<P, TG3>(), *s_r = s_x + T::TX * T::TY;
     __syncthreads();
     stage<P>(s_u, maps, [&](long long idx) { return ps[idx]; });
     stage_own<P>(s_x, x + o, g, gx0, gy0);
@@ -1241,7 +1534,7 @@ namespace lbfem_gpu
     __syncthreads();
     double part[2] = {0, 0};
     R *xs = x + o, *rs = r + o;
-    mass_apply<P>(s_u, s_t, maps, g, gx0, gy0, [&](int i, int j, int idx, bool image, R Ap) {
+    op_apply<P, TG3>(s_u, s_t, maps, g, gx0, gy0, sc, s, [&](int i, int j, int idx, bool image, R Ap) {
       const R pv = image ? ps[idx] : s_u[(i + P) * T::PF + j + P];
       if (image)
         Ap = pv;

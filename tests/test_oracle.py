@@ -86,7 +86,8 @@ def test_element_stencils(oracle_mod, p):
 
 
 def test_amplification_factor(oracle_mod):
-    """One TG2 streaming step of a Fourier mode (consistent mass) equals G_2d of analysis/tg_spectral.py."""
+    """One TG2 or TG3 streaming step of a Fourier mode (consistent mass; TG3 with
+    A = M + dt^2/6 K_e on the left) equals G_2d of analysis/tg_spectral.py."""
     gold = json.load(open(os.path.join(GOLDEN, "tg_spectral.json")))["cases"]
     n = 16
     m = unit_mesh(n, 1)
@@ -96,22 +97,25 @@ def test_amplification_factor(oracle_mod):
     I, J = I.ravel() % n, J.ravel() % n
     ind = m.independent()
     checked = 0
+    n_tg3 = 0
     for c in gold:
-        if c["tg3"]:
-            continue
         alpha = [k for k in range(1, 9) if tuple(d2q9.E[k]) == (c["ex"], c["ey"])][0]
         phi = 2 * np.pi * (c["mx"] * I + c["my"] * J) / n
         u = np.cos(phi)
         f = np.tile(u, (9, 1))
         r = o.advection(f, e, c["C"], 1.0)
-        x = o.mass_solve(r[alpha - 1])
+        if c["tg3"]:
+            x = o.mass_solve(r[alpha - 1], e=(c["ex"], c["ey"]), tg3_coefficient=c["C"] ** 2 / 6)
+            n_tg3 += 1
+        else:
+            x = o.mass_solve(r[alpha - 1])
         up = u + x
         cs, sn = np.cos(phi[ind]), np.sin(phi[ind])
         g_re = np.dot(up[ind], cs) / np.dot(cs, cs)
         g_im = -np.dot(up[ind], sn) / np.dot(sn, sn)
         assert abs(g_re - c["G_re"]) < 1e-12 and abs(g_im - c["G_im"]) < 1e-12, c
         checked += 1
-    assert checked >= 60
+    assert checked >= 120 and n_tg3 >= 60
 
 
 def test_stencil_bench_check_value(oracle_mod):
