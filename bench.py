@@ -15,6 +15,9 @@ A step is one Scheme::step of the whole mesh. Metric: Q.DoF updates/s =
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+  python bench.py --streaming tg3|tg3-split [--cfl C]   (Bardow FP64 TG3 step at
+  CFL C against TG2 at CFL 0.25 over the same simulated time)
+
 --impl reference times the CPU implementation of the same path on the host
 cores (the deal.II reference cannot be built here; the FP64 oracle port of its
 algorithm, OpenMP on all cores, stands in for it).
@@ -442,6 +445,74 @@ def run_batch(args):
     return 0
 
 
+def run_streaming(args):
+    """TG3 streaming (--streaming tg3 | tg3-split): the Bardow scheme in FP64 on the
+    Taylor-Green workload at CFL args.cfl, against TG2 at CFL 0.25 over the same
+    simulated time (the reference's comparison, docs/results.md:97-160)."""
+    import ctypes as C
+
+    import lbfem_gpu
+    from lbfem_gpu import cases, make_params
+
+    world, rank, local, pg = dist_setup()
+    tc, mesh, _, lam, f0, cfg = workload(args)
+    lib = lbfem_gpu.library()
+
+    def timed_run(streaming, cfl, steps, warmup):
+        dt = mesh.time_step(cfl)
+        prm = make_params("bardow", "cg", cg_tolerance=args.cg_tol, streaming=streaming, device=local)
+        h = lbfem_gpu.Solver(mesh, prm)
+        h.set_time_step(dt, lam)
+        h.set_initial_populations(f0)
+        h.step(warmup)
+        lib.lbfem_gpu_synchronize(h.h)
+        barrier(pg)
+        with Clocks(local) as clocks:
+            h._call("event_record", h.h, 0)
+            h.step(steps)
+            h._call("event_record", h.h, 1)
+            lib.lbfem_gpu_synchronize(h.h)
+        ms = C.c_float()
+        h._call("event_elapsed", h.h, 0, 1, C.byref(ms))
+        sec = allreduce_max(pg, ms.value * 1e-3)
+        its, launches = C.c_double(), C.c_int64()
+        h._call("last_step_stats", h.h, C.byref(its), C.byref(launches))
+        t = (warmup + steps) * dt
+        err = cases.diagnostics(tc, mesh, h.node_weight(), h.get_populations(), t)["rel_l2_u"]
+        h.close()
+        return {"sec": sec, "dt": dt, "its": its.value, "launches": int(launches.value), "clocks": clocks.summary(),
+                "rel_l2_u_vs_exact": err, "t": t}
+
+    tg3 = timed_run(args.streaming, args.cfl, args.steps, args.warmup)
+    ratio = int(round(args.cfl / 0.25))  # TG2 steps per TG3 step over the same simulated time
+    tg2 = timed_run("tg2", 0.25, args.steps * ratio, args.warmup * ratio)
+    if rank != 0:
+        return 0
+    units = 9 * mesh.n_unique() * args.steps * world
+    sim_rate = lambda r, n: n * r["dt"] / r["sec"]  # noqa: E731 (simulated time per second)
+    line = {
+        "metric": f"Q·DoF updates/s, Bardow {args.streaming} FP64 at CFL {args.cfl:g} (and time to solution "
+                  f"against TG2 at CFL 0.25)",
+        "value": units / tg3["sec"], "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tg3["sec"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Taylor-Green initial state)",
+        "config": dict(cfg, workload=cfg["workload"].replace(args.scheme, "bardow"), scheme="bardow",
+                       streaming=args.streaming, cfl=args.cfl,
+                       solver_iterations_per_solve=tg3["its"], parallelism=f"replicas x{world}" if world > 1
+                       else "single GPU"),
+        "tg2_cfl_0.25": {"value": 9 * mesh.n_unique() * args.steps * ratio * world / tg2["sec"],
+                         "ms_per_step": 1e3 * tg2["sec"] / (args.steps * ratio), "steps": args.steps * ratio,
+                         "solver_iterations_per_solve": tg2["its"], "rel_l2_u_vs_exact": tg2["rel_l2_u_vs_exact"]},
+        "rel_l2_u_vs_exact": tg3["rel_l2_u_vs_exact"],
+        "simulated_time_per_second": {args.streaming: sim_rate(tg3, args.steps),
+                                      "tg2": sim_rate(tg2, args.steps * ratio)},
+        "time_to_solution_speedup_vs_tg2": tg2["sec"] / tg3["sec"],
+        "clocks": tg3["clocks"], "gpu_launches": tg3["launches"],
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -454,6 +525,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--batch", type=int, default=0,
                     help="time N batched independent instances (the batched workload) instead of the default")
+    ap.add_argument("--streaming", default="tg2", choices=["tg2", "tg3", "tg3-split"],
+                    help="tg3 / tg3-split: time the Bardow FP64 TG3 step against TG2 at CFL 0.25 instead")
+    ap.add_argument("--cfl", type=float, default=1.0, help="CFL number of the --streaming tg3* run")
     ap.add_argument("--cg-tol", type=float, default=1e-8,
                     help="relative CG tolerance of both precisions (MassSettings default 1e-8, mass.h:33)")
     args = ap.parse_args()
@@ -461,6 +535,8 @@ def main():
         args.warmup = 3
     if args.batch and args.impl == "ours":
         return run_batch(args)
+    if args.streaming != "tg2" and args.impl == "ours":
+        return run_streaming(args)
     return run_reference(args) if args.impl == "reference" else run_ours(args)
 
 

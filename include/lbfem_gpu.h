@@ -196,6 +196,15 @@ int lbfem_gpu_advection(lbfem_gpu_ctx *ctx, const double *f, const double *feq, 
  */
 int lbfem_gpu_mass_solve(lbfem_gpu_ctx *ctx, double *x, const double *r, const double *e, double tg3_coefficient);
 
+/*
+ * compute_stream_function (io.h:31-95): psi with u = -dpsi/dy, v = dpsi/dx from
+ * (grad phi, grad psi) = (dphi/dx, v) - (dphi/dy, u), psi = 0 on every side of
+ * the box, Jacobi-PCG to 1e-12 |b| (at most 10000 iterations). velocity: u then
+ * v, two blocks of n_dofs (periodic images carry their source's value); psi:
+ * n_dofs. Host buffers; uses the context's solver scratch (call between steps).
+ */
+int lbfem_gpu_stream_function(lbfem_gpu_ctx *ctx, const double *velocity, double *psi);
+
 /* y <- M x, the MassOperator vmult (discretization.h:51), constrained rows the identity. Host buffers. */
 int lbfem_gpu_mass_vmult(lbfem_gpu_ctx *ctx, double *y, const double *x);
 

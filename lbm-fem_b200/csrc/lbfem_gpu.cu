@@ -169,12 +169,12 @@ namespace
       }
   }
 
-  template <int P, typename R, bool TG3 = false>
+  template <int P, typename R, int OPK = OPK_MASS>
   constexpr size_t
   cg_smem(int own, bool fp64_arith = false)
   {
     using T = Tile<P>;
-    return (fp64_arith ? sizeof(double) : sizeof(R)) * (T::NF + op_scratch<P, TG3>()) +
+    return (fp64_arith ? sizeof(double) : sizeof(R)) * (T::NF + op_scratch<P, OPK>()) +
            sizeof(R) * own * T::TX * T::TY;
   }
 
@@ -201,9 +201,13 @@ namespace
         (st = set_smem(ctx, k_cg_start<P, double, double, double>, cg_smem<P, double>(1))) ||
         (st = set_smem(ctx, k_cg_p<P, double>, cg_smem<P, double>(0))) ||
         (st = set_smem(ctx, k_cg_update<P, double>, cg_smem<P, double>(2))) ||
-        (st = set_smem(ctx, k_cg_start<P, double, double, double, true>, cg_smem<P, double, true>(1))) ||
-        (st = set_smem(ctx, k_cg_p<P, double, true>, cg_smem<P, double, true>(0))) ||
-        (st = set_smem(ctx, k_cg_update<P, double, true>, cg_smem<P, double, true>(2))) ||
+        (st = set_smem(ctx, k_cg_start<P, double, double, double, OPK_TG3>, cg_smem<P, double, OPK_TG3>(1))) ||
+        (st = set_smem(ctx, k_cg_p<P, double, OPK_TG3>, cg_smem<P, double, OPK_TG3>(0))) ||
+        (st = set_smem(ctx, k_cg_update<P, double, OPK_TG3>, cg_smem<P, double, OPK_TG3>(2))) ||
+        (st = set_smem(ctx, k_cg_start<P, double, double, double, OPK_LAPLACE>,
+                       cg_smem<P, double, OPK_LAPLACE>(1))) ||
+        (st = set_smem(ctx, k_cg_p<P, double, OPK_LAPLACE>, cg_smem<P, double, OPK_LAPLACE>(0))) ||
+        (st = set_smem(ctx, k_cg_update<P, double, OPK_LAPLACE>, cg_smem<P, double, OPK_LAPLACE>(2))) ||
         (st = set_smem(ctx, k_cg_start<P, float, float, float>, cg_smem<P, float>(1))) ||
         (st = set_smem(ctx, k_window_correct<P>, window_smem<P>())) ||
         (st = set_smem(ctx, k_richardson_pass<P, double>, cg_smem<P, double>(0))) ||
@@ -359,25 +363,36 @@ namespace
   }
 
   // One FP64 CG solve: x_new <- A^{-1} b for nsys systems, from the extrapolated
-  // start 2 x_cur - x_prev or from the given x_new. A is the mass matrix, or with
-  // tg3 the streaming matrix M + c K_e of each system (sc); the systems of skip
-  // are left alone (populations at rest in a split TG3 sweep).
+  // start 2 x_cur - x_prev or from the given x_new. A (opk) is the mass matrix, the
+  // streaming matrix M + c K_e of each system (sc), or the Laplace operator of the
+  // stream function; the systems of skip are left alone (populations at rest in a
+  // split TG3 sweep). tol / max_its < 0: the context's CG settings.
   struct CgCall
   {
     const double *b = nullptr;
     double *x_new = nullptr;
     const double *x_cur = nullptr, *x_prev = nullptr;
     int extrapolate = 0, nsys = NM;
-    bool tg3 = false;
+    int opk = OPK_MASS;
     StreamCoef sc{};
     int skip = 0;
+    double tol = -1;
+    int max_its = -1;
   };
 
   template <typename F>
   int
-  with_op(bool tg3, F &&f)
+  with_op(int opk, F &&f)
   {
-    return tg3 ? f(std::true_type()) : f(std::false_type());
+    switch (opk)
+      {
+        case OPK_TG3:
+          return f(std::integral_constant<int, OPK_TG3>());
+        case OPK_LAPLACE:
+          return f(std::integral_constant<int, OPK_LAPLACE>());
+        default:
+          return f(std::integral_constant<int, OPK_MASS>());
+      }
   }
 
   // r = b - A x_start and the start sums; *n_tiles: the tiles of one system.
@@ -390,9 +405,9 @@ namespace
       dim3 grid = tile_grid<P>(ctx->grid);
       *n_tiles = int(grid.x * grid.y);
       grid.z = c.nsys;
-      return with_op(c.tg3, [&](auto TT) -> int {
-        constexpr bool TG3 = decltype(TT)::value;
-        k_cg_start<P, double, double, double, TG3><<<grid, THREADS, cg_smem<P, double, TG3>(1, true), ctx->stream>>>(
+      return with_op(c.opk, [&](auto OO) -> int {
+        constexpr int OPK = decltype(OO)::value;
+        k_cg_start<P, double, double, double, OPK><<<grid, THREADS, cg_smem<P, double, OPK>(1, true), ctx->stream>>>(
           geo, c.b, c.x_cur, c.x_prev, c.x_new, w.r, c.extrapolate, w.partials, c.sc, c.skip);
         LAUNCHED();
         return LBFEM_OK;
@@ -409,9 +424,9 @@ namespace
       constexpr int P = decltype(PP)::value;
       dim3 grid = tile_grid<P>(ctx->grid);
       grid.z = c.nsys;
-      return with_op(c.tg3, [&](auto TT) -> int {
-        constexpr bool TG3 = decltype(TT)::value;
-        k_cg_p<P, double, TG3><<<grid, THREADS, cg_smem<P, double, TG3>(0), ctx->stream>>>(
+      return with_op(c.opk, [&](auto OO) -> int {
+        constexpr int OPK = decltype(OO)::value;
+        k_cg_p<P, double, OPK><<<grid, THREADS, cg_smem<P, double, OPK>(0), ctx->stream>>>(
           geo, w.r, w.p[pi], w.p[1 - pi], w.state, w.partials, c.sc);
         LAUNCHED();
         return LBFEM_OK;
@@ -428,9 +443,9 @@ namespace
       constexpr int P = decltype(PP)::value;
       dim3 grid = tile_grid<P>(ctx->grid);
       grid.z = c.nsys;
-      return with_op(c.tg3, [&](auto TT) -> int {
-        constexpr bool TG3 = decltype(TT)::value;
-        k_cg_update<P, double, TG3><<<grid, THREADS, cg_smem<P, double, TG3>(2), ctx->stream>>>(
+      return with_op(c.opk, [&](auto OO) -> int {
+        constexpr int OPK = decltype(OO)::value;
+        k_cg_update<P, double, OPK><<<grid, THREADS, cg_smem<P, double, OPK>(2), ctx->stream>>>(
           geo, c.x_new, w.r, w.p[pi], w.state, w.partials, c.sc);
         LAUNCHED();
         return LBFEM_OK;
@@ -444,8 +459,8 @@ namespace
   int
   cg_run(lbfem_gpu_ctx *ctx, const CgScratch<double> &w, const CgCall &c, int64_t *its_out)
   {
-    const double tol = ctx->prm.cg_tolerance;
-    const int max_its = ctx->prm.cg_max_iterations;
+    const double tol = c.tol >= 0 ? c.tol : ctx->prm.cg_tolerance;
+    const int max_its = c.max_its > 0 ? c.max_its : ctx->prm.cg_max_iterations;
     const int nsys = c.nsys;
     CK(cudaMemsetAsync(w.state, 0, sizeof(CgState), ctx->stream));
     int n_tiles = 0, st;
@@ -693,7 +708,7 @@ namespace
     c.b = b;
     c.x_new = x_new;
     c.nsys = nsys;
-    c.tg3 = tg3;
+    c.opk = tg3 ? OPK_TG3 : OPK_MASS;
     c.sc = sc;
     return cg_solve(ctx, c, its);
   }
@@ -772,8 +787,9 @@ namespace
     CgCall c;
     c.b = ctx->d_rhs;
     c.nsys = NM;
-    c.tg3 = ctx->prm.streaming != LBFEM_STREAMING_TG2;
-    c.sc = stream_coef(e, c.tg3 ? ctx->dt * ctx->dt / 6. : 0.);
+    const bool tg3 = ctx->prm.streaming != LBFEM_STREAMING_TG2;
+    c.opk = tg3 ? OPK_TG3 : OPK_MASS;
+    c.sc = stream_coef(e, tg3 ? ctx->dt * ctx->dt / 6. : 0.);
     if (n_sweeps(ctx) == 2)
       {
         c.x_new = ctx->d_x[s];
@@ -963,8 +979,8 @@ namespace
   int
   cg_graph(lbfem_gpu_ctx *ctx, const CgCall &c, int64_t *body_kernels)
   {
-    const double tol = ctx->prm.cg_tolerance;
-    const int max_its = ctx->prm.cg_max_iterations;
+    const double tol = c.tol >= 0 ? c.tol : ctx->prm.cg_tolerance;
+    const int max_its = c.max_its > 0 ? c.max_its : ctx->prm.cg_max_iterations;
     const CgScratch<double> w = ctx_scratch(ctx);
     cudaStreamCaptureStatus cs;
     cudaGraph_t graph = nullptr;
@@ -1975,6 +1991,42 @@ lbfem_gpu_mass_solve(lbfem_gpu_ctx *ctx, double *x, const double *r, const doubl
   if ((st = download(ctx, xn, x, 1)))
     return st;
   return solve_st;
+}
+
+int
+lbfem_gpu_stream_function(lbfem_gpu_ctx *ctx, const double *velocity, double *psi)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!velocity || !psi)
+    return fail(ctx, LBFEM_ERR_ARG, "stream_function: null buffer");
+  const long long N = ctx->grid.N;
+  double *vel = ctx->d_x[ctx->x_new], *b = ctx->d_rhs, *x = ctx->d_rhs + N; // scratch between steps
+  if ((st = upload(ctx, velocity, vel, 2)))
+    return st;
+  st = with_degree(ctx->P, [&](auto PP) -> int {
+    constexpr int P = decltype(PP)::value;
+    k_psi_rhs<P><<<n_pointwise_blocks(N), THREADS, 0, ctx->stream>>>(geo_of(ctx), vel, vel + N, b);
+    LAUNCHED();
+    return LBFEM_OK;
+  });
+  if (st)
+    return st;
+  CK(cudaMemsetAsync(x, 0, sizeof(double) * N, ctx->stream));
+  // SolverCG with the Laplace diagonal from zero to 1e-12 |b|, at most 10000 iterations (io.h:90-93)
+  CgCall c;
+  c.b = b;
+  c.x_new = x;
+  c.nsys = 1;
+  c.opk = OPK_LAPLACE;
+  c.tol = 1e-12;
+  c.max_its = 10000;
+  int64_t its = 0;
+  const int solve_st = cg_run(ctx, ctx_scratch(ctx), c, &its);
+  if (solve_st != LBFEM_OK)
+    return solve_st;
+  return download(ctx, x, psi, 1);
 }
 
 int

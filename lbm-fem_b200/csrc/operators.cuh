@@ -1149,13 +1149,14 @@ namespace lbfem_gpu
       }
   }
 
-  // x pass of the general form on one footprint row / x segment: Z1, Z2, Z3 into
+  // x pass of the general form on one footprint row / x segment (Z1 with wm Mx in
+  // place of Mx, so that wm = 0 gives the Laplace operator): Z1, Z2, Z3 into
   // s_y (three arrays of NY), Z4 into s_y4[slot] when the row is the first
   // (slot 0) or last (slot 1) row of a non-periodic y axis.
   template <int P, typename R>
   __device__ __forceinline__ void
   full_xpass(const R *__restrict__ s, R *__restrict__ s_y, R *__restrict__ s_y4, const TileMaps<P, R> &m, int fy,
-             int seg, R kxx, R kyy, R kxy, int gx0, int y4_slot, int bx_lo, int bx_hi)
+             int seg, R wm, R kxx, R kyy, R kxy, int gx0, int y4_slot, int bx_lo, int bx_hi)
   {
     using T = Tile<P>;
     const R *row = s + fy * T::PF;
@@ -1202,7 +1203,7 @@ namespace lbfem_gpu
                 else if (gx == bx_hi)
                   z2 = fma(kxy, u[0], z2);
               }
-            y1[j] = fma(kxx, vK, vM);
+            y1[j] = fma(kxx, vK, wm * vM);
             y2[j] = z2;
             y3[j] = kyy * vM;
             if (y4_slot >= 0)
@@ -1276,16 +1277,26 @@ namespace lbfem_gpu
       }
   }
 
-  // A u for every own node of the tile, u staged in s_u; s_t holds tg3_scratch<P>()
-  // elements. emit(i, j, storage index, image, Au) as mass_apply (images: identity row).
-  template <int P, typename R, typename Emit>
+  // Whether node (i, j) lies on a side of the box (psi = 0 there, periodic sides included).
+  __device__ __forceinline__ bool
+  on_box_side(int i, int j, const Grid &g)
+  {
+    return i == 0 || j == 0 || i == g.nfx - 1 || j == g.nfy - 1;
+  }
+
+  // A u for every own node of the tile, A = wm M + (the K_e part of kxx, kyy, kxy),
+  // u staged in s_u; s_t holds tg3_scratch<P>() elements. emit(i, j, storage index,
+  // fixed, Au) as mass_apply: a fixed row (a periodic image; with DIRICHLET also a
+  // node on a side of the box) is the identity row.
+  template <int P, bool DIRICHLET, typename R, typename Emit>
   __device__ __forceinline__ void
-  tg3_apply(const R *s_u, R *s_t, const TileMaps<P, R> &m, const Grid &g, int gx0, int gy0, R kxx, R kyy, R kxy,
-            Emit &&emit)
+  tg3_apply(const R *s_u, R *s_t, const TileMaps<P, R> &m, const Grid &g, int gx0, int gy0, R wm, R kxx, R kyy,
+            R kxy, Emit &&emit)
   {
     using T = Tile<P>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const bool sep = kxy == R(0);
+    // the product form needs wm = 1 and an axis-parallel e
+    const bool sep = wm == R(1) && kxy == R(0) && (kxx == R(0) || kyy == R(0));
     R *s_y4 = s_t + 3 * T::NY;
     if (warp < T::NSX && lane < T::FY)
       {
@@ -1295,7 +1306,7 @@ namespace lbfem_gpu
           {
             const int gy = gy0 - P + lane;
             const int y4_slot = g.py ? -1 : gy == 0 ? 0 : gy == g.nfy - 1 ? 1 : -1;
-            full_xpass<P>(s_u, s_t, s_y4, m, lane, warp, kxx, kyy, kxy, gx0, y4_slot, g.px ? -1 : 0,
+            full_xpass<P>(s_u, s_t, s_y4, m, lane, warp, wm, kxx, kyy, kxy, gx0, y4_slot, g.px ? -1 : 0,
                           g.px ? -1 : g.nfx - 1);
           }
       }
@@ -1307,7 +1318,7 @@ namespace lbfem_gpu
         auto out = [&](int i, R v) {
           const int gy = gy0 + i;
           if (gx < g.nfx && gy < g.nfy)
-            emit(i, j, gy * g.nfx + gx, is_image(gx, gy, g), v);
+            emit(i, j, gy * g.nfx + gx, DIRICHLET ? on_box_side(gx, gy, g) : is_image(gx, gy, g), v);
         };
         if (sep)
           sep_ypass<P>(s_t, m, j, seg, kyy, out);
@@ -1316,25 +1327,86 @@ namespace lbfem_gpu
       }
   }
 
-  // The operator of a CG kernel: the mass matrix, or with TG3 the streaming
-  // matrix of system s.
-  template <int P, bool TG3, typename R, typename Emit>
+  // The operators of the CG kernels.
+  enum
+  {
+    OPK_MASS = 0,   // M (MassOperator)
+    OPK_TG3 = 1,    // M + c K_e of system s (StreamingMatrix)
+    OPK_LAPLACE = 2 // K with zero rows on the sides of the box (the stream function, io.h:31-95)
+  };
+
+  template <int P, int OPK, typename R, typename Emit>
   __device__ __forceinline__ void
   op_apply(const R *s_u, R *s_t, const TileMaps<P, R> &m, const Grid &g, int gx0, int gy0, const StreamCoef &sc,
            int s, Emit &&emit)
   {
-    if constexpr (TG3)
-      tg3_apply<P>(s_u, s_t, m, g, gx0, gy0, R(sc.kxx[s]), R(sc.kyy[s]), R(sc.kxy[s]), emit);
+    if constexpr (OPK == OPK_TG3)
+      tg3_apply<P, false>(s_u, s_t, m, g, gx0, gy0, R(1), R(sc.kxx[s]), R(sc.kyy[s]), R(sc.kxy[s]), emit);
+    else if constexpr (OPK == OPK_LAPLACE)
+      tg3_apply<P, true>(s_u, s_t, m, g, gx0, gy0, R(0), R(1), R(1), R(0), emit);
     else
       mass_apply<P>(s_u, s_t, m, g, gx0, gy0, emit);
   }
 
   // Elements of the x-pass scratch of a CG kernel.
-  template <int P, bool TG3>
+  template <int P, int OPK>
   __host__ __device__ constexpr int
   op_scratch()
   {
-    return TG3 ? tg3_scratch<P>() : Tile<P>::NY;
+    return OPK == OPK_MASS ? Tile<P>::NY : tg3_scratch<P>();
+  }
+
+  // The inverse Jacobi diagonal of the Laplace operator at storage node (c, r):
+  // diag(My (x) Kx + Ky (x) Mx) from the assembled 1-D rows; 1 on the fixed nodes.
+  template <int P>
+  __device__ __forceinline__ double
+  laplace_inv_diag(const Geo &geo, int c, int r)
+  {
+    constexpr int K = 2 * P + 1;
+    const Grid &g = geo.g;
+    if (on_box_side(c, r, g))
+      return 1.0;
+    const long long nx = g.nfx, ny = g.nfy;
+    const double mx = geo.rowx[(0 * nx + c) * K + P], kx = geo.rowx[(3 * nx + c) * K + P];
+    const double my = geo.rowy[(0 * ny + r) * K + P], ky = geo.rowy[(3 * ny + r) * K + P];
+    return 1.0 / (my * kx + ky * mx);
+  }
+
+  // The right-hand side of the stream function (io.h:64-88): b = (dphi/dx, v) -
+  // (dphi/dy, u) = (My (x) Cx^T) v - (Cy^T (x) Mx) u from the assembled 1-D rows,
+  // 0 on the sides of the box. One thread per node.
+  template <int P>
+  __global__ void
+  k_psi_rhs(const Geo geo, const double *__restrict__ u, const double *__restrict__ v, double *__restrict__ b)
+  {
+    constexpr int K = 2 * P + 1;
+    const Grid &g = geo.g;
+    const long long nx = g.nfx, ny = g.nfy;
+    LBFEM_GRID_STRIDE(idx, g.N)
+    {
+      const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
+      double s = 0;
+      if (!on_box_side(i, j, g))
+        for (int k = 0; k < K; ++k)
+          {
+            const int r = wrap(j + k - P, g.py, g.nuy, g.nfy);
+            if (r < 0)
+              continue;
+            const double my = geo.rowy[(0 * ny + j) * K + k], cyt = geo.rowy[(2 * ny + j) * K + k];
+            double sv = 0, su = 0;
+            for (int l = 0; l < K; ++l)
+              {
+                const int c = wrap(i + l - P, g.px, g.nux, g.nfx);
+                if (c < 0)
+                  continue;
+                const long long id = (long long)r * g.nfx + c;
+                sv = fma(geo.rowx[(2 * nx + i) * K + l], v[id], sv);
+                su = fma(geo.rowx[(0 * nx + i) * K + l], u[id], su);
+              }
+            s += my * sv - cyt * su;
+          }
+      b[idx] = s;
+    }
   }
 
   // ---------------------------------------- iterated lumping (Richardson)
@@ -1395,12 +1467,24 @@ namespace lbfem_gpu
     return image ? 1.0 : m.ijx[j + P] * m.ijy[i + P];
   }
 
+  // The same for the operator of a CG kernel: the mass diagonal (M and the TG3
+  // matrix, RangeJacobi of mass.h:164-176), or the Laplace diagonal.
+  template <int P, int OPK, typename RM>
+  __device__ __forceinline__ double
+  cg_inv_jacobi(const Geo &geo, const TileMaps<P, RM> &m, int gx0, int gy0, int i, int j, bool fixed)
+  {
+    if constexpr (OPK == OPK_LAPLACE)
+      return fixed ? 1.0 : laplace_inv_diag<P>(geo, gx0 + j, gy0 + i);
+    else
+      return own_inv_jacobi(m, i, j, fixed);
+  }
+
   // r = b - A xg with xg = extrapolate ? 2 x_cur - x_prev (written to x_new) : x_new;
   // partials per system: b.b, r.r, r.D^{-1}r. Storage R, arithmetic A (A = double:
   // the FP64 residual of the refinement). One system per CTA.
   // TG3: A is the streaming matrix of sc; systems whose bit is set in skip are
   // not solved (zero sums: converged at the start, x untouched).
-  template <int P, typename R, typename X = R, typename A = R, bool TG3 = false>
+  template <int P, typename R, typename X = R, typename A = R, int OPK = OPK_MASS>
   __global__ void __launch_bounds__(THREADS)
     k_cg_start(const Geo geo, const R *__restrict__ b, const X *__restrict__ x_cur, const X *__restrict__ x_prev,
                X *__restrict__ x_new, R *__restrict__ r, int extrapolate, double *__restrict__ partials,
@@ -1409,7 +1493,7 @@ namespace lbfem_gpu
     using T = Tile<P>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     A *s_u = reinterpret_cast<A *>(sm_raw), *s_t = s_u + T::NF;
-    R *s_b = reinterpret_cast<R *>(s_t + op_scratch<P, TG3>());
+    R *s_b = reinterpret_cast<R *>(s_t + op_scratch<P, OPK>());
     __shared__ TileMaps<P, A> maps;
     const Grid &g = geo.g;
     const long long N = g.N;
@@ -1436,7 +1520,7 @@ namespace lbfem_gpu
     __syncthreads();
     double part[3] = {0, 0, 0};
     R *rs = r + o;
-    op_apply<P, TG3>(s_u, s_t, maps, g, gx0, gy0, sc, s, [&](int i, int j, int idx, bool image, A Ax) {
+    op_apply<P, OPK>(s_u, s_t, maps, g, gx0, gy0, sc, s, [&](int i, int j, int idx, bool image, A Ax) {
       const long long id = o + idx;
       A xg;
       if (image)
@@ -1453,7 +1537,7 @@ namespace lbfem_gpu
       rs[idx] = R(rr);
       part[0] += double(bb) * double(bb);
       part[1] += double(rr) * double(rr);
-      part[2] += double(rr) * (own_inv_jacobi(maps, i, j, image) * double(rr));
+      part[2] += double(rr) * (cg_inv_jacobi<P, OPK>(geo, maps, gx0, gy0, i, j, image) * double(rr));
     });
     const int nt = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
     // partial (quantity k of system s) at [(k*NM + s) * n_tiles + tile]
@@ -1461,7 +1545,7 @@ namespace lbfem_gpu
   }
 
   // p <- D^{-1} r + beta p (p <- D^{-1} r on the first iteration); partial p.Ap. One system per CTA.
-  template <int P, typename R, bool TG3 = false>
+  template <int P, typename R, int OPK = OPK_MASS>
   __global__ void __launch_bounds__(THREADS)
     k_cg_p(const Geo geo, const R *__restrict__ r, const R *__restrict__ p_in, R *__restrict__ p_out,
            const CgState *__restrict__ st, double *__restrict__ partials, const StreamCoef sc)
@@ -1484,13 +1568,13 @@ namespace lbfem_gpu
     __syncthreads();
     const R *rsys = r + o, *psys = p_in + o;
     stage_ij<P>(s_u, maps, [&](long long idx, int c, int rw) -> R {
-      const R z = R(geo.ijx[c] * geo.ijy[rw]) * rsys[idx];
+      const R z = R(OPK == OPK_LAPLACE ? laplace_inv_diag<P>(geo, c, rw) : geo.ijx[c] * geo.ijy[rw]) * rsys[idx];
       return first ? z : fma(beta, psys[idx], z);
     });
     __syncthreads();
     double part[1] = {0};
     R *posys = p_out + o;
-    op_apply<P, TG3>(s_u, s_t, maps, g, gx0, gy0, sc, s, [&](int i, int j, int idx, bool image, R Ap) {
+    op_apply<P, OPK>(s_u, s_t, maps, g, gx0, gy0, sc, s, [&](int i, int j, int idx, bool image, R Ap) {
       R pn;
       if (image)
         {
@@ -1506,7 +1590,7 @@ namespace lbfem_gpu
   }
 
   // v = A p recomputed; x += alpha p, r -= alpha v; partials r.r, r.D^{-1}r. One system per CTA.
-  template <int P, typename R, bool TG3 = false>
+  template <int P, typename R, int OPK = OPK_MASS>
   __global__ void __launch_bounds__(THREADS)
     k_cg_update(const Geo geo, R *__restrict__ x, R *__restrict__ r, const R *__restrict__ p,
                 const CgState *__restrict__ st, double *__restrict__ partials, const StreamCoef sc)
@@ -1526,7 +1610,7 @@ namespace lbfem_gpu
     const R al = R(st->alpha[s]);
     const long long o = s * N;
     const R *ps = p + o;
-    R *s_x = s_t + op_scratch<P, TG3>(), *s_r = s_x + T::TX * T::TY;
+    R *s_x = s_t + op_scratch<P, OPK>(), *s_r = s_x + T::TX * T::TY;
     __syncthreads();
     stage<P>(s_u, maps, [&](long long idx) { return ps[idx]; });
     stage_own<P>(s_x, x + o, g, gx0, gy0);
@@ -1534,7 +1618,7 @@ namespace lbfem_gpu
     __syncthreads();
     double part[2] = {0, 0};
     R *xs = x + o, *rs = r + o;
-    op_apply<P, TG3>(s_u, s_t, maps, g, gx0, gy0, sc, s, [&](int i, int j, int idx, bool image, R Ap) {
+    op_apply<P, OPK>(s_u, s_t, maps, g, gx0, gy0, sc, s, [&](int i, int j, int idx, bool image, R Ap) {
       const R pv = image ? ps[idx] : s_u[(i + P) * T::PF + j + P];
       if (image)
         Ap = pv;
@@ -1543,7 +1627,7 @@ namespace lbfem_gpu
       const R rr = s_r[t] + -al * Ap;
       rs[idx] = rr;
       part[0] += double(rr) * double(rr);
-      part[1] += double(rr) * (own_inv_jacobi(maps, i, j, image) * double(rr));
+      part[1] += double(rr) * (cg_inv_jacobi<P, OPK>(geo, maps, gx0, gy0, i, j, image) * double(rr));
     });
     block_reduce_store<2>(part, partials + (long long)s * nt, tile, NM * nt);
   }

@@ -171,6 +171,13 @@ class Handle:
         self._call("mass_solve", self.h, _dptr(x), _dptr(r), _dptr(e), C.c_double(tg3_coefficient))
         return x
 
+    def stream_function(self, velocity):
+        """compute_stream_function (io.h:31-95): psi from velocity = (u, v) (2 x n_dofs)."""
+        velocity = _f64(velocity).reshape(2, self.n)
+        psi = np.empty(self.n)
+        self._call("stream_function", self.h, _dptr(velocity), _dptr(psi))
+        return psi
+
     def mass_vmult(self, x):
         x = _f64(x)
         y = np.empty(self.n)
@@ -224,7 +231,7 @@ def declare(lib, prefix):
         "set_populations": [vp, dp], "get_populations": [vp, dp], "step": [vp, i32],
         "step_host": [vp, dp, i32], "synchronize": [vp],
         "advection": [vp, dp, dp, dp, d, d, i32, i32, dp],
-        "mass_solve": [vp, dp, dp, dp, d], "mass_vmult": [vp, dp, dp],
+        "mass_solve": [vp, dp, dp, dp, d], "mass_vmult": [vp, dp, dp], "stream_function": [vp, dp, dp],
         "cg_iterations": [vp, C.POINTER(i64)], "collide_bgk": [vp, dp, d],
         "compute_equilibrium": [vp, dp, dp], "predictor_corrector": [vp, dp, dp, dp, d],
         "node_weight": [vp, dp], "jacobi_diagonal": [vp, dp], "conservation": [vp, dp],

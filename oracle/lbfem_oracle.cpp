@@ -948,6 +948,178 @@ namespace
     predictor_corrector(o, o.f.data(), o.feq.data(), o.x0.data(), o.dt / o.lambda);
     return LBFEM_OK;
   }
+  // ------------------------------------------------------- stream function
+  // compute_stream_function (io.h:31-95): (grad phi, grad psi) = (dphi/dx, v) -
+  // (dphi/dy, u) with psi = 0 on every side of the box (make_zero_boundary_
+  // constraints covers all boundary faces, periodic ones included, and psi has
+  // no periodicity constraint), Jacobi-PCG to 1e-12 |b|, at most 10000
+  // iterations. psi's DoFs are all stored nodes, images included; the velocity
+  // is read through the periodic images (read_dof_values of index 0).
+  inline bool
+  psi_fixed(const lbfem_oracle &o, int i, int j)
+  {
+    return i == 0 || j == 0 || i == o.nfx - 1 || j == o.nfy - 1;
+  }
+
+  // mode 0: dst = b(u, v); mode 1: dst = K src (the Laplace cell integrals); mode 2:
+  // dst = the diagonal of K. Constrained rows are not treated here.
+  template <int P>
+  void
+  psi_cells(const lbfem_oracle &o, const double *u, const double *v, const double *src, double *dst, int mode)
+  {
+    constexpr int n = P + 1;
+    const Basis &B = *o.basis;
+    std::fill(dst, dst + o.N, 0.);
+    for_cells_coloured(o, [&](int cx, int cy) {
+      const double hx = o.vx[cx + 1] - o.vx[cx], hy = o.vy[cy + 1] - o.vy[cy];
+      int64_t own[n][n], src_idx[n][n];
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+          {
+            own[j][i] = int64_t(cy * P + j) * o.nfx + cx * P + i;
+            src_idx[j][i] = o.master(cx * P + i, cy * P + j);
+          }
+      double out[n][n] = {};
+      for (int q2 = 0; q2 < n; ++q2)
+        for (int q1 = 0; q1 < n; ++q1)
+          {
+            const double JxW = B.qw[q1] * B.qw[q2] * hx * hy;
+            if (mode == 2)
+              {
+                for (int bb = 0; bb < n; ++bb)
+                  for (int aa = 0; aa < n; ++aa)
+                    {
+                      const double gx = B.S[q2][bb] * B.D[q1][aa] / hx, gy = B.D[q2][bb] * B.S[q1][aa] / hy;
+                      out[bb][aa] += (gx * gx + gy * gy) * JxW;
+                    }
+                continue;
+              }
+            double fx = 0, fy = 0;
+            if (mode == 0)
+              {
+                double uq = 0, vq = 0;
+                for (int bb = 0; bb < n; ++bb)
+                  for (int aa = 0; aa < n; ++aa)
+                    {
+                      const double phi = B.S[q2][bb] * B.S[q1][aa];
+                      uq += phi * u[src_idx[bb][aa]];
+                      vq += phi * v[src_idx[bb][aa]];
+                    }
+                fx = vq;
+                fy = -uq;
+              }
+            else
+              {
+                for (int bb = 0; bb < n; ++bb)
+                  for (int aa = 0; aa < n; ++aa)
+                    {
+                      fx += B.S[q2][bb] * B.D[q1][aa] / hx * src[own[bb][aa]];
+                      fy += B.D[q2][bb] * B.S[q1][aa] / hy * src[own[bb][aa]];
+                    }
+              }
+            for (int bb = 0; bb < n; ++bb)
+              for (int aa = 0; aa < n; ++aa)
+                out[bb][aa] += (B.S[q2][bb] * B.D[q1][aa] / hx * fx + B.D[q2][bb] * B.S[q1][aa] / hy * fy) * JxW;
+          }
+      for (int bb = 0; bb < n; ++bb)
+        for (int aa = 0; aa < n; ++aa)
+          dst[own[bb][aa]] += out[bb][aa];
+    });
+  }
+
+  void
+  psi_cells_dispatch(const lbfem_oracle &o, const double *u, const double *v, const double *src, double *dst,
+                     int mode)
+  {
+    switch (o.p)
+      {
+        case 1:
+          psi_cells<1>(o, u, v, src, dst, mode);
+          break;
+        case 2:
+          psi_cells<2>(o, u, v, src, dst, mode);
+          break;
+        case 3:
+          psi_cells<3>(o, u, v, src, dst, mode);
+          break;
+        default:
+          psi_cells<4>(o, u, v, src, dst, mode);
+      }
+  }
+
+  // The Laplace operator of psi with identity rows on the fixed (boundary) nodes;
+  // their entries of src are read as zero (homogeneous constraints).
+  void
+  laplace_vmult(const lbfem_oracle &o, double *dst, const double *src, std::vector<double> &tmp)
+  {
+    tmp.assign(src, src + o.N);
+    for (int j = 0; j < o.nfy; ++j)
+      for (int i = 0; i < o.nfx; ++i)
+        if (psi_fixed(o, i, j))
+          tmp[int64_t(j) * o.nfx + i] = 0.;
+    psi_cells_dispatch(o, nullptr, nullptr, tmp.data(), dst, 1);
+    for (int j = 0; j < o.nfy; ++j)
+      for (int i = 0; i < o.nfx; ++i)
+        if (psi_fixed(o, i, j))
+          dst[int64_t(j) * o.nfx + i] = src[int64_t(j) * o.nfx + i];
+  }
+
+  int
+  stream_function(lbfem_oracle &o, const double *u, const double *v, double *psi, int64_t *its)
+  {
+    const int64_t N = o.N;
+    std::vector<double> b(N), diag(N), r(N), z(N), p(N), w(N), tmp;
+    psi_cells_dispatch(o, u, v, nullptr, b.data(), 0);
+    psi_cells_dispatch(o, nullptr, nullptr, nullptr, diag.data(), 2);
+    for (int j = 0; j < o.nfy; ++j)
+      for (int i = 0; i < o.nfx; ++i)
+        if (psi_fixed(o, i, j))
+          {
+            b[int64_t(j) * o.nfx + i] = 0.; // distribute_local_to_global drops constrained rows
+            diag[int64_t(j) * o.nfx + i] = 1.;
+          }
+    std::fill(psi, psi + N, 0.);
+    // SolverCG with the Jacobi preconditioner from zero, tolerance 1e-12 |b| (io.h:90-92)
+    const double tol = 1e-12 * std::sqrt(dot(b.data(), b.data(), N));
+    std::copy(b.begin(), b.end(), r.begin());
+    double res = std::sqrt(dot(r.data(), r.data(), N)), rz = 0;
+    *its = 0;
+    if (res <= tol)
+      return LBFEM_OK;
+    for (int it = 1;; ++it)
+      {
+        for (int64_t k = 0; k < N; ++k)
+          z[k] = r[k] / diag[k];
+        const double rz_prev = rz;
+        rz = dot(r.data(), z.data(), N);
+        if (it > 1)
+          for (int64_t k = 0; k < N; ++k)
+            p[k] = (rz / rz_prev) * p[k] + z[k];
+        else
+          std::copy(z.begin(), z.end(), p.begin());
+        laplace_vmult(o, w.data(), p.data(), tmp);
+        const double alpha = rz / dot(p.data(), w.data(), N);
+        for (int64_t k = 0; k < N; ++k)
+          {
+            psi[k] += alpha * p[k];
+            r[k] += -alpha * w[k];
+          }
+        res = std::sqrt(dot(r.data(), r.data(), N));
+        *its = it;
+        if (std::isnan(res))
+          return LBFEM_ERR_NONFINITE;
+        if (res <= tol)
+          break;
+        if (it >= 10000)
+          return LBFEM_ERR_NO_CONVERGENCE;
+      }
+    // zero.distribute(psi): the fixed nodes are 0
+    for (int j = 0; j < o.nfy; ++j)
+      for (int i = 0; i < o.nfx; ++i)
+        if (psi_fixed(o, i, j))
+          psi[int64_t(j) * o.nfx + i] = 0.;
+    return LBFEM_OK;
+  }
 } // namespace
 
 extern "C" {
@@ -1291,4 +1463,13 @@ lbfem_oracle_conservation(lbfem_oracle *h, double out[5])
   return LBFEM_OK;
 }
 
+
+int
+lbfem_oracle_stream_function(lbfem_oracle *h, const double *velocity, double *psi)
+{
+  if (!h || !velocity || !psi)
+    return LBFEM_ERR_ARG;
+  int64_t its = 0;
+  return stream_function(*h, velocity, velocity + h->N, psi, &its);
+}
 } // extern "C"

@@ -50,6 +50,8 @@ int lbfem_oracle_predictor_corrector(lbfem_oracle *h, double *f, const double *f
 int lbfem_oracle_node_weight(lbfem_oracle *h, double *w);
 int lbfem_oracle_jacobi_diagonal(lbfem_oracle *h, double *d);
 int lbfem_oracle_conservation(lbfem_oracle *h, double out[5]);
+/* compute_stream_function (io.h:31-95): velocity = (u, v), 2 blocks of n_dofs; psi: n_dofs. */
+int lbfem_oracle_stream_function(lbfem_oracle *h, const double *velocity, double *psi);
 /* 1-D reference data of FE_Q(p): Gauss-Lobatto support points (p+1), Gauss points and weights (p+1). */
 int lbfem_oracle_basis_1d(int32_t p, double *support, double *gauss_points, double *gauss_weights);
 

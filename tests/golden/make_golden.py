@@ -15,7 +15,11 @@ It writes
                          its plotting code uses);
   stencil_bench.json  -- the check value printed by the reference's
                          benchmarks/stencil_bench.cc (Q1 lumped Lax-Wendroff
-                         streaming, periodic N x N grid, dt = h/4) for several N.
+                         streaming, periodic N x N grid, dt = h/4) for several N;
+  cavity_Re1000.dat.gz -- the reference's own steady cavity result
+                         data/cavity/cavity_Re1000.dat (gnuplot rows
+                         x y u/U0 v/U0 psi/(U0 L) rho-rho0 of 32^2 Q2 elements,
+                         stretch 1.2, and the vortex extrema), gzipped as is.
 
 The fixtures are committed; tests never read the reference at run time.
 """
@@ -105,7 +109,18 @@ def make_stencil_bench():
             "dt_over_h": 0.25, "rows": rows}
 
 
+def copy_cavity(name="cavity_Re1000.dat"):
+    import gzip
+
+    with open(os.path.join(REF, "data", "cavity", name), "rb") as src:
+        data = src.read()
+    with gzip.GzipFile(os.path.join(HERE, name + ".gz"), "wb", mtime=0) as dst:
+        dst.write(data)
+    print("wrote", name + ".gz")
+
+
 if __name__ == "__main__":
+    copy_cavity()
     for name, fn in (("stencils.json", make_stencils), ("tg_spectral.json", make_tg_spectral),
                      ("stencil_bench.json", make_stencil_bench)):
         with open(os.path.join(HERE, name), "w") as fh:

@@ -225,6 +225,57 @@ def test_tg3_needs_bardow_and_consistent_mass(oracle_mod):
             oracle_mod.Oracle(m, make_params(scheme, mass, streaming="tg3-split"))
 
 
+def _cavity_golden():
+    """data/cavity/cavity_Re1000.dat of the reference (32^2 Q2, stretch 1.2, Ma 0.1):
+    its text and its rows x y u/U0 v/U0 psi/(U0 L) rho-rho0."""
+    import gzip
+
+    text = gzip.open(os.path.join(GOLDEN, "cavity_Re1000.dat.gz"), "rt").read()
+    rows = np.array([ln.split() for ln in text.splitlines() if ln.strip() and not ln.startswith("#")], float)
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    tc.set_reynolds(1000)
+    return text, rows, tc, cases.build_mesh(tc, 32, 2)
+
+
+def test_stream_function_reproduces_the_reference_cavity(oracle_mod):
+    """compute_stream_function (io.h:31-95) of the reference's own steady cavity
+    velocities gives its printed psi to the print resolution, on the same nodes."""
+    text, rows, tc, m = _cavity_golden()
+    x, y = m.nodes()
+    assert np.max(np.abs(rows[:, 0] - x)) < 1e-6 and np.max(np.abs(rows[:, 1] - y)) < 1e-6
+    o = oracle_mod.Oracle(m, make_params("bardow", "lumped"))
+    psi = o.stream_function(np.stack([rows[:, 2], rows[:, 3]])) / tc.L
+    assert np.max(np.abs(psi - rows[:, 4])) < 1e-6, np.max(np.abs(psi - rows[:, 4]))
+    assert np.all(psi[m.constrained() | (x == 0) | (y == 0) | (x == 1) | (y == 1)] == 0)
+
+
+def test_gnuplot_writer_reproduces_the_reference_cavity_file(oracle_mod):
+    """cgdbe.cc:399-472: the same header, row order, blank lines, number format
+    and vortex lines as the reference's file, from populations with its moments."""
+    from lbfem_gpu import io
+
+    text, rows, tc, m = _cavity_golden()
+    o = oracle_mod.Oracle(m, make_params("bardow", "lumped"))
+    o.set_time_step(1e-3, 1e-3)
+    o.set_populations(d2q9.equilibrium(1 + rows[:, 5], rows[:, 2] * tc.U0, rows[:, 3] * tc.U0))
+    out = io.gnuplot_text(o, m, tc, t_over_tref=32.9998, step=391314, reynolds=1000, mach=0.1, n_cells=32)
+    a, b = text.splitlines(), out.splitlines()
+    assert len(a) == len(b) and a[:2] == b[:2]
+    assert [ln == "" for ln in a] == [ln == "" for ln in b]
+    same = 0
+    for la, lb in zip(a, b):
+        if la == lb:
+            same += 1
+            continue
+        va, vb = [float(t) for t in la.split()[-6:] if t[0] in "-.0123456789"], \
+                 [float(t) for t in lb.split()[-6:] if t[0] in "-.0123456789"]
+        # the last printed digit of psi may differ: the velocities it is solved from are rounded to 6 digits
+        assert np.allclose(va, vb, rtol=5e-5, atol=1e-6), (la, lb)
+    assert same > 0.8 * len(a)
+    assert [ln.split(":")[0] for ln in a[-3:]] == ["# primary vortex", "# lower left vortex", "# lower right vortex"]
+    assert a[-3] == b[-3] and a[-1] == b[-1]
+
+
 def test_couette_steady_profile(oracle_mod):
     """docs/results.md:253-260: the steady linear profile to solver tolerance (16 elements, Re 10, t = 2 L^2/nu)."""
     tc = cases.CouetteFlow(0.1)
