@@ -1819,6 +1819,7 @@ namespace lbfem_gpu
     double *s_my = reinterpret_cast<double *>(s_w + PF * FY);       // [TY][K] My rows of the own rows
     __shared__ __align__(16) float s_lx[FX * NC], s_ly[FY * NC];     // factors (apart from the window: no aliasing)
     __shared__ int s_col[FX], s_row[FY];                             // storage column / row, -1 outside the grid
+    __shared__ long long s_rowoff[FY];                               // storage offset of a window row, -1 outside
     __shared__ double s_ijy[S::TY];                                  // inverse Jacobi factors of the own rows
     const int s = blockIdx.z;
     const Grid &g = geo.g;
@@ -1854,7 +1855,11 @@ namespace lbfem_gpu
     for (int t = tid; t < FX; t += NT)
       s_col[t] = wrap(gx0 - W + t, g.px, g.nux, g.nfx);
     for (int t = tid; t < FY; t += NT)
-      s_row[t] = wrap(gy0 - W + t, g.py, g.nuy, g.nfy);
+      {
+        const int r = wrap(gy0 - W + t, g.py, g.nuy, g.nfy);
+        s_row[t] = r;
+        s_rowoff[t] = r < 0 ? -1 : (long long)r * g.nfx;
+      }
     for (int t = tid; t < S::TY * K; t += NT)
       {
         const int i = t / K, k = t - i * K, gy = gy0 + i;
@@ -1863,14 +1868,19 @@ namespace lbfem_gpu
     for (int t = tid; t < S::TY; t += NT)
       s_ijy[t] = gy0 + t < g.nfy ? geo.ijy[gy0 + t] : 0.0;
     __syncthreads();
-    // the window of r_in by asynchronous copies, all in flight at once; meanwhile
-    // this thread's column of x_in (own rows and a halo of P) and of b into registers
-    for (int t = tid; t < FX * FY; t += NT)
+    // the window of r_in by asynchronous copies, all in flight at once, a window
+    // column per thread (consecutive threads: consecutive addresses); meanwhile
+    // this thread's column of x_in (own rows and a halo of P) into registers
+    for (int c = tid; c < FX; c += NT)
       {
-        const int q = t / FX, c = t - q * FX;
-        const int row = s_row[q], col = s_col[c];
-        const bool ok = row >= 0 && col >= 0;
-        cp_async4(&s_w[q * PF + c], ok ? rs + ((long long)row * g.nfx + col) : rs, ok);
+        const int col = s_col[c];
+#pragma unroll 8
+        for (int q = 0; q < FY; ++q)
+          {
+            const long long ro = s_rowoff[q];
+            const bool ok = ro >= 0 && col >= 0;
+            cp_async4(&s_w[q * PF + c], ok ? rs + (ro + col) : rs, ok);
+          }
       }
     const int cw = W - P + tid; // window column of this thread's y solve
     float xr[S::TY + 2 * P];
