@@ -153,7 +153,7 @@ namespace lbfem_gpu
 
   // predictor_corrector on FP32 deviations d = f - w with the FP32 increment x, in
   // FP64 arithmetic (the corrector's theta (feq(fhat) - feq(f)) cancels).
-  __global__ void
+  __global__ void __launch_bounds__(THREADS, 4) // 4 CTAs per SM: more loads in flight, a few spills
   k_predictor_corrector_dev(const Geo geo, DevStats *__restrict__ ds, float *__restrict__ d,
                             const float *__restrict__ x, double theta)
   {
@@ -1652,6 +1652,7 @@ namespace lbfem_gpu
     static constexpr int PF = FX + 4;
     static constexpr int NC = P == 1 ? 2 : P <= 3 ? 4 : 8; // factor floats per window position (padded)
     static constexpr int K = 2 * P + 1;                    // entries of an assembled 1-D row
+    static constexpr int KP = K + 1;                       // row pitch of the My rows (16-byte pairs)
     static constexpr int THREADS = 160;
     static_assert(FY <= THREADS && TX + 2 * P <= THREADS, "one thread per window row and per own-plus-halo column");
     static_assert(FX % 8 == 0 && FY % 4 == 0 && W - P >= 3, "whole chunks; the backward sweeps stop at W - P");
@@ -1662,7 +1663,7 @@ namespace lbfem_gpu
   window_smem()
   {
     using S = WinShape<P>;
-    return sizeof(float) * size_t(S::PF) * S::FY + sizeof(double) * S::TY * S::K;
+    return sizeof(float) * size_t(S::PF) * S::FY + sizeof(double) * S::TY * S::KP;
   }
 
   // The factor row of window position q: l[k-1] = l_{q,q-k}, l[P] = 1/d_q (one
@@ -1762,21 +1763,30 @@ namespace lbfem_gpu
 #pragma unroll
     for (int k = 0; k < P; ++k)
       y[k] = 0.f; // y[k]: the value k + 1 positions ahead
+    // the factor rows of the P positions after the chunk: the first P rows of the
+    // previous chunk (none after the last position)
+    float lp[P][P + 1];
+#pragma unroll
+    for (int u = 0; u < P; ++u)
+#pragma unroll
+      for (int k = 0; k <= P; ++k)
+        lp[u][k] = 0.f;
 #pragma unroll 2
     for (int q0 = n - CH; q0 + CH > stop; q0 -= CH) // the last chunk may reach below stop
       {
         float v[CH], l[CH + P][P + 1];
         load4(q0, v);
 #pragma unroll
-        for (int u = 0; u < CH + P; ++u)
-          {
-            if (q0 + u < n)
-              ldl_row<P, NC>(c, q0 + u, l[u]);
-            else
+        for (int u = 0; u < CH; ++u)
+          ldl_row<P, NC>(c, q0 + u, l[u]);
 #pragma unroll
-              for (int k = 0; k <= P; ++k)
-                l[u][k] = 0.f;
-          }
+        for (int u = 0; u < P; ++u)
+#pragma unroll
+          for (int k = 0; k <= P; ++k)
+            {
+              l[CH + u][k] = lp[u][k];
+              lp[u][k] = l[u][k];
+            }
 #pragma unroll
         for (int u = CH - 1; u >= 0; --u)
           {
@@ -1816,7 +1826,7 @@ namespace lbfem_gpu
     constexpr int W = S::W, FX = S::FX, FY = S::FY, PF = S::PF, NC = S::NC, K = S::K, NT = S::THREADS;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     float *s_w = reinterpret_cast<float *>(sm_raw);                  // [FY][PF] the window
-    double *s_my = reinterpret_cast<double *>(s_w + PF * FY);       // [TY][K] My rows of the own rows
+    double *s_my = reinterpret_cast<double *>(s_w + PF * FY);       // [TY][KP] My rows of the own rows (zero padded)
     __shared__ __align__(16) float s_lx[FX * NC], s_ly[FY * NC];     // factors (apart from the window: no aliasing)
     __shared__ int s_col[FX], s_row[FY];                             // storage column / row, -1 outside the grid
     __shared__ long long s_rowoff[FY];                               // storage offset of a window row, -1 outside
@@ -1860,10 +1870,10 @@ namespace lbfem_gpu
         s_row[t] = r;
         s_rowoff[t] = r < 0 ? -1 : (long long)r * g.nfx;
       }
-    for (int t = tid; t < S::TY * K; t += NT)
+    for (int t = tid; t < S::TY * S::KP; t += NT)
       {
-        const int i = t / K, k = t - i * K, gy = gy0 + i;
-        s_my[t] = (gy < g.nfy && !(g.py && gy == g.nuy)) ? geo.rowy[(long long)gy * K + k] : 0.0;
+        const int i = t / S::KP, k = t - i * S::KP, gy = gy0 + i;
+        s_my[t] = (k < K && gy < g.nfy && !(g.py && gy == g.nuy)) ? geo.rowy[(long long)gy * K + k] : 0.0;
       }
     for (int t = tid; t < S::TY; t += NT)
       s_ijy[t] = gy0 + t < g.nfy ? geo.ijy[gy0 + t] : 0.0;
@@ -1984,13 +1994,17 @@ namespace lbfem_gpu
             else
               {
                 xv = s_w[(W + i) * PF + c];
-                double a0 = s_my[i * K] * t[0], a1 = s_my[i * K + 1] * t[1];
+                // the row's coefficients in 16-byte pairs (broadcast loads)
+                const double2 *my = reinterpret_cast<const double2 *>(s_my + i * S::KP);
+                const double2 m0 = my[0];
+                double a0 = m0.x * t[0], a1 = m0.y * t[1];
 #pragma unroll
                 for (int k = 2; k < K; k += 2)
                   {
-                    a0 = fma(s_my[i * K + k], t[k], a0);
+                    const double2 mk = my[k / 2];
+                    a0 = fma(mk.x, t[k], a0);
                     if (k + 1 < K)
-                      a1 = fma(s_my[i * K + k + 1], t[k + 1], a1);
+                      a1 = fma(mk.y, t[k + 1], a1);
                   }
                 ax = a0 + a1;
               }
