@@ -1645,6 +1645,8 @@ namespace lbfem_gpu
     // check then finds the residual at about 1e-5 of the round's start residual
     static constexpr int W = P == 1 ? 8 : P == 2 ? 12 : P == 3 ? 16 : 20;
     static constexpr int TX = 128, TY = 64;                // own nodes
+    // CTAs per SM the registers are sized for (shared memory admits 4 / 3 / 3 / 2)
+    static constexpr int MIN_CTAS = P == 1 ? 4 : P == 4 ? 2 : 3;
     static constexpr int FX = TX + 2 * W, FY = TY + 2 * W; // window
     // pitch = 4 (mod 8): rows are 16-byte aligned, and eight lanes on eight rows hit
     // distinct bank groups with 16-byte accesses (row sweeps) as with 4-byte ones
@@ -1816,7 +1818,7 @@ namespace lbfem_gpu
   // round in the same buffers. x and r are never updated in place (the halos
   // read the inputs). Periodic images have identity rows.
   template <int P>
-  __global__ void __launch_bounds__(WinShape<P>::THREADS, 2)
+  __global__ void __launch_bounds__(WinShape<P>::THREADS, WinShape<P>::MIN_CTAS)
     k_window_correct(const Geo geo, const float *__restrict__ lx, const float *__restrict__ ly,
                      const float *__restrict__ r_in, const float *__restrict__ x_in, const float *__restrict__ b,
                      float *__restrict__ x_out, float *__restrict__ r_out, const CgState *__restrict__ st, int all,
