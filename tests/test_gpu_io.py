@@ -75,3 +75,30 @@ def test_gnuplot_writer_through_the_gpu(gpu_lib, oracle_mod):
     assert len(a) == len(b) == len(text.splitlines())
     diff = [(la, lb) for la, lb in zip(a, b) if la != lb]
     assert len(diff) <= 0.01 * len(a), diff[:5]
+
+
+def test_cavity_continuation_against_ghia(gpu_lib, oracle_mod):
+    """The reference's CI run (ci.yml:44-58: cavity 16^2 Q1, Bardow, lumped, CFL 0.4,
+    Re 100 then 400) on the GPU: the same steady states as the oracle (same step
+    counts, psi within 1e-9) and psi_max within 10% of Ghia, Ghia & Shin."""
+    from helpers import setup_case
+    from lbfem_gpu import driver, io
+
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    tc.set_reynolds(100)
+    m = cases.build_mesh(tc, 16, 1)
+    dt = m.time_step(0.4)
+    prm = make_params("bardow", "lumped")
+    g = setup_case(_gpu, tc, m, prm, dt, tc.relaxation_time())
+    o = setup_case(oracle_mod.Oracle, tc, m, prm, dt, tc.relaxation_time())
+    for Re, ghia in ((100, 0.1034), (400, 0.1139)):
+        if Re != 100:
+            tc.set_reynolds(Re)
+            g.set_time_step(dt, tc.relaxation_time())
+            o.set_time_step(dt, tc.relaxation_time())
+        sg, cg, _ = driver.steady_state(g, m, tc, dt)
+        so, co, _ = driver.steady_state(o, m, tc, dt)
+        assert cg and co and sg == so
+        psi = [io.nodal_rows(h, m, tc, True)[:, 4] for h in (g, o)]
+        assert rel_l2(psi[0], psi[1]) <= 1e-9, rel_l2(psi[0], psi[1])
+        assert abs(psi[0].max() - ghia) <= 0.1 * ghia, (Re, psi[0].max())

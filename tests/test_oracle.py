@@ -276,6 +276,29 @@ def test_gnuplot_writer_reproduces_the_reference_cavity_file(oracle_mod):
     assert a[-3] == b[-3] and a[-1] == b[-1]
 
 
+def test_cavity_continuation_against_ghia(oracle_mod):
+    """The reference's CI check (ci.yml:44-58): cavity, 16^2 Q1, Bardow, lumped mass,
+    CFL 0.4, Re 100 to a steady state, then continued to Re 400; psi_max within 10%
+    of Ghia, Ghia & Shin (1982): 0.1034 and 0.1139."""
+    from lbfem_gpu import driver, io
+
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    tc.set_reynolds(100)
+    m = cases.build_mesh(tc, 16, 1)
+    dt = m.time_step(0.4)
+    o = setup_case(oracle_mod.Oracle, tc, m, make_params("bardow", "lumped"), dt, tc.relaxation_time())
+    for Re, ghia in ((100, 0.1034), (400, 0.1139)):
+        if Re != 100:
+            tc.set_reynolds(Re)
+            o.set_time_step(dt, tc.relaxation_time())
+        steps, converged, rate = driver.steady_state(o, m, tc, dt)
+        assert converged, (Re, steps, rate)
+        text = io.gnuplot_text(o, m, tc, t_over_tref=steps * dt / tc.reference_time(), step=steps, reynolds=Re,
+                               mach=0.1, n_cells=16)
+        psi_max = float([ln for ln in text.splitlines() if ln.startswith("# primary vortex")][0].split()[5])
+        assert abs(psi_max - ghia) <= 0.1 * ghia, (Re, psi_max)
+
+
 def test_couette_steady_profile(oracle_mod):
     """docs/results.md:253-260: the steady linear profile to solver tolerance (16 elements, Re 10, t = 2 L^2/nu)."""
     tc = cases.CouetteFlow(0.1)
