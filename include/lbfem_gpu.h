@@ -130,6 +130,8 @@ int lbfem_gpu_device_count(void);
  * Creates a context: exports the discretisation to flat device arrays and
  * builds the operators (Discretization::reinit + Scheme constructor,
  * discretization.h:78-144, schemes.h:85-90,111-116, streaming.h:41-60).
+ * A mesh of 2^31 or more nodes is refused with LBFEM_ERR_UNSUPPORTED (the
+ * kernels index a population array with 32-bit indices).
  */
 int lbfem_gpu_create(const lbfem_mesh_desc *mesh, const lbfem_params *params, lbfem_gpu_ctx **ctx);
 int lbfem_gpu_destroy(lbfem_gpu_ctx *ctx);

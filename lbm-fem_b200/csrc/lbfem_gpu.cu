@@ -1480,6 +1480,9 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
   if (!(prm->cg_tolerance >= 0) || prm->cg_max_iterations < 1 || !(prm->mixed_tolerance >= 0))
     return LBFEM_ERR_ARG;
   const int P = m->degree;
+  // the kernels index a population array with 32-bit storage indices: fewer than 2^31 nodes
+  if (((long long)P * m->n_cells_x + 1) * ((long long)P * m->n_cells_y + 1) >= (1LL << 31))
+    return LBFEM_ERR_UNSUPPORTED;
   const int nfx = P * m->n_cells_x + 1, nfy = P * m->n_cells_y + 1;
   const long long N = (long long)nfx * nfy;
   if (m->dof_index == nullptr && m->n_dofs != N)

@@ -54,6 +54,24 @@ def test_no_gpu_fails_loudly():
     assert ei.value.status == _abi.LBFEM_ERR_CUDA
 
 
+def test_meshes_of_2_31_nodes_are_refused():
+    """The kernels index a population array with 32-bit storage indices: create
+    refuses a mesh of 2^31 or more nodes before it touches the device."""
+    import lbfem_gpu
+
+    lib = lbfem_gpu.library()
+    for p, n in ((4, 11586), (1, 46341)):
+        vx = np.arange(n + 1, dtype=np.float64)
+        nd = (p * n + 1) ** 2
+        assert nd >= 2 ** 31
+        desc = _abi.MeshDesc(p, n, n, 1, 1, vx.ctypes.data_as(C.POINTER(C.c_double)),
+                             vx.ctypes.data_as(C.POINTER(C.c_double)), nd, None, 0, None, None)
+        prm = lbfem_gpu.make_params()
+        h = C.c_void_p()
+        assert lib.lbfem_gpu_create(C.byref(desc), C.byref(prm), C.byref(h)) == _abi.LBFEM_ERR_UNSUPPORTED
+        assert not h.value
+
+
 def test_gauss_lobatto_points_match_oracle(oracle_mod):
     for p in (1, 2, 3, 4):
         s, _, _ = oracle_mod.basis_1d(p)
