@@ -1483,7 +1483,9 @@ namespace lbfem_gpu
   // partials per system: b.b, r.r, r.D^{-1}r. Storage R, arithmetic A (A = double:
   // the FP64 residual of the refinement). One system per CTA.
   // TG3: A is the streaming matrix of sc; systems whose bit is set in skip are
-  // not solved (zero sums: converged at the start, x untouched).
+  // not solved (zero sums: converged at the start, x untouched). With FP32
+  // arithmetic (the start of the mixed solve, whose rounds form their own sums)
+  // no partials are written.
   template <int P, typename R, typename X = R, typename A = R, int OPK = OPK_MASS>
   __global__ void __launch_bounds__(THREADS)
     k_cg_start(const Geo geo, const R *__restrict__ b, const X *__restrict__ x_cur, const X *__restrict__ x_prev,
@@ -1518,6 +1520,7 @@ namespace lbfem_gpu
     });
     stage_own<P>(s_b, b + o, g, gx0, gy0);
     __syncthreads();
+    constexpr bool SUMS = sizeof(A) == sizeof(double);
     double part[3] = {0, 0, 0};
     R *rs = r + o;
     op_apply<P, OPK>(s_u, s_t, maps, g, gx0, gy0, sc, s, [&](int i, int j, int idx, bool image, A Ax) {
@@ -1535,13 +1538,19 @@ namespace lbfem_gpu
       const A bb = A(s_b[i * T::TX + j]);
       const A rr = -Ax + bb;
       rs[idx] = R(rr);
-      part[0] += double(bb) * double(bb);
-      part[1] += double(rr) * double(rr);
-      part[2] += double(rr) * (cg_inv_jacobi<P, OPK>(geo, maps, gx0, gy0, i, j, image) * double(rr));
+      if constexpr (SUMS)
+        {
+          part[0] += double(bb) * double(bb);
+          part[1] += double(rr) * double(rr);
+          part[2] += double(rr) * (cg_inv_jacobi<P, OPK>(geo, maps, gx0, gy0, i, j, image) * double(rr));
+        }
     });
-    const int nt = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
-    // partial (quantity k of system s) at [(k*NM + s) * n_tiles + tile]
-    block_reduce_store<3>(part, partials + (long long)s * nt, tile, NM * nt);
+    if constexpr (SUMS)
+      {
+        const int nt = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
+        // partial (quantity k of system s) at [(k*NM + s) * n_tiles + tile]
+        block_reduce_store<3>(part, partials + (long long)s * nt, tile, NM * nt);
+      }
   }
 
   // p <- D^{-1} r + beta p (p <- D^{-1} r on the first iteration); partial p.Ap. One system per CTA.
