@@ -622,7 +622,7 @@ namespace
           return st;
         std::swap(xi, xo);
         std::swap(r_in, r_out);
-        if ((st = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, 3 * NM)))
+        if ((st = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, 2 * NM)))
           return st;
         k_mixed_round<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nullptr, nsys, tol, max_rounds, 0, 0);
         LAUNCHED();
@@ -1062,7 +1062,7 @@ namespace
         LAUNCHED();
         return LBFEM_OK;
       });
-      if (s2 || (s2 = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, 3 * NM)))
+      if (s2 || (s2 = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, 2 * NM)))
         return s2;
       k_mixed_round<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, ctx->d_stats, NM, tol, max_rounds, h, set);
       LAUNCHED();

@@ -1819,7 +1819,7 @@ namespace lbfem_gpu
   // systems (all of them when all is set):
   //   x_out = x_in + M^{-1} r_in   (FP32 window solves),
   //   r_out = b - A x_out           (FP64 arithmetic on the FP32 values),
-  // with the partial sums b.b, r.r and r.D^{-1}r of each system. The window
+  // with the partial sums b.b and r.r of each system. The window
   // solves give the correction on the own nodes and on a halo of P nodes, so
   // that A x_out follows without another pass; the halo's correction is the
   // window solve's own, within a few 1e-8 of the neighbouring tile's. An
@@ -1841,7 +1841,6 @@ namespace lbfem_gpu
     __shared__ __align__(16) float s_lx[FX * NC], s_ly[FY * NC];     // factors (apart from the window: no aliasing)
     __shared__ int s_col[FX], s_row[FY];                             // storage column / row, -1 outside the grid
     __shared__ long long s_rowoff[FY];                               // storage offset of a window row, -1 outside
-    __shared__ double s_ijy[S::TY];                                  // inverse Jacobi factors of the own rows
     const int s = blockIdx.z;
     const Grid &g = geo.g;
     const long long N = g.N;
@@ -1850,7 +1849,7 @@ namespace lbfem_gpu
     const int n_tiles = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
     const float *rs = r_in + (long long)s * N, *xs = x_in + (long long)s * N, *bs = b + (long long)s * N;
     float *xo = x_out + (long long)s * N, *ro = r_out + (long long)s * N;
-    double part[3] = {0, 0, 0};
+    double part[2] = {0, 0};
     if (!all && !st->active[s])
       {
         // converged: carried over to the output buffers
@@ -1865,7 +1864,7 @@ namespace lbfem_gpu
                 ro[idx] = rs[idx];
               }
           }
-        block_reduce_store_n<3, NT>(part, partials + (long long)s * n_tiles, tile, NM * n_tiles);
+        block_reduce_store_n<2, NT>(part, partials + (long long)s * n_tiles, tile, NM * n_tiles);
         return;
       }
     const float *lxt = lx + (size_t)blockIdx.x * FX * NC, *lyt = ly + (size_t)blockIdx.y * FY * NC;
@@ -1886,8 +1885,6 @@ namespace lbfem_gpu
         const int i = t / S::KP, k = t - i * S::KP, gy = gy0 + i;
         s_my[t] = (k < K && gy < g.nfy && !(g.py && gy == g.nuy)) ? geo.rowy[(long long)gy * K + k] : 0.0;
       }
-    for (int t = tid; t < S::TY; t += NT)
-      s_ijy[t] = gy0 + t < g.nfy ? geo.ijy[gy0 + t] : 0.0;
     __syncthreads();
     // the window of r_in by asynchronous copies, all in flight at once, a window
     // column per thread (consecutive threads: consecutive addresses); meanwhile
@@ -1945,7 +1942,6 @@ namespace lbfem_gpu
 #pragma unroll
         for (int k = 0; k < K; ++k)
           mx[k] = (col_ok && !img_col) ? geo.rowx[(long long)gx * K + k] : 0.0;
-        const double ijx = col_ok ? geo.ijx[gx] : 0.0;
         // this column of b in batches of BR rows, the next batch in flight while one is used
         constexpr int BR = 16;
         static_assert(S::TY % BR == 0, "whole batches");
@@ -2024,11 +2020,10 @@ namespace lbfem_gpu
             ro[idx] = float(rr);
             part[0] += bb * bb;
             part[1] += rr * rr;
-            part[2] += rr * ((image ? 1.0 : ijx * s_ijy[i]) * rr);
           }
         }
       }
-    block_reduce_store_n<3, NT>(part, partials + (long long)s * n_tiles, tile, NM * n_tiles);
+    block_reduce_store_n<2, NT>(part, partials + (long long)s * n_tiles, tile, NM * n_tiles);
   }
 
   // The scalar work of one CG phase, one thread per system, from the reduced sums.
@@ -2126,7 +2121,7 @@ namespace lbfem_gpu
   }
 
   // The bookkeeping of one round of the mixed-precision mass solve, after the
-  // round's correction kernel and the reduction of its sums [bb, rr, rz]: a
+  // round's correction kernel and the reduction of its sums [bb, rr]: a
   // corrected system whose residual meets tol stops; a round that halves no
   // active residual means the tolerance lies below the FP32 resolution of the
   // solution (status 4); round max_rounds is the cap (status 2). Corrections
