@@ -21,9 +21,10 @@ def _g(v):
 
 def nodal_rows(handle, mesh, tc, steady):
     """The rows of every stored node (cgdbe.cc:405-446): moments of the
-    populations, the wall velocity on the wall nodes, and for a steady case the
-    stream function psi / L in column 4."""
-    f = handle.get_populations()
+    populations (the periodic images take their source's populations first, as
+    constraints.distribute does), the wall velocity on the wall nodes, and for a
+    steady case the stream function psi / L in column 4."""
+    f = handle.get_populations()[:, mesh.master()]
     rho, ux, uy = d2q9.moments(f)
     x, y = mesh.nodes()
     u, v = ux / tc.U0, uy / tc.U0

@@ -299,6 +299,29 @@ def test_cavity_continuation_against_ghia(oracle_mod):
         assert abs(psi_max - ghia) <= 0.1 * ghia, (Re, psi_max)
 
 
+def test_gnuplot_writer_unsteady_rows(oracle_mod):
+    """cgdbe.cc:399-446 for an unsteady case: rows x y u/U0 v/U0 |u|/U0 of every
+    node (the periodic images with their source's values), grid rows separated by
+    blank lines, no vortex lines."""
+    from lbfem_gpu import io
+
+    tc, m = tgv(6, p=2)
+    o = setup_case(oracle_mod.Oracle, tc, m, make_params("bardow", "cg"), m.time_step(0.25),
+                   tc.relaxation_time())
+    o.step(3)
+    text = io.gnuplot_text(o, m, tc, t_over_tref=0.5, step=3, reynolds=100, mach=0.05, n_cells=6)
+    lines = text.splitlines()
+    assert lines[0] == "# t/t_ref = 0.5 (step 3), Re = 100, Ma = 0.05, 6^2 Q2 elements"
+    assert lines[1] == "# x y u/U0 v/U0 |u|/U0"
+    rows = [ln for ln in lines[2:] if ln]
+    assert len(rows) == m.n_dofs and lines[2:].count("") == m.nfy - 1
+    a = np.array([r.split() for r in rows], float)
+    assert a.shape[1] == 5 and np.allclose(a[:, 4], np.hypot(a[:, 2], a[:, 3]), rtol=1e-5, atol=1e-6)
+    # the image row y = 1 repeats the row y = 0, the image column x = 1 the column x = 0
+    g = a.reshape(m.nfy, m.nfx, 5)
+    assert np.array_equal(g[-1, :, 2:], g[0, :, 2:]) and np.array_equal(g[:, -1, 2:], g[:, 0, 2:])
+
+
 def test_couette_steady_profile(oracle_mod):
     """docs/results.md:253-260: the steady linear profile to solver tolerance (16 elements, Re 10, t = 2 L^2/nu)."""
     tc = cases.CouetteFlow(0.1)
