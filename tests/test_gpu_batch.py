@@ -65,3 +65,27 @@ def test_batch_failure_of_one_instance(gpu_lib):
     assert np.array_equal(handles[1].get_populations(), before)
     assert np.array_equal(handles[2].get_populations(), ref.get_populations())
     b.close()
+
+
+def test_batch_with_tg3_instances(gpu_lib):
+    """TG3 and split-TG3 instances (two solver loops per split step) in one batch
+    with a TG2 instance: each ends where it ends alone, bitwise."""
+    import lbfem_gpu
+
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    tc.set_reynolds(400)
+    table = [(12, 1, "tg3-split"), (8, 2, "tg3"), (10, 2, "tg2")]
+    batch_handles, single_handles = [], []
+    for n, p, streaming in table:
+        m = cases.build_mesh(tc, n, p)
+        prm = make_params("bardow", "cg", cg_tolerance=1e-10, streaming=streaming)
+        dt = m.time_step(0.8)
+        batch_handles.append(setup_case(lbfem_gpu.Solver, tc, m, prm, dt, tc.relaxation_time()))
+        single_handles.append(setup_case(lbfem_gpu.Solver, tc, m, prm, dt, tc.relaxation_time()))
+    b = lbfem_gpu.Batch(batch_handles)
+    b.step(6)
+    for h in single_handles:
+        h.step(6)
+    for hb, hs in zip(batch_handles, single_handles):
+        assert np.array_equal(hb.get_populations(), hs.get_populations())
+    b.close()
