@@ -143,3 +143,23 @@ def test_tg3_settings_rejected(gpu_lib):
     with pytest.raises(_abi.LbfemError) as ei:
         _gpu(m, make_params("bardow", "cg", streaming="tg3-split", precision="mixed"))
     assert ei.value.status == _abi.LBFEM_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("N,streaming,cfl,expected", [
+    (64, "tg2", 0.25, 7.58e-3),
+    (96, "tg2", 0.25, 2.89e-3),
+    (64, "tg3", 1.0, 6.76e-3),
+    (96, "tg3", 1.0, 2.84e-3),
+    (64, "tg3-split", 1.0, 3.56e-3),
+    (96, "tg3-split", 1.0, 2.16e-3),
+])
+def test_error_tables_at_larger_meshes(gpu_lib, N, streaming, cfl, expected):
+    """docs/results.md:97-107,143-149 at N = 64 and 96 (bardow, consistent mass,
+    modes (1,4), Re 100, t = t_ref/4, Ma 0.05), to the printed digits: the sizes
+    the CPU oracle tests leave out."""
+    tc, m = tgv(N)
+    dt, n = cases.run_length(tc, m, cfl, 0.25)
+    g = setup_case(_gpu, tc, m, make_params("bardow", "cg", streaming=streaming), dt, tc.relaxation_time())
+    g.step(n)
+    err = cases.diagnostics(tc, m, g.node_weight(), g.get_populations(), n * dt)["rel_l2_u"]
+    assert float(f"{err:.2e}") == expected, err

@@ -166,10 +166,13 @@ def test_tgv_error_table(oracle_mod, N, scheme, mass, p, expected):
     (32, "tg3-split", 1.0, 0.05, 2.15e-2, None),
     (48, "tg3-split", 1.0, 0.05, 5.75e-3, None),
     (24, "tg3-split", 1.0, 1.6 / 24, 5.38e-2, None),
+    (96, "tg2", 0.25, 0.05, 2.89e-3, None),
+    (96, "tg3", 1.0, 0.05, 2.84e-3, 2.1),
+    (96, "tg3-split", 1.0, 0.05, 2.16e-3, None),
 ])
 def test_tg3_error_table(oracle_mod, N, streaming, cfl, mach, expected, its):
-    """docs/results.md:97-107 (TG3 at CFL 0.25 and 1, with the mean CG iterations
-    per solve at CFL 1) and :143-149 (split TG3 at CFL 1, Ma 0.05 and 1.6/N):
+    """docs/results.md:97-107 (TG2 at CFL 0.25, TG3 at CFL 0.25 and 1, with the mean
+    CG iterations per solve at CFL 1) and :143-149 (split TG3 at CFL 1, Ma 0.05 and 1.6/N):
     bardow, consistent mass, modes (1,4), Re 100, t = t_ref/4, to the printed digits."""
     tc, m = tgv(N, mach=mach)
     dt, n = cases.run_length(tc, m, cfl, 0.25)
