@@ -1619,11 +1619,8 @@ namespace lbfem_gpu
     const R al = R(st->alpha[s]);
     const long long o = s * N;
     const R *ps = p + o;
-    R *s_x = s_t + op_scratch<P, OPK>(), *s_r = s_x + T::TX * T::TY;
     __syncthreads();
     stage<P>(s_u, maps, [&](long long idx) { return ps[idx]; });
-    stage_own<P>(s_x, x + o, g, gx0, gy0);
-    stage_own<P>(s_r, r + o, g, gx0, gy0);
     __syncthreads();
     double part[2] = {0, 0};
     R *xs = x + o, *rs = r + o;
@@ -1631,9 +1628,9 @@ namespace lbfem_gpu
       const R pv = image ? ps[idx] : s_u[(i + P) * T::PF + j + P];
       if (image)
         Ap = pv;
-      const int t = i * T::TX + j;
-      xs[idx] = s_x[t] + al * pv;
-      const R rr = s_r[t] + -al * Ap;
+      // x and r of the own node straight from global memory (no staging: more CTAs per SM)
+      xs[idx] = xs[idx] + al * pv;
+      const R rr = rs[idx] + -al * Ap;
       rs[idx] = rr;
       part[0] += double(rr) * double(rr);
       part[1] += double(rr) * (cg_inv_jacobi<P, OPK>(geo, maps, gx0, gy0, i, j, image) * double(rr));
