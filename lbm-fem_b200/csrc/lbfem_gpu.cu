@@ -407,7 +407,7 @@ namespace
       grid.z = c.nsys;
       return with_op(c.opk, [&](auto OO) -> int {
         constexpr int OPK = decltype(OO)::value;
-        k_cg_start<P, double, double, double, OPK><<<grid, THREADS, cg_smem<P, double, OPK>(1, true), ctx->stream>>>(
+        k_cg_start<P, double, double, double, OPK><<<grid, THREADS, cg_smem<P, double, OPK>(0, true), ctx->stream>>>(
           geo, c.b, c.x_cur, c.x_prev, c.x_new, w.r, c.extrapolate, w.partials, c.sc, c.skip);
         LAUNCHED();
         return LBFEM_OK;

@@ -1486,8 +1486,10 @@ namespace lbfem_gpu
   // not solved (zero sums: converged at the start, x untouched). With FP32
   // arithmetic (the start of the mixed solve, whose rounds form their own sums)
   // no partials are written.
+  // FP32 storage stages b in shared memory (8 CTAs per SM at 32 registers); FP64
+  // reads it in place, which leaves room for 6 CTAs of the mass start per SM.
   template <int P, typename R, typename X = R, typename A = R, int OPK = OPK_MASS>
-  __global__ void __launch_bounds__(THREADS)
+  __global__ void __launch_bounds__(THREADS, OPK != OPK_MASS ? 2 : sizeof(R) == sizeof(float) ? 8 : 6)
     k_cg_start(const Geo geo, const R *__restrict__ b, const X *__restrict__ x_cur, const X *__restrict__ x_prev,
                X *__restrict__ x_new, R *__restrict__ r, int extrapolate, double *__restrict__ partials,
                const StreamCoef sc, int skip)
@@ -1518,7 +1520,9 @@ namespace lbfem_gpu
     stage<P>(s_u, maps, [&](long long idx) -> A {
       return extrapolate ? A(X(-A(x_prev[o + idx]) + A(2) * A(x_cur[o + idx]))) : A(x_new[o + idx]);
     });
-    stage_own<P>(s_b, b + o, g, gx0, gy0);
+    constexpr bool STAGE_B = sizeof(R) == sizeof(float);
+    if constexpr (STAGE_B)
+      stage_own<P>(s_b, b + o, g, gx0, gy0);
     __syncthreads();
     constexpr bool SUMS = sizeof(A) == sizeof(double);
     double part[3] = {0, 0, 0};
@@ -1535,7 +1539,7 @@ namespace lbfem_gpu
         xg = s_u[(i + P) * T::PF + j + P];
       if (extrapolate)
         x_new[id] = X(xg);
-      const A bb = A(s_b[i * T::TX + j]);
+      const A bb = A(STAGE_B ? s_b[i * T::TX + j] : b[id]);
       const A rr = -Ax + bb;
       rs[idx] = R(rr);
       if constexpr (SUMS)
