@@ -1559,7 +1559,7 @@ namespace lbfem_gpu
 
   // p <- D^{-1} r + beta p (p <- D^{-1} r on the first iteration); partial p.Ap. One system per CTA.
   template <int P, typename R, int OPK = OPK_MASS>
-  __global__ void __launch_bounds__(THREADS)
+  __global__ void __launch_bounds__(THREADS, OPK == OPK_MASS ? 8 : 2)
     k_cg_p(const Geo geo, const R *__restrict__ r, const R *__restrict__ p_in, R *__restrict__ p_out,
            const CgState *__restrict__ st, double *__restrict__ partials, const StreamCoef sc)
   {
@@ -1604,7 +1604,7 @@ namespace lbfem_gpu
 
   // v = A p recomputed; x += alpha p, r -= alpha v; partials r.r, r.D^{-1}r. One system per CTA.
   template <int P, typename R, int OPK = OPK_MASS>
-  __global__ void __launch_bounds__(THREADS)
+  __global__ void __launch_bounds__(THREADS, OPK == OPK_MASS ? 8 : 2)
     k_cg_update(const Geo geo, R *__restrict__ x, R *__restrict__ r, const R *__restrict__ p,
                 const CgState *__restrict__ st, double *__restrict__ partials, const StreamCoef sc)
   {
