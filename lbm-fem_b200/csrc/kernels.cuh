@@ -401,7 +401,7 @@ namespace lbfem_gpu
   {
     int col[Tile<P>::FX];
     int rowi[Tile<P>::FY];
-    long long row[Tile<P>::FY];
+    int row[Tile<P>::FY]; // storage offset of the row (a population array holds fewer than 2^31 nodes)
     R hx[Tile<P>::CX + 1], hxi[Tile<P>::CX + 1], cx[Tile<P>::CX + 1];
     R hy[Tile<P>::CY + 1], hyi[Tile<P>::CY + 1], cy[Tile<P>::CY + 1];
     double ijx[Tile<P>::FX], ijy[Tile<P>::FY]; // inverse Jacobi diagonal factors of the footprint's storage nodes
@@ -423,7 +423,7 @@ namespace lbfem_gpu
       {
         const int r = wrap(gy0 - P + t, g.py, g.nuy, g.nfy);
         m.rowi[t] = r;
-        m.row[t] = r < 0 ? -1 : (long long)r * g.nfx;
+        m.row[t] = r < 0 ? -1 : r * g.nfx;
         m.ijy[t] = r < 0 ? 0.0 : geo.ijy[r];
       }
     const int cx0 = gx0 / P - 1, cy0 = gy0 / P - 1;
@@ -460,7 +460,7 @@ namespace lbfem_gpu
         if (t < NT)
           {
             const int fy = t / T::FX, fx = t - fy * T::FX;
-            const long long r = m.row[fy];
+            const int r = m.row[fy];
             const int c = m.col[fx];
             if (r >= 0 && c >= 0)
               v[k] = R(value_at(r + c));
@@ -494,7 +494,7 @@ namespace lbfem_gpu
         if (t < NT)
           {
             const int fy = t / T::FX, fx = t - fy * T::FX;
-            const long long r = m.row[fy];
+            const int r = m.row[fy];
             const int c = m.col[fx];
             if (r >= 0 && c >= 0)
               v[k] = R(value_at(r + c, c, m.rowi[fy]));

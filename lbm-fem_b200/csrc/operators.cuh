@@ -727,7 +727,7 @@ namespace lbfem_gpu
         for (int t0 = threadIdx.x; t0 < NT; t0 += 2 * THREADS)
           {
             R v[2][Q];
-            long long idx[2];
+            int idx[2];
             int wk[2];
 #pragma unroll
             for (int h = 0; h < 2; ++h)
@@ -738,7 +738,7 @@ namespace lbfem_gpu
                 if (t < NT)
                   {
                     const int fy = t / T::FX, fx = t - fy * T::FX;
-                    const long long r = maps.row[fy];
+                    const int r = maps.row[fy];
                     const int c = maps.col[fx];
                     if (r >= 0 && c >= 0)
                       idx[h] = r + c;
@@ -807,7 +807,7 @@ namespace lbfem_gpu
             for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
               {
                 const int fy = t / T::FX, fx = t - fy * T::FX, st = fy * T::PF + fx;
-                const long long r = maps.row[fy];
+                const int r = maps.row[fy];
                 const int c = maps.col[fx];
                 if (r < 0 || c < 0)
                   continue;
@@ -1841,7 +1841,7 @@ namespace lbfem_gpu
     double *s_my = reinterpret_cast<double *>(s_w + PF * FY);       // [TY][KP] My rows of the own rows (zero padded)
     __shared__ __align__(16) float s_lx[FX * NC], s_ly[FY * NC];     // factors (apart from the window: no aliasing)
     __shared__ int s_col[FX], s_row[FY];                             // storage column / row, -1 outside the grid
-    __shared__ long long s_rowoff[FY];                               // storage offset of a window row, -1 outside
+    __shared__ int s_rowoff[FY];                                     // storage offset of a window row, -1 outside
     const int s = blockIdx.z;
     const Grid &g = geo.g;
     const long long N = g.N;
@@ -1879,7 +1879,7 @@ namespace lbfem_gpu
       {
         const int r = wrap(gy0 - W + t, g.py, g.nuy, g.nfy);
         s_row[t] = r;
-        s_rowoff[t] = r < 0 ? -1 : (long long)r * g.nfx;
+        s_rowoff[t] = r < 0 ? -1 : r * g.nfx;
       }
     for (int t = tid; t < S::TY * S::KP; t += NT)
       {
@@ -1896,7 +1896,7 @@ namespace lbfem_gpu
 #pragma unroll 8
         for (int q = 0; q < FY; ++q)
           {
-            const long long ro = s_rowoff[q];
+            const int ro = s_rowoff[q];
             const bool ok = ro >= 0 && col >= 0;
             cp_async4(&s_w[q * PF + c], ok ? rs + (ro + col) : rs, ok);
           }
@@ -1908,8 +1908,8 @@ namespace lbfem_gpu
 #pragma unroll
       for (int q = 0; q < S::TY + 2 * P; ++q)
         {
-          const int row = s_row[W - P + q];
-          xr[q] = (row >= 0 && col >= 0) ? xs[(long long)row * g.nfx + col] : 0.f;
+          const int ro = s_rowoff[W - P + q];
+          xr[q] = (ro >= 0 && col >= 0) ? xs[ro + col] : 0.f;
         }
     }
     cp_async_wait_all();
@@ -1947,10 +1947,13 @@ namespace lbfem_gpu
         constexpr int BR = 16;
         static_assert(S::TY % BR == 0, "whole batches");
         float bn[BR];
+        // this column's own nodes, by 32-bit offsets (a population array holds fewer than 2^31 nodes)
+        const int col0 = gy0 * g.nfx + gx, pitch = g.nfx;
+        const int rows_in = g.nfy - gy0; // own rows inside the grid
         auto load_b = [&](int i0) {
 #pragma unroll
           for (int u = 0; u < BR; ++u)
-            bn[u] = (col_ok && gy0 + i0 + u < g.nfy) ? bs[(long long)(gy0 + i0 + u) * g.nfx + gx] : 0.f;
+            bn[u] = (col_ok && i0 + u < rows_in) ? bs[col0 + (i0 + u) * pitch] : 0.f;
         };
         load_b(0);
         // t[k] = (Mx x)(row i - P + k) of this column, a sliding window of 2P + 1 rows;
@@ -1989,9 +1992,9 @@ namespace lbfem_gpu
               t[k] = t[k + 1];
             t[K - 1] = xrow(W + i + P);
             const int gy = gy0 + i;
-            if (!col_ok || gy >= g.nfy)
+            if (!col_ok || i >= rows_in)
               continue;
-            const long long idx = (long long)gy * g.nfx + gx;
+            const int idx = col0 + i * pitch;
             const bool image = img_col || (g.py && gy == g.nuy);
             double xv, ax;
             if (image)

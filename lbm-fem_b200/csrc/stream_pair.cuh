@@ -415,10 +415,10 @@ namespace lbfem_gpu
       for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
         {
           const int fy = t / T::FX, fx = t - fy * T::FX, st = fy * T::PF + fx;
-          const long long r = maps.row[fy];
+          const int r = maps.row[fy];
           const int c = maps.col[fx];
           const bool ok = r >= 0 && c >= 0;
-          const long long idx = ok ? r + c : 0;
+          const int idx = ok ? r + c : 0;
           cp_async4(&buf[st].x, d + a * N + idx, ok);
           cp_async4(&buf[st].y, d + ab * N + idx, ok);
         }
@@ -434,7 +434,7 @@ namespace lbfem_gpu
       for (int t0 = threadIdx.x; t0 < NT; t0 += 2 * THREADS)
         {
           float v[2][Q];
-          long long idx[2];
+          int idx[2];
           int wk[2];
 #pragma unroll
           for (int hh = 0; hh < 2; ++hh)
@@ -445,7 +445,7 @@ namespace lbfem_gpu
               if (t < NT)
                 {
                   const int fy = t / T::FX, fx = t - fy * T::FX;
-                  const long long r = maps.row[fy];
+                  const int r = maps.row[fy];
                   const int c = maps.col[fx];
                   if (r >= 0 && c >= 0)
                     idx[hh] = r + c;
@@ -536,7 +536,7 @@ namespace lbfem_gpu
             for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
               {
                 const int fy = t / T::FX, fx = t - fy * T::FX, st = fy * T::PF + fx;
-                const long long r = maps.row[fy];
+                const int r = maps.row[fy];
                 const int c = maps.col[fx];
                 float2 gs = make_float2(0.f, 0.f);
                 if (r >= 0 && c >= 0)
@@ -595,7 +595,7 @@ namespace lbfem_gpu
               const int gy = gy0 + i;
               if (gx < g.nfx && gy < g.nfy)
                 {
-                  const long long idx = (long long)gy * g.nfx + gx;
+                  const int idx = gy * g.nfx + gx; // a population array holds fewer than 2^31 nodes
                   const bool img = is_image(gx, gy, g);
                   oa[idx] = img ? 0.f : r.x;
                   ob[idx] = img ? 0.f : r.y;
