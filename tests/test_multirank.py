@@ -52,7 +52,7 @@ def test_max_over_ranks_with_gloo():
 
 @pytest.mark.timeout(300)
 def test_reference_arm_under_torchrun():
-    """bench.py --impl reference launched as the driver launches it with 2 ranks:
+    """bench.py --impl reference launched under torchrun with 2 ranks (one process per GPU):
     rank 0 alone runs the CPU reference and prints one JSON line; the other
     rank exits 0 without work."""
     env = dict(os.environ, LBFEM_CPU_BUDGET_S="1", OMP_NUM_THREADS="2")
