@@ -152,34 +152,70 @@ namespace lbfem_gpu
   }
 
   // predictor_corrector on FP32 deviations d = f - w with the FP32 increment x, in
-  // FP64 arithmetic (the corrector's theta (feq(fhat) - feq(f)) cancels).
-  __global__ void __launch_bounds__(THREADS, 4) // 4 CTAs per SM: more loads in flight, a few spills
+  // FP32 arithmetic. The corrector's theta (feq(fhat) - feq(f)) is formed from the
+  // moment changes of the predictor, exact in real arithmetic because feq(f) has
+  // the moments of f (and its density at a wall): with inv = 1 / (1 + theta),
+  //   rho_hat - rho = inv sum x,   J_hat - J = inv sum e x  (J = rho u; a wall
+  //   node keeps its imposed u), so that
+  //   feq_a(fhat) - feq_a(f) = w_a (d rho + 3 e.dJ + 4.5 d[(e.J)^2 / rho] - 1.5 d[J.J / rho]),
+  // each difference written out in the small changes. No difference of two
+  // O(1e-2) equilibria is rounded (the reason the corrector once ran in FP64).
+  __global__ void __launch_bounds__(THREADS, 4)
   k_predictor_corrector_dev(const Geo geo, DevStats *__restrict__ ds, float *__restrict__ d,
                             const float *__restrict__ x, double theta)
   {
     if (step_skipped(ds))
       return;
     const long long N = geo.g.N;
-    const double inv = 1. / (1. + theta);
+    const float th = float(theta), inv = float(1. / (1. + theta));
     LBFEM_GRID_STRIDE(i, N)
     {
-      double di[Q], fe[Q], fh[Q], dr;
+      float di[Q], xa[Q];
 #pragma unroll
       for (int a = 0; a < Q; ++a)
         di[a] = d[a * N + i];
-      const Mom m = impose(moments_dev64(di, dr), i, geo);
-#pragma unroll
-      for (int a = 0; a < Q; ++a)
-        fe[a] = feqd64_a(a, m, dr);
-      fh[0] = inv * (di[0] + theta * fe[0]);
+      xa[0] = 0.f;
 #pragma unroll
       for (int a = 1; a < Q; ++a)
-        fh[a] = inv * (di[a] + theta * fe[a] + x[(a - 1) * N + i]);
-      double drh;
-      const Mom mh = impose(moments_dev64(fh, drh), i, geo);
+        xa[a] = x[(a - 1) * N + i];
+      const int wk = geo.wall ? geo.wall[i] : 0;
+      const MomF m = impose_class(moments_dev(di), wk, geo);
+      float sx = 0.f, sjx = 0.f, sjy = 0.f;
+#pragma unroll
+      for (int a = 1; a < Q; ++a)
+        {
+          sx += xa[a];
+          sjx += float(c_EX[a]) * xa[a];
+          sjy += float(c_EY[a]) * xa[a];
+        }
+      const float dr = inv * sx;
+      const float rho = m.rho, rh = rho + dr, den = 1.f / (rho * rh);
+      const float Jx = rho * m.ux, Jy = rho * m.uy;
+      const float djx = wk ? 0.f : inv * sjx, djy = wk ? 0.f : inv * sjy;
+      // d[J.J / rho] and the wall's density-only change
+      const float duu = ((2.f * (Jx * djx + Jy * djy) + djx * djx + djy * djy) * rho - (Jx * Jx + Jy * Jy) * dr) * den;
+      const float uu = m.ux * m.ux + m.uy * m.uy;
 #pragma unroll
       for (int a = 0; a < Q; ++a)
-        d[a * N + i] = float(fh[a] + theta * (feqd64_a(a, mh, drh) - fe[a]));
+        {
+          const float ex = float(c_EX[a]), ey = float(c_EY[a]);
+          // fhat - d = inv (theta (feq - d) + x): the update is formed apart from d
+          // and added to it once (as the FP64 form rounds once)
+          const float up = inv * fmaf(th, feqd_a(a, m) - di[a], xa[a]);
+          float dq;
+          if (wk)
+            {
+              const float eu = ex * m.ux + ey * m.uy;
+              dq = dr * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * uu);
+            }
+          else
+            {
+              const float eJ = ex * Jx + ey * Jy, edJ = ex * djx + ey * djy;
+              const float de = (edJ * (2.f * eJ + edJ) * rho - eJ * eJ * dr) * den;
+              dq = dr + 3.f * edJ + 4.5f * de - 1.5f * duu;
+            }
+          d[a * N + i] = di[a] + fmaf(th, float(c_W[a]) * dq, up);
+        }
     }
   }
 
