@@ -452,14 +452,17 @@ namespace lbfem_gpu
     // all loads of a thread are issued before its first shared store (memory-level parallelism)
     constexpr int NT = T::FY * T::FX, IT = (NT + THREADS - 1) / THREADS;
     R v[IT];
+    int si[IT]; // shared-memory index of each element (the division is done once)
 #pragma unroll
     for (int k = 0; k < IT; ++k)
       {
         const int t = threadIdx.x + k * THREADS;
         v[k] = R{};
+        si[k] = -1;
         if (t < NT)
           {
             const int fy = t / T::FX, fx = t - fy * T::FX;
+            si[k] = fy * T::PF + fx;
             const int r = m.row[fy];
             const int c = m.col[fx];
             if (r >= 0 && c >= 0)
@@ -468,14 +471,8 @@ namespace lbfem_gpu
       }
 #pragma unroll
     for (int k = 0; k < IT; ++k)
-      {
-        const int t = threadIdx.x + k * THREADS;
-        if (t < NT)
-          {
-            const int fy = t / T::FX, fx = t - fy * T::FX;
-            s[fy * T::PF + fx] = v[k];
-          }
-      }
+      if (si[k] >= 0)
+        s[si[k]] = v[k];
   }
 
   // The same with the storage coordinates: value_at(storage index, column, row).
@@ -486,14 +483,17 @@ namespace lbfem_gpu
     using T = Tile<P>;
     constexpr int NT = T::FY * T::FX, IT = (NT + THREADS - 1) / THREADS;
     R v[IT];
+    int si[IT];
 #pragma unroll
     for (int k = 0; k < IT; ++k)
       {
         const int t = threadIdx.x + k * THREADS;
         v[k] = R{};
+        si[k] = -1;
         if (t < NT)
           {
             const int fy = t / T::FX, fx = t - fy * T::FX;
+            si[k] = fy * T::PF + fx;
             const int r = m.row[fy];
             const int c = m.col[fx];
             if (r >= 0 && c >= 0)
@@ -502,14 +502,8 @@ namespace lbfem_gpu
       }
 #pragma unroll
     for (int k = 0; k < IT; ++k)
-      {
-        const int t = threadIdx.x + k * THREADS;
-        if (t < NT)
-          {
-            const int fy = t / T::FX, fx = t - fy * T::FX;
-            s[fy * T::PF + fx] = v[k];
-          }
-      }
+      if (si[k] >= 0)
+        s[si[k]] = v[k];
   }
 
   // s[i*TX + j] <- src at own node (gx0 + j, gy0 + i) of the tile (0 past the grid).

@@ -1553,9 +1553,10 @@ namespace lbfem_gpu
     __syncthreads();
     const long long o = s * N;
     // the start as stored (rounded to X), so that r is the residual of the stored x
-    stage<P>(s_u, maps, [&](long long idx) -> A {
-      return extrapolate ? A(X(-A(x_prev[o + idx]) + A(2) * A(x_cur[o + idx]))) : A(x_new[o + idx]);
-    });
+    if (extrapolate)
+      stage<P>(s_u, maps, [&](long long idx) -> A { return A(X(-A(x_prev[o + idx]) + A(2) * A(x_cur[o + idx]))); });
+    else
+      stage<P>(s_u, maps, [&](long long idx) -> A { return A(x_new[o + idx]); });
     constexpr bool STAGE_B = sizeof(R) == sizeof(float);
     if constexpr (STAGE_B)
       stage_own<P>(s_b, b + o, g, gx0, gy0);
