@@ -520,7 +520,7 @@ namespace lbfem_gpu
         const int t = threadIdx.x + k * THREADS;
         const int i = t / T::TX, j = t - i * T::TX;
         const int gx = gx0 + j, gy = gy0 + i;
-        v[k] = (t < NT && gx < g.nfx && gy < g.nfy) ? src[(long long)gy * g.nfx + gx] : R(0);
+        v[k] = (t < NT && gx < g.nfx && gy < g.nfy) ? src[gy * g.nfx + gx] : R(0); // fewer than 2^31 nodes
       }
 #pragma unroll
     for (int k = 0; k < IT; ++k)

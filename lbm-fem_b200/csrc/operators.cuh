@@ -1564,19 +1564,22 @@ namespace lbfem_gpu
     constexpr bool SUMS = sizeof(A) == sizeof(double);
     double part[3] = {0, 0, 0};
     R *rs = r + o;
+    // this system's vectors, indexed by 32-bit node offsets
+    X *xns = x_new + o;
+    const X *xcs = extrapolate ? x_cur + o : nullptr, *xps = extrapolate ? x_prev + o : nullptr;
+    const R *bs = b + o;
     op_apply<P, OPK>(s_u, s_t, maps, g, gx0, gy0, sc, s, [&](int i, int j, int idx, bool image, A Ax) {
-      const long long id = o + idx;
       A xg;
       if (image)
         {
-          xg = extrapolate ? A(X(-A(x_prev[id]) + A(2) * A(x_cur[id]))) : A(x_new[id]);
+          xg = extrapolate ? A(X(-A(xps[idx]) + A(2) * A(xcs[idx]))) : A(xns[idx]);
           Ax = xg;
         }
       else
         xg = s_u[(i + P) * T::PF + j + P];
       if (extrapolate)
-        x_new[id] = X(xg);
-      const A bb = A(STAGE_B ? s_b[i * T::TX + j] : b[id]);
+        xns[idx] = X(xg);
+      const A bb = A(STAGE_B ? s_b[i * T::TX + j] : bs[idx]);
       const A rr = -Ax + bb;
       rs[idx] = R(rr);
       if constexpr (SUMS)
