@@ -203,11 +203,11 @@ namespace
         (st = set_smem(ctx, k_cg_update<P, double>, cg_smem<P, double>(0))) ||
         (st = set_smem(ctx, k_cg_start<P, double, double, double, OPK_TG3>, cg_smem<P, double, OPK_TG3>(1))) ||
         (st = set_smem(ctx, k_cg_p<P, double, OPK_TG3>, cg_smem<P, double, OPK_TG3>(0))) ||
-        (st = set_smem(ctx, k_cg_update<P, double, OPK_TG3>, cg_smem<P, double, OPK_TG3>(0))) ||
+        (st = set_smem(ctx, k_cg_update<P, double, OPK_TG3>, cg_smem<P, double, OPK_TG3>(2))) ||
         (st = set_smem(ctx, k_cg_start<P, double, double, double, OPK_LAPLACE>,
                        cg_smem<P, double, OPK_LAPLACE>(1))) ||
         (st = set_smem(ctx, k_cg_p<P, double, OPK_LAPLACE>, cg_smem<P, double, OPK_LAPLACE>(0))) ||
-        (st = set_smem(ctx, k_cg_update<P, double, OPK_LAPLACE>, cg_smem<P, double, OPK_LAPLACE>(0))) ||
+        (st = set_smem(ctx, k_cg_update<P, double, OPK_LAPLACE>, cg_smem<P, double, OPK_LAPLACE>(2))) ||
         (st = set_smem(ctx, k_cg_start<P, float, float, float>, cg_smem<P, float>(1))) ||
         (st = set_smem(ctx, k_window_correct<P>, window_smem<P>())) ||
         (st = set_smem(ctx, k_richardson_pass<P, double>, cg_smem<P, double>(0))) ||
@@ -407,7 +407,7 @@ namespace
       grid.z = c.nsys;
       return with_op(c.opk, [&](auto OO) -> int {
         constexpr int OPK = decltype(OO)::value;
-        k_cg_start<P, double, double, double, OPK><<<grid, THREADS, cg_smem<P, double, OPK>(0, true), ctx->stream>>>(
+        k_cg_start<P, double, double, double, OPK><<<grid, THREADS, cg_smem<P, double, OPK>(OPK == OPK_MASS ? 0 : 1, true), ctx->stream>>>(
           geo, c.b, c.x_cur, c.x_prev, c.x_new, w.r, c.extrapolate, w.partials, c.sc, c.skip);
         LAUNCHED();
         return LBFEM_OK;
@@ -445,7 +445,7 @@ namespace
       grid.z = c.nsys;
       return with_op(c.opk, [&](auto OO) -> int {
         constexpr int OPK = decltype(OO)::value;
-        k_cg_update<P, double, OPK><<<grid, THREADS, cg_smem<P, double, OPK>(0), ctx->stream>>>(
+        k_cg_update<P, double, OPK><<<grid, THREADS, cg_smem<P, double, OPK>(OPK == OPK_MASS ? 0 : 2), ctx->stream>>>(
           geo, c.x_new, w.r, w.p[pi], w.state, w.partials, c.sc);
         LAUNCHED();
         return LBFEM_OK;

@@ -1522,8 +1522,9 @@ namespace lbfem_gpu
   // not solved (zero sums: converged at the start, x untouched). With FP32
   // arithmetic (the start of the mixed solve, whose rounds form their own sums)
   // no partials are written.
-  // FP32 storage stages b in shared memory (8 CTAs per SM at 32 registers); FP64
-  // reads it in place, which leaves room for 6 CTAs of the mass start per SM.
+  // FP32 storage and the register-bound TG3 / Laplace operators stage b in shared
+  // memory (the FP32 start runs 8 CTAs per SM at 32 registers); the FP64 mass start
+  // reads it in place, which leaves room for 6 CTAs per SM.
   template <int P, typename R, typename X = R, typename A = R, int OPK = OPK_MASS>
   __global__ void __launch_bounds__(THREADS, OPK != OPK_MASS ? 2 : sizeof(R) == sizeof(float) ? 8 : 6)
     k_cg_start(const Geo geo, const R *__restrict__ b, const X *__restrict__ x_cur, const X *__restrict__ x_prev,
@@ -1557,7 +1558,7 @@ namespace lbfem_gpu
       stage<P>(s_u, maps, [&](long long idx) -> A { return A(X(-A(x_prev[o + idx]) + A(2) * A(x_cur[o + idx]))); });
     else
       stage<P>(s_u, maps, [&](long long idx) -> A { return A(x_new[o + idx]); });
-    constexpr bool STAGE_B = sizeof(R) == sizeof(float);
+    constexpr bool STAGE_B = sizeof(R) == sizeof(float) || OPK != OPK_MASS;
     if constexpr (STAGE_B)
       stage_own<P>(s_b, b + o, g, gx0, gy0);
     __syncthreads();
@@ -1663,18 +1664,28 @@ namespace lbfem_gpu
     const R al = R(st->alpha[s]);
     const long long o = s * N;
     const R *ps = p + o;
+    R *xs = x + o, *rs = r + o;
+    // The mass update reads the own x and r in place (less shared memory: more CTAs
+    // per SM); the TG3 and Laplace updates, held at 2 CTAs per SM by their registers,
+    // stage them with the footprint so that their loads are in flight together.
+    constexpr bool STAGE_XR = OPK != OPK_MASS;
+    R *s_x = s_t + op_scratch<P, OPK>(), *s_r = s_x + T::TX * T::TY;
     __syncthreads();
     stage<P>(s_u, maps, [&](long long idx) { return ps[idx]; });
+    if constexpr (STAGE_XR)
+      {
+        stage_own<P>(s_x, xs, g, gx0, gy0);
+        stage_own<P>(s_r, rs, g, gx0, gy0);
+      }
     __syncthreads();
     double part[2] = {0, 0};
-    R *xs = x + o, *rs = r + o;
     op_apply<P, OPK>(s_u, s_t, maps, g, gx0, gy0, sc, s, [&](int i, int j, int idx, bool image, R Ap) {
       const R pv = image ? ps[idx] : s_u[(i + P) * T::PF + j + P];
       if (image)
         Ap = pv;
-      // x and r of the own node straight from global memory (no staging: more CTAs per SM)
-      xs[idx] = xs[idx] + al * pv;
-      const R rr = rs[idx] + -al * Ap;
+      const int t = i * T::TX + j;
+      xs[idx] = (STAGE_XR ? s_x[t] : xs[idx]) + al * pv;
+      const R rr = (STAGE_XR ? s_r[t] : rs[idx]) + -al * Ap;
       rs[idx] = rr;
       part[0] += double(rr) * double(rr);
       part[1] += double(rr) * (cg_inv_jacobi<P, OPK>(geo, maps, gx0, gy0, i, j, image) * double(rr));
