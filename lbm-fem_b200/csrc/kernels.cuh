@@ -475,7 +475,8 @@ namespace lbfem_gpu
         s[si[k]] = v[k];
   }
 
-  // The same with the storage coordinates: value_at(storage index, column, row).
+  // The same with the storage coordinates and the footprint position:
+  // value_at(storage index, column, row, footprint column, footprint row).
   template <int P, typename R, typename RM, typename F>
   __device__ __forceinline__ void
   stage_ij(R *s, const TileMaps<P, RM> &m, F &&value_at)
@@ -497,7 +498,7 @@ namespace lbfem_gpu
             const int r = m.row[fy];
             const int c = m.col[fx];
             if (r >= 0 && c >= 0)
-              v[k] = R(value_at(r + c, c, m.rowi[fy]));
+              v[k] = R(value_at(r + c, c, m.rowi[fy], fx, fy));
           }
       }
 #pragma unroll

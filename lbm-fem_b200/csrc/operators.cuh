@@ -1621,8 +1621,9 @@ namespace lbfem_gpu
     const long long o = s * N;
     __syncthreads();
     const R *rsys = r + o, *psys = p_in + o;
-    stage_ij<P>(s_u, maps, [&](long long idx, int c, int rw) -> R {
-      const R z = R(OPK == OPK_LAPLACE ? laplace_inv_diag<P>(geo, c, rw) : geo.ijx[c] * geo.ijy[rw]) * rsys[idx];
+    stage_ij<P>(s_u, maps, [&](long long idx, int c, int rw, int fx, int fy) -> R {
+      // the mass Jacobi factors from the tile maps (shared memory), not from global memory
+      const R z = R(OPK == OPK_LAPLACE ? laplace_inv_diag<P>(geo, c, rw) : maps.ijx[fx] * maps.ijy[fy]) * rsys[idx];
       return first ? z : fma(beta, psys[idx], z);
     });
     __syncthreads();
