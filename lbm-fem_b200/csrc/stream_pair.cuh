@@ -8,7 +8,8 @@
 //   k1 = ex, k3 = ey flip sign; c ex^2, -2 c ex ey, c ey^2, c ex ey do not.
 // The kernel stages each pair as float2 {u_a, u_abar} and runs the x and y
 // passes with packed FP32 arithmetic (fma.rn.f32x2, sm_100): one instruction,
-// one shared-memory access and one barrier serve two populations. In the
+// one shared-memory access and one barrier serve two populations (the
+// element-matrix products of degree 3 and 4 excepted, see elem2_row). In the
 // Lee-Lin right-hand side the equilibria of a pair share their even part:
 //   feq_a - w = E + O, feq_abar - w = E - O,
 //   E = w (drho + rho (4.5 (e.u)^2 - 1.5 u.u)), O = 3 w rho e.u;
@@ -78,30 +79,53 @@ namespace lbfem_gpu
     return c_ref2[P - 1][OP][a][b];
   }
 
+  // Row a of reference matrix OP applied to u, both lanes. The matrix entries
+  // are uniform constants. From degree 3 on they enter as scalar FMA operands
+  // read from constant memory (two FP32 FMAs per entry): the packed form
+  // needs each entry as a lane-duplicated register pair, and at p = 4 those
+  // pairs spill (p = 4 K1 1.3x faster scalar, p = 3 even). Below degree 3 the
+  // packed form is kept (about 1% faster there).
+  template <int P, int OP>
+  __device__ __forceinline__ float2
+  elem2_row(int a, const float2 (&u)[P + 1])
+  {
+    if constexpr (P >= 3)
+      {
+        float c = ref<float, P, OP>(a, 0);
+        float sx = c * u[0].x, sy = c * u[0].y;
+#pragma unroll
+        for (int b = 1; b <= P; ++b)
+          {
+            c = ref<float, P, OP>(a, b);
+            sx = fmaf(c, u[b].x, sx);
+            sy = fmaf(c, u[b].y, sy);
+          }
+        return make_float2(sx, sy);
+      }
+    else
+      {
+        float2 s = mul2(ref2<P, OP>(a, 0), u[0]);
+#pragma unroll
+        for (int b = 1; b <= P; ++b)
+          s = fma2(ref2<P, OP>(a, b), u[b], s);
+        return s;
+      }
+  }
+
   template <int P, int OP>
   __device__ __forceinline__ void
   elem2(const float2 (&u)[P + 1], float2 (&y)[P + 1])
   {
 #pragma unroll
     for (int a = 0; a <= P; ++a)
-      {
-        float2 s = mul2(ref2<P, OP>(a, 0), u[0]);
-#pragma unroll
-        for (int b = 1; b <= P; ++b)
-          s = fma2(ref2<P, OP>(a, b), u[b], s);
-        y[a] = s;
-      }
+      y[a] = elem2_row<P, OP>(a, u);
   }
 
   template <int P, int OP>
   __device__ __forceinline__ float2
   elem2_last(const float2 (&u)[P + 1])
   {
-    float2 s = mul2(ref2<P, OP>(P, 0), u[0]);
-#pragma unroll
-    for (int b = 1; b <= P; ++b)
-      s = fma2(ref2<P, OP>(P, b), u[b], s);
-    return s;
+    return elem2_row<P, OP>(P, u);
   }
 
   // Per-cell scales of the footprint, lane-duplicated: width, 1 / width, and 1 / 0 for
@@ -153,18 +177,6 @@ namespace lbfem_gpu
       }
     else
       h = mul2(k.A, u);
-  }
-
-  // Row a of reference matrix OP applied to u.
-  template <int P, int OP>
-  __device__ __forceinline__ float2
-  elem2_row(int a, const float2 (&u)[P + 1])
-  {
-    float2 s = mul2(ref2<P, OP>(a, 0), u[0]);
-#pragma unroll
-    for (int b = 1; b <= P; ++b)
-      s = fma2(ref2<P, OP>(a, b), u[b], s);
-    return s;
   }
 
   // x pass of one footprint row fy and one x segment. CLS: 0 e = (ex, 0), 1 e = (0, ey), 2 diagonal.
