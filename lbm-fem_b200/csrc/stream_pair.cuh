@@ -210,7 +210,8 @@ namespace lbfem_gpu
     if constexpr (DG)
       pCu = mul2(m.cx[q0], elem2_row<P, OP_C>(P, u));
     float2 *y1 = s_y + fy * T::PY, *y2 = y1 + T::NY, *y3 = y2 + T::NY;
-#pragma unroll 1
+    // unrolled up to p = 3 (K1 3-5% faster); at p = 4 the unrolled loop spills
+#pragma unroll(P >= 4 ? 1 : T::KX)
     for (int q = 1; q <= T::KX; ++q)
       {
         const int qc = q0 + q;
