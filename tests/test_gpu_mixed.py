@@ -57,6 +57,8 @@ def test_mixed_population_roundtrip(gpu_lib):
     ("bardow", "richardson", "cavity", 2, 16, 400, 0.4),
     ("leelin", "cg", "couette", 1, 16, 600, 0.25),
     ("bardow", "cg", "cavity", 1, 24, 300, 0.4),
+    ("leelin", "cg", "tgv", 4, 16, 150, 0.5),
+    ("bardow", "cg", "cavity", 4, 20, 200, 0.4),
 ])
 def test_mixed_matches_fp64(gpu_lib, scheme, mass, case, p, n, steps, cfl):
     if case == "tgv":
