@@ -445,6 +445,73 @@ def run_batch(args):
     return 0
 
 
+def run_ladder(args):
+    """The Reynolds-continuation ladder of the throughput scan: args.ladder lid-driven
+    cavities on args.ladder_cells^2 Q2 cells (lid 0.1, stretch 1.2, CFL 0.4, Bardow,
+    lumped mass as in the reference's cavity continuations, mixed precision), Re
+    geometric from 100 to 3200, each rung warm-started from the previous one
+    (driver.batched_ladder), args.steps steps per stage. The batched ladder is timed
+    against the same ladder stepped one rung at a time. The default mesh is 128^2:
+    on 256^2 the Re = 100 rung of this scheme grows without bound within 100 steps
+    (both schemes, both masses, CFL 0.4 and 0.2, in the FP64 oracle as well), while
+    128^2 holds every rung."""
+    import lbfem_gpu
+    from lbfem_gpu import cases, driver, make_params
+
+    world, rank, local, pg = dist_setup()
+    lib = lbfem_gpu.library()
+    reynolds = driver.reynolds_ladder(100.0, 3200.0, args.ladder)
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    mesh = cases.build_mesh(tc, args.ladder_cells, 2)
+    dt = mesh.time_step(0.4)
+    x, y = mesh.nodes()
+
+    def make():
+        hs = []
+        for k, re in enumerate(reynolds):
+            tc.set_reynolds(re)
+            h = lbfem_gpu.Solver(mesh, make_params("bardow", "lumped", precision="mixed", device=local))
+            h.set_time_step(dt, tc.relaxation_time())
+            if k == 0:
+                h.set_initial_populations(tc.initial_populations(x, y, tc.relaxation_time()))
+            hs.append(h)
+        return hs
+
+    def timed(batch):
+        hs = make()
+        lib.lbfem_gpu_synchronize(hs[0].h)
+        barrier(pg)
+        t0 = time.perf_counter()
+        taken = driver.batched_ladder(hs, args.steps, batch=batch)
+        for h in hs:
+            lib.lbfem_gpu_synchronize(h.h)
+        sec = allreduce_max(pg, time.perf_counter() - t0)
+        rho = [float(h.conservation()[1] / h.conservation()[0]) for h in hs]
+        for h in hs:
+            h.close()
+        return sec, taken, rho
+
+    t_batch, taken, rho = timed(True)
+    t_single, _, _ = timed(False)
+    units = 9 * mesh.n_unique() * sum(taken) * world
+    if rank == 0:
+        line = {"metric": "aggregate Q·DoF updates/s of a batched Reynolds-continuation ladder (warm-started rungs)",
+                "value": units / t_batch, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": 0, "ms_per_stage": 1e3 * t_batch / len(reynolds), "higher_is_better": True,
+                "scaling": "weak",
+                "one_at_a_time": {"value": units / t_single, "sec": t_single},
+                "speedup_vs_one_at_a_time": t_single / t_batch, "dtype": "f32 mixed", "data": "synthetic",
+                "config": {"workload": f"ladder of {len(reynolds)} lid-driven cavities, Q2 "
+                                       f"{args.ladder_cells}x{args.ladder_cells} cells, Re 100 -> 3200",
+                           "reynolds": [round(r, 2) for r in reynolds], "steps_per_rung": taken,
+                           "nodes_distinct_per_rung": int(mesh.n_unique()), "scheme": "bardow", "mass": "lumped",
+                           "cfl": 0.4, "mean_density_per_rung": rho},
+                "timing": "host wall clock around the whole ladder, warm starts and graph captures included; "
+                          "the first stage steps from the cavity at rest"}
+        print(json.dumps(line))
+    return 0
+
+
 def run_streaming(args):
     """TG3 streaming (--streaming tg3 | tg3-split): the Bardow scheme in FP64 on the
     Taylor-Green workload at CFL args.cfl, against TG2 at CFL 0.25 over the same
@@ -525,6 +592,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--batch", type=int, default=0,
                     help="time N batched independent instances (the batched workload) instead of the default")
+    ap.add_argument("--ladder", type=int, default=0,
+                    help="time a Reynolds-continuation ladder of N cavities (Re 100 -> 3200) instead of the default")
+    ap.add_argument("--ladder-cells", type=int, default=128, help="cells per side of each ladder cavity (Q2)")
     ap.add_argument("--streaming", default="tg2", choices=["tg2", "tg3", "tg3-split"],
                     help="tg3 / tg3-split: time the Bardow FP64 TG3 step against TG2 at CFL 0.25 instead")
     ap.add_argument("--cfl", type=float, default=1.0, help="CFL number of the --streaming tg3* run")
@@ -535,6 +605,8 @@ def main():
         args.warmup = 3
     if args.batch and args.impl == "ours":
         return run_batch(args)
+    if args.ladder and args.impl == "ours":
+        return run_ladder(args)
     if args.streaming != "tg2" and args.impl == "ours":
         return run_streaming(args)
     return run_reference(args) if args.impl == "reference" else run_ours(args)

@@ -35,3 +35,47 @@ def steady_state(handle, mesh, tc, dt, *, steady_tol=1e-4, t_end=100.0):
         if rate < steady_tol:
             return steps, True, rate
     return steps, False, rate
+
+
+def reynolds_ladder(first, last, n):
+    """n Reynolds numbers from first to last, geometrically spaced: the stages of a
+    continuation (cgdbe's --Re list, cgdbe.cc:280-290)."""
+    if n < 1:
+        raise ValueError("a ladder has at least one rung")
+    if n == 1:
+        return [float(first)]
+    return [first * (last / first) ** (k / (n - 1)) for k in range(n)]
+
+
+def batched_ladder(solvers, steps_per_stage, *, batch=True):
+    """A Reynolds-continuation ladder with its rungs as concurrent instances.
+
+    cgdbe continues one Reynolds number after the other on the same populations:
+    set_time_step with the next relaxation time, Scheme::f kept (cgdbe.cc:280-290).
+    Here rung k is its own context, created with its own time step. Rung 0
+    starts from the populations it holds. At stage k, rung k is warm-started from
+    rung k - 1's populations at that moment (set_populations: the state only; the
+    solver's start history restarts). Rungs 0..k then take steps_per_stage steps
+    together, one graph launch per step of all of them (Batch) when batch is true,
+    one rung after the other otherwise. The two give the same populations.
+    Returns the steps each rung took."""
+    from . import Batch
+
+    n = len(solvers)
+    taken = [0] * n
+    for s in range(n):
+        if s > 0:
+            solvers[s].set_populations(solvers[s - 1].get_populations())
+        active = solvers[: s + 1]
+        if batch and len(active) > 1:
+            b = Batch(active)
+            try:
+                b.step(steps_per_stage)
+            finally:
+                b.close()
+        else:
+            for h in active:
+                h.step(steps_per_stage)
+        for k in range(s + 1):
+            taken[k] += steps_per_stage
+    return taken

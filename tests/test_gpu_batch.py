@@ -89,3 +89,51 @@ def test_batch_with_tg3_instances(gpu_lib):
     for hb, hs in zip(batch_handles, single_handles):
         assert np.array_equal(hb.get_populations(), hs.get_populations())
     b.close()
+
+
+def _ladder(factory, precision, n_rungs, cells, p):
+    """A continuation ladder of lid-driven cavities, Re 100 -> 400, rungs warm-started
+    by driver.batched_ladder."""
+    from lbfem_gpu import driver
+
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    m = cases.build_mesh(tc, cells, p)
+    dt = m.time_step(0.4)
+    x, y = m.nodes()
+    hs = []
+    for k, re in enumerate(driver.reynolds_ladder(100.0, 400.0, n_rungs)):
+        tc.set_reynolds(re)
+        h = factory(m, make_params("bardow", "cg", cg_tolerance=1e-12, precision=precision))
+        h.set_time_step(dt, tc.relaxation_time())
+        if k == 0:
+            h.set_initial_populations(tc.initial_populations(x, y, tc.relaxation_time()))
+        hs.append(h)
+    return hs
+
+
+def test_ladder_against_the_oracle(gpu_lib, oracle_mod):
+    """The batched continuation ladder (one graph launch per step of the active
+    rungs) against the same ladder on the FP64 oracle, rung by rung."""
+    import lbfem_gpu
+    from lbfem_gpu import driver
+
+    g = _ladder(lbfem_gpu.Solver, "fp64", 3, 10, 1)
+    o = _ladder(lambda m, prm: oracle_mod.Oracle(m, prm), "fp64", 3, 10, 1)
+    assert driver.batched_ladder(g, 6, batch=True) == driver.batched_ladder(o, 6, batch=False) == [18, 12, 6]
+    for a, b in zip(g, o):
+        fa, fb = a.get_populations(), b.get_populations()
+        assert np.linalg.norm(fa - fb) <= 1e-12 * np.linalg.norm(fb)
+
+
+def test_ladder_batched_equals_one_at_a_time(gpu_lib):
+    """Mixed precision, Q2: the batched ladder and the ladder stepped one rung at a
+    time end bitwise equal."""
+    import lbfem_gpu
+    from lbfem_gpu import driver
+
+    a = _ladder(lbfem_gpu.Solver, "mixed", 4, 8, 2)
+    b = _ladder(lbfem_gpu.Solver, "mixed", 4, 8, 2)
+    driver.batched_ladder(a, 5, batch=True)
+    driver.batched_ladder(b, 5, batch=False)
+    for x, y in zip(a, b):
+        assert np.array_equal(x.get_populations(), y.get_populations())

@@ -426,3 +426,40 @@ def test_checkpoint_format(oracle_mod, tmp_path):
     f[:, :5].tofile(name + ".5")
     with pytest.raises(_abi.LbfemError):
         o.read_checkpoint(name, rank=5)
+
+
+def test_reynolds_ladder_rungs():
+    """The continuation ladder's Reynolds numbers: geometric, ends included."""
+    from lbfem_gpu import driver
+
+    re = driver.reynolds_ladder(100.0, 3200.0, 16)
+    assert len(re) == 16 and re[0] == 100.0 and abs(re[-1] - 3200.0) < 1e-9
+    ratios = np.array(re[1:]) / np.array(re[:-1])
+    assert np.allclose(ratios, 32.0 ** (1 / 15), rtol=1e-13)
+    assert driver.reynolds_ladder(400.0, 800.0, 1) == [400.0]
+
+
+def test_ladder_warm_start_on_the_oracle(oracle_mod):
+    """batched_ladder's warm start (cgdbe.cc:280-290 keeps Scheme::f from one
+    Reynolds number to the next): with every rung at the same Reynolds number and
+    the lumped mass (no solver history), rung k, warm-started from rung k - 1 at
+    stage k, ends bitwise where rung 0 ends; the steps taken count down by stage."""
+    from lbfem_gpu import driver
+
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    tc.set_reynolds(400)
+    m = cases.build_mesh(tc, 8, 1)
+    dt, lam = m.time_step(0.4), tc.relaxation_time()
+    x, y = m.nodes()
+    hs = []
+    for k in range(3):
+        h = oracle_mod.Oracle(m, make_params("bardow", "lumped"))
+        h.set_time_step(dt, lam)
+        if k == 0:
+            h.set_initial_populations(tc.initial_populations(x, y, lam))
+        hs.append(h)
+    taken = driver.batched_ladder(hs, 4, batch=False)
+    assert taken == [12, 8, 4]
+    f0 = hs[0].get_populations()
+    for h in hs[1:]:
+        assert np.array_equal(h.get_populations(), f0)
