@@ -392,18 +392,20 @@ def batch_instances(n, seed=20261203):
 
 
 def run_batch(args):
-    """Aggregate throughput of the batched instances, against stepping them one at a time."""
+    """Aggregate throughput of the batched instances, against stepping them one at a
+    time, in mixed precision and on the plain FP64 path."""
     import lbfem_gpu
+    from lbfem_gpu import d2q9, make_params
 
     world, rank, local, pg = dist_setup()
     inst = batch_instances(args.batch)
     lib = lbfem_gpu.library()
 
-    def make():
+    def make(fp64=False):
         hs = []
         for it in inst:
             m, tc = it["mesh"], it["tc"]
-            h = lbfem_gpu.Solver(m, it["params"])
+            h = lbfem_gpu.Solver(m, make_params(it["scheme"], "cg") if fp64 else it["params"])
             dt, lam = m.time_step(0.4), tc.relaxation_time()
             x, y = m.nodes()
             h.set_time_step(dt, lam)
@@ -420,6 +422,7 @@ def run_batch(args):
     b.step(args.steps)  # returns after the device finished (one synchronisation)
     t_batch = time.perf_counter() - t0
     b.close()
+    f_mixed = [h.get_populations() for h in hs]  # the batched mixed run's end states
     for h in hs:
         h.close()
     hs = make()
@@ -431,12 +434,34 @@ def run_batch(args):
     t_single = time.perf_counter() - t0
     for h in hs:
         h.close()
+    # the plain FP64 path on the same instances, one at a time
+    hs = make(fp64=True)
+    for h in hs:
+        h.step(args.warmup)
+    t0 = time.perf_counter()
+    for h in hs:
+        h.step(args.steps)
+    t_fp64 = time.perf_counter() - t0
+    # relative L2 velocity error of each batched mixed instance against its FP64 run
+    errs = []
+    for it, h, fm in zip(inst, hs, f_mixed):
+        ind = it["mesh"].independent()
+        _, uxm, uym = d2q9.moments(fm[:, ind])
+        _, uxr, uyr = d2q9.moments(h.get_populations()[:, ind])
+        errs.append(float(np.linalg.norm(np.stack([uxm - uxr, uym - uyr])) / np.linalg.norm(np.stack([uxr, uyr]))))
+    for h in hs:
+        h.close()
     if rank == 0:
         line = {"metric": "aggregate Q·DoF updates/s of batched independent instances (one graph launch per step)",
                 "value": units / t_batch, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * t_batch / args.steps, "higher_is_better": True,
                 "one_at_a_time": {"value": units / t_single, "ms_per_step": 1e3 * t_single / args.steps},
-                "speedup_vs_one_at_a_time": t_single / t_batch, "dtype": "f32 mixed", "data": "synthetic",
+                "speedup_vs_one_at_a_time": t_single / t_batch,
+                "fp64_one_at_a_time": {"value": units / t_fp64, "ms_per_step": 1e3 * t_fp64 / args.steps},
+                "speedup_vs_fp64_one_at_a_time": t_fp64 / t_batch,
+                "accuracy": {"max_rel_l2_u_mixed_vs_fp64": max(errs), "median": float(np.median(errs)), "target": 1e-5,
+                             "note": f"per instance, after {args.warmup + args.steps} steps of both runs"},
+                "dtype": "f32 mixed", "data": "synthetic",
                 "config": {"workload": f"{args.batch} instances (cavities and Taylor-Green vortices)",
                            "nodes_distinct_total": int(sum(it["mesh"].n_unique() for it in inst)),
                            "instances": [{k: it[k] for k in ("case", "edge", "p", "Re", "U0", "scheme")} for it in inst]},
@@ -500,7 +525,12 @@ def run_ladder(args):
                 "warmup": 0, "ms_per_stage": 1e3 * t_batch / len(reynolds), "higher_is_better": True,
                 "scaling": "weak",
                 "one_at_a_time": {"value": units / t_single, "sec": t_single},
-                "speedup_vs_one_at_a_time": t_single / t_batch, "dtype": "f32 mixed", "data": "synthetic",
+                "speedup_vs_one_at_a_time": t_single / t_batch,
+                "fp64_one_at_a_time": {"value": units / t_fp64, "ms_per_step": 1e3 * t_fp64 / args.steps},
+                "speedup_vs_fp64_one_at_a_time": t_fp64 / t_batch,
+                "accuracy": {"max_rel_l2_u_mixed_vs_fp64": max(errs), "median": float(np.median(errs)), "target": 1e-5,
+                             "note": f"per instance, after {args.warmup + args.steps} steps of both runs"},
+                "dtype": "f32 mixed", "data": "synthetic",
                 "config": {"workload": f"ladder of {len(reynolds)} lid-driven cavities, Q2 "
                                        f"{args.ladder_cells}x{args.ladder_cells} cells, Re 100 -> 3200",
                            "reynolds": [round(r, 2) for r in reynolds], "steps_per_rung": taken,
