@@ -331,6 +331,10 @@ def run_ours(args):
         cpu = {"value": cval, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{cn} step(s) of the full mesh after 1 warm-up step ({csec:.1f} s), CPU FP64 oracle port, "
                          f"{threads} OpenMP threads, {cpu_model()}"}
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        batched = batch_measure(64, 100, 5)
+        batched.pop("instances")
     if rank != 0:
         return 0
     line = {
@@ -358,6 +362,7 @@ def run_ours(args):
                 "call": "lbfem_gpu_step_host on the mixed context (FP64 host populations in, one step, out)"},
         "clocks": mix["clocks"],
         "gpu_launches": mix["launches"],
+        "batched": batched,
     }
     print(json.dumps(line))
     return 0
@@ -391,14 +396,16 @@ def batch_instances(n, seed=20261203):
     return out
 
 
-def run_batch(args):
-    """Aggregate throughput of the batched instances, against stepping them one at a
-    time, in mixed precision and on the plain FP64 path."""
+def batch_measure(n, steps, warmup):
+    """The batched workload of n instances: batched mixed steps (one graph launch per
+    step of all of them), the same instances stepped one at a time in mixed precision
+    and on the plain FP64 path, and each batched mixed instance's relative L2 velocity
+    error against its FP64 run. Host wall clock around calls that each end with one
+    device synchronisation."""
     import lbfem_gpu
     from lbfem_gpu import d2q9, make_params
 
-    world, rank, local, pg = dist_setup()
-    inst = batch_instances(args.batch)
+    inst = batch_instances(n)
     lib = lbfem_gpu.library()
 
     def make(fp64=False):
@@ -413,36 +420,32 @@ def run_batch(args):
             hs.append(h)
         return hs
 
-    units = 9 * sum(it["mesh"].n_unique() for it in inst) * args.steps
+    def one_at_a_time(hs):
+        for h in hs:
+            h.step(warmup)
+        t0 = time.perf_counter()
+        for h in hs:
+            h.step(steps)
+        return time.perf_counter() - t0
+
+    units = 9 * sum(it["mesh"].n_unique() for it in inst) * steps
     hs = make()
     b = lbfem_gpu.Batch(hs)
-    b.step(args.warmup)
+    b.step(warmup)
     lib.lbfem_gpu_synchronize(hs[0].h)
     t0 = time.perf_counter()
-    b.step(args.steps)  # returns after the device finished (one synchronisation)
+    b.step(steps)  # returns after the device finished (one synchronisation)
     t_batch = time.perf_counter() - t0
     b.close()
     f_mixed = [h.get_populations() for h in hs]  # the batched mixed run's end states
     for h in hs:
         h.close()
     hs = make()
-    for h in hs:
-        h.step(args.warmup)
-    t0 = time.perf_counter()
-    for h in hs:
-        h.step(args.steps)
-    t_single = time.perf_counter() - t0
+    t_single = one_at_a_time(hs)
     for h in hs:
         h.close()
-    # the plain FP64 path on the same instances, one at a time
     hs = make(fp64=True)
-    for h in hs:
-        h.step(args.warmup)
-    t0 = time.perf_counter()
-    for h in hs:
-        h.step(args.steps)
-    t_fp64 = time.perf_counter() - t0
-    # relative L2 velocity error of each batched mixed instance against its FP64 run
+    t_fp64 = one_at_a_time(hs)
     errs = []
     for it, h, fm in zip(inst, hs, f_mixed):
         ind = it["mesh"].independent()
@@ -451,21 +454,35 @@ def run_batch(args):
         errs.append(float(np.linalg.norm(np.stack([uxm - uxr, uym - uyr])) / np.linalg.norm(np.stack([uxr, uyr]))))
     for h in hs:
         h.close()
+    return {"value": units / t_batch, "ms_per_step": 1e3 * t_batch / steps, "steps": steps, "warmup": warmup,
+            "one_at_a_time": {"value": units / t_single, "ms_per_step": 1e3 * t_single / steps},
+            "speedup_vs_one_at_a_time": t_single / t_batch,
+            "fp64_one_at_a_time": {"value": units / t_fp64, "ms_per_step": 1e3 * t_fp64 / steps},
+            "speedup_vs_fp64_one_at_a_time": t_fp64 / t_batch,
+            "accuracy": {"max_rel_l2_u_mixed_vs_fp64": max(errs), "median": float(np.median(errs)), "target": 1e-5,
+                         "note": f"per instance, after {warmup + steps} steps of both runs"},
+            "workload": f"{n} instances (cavities and Taylor-Green vortices)",
+            "nodes_distinct_total": int(sum(it["mesh"].n_unique() for it in inst)),
+            "instances": [{k: it[k] for k in ("case", "edge", "p", "Re", "U0", "scheme")} for it in inst],
+            "timing": "host wall clock around the call (each call ends with a device synchronisation)"}
+
+
+def run_batch(args):
+    """Aggregate throughput of the batched instances, against stepping them one at a
+    time, in mixed precision and on the plain FP64 path."""
+    world, rank, local, pg = dist_setup()
+    r = batch_measure(args.batch, args.steps, args.warmup)
     if rank == 0:
         line = {"metric": "aggregate Q·DoF updates/s of batched independent instances (one graph launch per step)",
-                "value": units / t_batch, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": 1e3 * t_batch / args.steps, "higher_is_better": True,
-                "one_at_a_time": {"value": units / t_single, "ms_per_step": 1e3 * t_single / args.steps},
-                "speedup_vs_one_at_a_time": t_single / t_batch,
-                "fp64_one_at_a_time": {"value": units / t_fp64, "ms_per_step": 1e3 * t_fp64 / args.steps},
-                "speedup_vs_fp64_one_at_a_time": t_fp64 / t_batch,
-                "accuracy": {"max_rel_l2_u_mixed_vs_fp64": max(errs), "median": float(np.median(errs)), "target": 1e-5,
-                             "note": f"per instance, after {args.warmup + args.steps} steps of both runs"},
+                "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+                "one_at_a_time": r["one_at_a_time"], "speedup_vs_one_at_a_time": r["speedup_vs_one_at_a_time"],
+                "fp64_one_at_a_time": r["fp64_one_at_a_time"],
+                "speedup_vs_fp64_one_at_a_time": r["speedup_vs_fp64_one_at_a_time"], "accuracy": r["accuracy"],
                 "dtype": "f32 mixed", "data": "synthetic",
-                "config": {"workload": f"{args.batch} instances (cavities and Taylor-Green vortices)",
-                           "nodes_distinct_total": int(sum(it["mesh"].n_unique() for it in inst)),
-                           "instances": [{k: it[k] for k in ("case", "edge", "p", "Re", "U0", "scheme")} for it in inst]},
-                "timing": "host wall clock around the call (each call ends with a device synchronisation)"}
+                "config": {"workload": r["workload"], "nodes_distinct_total": r["nodes_distinct_total"],
+                           "instances": r["instances"]},
+                "timing": r["timing"]}
         print(json.dumps(line))
     return 0
 
@@ -620,6 +637,8 @@ def main():
     ap.add_argument("--degree", type=int, default=3)
     ap.add_argument("--scheme", default="leelin", choices=["leelin", "bardow"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched-workload leg (64 instances, mixed batched vs one at a time and FP64)")
     ap.add_argument("--batch", type=int, default=0,
                     help="time N batched independent instances (the batched workload) instead of the default")
     ap.add_argument("--ladder", type=int, default=0,
