@@ -489,7 +489,7 @@ def run_batch(args):
 
 def run_ladder(args):
     """The Reynolds-continuation ladder of the throughput scan: args.ladder lid-driven
-    cavities on args.ladder_cells^2 Q2 cells (lid 0.1, stretch 1.2, CFL 0.4, Bardow,
+    cavities on args.ladder_cells^2 Q2 cells (Ma 0.1, stretch 1.2, CFL 0.4, Bardow,
     lumped mass as in the reference's cavity continuations, mixed precision), Re
     geometric from 100 to 3200, each rung warm-started from the previous one
     (driver.batched_ladder), args.steps steps per stage. The batched ladder is timed

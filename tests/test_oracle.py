@@ -408,6 +408,30 @@ def test_leelin_q1_checkerboard_stability_limit(oracle_mod, cfl, grows):
         assert a200 < a100 < 1e-9, (a100, a200)  # decays from the 1e-7 seed
 
 
+@pytest.mark.timeout(300)
+@pytest.mark.parametrize("cells,grows", [(256, True), (128, False)])
+def test_cavity_ladder_first_rung_stability(oracle_mod, cells, grows):
+    """The first rung of the continuation ladder (lid-driven cavity, Ma 0.1, Re 100,
+    Q2, stretch 1.2, CFL 0.4, Bardow, lumped mass) in the reference's own algorithm:
+    on 256^2 cells the peak velocity grows without bound within 100 steps; on
+    128^2 it stays at the lid's scale. The ladder runs on 128^2 for this reason."""
+    tc = cases.LidDrivenCavity(0.1, 1.2)
+    tc.set_reynolds(100)
+    m = cases.build_mesh(tc, cells, 2)
+    dt, lam = m.time_step(0.4), tc.relaxation_time()
+    x, y = m.nodes()
+    o = oracle_mod.Oracle(m, make_params("bardow", "lumped"))
+    o.set_time_step(dt, lam)
+    o.set_initial_populations(tc.initial_populations(x, y, lam))
+    o.step(100)
+    _, ux, uy = d2q9.moments(o.get_populations())
+    peak = float(np.max(np.hypot(ux, uy)))
+    if grows:
+        assert peak > 10 * tc.U0, peak
+    else:
+        assert peak < 2 * tc.U0, peak
+
+
 def test_checkpoint_format(oracle_mod, tmp_path):
     """write_checkpoint / read_checkpoint (io.h:137-165): name.rank holds the nine
     blocks of Scheme::f one after the other, raw FP64; a torn or foreign file is refused."""
