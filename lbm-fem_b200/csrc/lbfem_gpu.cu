@@ -2293,8 +2293,16 @@ namespace
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     int st = LBFEM_OK;
     cudaError_t ce = cudaEventRecord(b->fork, b->stream);
-    for (size_t k = 0; k < b->ctxs.size() && !st && ce == cudaSuccess; ++k)
+    // the largest instances are recorded first, so that their branches start first;
+    // results and failure indices stay those of the instance order
+    std::vector<size_t> order(b->ctxs.size());
+    for (size_t k = 0; k < order.size(); ++k)
+      order[k] = k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t x, size_t y) { return b->ctxs[x]->grid.N > b->ctxs[y]->grid.N; });
+    for (size_t o = 0; o < order.size() && !st && ce == cudaSuccess; ++o)
       {
+        const size_t k = order[o];
         lbfem_gpu_ctx *c = b->ctxs[k];
         ce = cudaStreamWaitEvent(c->stream, b->fork, 0);
         if (ce != cudaSuccess)
