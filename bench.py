@@ -139,8 +139,10 @@ def barrier(pg):
         pg.barrier()
 
 
-def cpu_run(tc, mesh, dt, lam, f0, args, budget_s, max_steps):
-    """The FP64 oracle port on the host cores: warm-up 1 step, then steps until budget_s or max_steps."""
+def cpu_run(tc, mesh, dt, lam, f0, args, budget_s, max_steps, keep=False):
+    """The FP64 oracle port on the host cores: warm-up 1 step, then steps until
+    budget_s or max_steps. keep: also return the oracle's populations after its
+    1 + n steps (the parity check of the FP64 GPU path on the same mesh)."""
     import oracle
     from lbfem_gpu import make_params
 
@@ -156,8 +158,10 @@ def cpu_run(tc, mesh, dt, lam, f0, args, budget_s, max_steps):
         if time.perf_counter() - t0 > budget_s:
             break
     sec = time.perf_counter() - t0
+    f_end = h.get_populations() if keep else None
     h.close()
-    return 9 * mesh.n_unique() * n / sec, n, sec, threads
+    out = (9 * mesh.n_unique() * n / sec, n, sec, threads)
+    return out + (f_end,) if keep else out
 
 
 def cpu_model():
@@ -209,7 +213,43 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def run_precision(args, precision, tc, mesh, dt, lam, f0, local, pg, world):
+def gpu_states(args, mesh, dt, lam, f0, local, steps, precision="fp64", cg_tol=None):
+    """A fresh GPU context of the workload stepped `steps` times from f0 (untimed);
+    its populations (FP64, stored numbering)."""
+    import lbfem_gpu
+    from lbfem_gpu import make_params
+
+    prm = make_params(args.scheme, "cg", cg_tolerance=cg_tol or args.cg_tol, precision=precision, device=local)
+    h = lbfem_gpu.Solver(mesh, prm)
+    h.set_time_step(dt, lam)
+    h.set_initial_populations(f0)
+    h.step(steps)
+    f = h.get_populations()
+    h.close()
+    return f
+
+
+def accuracy_leg(args, mesh, dt, lam, f0, local, steps):
+    """Mixed against FP64 on the GPU after `steps` steps of both from f0: relative L2
+    of the velocity and of the density deviation over the independent nodes, and
+    each run's drift of the mean density."""
+    from lbfem_gpu import d2q9
+
+    ind = mesh.independent()
+    mom = {}
+    for precision in ("fp64", "mixed"):
+        f = gpu_states(args, mesh, dt, lam, f0, local, steps, precision)[:, ind]
+        mom[precision] = d2q9.moments(f)
+    (r64, ux64, uy64), (rm, uxm, uym) = mom["fp64"], mom["mixed"]
+    u64 = np.stack([ux64, uy64])
+    return {"steps": steps,
+            "rel_l2_u_mixed_vs_fp64": float(np.linalg.norm(np.stack([uxm, uym]) - u64) / np.linalg.norm(u64)),
+            "rel_l2_drho_mixed_vs_fp64": float(np.linalg.norm(rm - r64) / np.linalg.norm(r64 - 1.0)),
+            "mean_density_drift": {"fp64": float(np.mean(r64) - 1.0), "mixed": float(np.mean(rm) - 1.0)},
+            "target": 1e-5}
+
+
+def run_precision(args, precision, tc, mesh, dt, lam, f0, local, pg, world, cg_tol=None, rooflines=True):
     """One timed run of the workload in one precision; returns its figures and final velocity."""
     import ctypes as C
 
@@ -217,7 +257,8 @@ def run_precision(args, precision, tc, mesh, dt, lam, f0, local, pg, world):
     from lbfem_gpu import make_params
 
     lib = lbfem_gpu.library()
-    prm = make_params(args.scheme, "cg", cg_tolerance=args.cg_tol, precision=precision, device=local)
+    cg_tol = cg_tol or args.cg_tol
+    prm = make_params(args.scheme, "cg", cg_tolerance=cg_tol, precision=precision, device=local)
     h = lbfem_gpu.Solver(mesh, prm)
     h.set_time_step(dt, lam)
     h.set_initial_populations(f0)
@@ -245,6 +286,10 @@ def run_precision(args, precision, tc, mesh, dt, lam, f0, local, pg, world):
     rho, ux, uy = (np.empty(mesh.n_dofs) for _ in range(3))
     P = C.POINTER(C.c_double)
     h._call("moments", ctx, rho.ctypes.data_as(P), ux.ctypes.data_as(P), uy.ctypes.data_as(P))
+
+    if not rooflines:
+        h.close()
+        return {"sec": sec, "its": its.value, "launches": int(launches.value), "clocks": clocks.summary()}
 
     # rooflines, each kernel timed alone on the context's stream (CUDA events, 10 launches)
     reps = 10
@@ -324,13 +369,28 @@ def run_ours(args):
     lib.lbfem_gpu_host_free(fbuf_ptr)
     h.close()
 
-    cpu = None
+    # the FP64 path at config 0's CG tolerance (1e-12), beside the reference default 1e-8 above
+    f64_tight = None
+    if not args.no_accuracy:
+        f64_tight = run_precision(args, "fp64", tc, mesh, dt, lam, f0, local, pg, world, cg_tol=1e-12,
+                                  rooflines=False)
+
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
         budget = float(os.environ.get("LBFEM_CPU_BUDGET_S", "20"))
-        cval, cn, csec, threads = cpu_run(tc, mesh, dt, lam, f0, args, budget, 1000)
+        cval, cn, csec, threads, f_oracle = cpu_run(tc, mesh, dt, lam, f0, args, budget, 1000, keep=True)
         cpu = {"value": cval, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{cn} step(s) of the full mesh after 1 warm-up step ({csec:.1f} s), CPU FP64 oracle port, "
                          f"{threads} OpenMP threads, {cpu_model()}"}
+        # the FP64 GPU path against the oracle on the same mesh, from the same f0, after the same steps
+        f_gpu = gpu_states(args, mesh, dt, lam, f0, local, 1 + cn)
+        parity = {"rel_l2_fp64_vs_oracle": float(np.linalg.norm(f_gpu - f_oracle) / np.linalg.norm(f_oracle)),
+                  "max_abs_fp64_vs_oracle": float(np.max(np.abs(f_gpu - f_oracle))), "steps": 1 + cn,
+                  "target": 1e-12, "note": "all 9 population arrays, images included, CG tolerance "
+                                           f"{args.cg_tol:g} in both"}
+    accuracy_long = None
+    if rank == 0 and not args.no_accuracy:
+        accuracy_long = accuracy_leg(args, mesh, dt, lam, f0, local, args.accuracy_steps)
     batched = None
     if rank == 0 and world == 1 and not args.no_batch:
         batched = batch_measure(64, 100, 5)
@@ -349,11 +409,18 @@ def run_ours(args):
                        solver_iterations_per_solve={"mixed (window corrections)": mix["its"],
                                                     "fp64 (Jacobi-PCG)": f64["its"]}),
         "fp64": {"value": units / f64["sec"], "ms_per_step": 1e3 * f64["sec"] / args.steps,
-                 "roofline": f64["roofline"], "gpu_launches": f64["launches"]},
+                 "cg_tolerance": args.cg_tol, "roofline": f64["roofline"], "gpu_launches": f64["launches"]},
+        "fp64_cg_1e-12": None if f64_tight is None else {
+            "value": units / f64_tight["sec"], "ms_per_step": 1e3 * f64_tight["sec"] / args.steps,
+            "cg_iterations_per_solve": f64_tight["its"], "gpu_launches": f64_tight["launches"],
+            "mixed_vs_this_speedup": f64_tight["sec"] / mix["sec"],
+            "note": "config 0's CG tolerance, the other reading of the throughput scan's unstated one"},
         "streaming_kernel": mix["streaming"],
         "accuracy": {"rel_l2_u_mixed_vs_fp64": rel_u, "target": 1e-5, "mean_density_fp64": f64["mass"],
                      "mean_density_mixed": mix["mass"],
                      "note": f"after {args.warmup + args.steps} steps of both runs from the same initial state"},
+        "accuracy_long": accuracy_long,
+        "parity": parity,
         "mixed_vs_fp64_speedup": f64["sec"] / mix["sec"],
         "roofline": mix["roofline"],
         "cpu_baseline": cpu,
@@ -543,10 +610,6 @@ def run_ladder(args):
                 "scaling": "weak",
                 "one_at_a_time": {"value": units / t_single, "sec": t_single},
                 "speedup_vs_one_at_a_time": t_single / t_batch,
-                "fp64_one_at_a_time": {"value": units / t_fp64, "ms_per_step": 1e3 * t_fp64 / args.steps},
-                "speedup_vs_fp64_one_at_a_time": t_fp64 / t_batch,
-                "accuracy": {"max_rel_l2_u_mixed_vs_fp64": max(errs), "median": float(np.median(errs)), "target": 1e-5,
-                             "note": f"per instance, after {args.warmup + args.steps} steps of both runs"},
                 "dtype": "f32 mixed", "data": "synthetic",
                 "config": {"workload": f"ladder of {len(reynolds)} lid-driven cavities, Q2 "
                                        f"{args.ladder_cells}x{args.ladder_cells} cells, Re 100 -> 3200",
@@ -647,6 +710,10 @@ def main():
     ap.add_argument("--streaming", default="tg2", choices=["tg2", "tg3", "tg3-split"],
                     help="tg3 / tg3-split: time the Bardow FP64 TG3 step against TG2 at CFL 0.25 instead")
     ap.add_argument("--cfl", type=float, default=1.0, help="CFL number of the --streaming tg3* run")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the untimed accuracy legs (mixed vs FP64 over --accuracy-steps, FP64 at CG 1e-12)")
+    ap.add_argument("--accuracy-steps", type=int, default=500,
+                    help="steps of the mixed-vs-FP64 accuracy leg (the throughput scan's 500)")
     ap.add_argument("--cg-tol", type=float, default=1e-8,
                     help="relative CG tolerance of both precisions (MassSettings default 1e-8, mass.h:33)")
     args = ap.parse_args()

@@ -223,6 +223,42 @@ int lbfem_gpu_compute_equilibrium(lbfem_gpu_ctx *ctx, const double *f, double *f
 int lbfem_gpu_predictor_corrector(lbfem_gpu_ctx *ctx, double *f, const double *feq, const double *incr,
                                   double theta);
 
+/*
+ * Device-pointer forms of the operators, for a caller that keeps the vectors
+ * in device memory (a shim whose deal.II vectors have device mirrors) and
+ * swaps only the operators of Scheme::step: no host copy per call. Vectors are
+ * DEVICE pointers with the same block layout and the caller's DoF numbering
+ * (permuted on the device when the context has a dof_index; with the
+ * structured numbering the kernels work on the caller's buffers in place).
+ * The small parameter arrays (e: 9 x 2 or 2 doubles) stay on the host.
+ *
+ * `stream` is the caller's cudaStream_t passed as a pointer (NULL: the legacy
+ * default stream). The call's device work is ordered after the work queued on
+ * `stream` before the call, and the work queued on `stream` after the call
+ * waits for it (events; the host does not wait). The exceptions are
+ * lbfem_gpu_mass_solve_dev with consistent mass, whose Jacobi-PCG reads its
+ * state back once per iteration and returns when the solve is done, and
+ * lbfem_gpu_step_stream, which reads the step's status as lbfem_gpu_step does.
+ */
+/* AdvectionOperator::apply (advection.h:49-58, 219-241, 263-289): as lbfem_gpu_advection. */
+int lbfem_gpu_advection_dev(lbfem_gpu_ctx *ctx, const double *f, const double *feq, const double *e, double dt,
+                            double lambda, int32_t kind, int32_t remove_wall_mass_flux, double *rhs, void *stream);
+/* MassSolver::solve (mass.h:185-213): as lbfem_gpu_mass_solve, x and r device vectors. */
+int lbfem_gpu_mass_solve_dev(lbfem_gpu_ctx *ctx, double *x, const double *r, const double *e, double tg3_coefficient,
+                             void *stream);
+/* collide_bgk (collision.h:152-168): as lbfem_gpu_collide_bgk, g a device vector. */
+int lbfem_gpu_collide_bgk_dev(lbfem_gpu_ctx *ctx, double *g, double omega, void *stream);
+/* compute_equilibrium (collision.h:105-113): as lbfem_gpu_compute_equilibrium. */
+int lbfem_gpu_compute_equilibrium_dev(lbfem_gpu_ctx *ctx, const double *f, double *feq, void *stream);
+/* predictor_corrector (collision.h:119-145): as lbfem_gpu_predictor_corrector. */
+int lbfem_gpu_predictor_corrector_dev(lbfem_gpu_ctx *ctx, double *f, const double *feq, const double *incr,
+                                      double theta, void *stream);
+/* Scheme::f (schemes.h:63) to and from a device vector of 9 blocks. */
+int lbfem_gpu_set_populations_dev(lbfem_gpu_ctx *ctx, const double *f, void *stream);
+int lbfem_gpu_get_populations_dev(lbfem_gpu_ctx *ctx, double *f, void *stream);
+/* Scheme::step (schemes.h:92-98, 118-124) n_steps times, ordered on the caller's stream. */
+int lbfem_gpu_step_stream(lbfem_gpu_ctx *ctx, int32_t n_steps, void *stream);
+
 /* Discretization::node_weight (discretization.h:164-169): the lumped mass diagonal, n_dofs values (1 on periodic images). */
 int lbfem_gpu_node_weight(lbfem_gpu_ctx *ctx, double *w);
 
@@ -297,21 +333,31 @@ int lbfem_gpu_batch_destroy(lbfem_gpu_batch *batch);
 
 /*
  * The mass solve of lbfem_gpu_mass_solve (consistent mass, Jacobi-PCG) for
- * callers that cannot allocate device memory at the time of the call: for
- * example code that runs while a CUDA stream is being captured, or a host
- * framework that must own every device allocation. It has no counterpart in
- * the reference.
+ * callers that cannot allocate device memory at the time of the call: a host
+ * framework that owns every device allocation and hands out only its own
+ * buffers, or a solver embedded in a code whose memory pool is sized once at
+ * start-up. It has no counterpart in the reference.
  *
  * x (in: start, out: solution) and r are DEVICE pointers to n_dofs doubles in
  * the structured numbering (the context must have been created without
  * dof_index). The CG work buffers are not the context's: they live in one
  * fixed file-scope device array of the library (about 3.8 MiB, held by every
  * GPU that loads the library until the process exits), so the call allocates
- * nothing. Limits: at most 131072 nodes and 4096 tiles; larger meshes are
- * rejected with LBFEM_ERR_ARG. The first call on a device looks up the array's
- * device address; make that first call before any stream capture. All calls
- * share the array: calls that overlap on the GPU race. Iterations are not
- * added to lbfem_gpu_cg_iterations. Returns when the solve has finished.
+ * nothing. Limits: at most 131072 nodes; larger meshes are rejected with
+ * LBFEM_ERR_ARG. (The array also bounds the tiles at 4096, which no mesh of at
+ * most 131072 nodes reaches: the most is 2731, Q1 with one cell across.)
+ *
+ * The call runs eagerly on the context's own stream and is host-synchronous:
+ * it reads the solver state back to the host once per CG iteration and
+ * returns when the solve has finished. It therefore cannot itself be recorded
+ * into a CUDA graph. The solve reads x and r on the context's stream, which is
+ * not ordered with the caller's streams: the caller must have finished
+ * writing x and r before the call (for example with cudaStreamSynchronize on
+ * the stream that wrote them). The first call on a device looks up the
+ * array's device address. All calls share the array, so calls that overlap on
+ * the GPU (from several threads or contexts) race, and a call must not overlap
+ * any other call on the same context. Iterations are not added to
+ * lbfem_gpu_cg_iterations.
  */
 int lbfem_gpu_mass_solve_noalloc(lbfem_gpu_ctx *ctx, double *x, const double *r);
 

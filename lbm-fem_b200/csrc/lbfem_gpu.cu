@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <utility>
@@ -28,6 +29,7 @@ struct lbfem_gpu_ctx
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[16] = {};
+  cudaEvent_t ev_join[2] = {}; // orders the context's stream with a caller's stream (no timing)
   lbfem_params prm{};
   int P = 1;
   Grid grid{};
@@ -453,6 +455,16 @@ namespace
     });
   }
 
+  // x <- 0 for the systems flagged by the solver's start (right-hand side exactly zero).
+  template <typename R>
+  int
+  zero_flagged(lbfem_gpu_ctx *ctx, R *x, const CgState *state, int nsys)
+  {
+    k_zero_flagged<R><<<dim3(148, nsys), THREADS, 0, ctx->stream>>>(x, state, ctx->grid.N, nsys);
+    LAUNCHED();
+    return LBFEM_OK;
+  }
+
   // Jacobi-PCG in the order of updates of deal.II SolverCG (mass.h:204-211),
   // host-driven, with the work buffers w. *its_out: CG iterations summed over
   // the systems.
@@ -468,6 +480,8 @@ namespace
       return st;
     k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 0, tol, max_its);
     LAUNCHED();
+    if ((st = zero_flagged(ctx, c.x_new, w.state, nsys)))
+      return st;
     int pi = 0;
     for (int it = 0;; ++it)
       {
@@ -626,6 +640,8 @@ namespace
           return st;
         k_mixed_round<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nullptr, nsys, tol, max_rounds, 0, 0);
         LAUNCHED();
+        if (round == 0 && (st = zero_flagged(ctx, ctx->d_x_s[xi], ctx->d_cg, nsys)))
+          return st; // xi: the round's output after the swap above
         CK(cudaMemcpyAsync(ctx->h_cg, ctx->d_cg, sizeof(CgState), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
         if (ctx->trace)
@@ -744,6 +760,63 @@ namespace
     LAUNCHED();
     CK(cudaMemcpyAsync(host, ctx->d_stage, sizeof(double) * nb * ctx->n_dofs, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    return LBFEM_OK;
+  }
+
+  // Copies nb blocks of a caller-numbered DEVICE vector into structured device
+  // storage (a permutation gather; with the structured numbering the caller's
+  // buffer is used in place and nothing is copied: *use points at it).
+  int
+  gather_dev(lbfem_gpu_ctx *ctx, const double *src, double *dst, int nb, const double **use)
+  {
+    if (ctx->identity)
+      {
+        *use = src;
+        return LBFEM_OK;
+      }
+    k_gather<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(src, ctx->d_dof, dst, ctx->grid.N,
+                                                                           ctx->n_dofs, nb);
+    LAUNCHED();
+    *use = dst;
+    return LBFEM_OK;
+  }
+
+  // The output side of gather_dev: where a kernel writes so that the caller's
+  // device vector dst ends up holding the result (dst itself with the
+  // structured numbering, else the context's scratch, scattered by scatter_dev).
+  double *
+  out_dev(const lbfem_gpu_ctx *ctx, double *dst, double *scratch)
+  {
+    return ctx->identity ? dst : scratch;
+  }
+
+  int
+  scatter_dev(lbfem_gpu_ctx *ctx, const double *src, double *dst, int nb)
+  {
+    if (ctx->identity)
+      return LBFEM_OK;
+    k_scatter<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(src, ctx->d_dof, dst, ctx->grid.N,
+                                                                            ctx->n_dofs, nb);
+    LAUNCHED();
+    return LBFEM_OK;
+  }
+
+  // Orders the context's stream after the work queued so far on the caller's
+  // stream (an event wait on the device; the host does not wait).
+  int
+  join_caller(lbfem_gpu_ctx *ctx, void *stream)
+  {
+    CK(cudaEventRecord(ctx->ev_join[0], static_cast<cudaStream_t>(stream)));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join[0], 0));
+    return LBFEM_OK;
+  }
+
+  // Makes the work queued later on the caller's stream wait for the context's stream.
+  int
+  release_caller(lbfem_gpu_ctx *ctx, void *stream)
+  {
+    CK(cudaEventRecord(ctx->ev_join[1], ctx->stream));
+    CK(cudaStreamWaitEvent(static_cast<cudaStream_t>(stream), ctx->ev_join[1], 0));
     return LBFEM_OK;
   }
 
@@ -993,6 +1066,8 @@ namespace
       return st;
     k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, c.nsys, 0, tol, max_its);
     LAUNCHED();
+    if ((st = zero_flagged(ctx, c.x_new, w.state, c.nsys)))
+      return st;
     k_cg_control<<<1, 32, 0, ctx->stream>>>(w.state, ctx->d_stats, h, 0);
     LAUNCHED();
     auto iteration = [&](int pi) -> int {
@@ -1069,7 +1144,7 @@ namespace
       return LBFEM_OK;
     };
     float *r0 = ctx->d_r_s, *r1 = ctx->d_p_s[0];
-    if ((st = round(r0, xn, xp, r1, 1, 1)))
+    if ((st = round(r0, xn, xp, r1, 1, 1)) || (st = zero_flagged(ctx, xp, ctx->d_cg, NM)))
       return st;
     return capture_while(
       ctx, h,
@@ -1441,6 +1516,9 @@ lbfem_gpu_destroy(lbfem_gpu_ctx *ctx)
   for (auto &e : ctx->ev)
     if (e)
       cudaEventDestroy(e);
+  for (auto &e : ctx->ev_join)
+    if (e)
+      cudaEventDestroy(e);
   if (ctx->stream)
     cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -1513,6 +1591,8 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
   CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   for (auto &e : ctx->ev)
     CK(cudaEventCreate(&e));
+  for (auto &e : ctx->ev_join)
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   ctx->basis = std::make_unique<Basis1D>(P);
   ctx->ax = make_axis(*ctx->basis, m->vertex_x, m->n_cells_x, m->periodic_x != 0);
   ctx->ay = make_axis(*ctx->basis, m->vertex_y, m->n_cells_y, m->periodic_y != 0);
@@ -2112,6 +2192,216 @@ lbfem_gpu_predictor_corrector(lbfem_gpu_ctx *ctx, double *f, const double *feq, 
   return download(ctx, d, f, Q);
 }
 
+// ---------------------------------------------------------------------------
+// Device-pointer forms of the operators, ordered on the caller's stream.
+int
+lbfem_gpu_advection_dev(lbfem_gpu_ctx *ctx, const double *f, const double *feq, const double *e, double dt,
+                        double lambda, int32_t kind, int32_t remove, double *rhs, void *stream)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!f || !e || !rhs || !(dt > 0))
+    return fail(ctx, LBFEM_ERR_ARG, "advection_dev: bad argument");
+  const bool leelin = kind == LBFEM_ADVECTION_LEELIN;
+  if (!leelin && kind != LBFEM_ADVECTION_TAYLOR_GALERKIN)
+    return fail(ctx, LBFEM_ERR_ARG, "advection_dev: unknown kind %d", kind);
+  if (leelin && (!feq || !(lambda > 0)))
+    return fail(ctx, LBFEM_ERR_ARG, "LeeLinAdvection needs the equilibria");
+  if ((st = join_caller(ctx, stream)))
+    return st;
+  const double *fs = nullptr, *feqs = nullptr;
+  if ((st = gather_dev(ctx, f, ctx->d_f[1 - ctx->cur], Q, &fs)))
+    return st;
+  if (leelin && (st = gather_dev(ctx, feq, ctx->d_feq, Q, &feqs)))
+    return st;
+  AdvCoef ac;
+  if (leelin)
+    {
+      const double b = -0.5 * dt * dt / lambda;
+      ac = adv_coef(-dt - b, b, -0.5 * dt * dt, e, 0.);
+    }
+  else
+    ac = adv_coef(-dt, 0., -0.5 * dt * dt, e, 0.);
+  double *out = out_dev(ctx, rhs, ctx->d_rhs);
+  if ((st = launch_advection<double>(ctx, leelin ? ADV_LEELIN_FEQ : ADV_TG, fs, feqs, nullptr, out, ac)))
+    return st;
+  const bool rmv = remove < 0 ? !leelin : remove != 0;
+  if ((st = launch_wall_faces<double>(ctx, fs, out, e, dt, rmv)) || (st = scatter_dev(ctx, out, rhs, NM)))
+    return st;
+  return release_caller(ctx, stream);
+}
+
+int
+lbfem_gpu_mass_solve_dev(lbfem_gpu_ctx *ctx, double *x, const double *r, const double *e, double tg3, void *stream)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!x || !r)
+    return fail(ctx, LBFEM_ERR_ARG, "mass_solve_dev: null buffer");
+  if (tg3 != 0. && !e)
+    return fail(ctx, LBFEM_ERR_ARG, "mass_solve_dev: the TG3 matrix needs the direction e");
+  if (tg3 != 0. && ctx->prm.mass == LBFEM_MASS_RICHARDSON)
+    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_dev: the TG3 matrix with iterated lumping is not implemented");
+  StreamCoef sc{};
+  if (tg3 != 0.)
+    {
+      sc.kxx[0] = tg3 * e[0] * e[0];
+      sc.kyy[0] = tg3 * e[1] * e[1];
+      sc.kxy[0] = tg3 * e[0] * e[1];
+    }
+  if ((st = join_caller(ctx, stream)))
+    return st;
+  const double *b = nullptr;
+  if ((st = gather_dev(ctx, r, ctx->d_rhs, 1, &b)))
+    return st;
+  double *xn = ctx->d_x[ctx->x_new];
+  if (ctx->identity)
+    xn = x;
+  else
+    {
+      k_gather<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(x, ctx->d_dof, xn, ctx->grid.N,
+                                                                             ctx->n_dofs, 1);
+      LAUNCHED();
+    }
+  const int solve_st = mass_solve_dev(ctx, b, xn, tg3 != 0., sc, nullptr);
+  if (solve_st != LBFEM_OK && solve_st != LBFEM_ERR_NO_CONVERGENCE && solve_st != LBFEM_ERR_NONFINITE)
+    return solve_st;
+  if ((st = scatter_dev(ctx, xn, x, 1)) || (st = release_caller(ctx, stream)))
+    return st;
+  return solve_st;
+}
+
+int
+lbfem_gpu_collide_bgk_dev(lbfem_gpu_ctx *ctx, double *g, double omega, void *stream)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!g)
+    return fail(ctx, LBFEM_ERR_ARG, "collide_bgk_dev: null buffer");
+  if ((st = join_caller(ctx, stream)))
+    return st;
+  const double *gs = nullptr;
+  if ((st = gather_dev(ctx, g, ctx->d_f[1 - ctx->cur], Q, &gs)))
+    return st;
+  double *d = const_cast<double *>(gs); // g itself, or the context's gathered copy
+  k_collide<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), d, omega);
+  LAUNCHED();
+  if ((st = scatter_dev(ctx, d, g, Q)))
+    return st;
+  return release_caller(ctx, stream);
+}
+
+int
+lbfem_gpu_compute_equilibrium_dev(lbfem_gpu_ctx *ctx, const double *f, double *feq, void *stream)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!f || !feq)
+    return fail(ctx, LBFEM_ERR_ARG, "compute_equilibrium_dev: null buffer");
+  if ((st = join_caller(ctx, stream)))
+    return st;
+  const double *fs = nullptr;
+  if ((st = gather_dev(ctx, f, ctx->d_f[1 - ctx->cur], Q, &fs)))
+    return st;
+  double *out = out_dev(ctx, feq, ctx->d_feq);
+  k_equilibrium<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), fs, out);
+  LAUNCHED();
+  if ((st = scatter_dev(ctx, out, feq, Q)))
+    return st;
+  return release_caller(ctx, stream);
+}
+
+int
+lbfem_gpu_predictor_corrector_dev(lbfem_gpu_ctx *ctx, double *f, const double *feq, const double *incr,
+                                  double theta, void *stream)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!f || !feq || !incr)
+    return fail(ctx, LBFEM_ERR_ARG, "predictor_corrector_dev: null buffer");
+  if ((st = join_caller(ctx, stream)))
+    return st;
+  const double *fs = nullptr, *feqs = nullptr, *xs = nullptr;
+  if ((st = gather_dev(ctx, f, ctx->d_f[1 - ctx->cur], Q, &fs)) || (st = gather_dev(ctx, feq, ctx->d_feq, Q, &feqs)) ||
+      (st = gather_dev(ctx, incr, ctx->d_r, NM, &xs)))
+    return st;
+  double *d = const_cast<double *>(fs); // f itself, or the context's gathered copy
+  k_predictor_corrector<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), nullptr, d, feqs,
+                                                                                      xs, theta);
+  LAUNCHED();
+  if ((st = scatter_dev(ctx, d, f, Q)))
+    return st;
+  return release_caller(ctx, stream);
+}
+
+int
+lbfem_gpu_set_populations_dev(lbfem_gpu_ctx *ctx, const double *f, void *stream)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!f)
+    return fail(ctx, LBFEM_ERR_ARG, "set_populations_dev: null buffer");
+  if ((st = join_caller(ctx, stream)))
+    return st;
+  double *dst = ctx->d_f[ctx->cur];
+  if (ctx->identity)
+    CK(cudaMemcpyAsync(dst, f, sizeof(double) * Q * ctx->grid.N, cudaMemcpyDeviceToDevice, ctx->stream));
+  else
+    {
+      k_gather<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(f, ctx->d_dof, dst, ctx->grid.N,
+                                                                             ctx->n_dofs, Q);
+      LAUNCHED();
+    }
+  if (ctx->mixed)
+    {
+      k_to_dev<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(dst, ctx->d_fs[ctx->cur], ctx->grid.N);
+      LAUNCHED();
+    }
+  return release_caller(ctx, stream);
+}
+
+int
+lbfem_gpu_get_populations_dev(lbfem_gpu_ctx *ctx, double *f, void *stream)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!f)
+    return fail(ctx, LBFEM_ERR_ARG, "get_populations_dev: null buffer");
+  if ((st = join_caller(ctx, stream)))
+    return st;
+  double *src = ctx->d_f[ctx->cur];
+  if (ctx->mixed)
+    {
+      k_from_dev<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(ctx->d_fs[ctx->cur], src, ctx->grid.N);
+      LAUNCHED();
+    }
+  if (ctx->identity)
+    CK(cudaMemcpyAsync(f, src, sizeof(double) * Q * ctx->grid.N, cudaMemcpyDeviceToDevice, ctx->stream));
+  else if ((st = scatter_dev(ctx, src, f, Q)))
+    return st;
+  return release_caller(ctx, stream);
+}
+
+int
+lbfem_gpu_step_stream(lbfem_gpu_ctx *ctx, int32_t n_steps, void *stream)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if ((st = join_caller(ctx, stream)))
+    return st;
+  if ((st = lbfem_gpu_step(ctx, n_steps)))
+    return st;
+  return release_caller(ctx, stream);
+}
+
 int
 lbfem_gpu_node_weight(lbfem_gpu_ctx *ctx, double *w)
 {
@@ -2464,14 +2754,17 @@ lbfem_gpu_batch_step(lbfem_gpu_batch *b, int32_t n_steps)
 // ---------------------------------------------------------------------------
 // Mass solve without allocation.
 //
-// For callers that may not allocate device memory when they call in (code that
-// runs while a stream is being captured, or inside a host framework that owns
-// every device allocation): the CG work buffers of this entry point live in
+// For callers that may not allocate device memory when they call in (a host
+// framework that owns every device allocation, or a code whose memory pool is
+// sized once at start-up): the CG work buffers of this entry point live in
 // one file-scope device array of fixed size, which every GPU that loads the
 // library holds until the process exits. Its device address is looked up once
-// per device, on the first call with that device current. Calls share the
-// array, so calls that overlap on the GPU (from several threads or streams)
-// race; the solver state is cleared at the start of every call.
+// per device, on the first call with that device current (std::call_once, so
+// two host threads making their first call together do not race on the
+// cache). Calls share the array, so calls that overlap on the GPU (from
+// several threads or streams) race; the solver state is cleared at the start
+// of every call. The solve is host-driven: one small state read per CG
+// iteration, so the call is synchronous and cannot be captured into a graph.
 namespace
 {
   constexpr long long NOALLOC_MAX_NODES = 1LL << 17; // 131072 nodes
@@ -2484,6 +2777,21 @@ namespace
 
   constexpr int NOALLOC_MAX_DEVICES = 64;
   double *noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+  cudaError_t noalloc_err[NOALLOC_MAX_DEVICES] = {};
+  std::once_flag noalloc_once[NOALLOC_MAX_DEVICES];
+
+  // The array's device address on the current device (looked up once per device).
+  cudaError_t
+  noalloc_base(int device, double **out)
+  {
+    std::call_once(noalloc_once[device], [device] {
+      void *p = nullptr;
+      noalloc_err[device] = cudaGetSymbolAddress(&p, noalloc_scratch);
+      noalloc_ptr[device] = static_cast<double *>(p);
+    });
+    *out = noalloc_ptr[device];
+    return noalloc_err[device];
+  }
 } // namespace
 
 extern "C" int
@@ -2512,12 +2820,8 @@ lbfem_gpu_mass_solve_noalloc(lbfem_gpu_ctx *ctx, double *x, const double *r)
     return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: the consistent mass (CG) only");
   if (ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES)
     return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: device ordinal %d too large", ctx->device);
-  double *base = noalloc_ptr[ctx->device];
-  if (!base)
-    {
-      CK(cudaGetSymbolAddress((void **)&base, noalloc_scratch));
-      noalloc_ptr[ctx->device] = base;
-    }
+  double *base = nullptr; // check_ctx made ctx's device current
+  CK(noalloc_base(ctx->device, &base));
   CgScratch<double> w{};
   w.r = base;
   w.p[0] = base + NOALLOC_MAX_NODES;

@@ -1485,9 +1485,26 @@ namespace lbfem_gpu
   {
     double tol[NM], rz[NM], rz_prev[NM], beta[NM], alpha[NM], res[NM];
     int it[NM], its_total[NM], active[NM];
+    int zero[NM]; // the system's right-hand side is exactly zero: its solution is 0 (k_zero_flagged)
     int status, n_active, iter;
     unsigned long long total_its;
   };
+
+  // x_s <- 0 for the systems whose right-hand side is exactly zero. deal.II's
+  // SolverCG would iterate from a nonzero (extrapolated) start toward the
+  // tolerance cg_tol |b| = 0, which it cannot meet, and throw NoConvergence at
+  // the cap; the exact solution 0 is returned instead, with no iterations.
+  template <typename R>
+  __global__ void
+  k_zero_flagged(R *__restrict__ x, const CgState *__restrict__ st, long long N, int nsys)
+  {
+    const int s = blockIdx.y;
+    if (s >= nsys || !st->zero[s])
+      return;
+    R *xs = x + s * N;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+      xs[i] = R(0);
+  }
 
   __device__ __forceinline__ double
   inv_jacobi_at(const Geo &geo, int i, int j)
@@ -2101,13 +2118,14 @@ namespace lbfem_gpu
                 st->rz[s] = sums[2 * NM + s];
                 st->it[s] = 0;
                 st->beta[s] = 0;
+                st->zero[s] = sums[s] == 0.0;
                 if (isnan(res))
                   {
                     st->active[s] = 0;
                     atomicExch(&st->status, 3); // LBFEM_ERR_NONFINITE
                   }
                 else
-                  st->active[s] = res <= st->tol[s] ? 0 : 1;
+                  st->active[s] = (res <= st->tol[s] || st->zero[s]) ? 0 : 1;
               }
             else
               st->active[s] = 0;
@@ -2197,6 +2215,8 @@ namespace lbfem_gpu
           {
             const double res = sqrt(sums[NM + s]), tv = tol * sqrt(sums[s]);
             st->tol[s] = tv;
+            if (sums[s] == 0.0)
+              st->zero[s] = 1; // b = 0 exactly: x = 0 (k_zero_flagged), no further rounds
             if (isnan(res))
               {
                 st->active[s] = 0;
@@ -2204,7 +2224,7 @@ namespace lbfem_gpu
               }
             else
               {
-                st->active[s] = res > tv ? 1 : 0;
+                st->active[s] = (res > tv && !st->zero[s]) ? 1 : 0;
                 progress[s] = st->active[s] && (round == 0 || res <= 0.5 * st->res[s]);
               }
             st->res[s] = res;

@@ -206,6 +206,35 @@ class Handle:
         self._call("predictor_corrector", self.h, _dptr(f), _dptr(feq), _dptr(incr), C.c_double(theta))
         return f
 
+    # -- device-pointer forms: arguments are device addresses (ints) and the
+    #    caller's cudaStream_t as an int (0: the legacy default stream)
+    def advection_dev(self, f, e, dt, lam, rhs, kind="taylor_galerkin", feq=0, remove_wall_mass_flux=-1, stream=0):
+        e = _f64(e)
+        self._call("advection_dev", self.h, f, feq or None, _dptr(e), C.c_double(dt), C.c_double(lam),
+                   C.c_int32(ADVECTION[kind]), C.c_int32(remove_wall_mass_flux), rhs, stream or None)
+
+    def mass_solve_dev(self, x, r, e=(0.0, 0.0), tg3_coefficient=0.0, stream=0):
+        e = _f64(e)
+        self._call("mass_solve_dev", self.h, x, r, _dptr(e), C.c_double(tg3_coefficient), stream or None)
+
+    def collide_bgk_dev(self, g, omega, stream=0):
+        self._call("collide_bgk_dev", self.h, g, C.c_double(omega), stream or None)
+
+    def compute_equilibrium_dev(self, f, feq, stream=0):
+        self._call("compute_equilibrium_dev", self.h, f, feq, stream or None)
+
+    def predictor_corrector_dev(self, f, feq, incr, theta, stream=0):
+        self._call("predictor_corrector_dev", self.h, f, feq, incr, C.c_double(theta), stream or None)
+
+    def set_populations_dev(self, f, stream=0):
+        self._call("set_populations_dev", self.h, f, stream or None)
+
+    def get_populations_dev(self, f, stream=0):
+        self._call("get_populations_dev", self.h, f, stream or None)
+
+    def step_stream(self, n=1, stream=0):
+        self._call("step_stream", self.h, C.c_int32(n), stream or None)
+
     def node_weight(self):
         w = np.empty(self.n)
         self._call("node_weight", self.h, _dptr(w))
@@ -240,6 +269,11 @@ def declare(lib, prefix):
         "solve_round_resident": [vp],
         "last_step_stats": [vp, dp, C.POINTER(i64)],
         "write_checkpoint": [vp, C.c_char_p, i32], "read_checkpoint": [vp, C.c_char_p, i32],
+        # device-pointer forms (vp: device addresses and the caller's cudaStream_t)
+        "advection_dev": [vp, vp, vp, dp, d, d, i32, i32, vp, vp],
+        "mass_solve_dev": [vp, vp, vp, dp, d, vp], "collide_bgk_dev": [vp, vp, d, vp],
+        "compute_equilibrium_dev": [vp, vp, vp, vp], "predictor_corrector_dev": [vp, vp, vp, vp, d, vp],
+        "set_populations_dev": [vp, vp, vp], "get_populations_dev": [vp, vp, vp], "step_stream": [vp, i32, vp],
     }
     for name, args in sig.items():
         fn = getattr(lib, prefix + name, None)

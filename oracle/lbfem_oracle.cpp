@@ -698,7 +698,18 @@ namespace
   {
     const int64_t N = o.N;
     double *r = o.cg_r.data(), *p = o.cg_p.data(), *v = o.cg_v.data(), *z = o.cg_z.data();
-    const double tol = o.prm.cg_tolerance * std::sqrt(dot(b, b, N));
+    const double bb = dot(b, b, N);
+    const double tol = o.prm.cg_tolerance * std::sqrt(bb);
+    *its = 0;
+    if (bb == 0.)
+      {
+        // an exactly zero right-hand side: the solution 0. deal.II's SolverCG would
+        // iterate from a nonzero (extrapolated) start toward the tolerance 0 and
+        // throw NoConvergence at the cap (the x-axis populations of the start-up
+        // Couette flow on 32 x 256 cells meet this after a few steps).
+        std::fill(x, x + N, 0.);
+        return LBFEM_OK;
+      }
     bool zero = true;
     for (int64_t i = 0; i < N && zero; ++i)
       zero = x[i] == 0.;

@@ -1,9 +1,9 @@
 """Generates the golden fixtures of tests/golden/ from the reference itself.
 
-Run in a container that has the reference sources (default /root/reference,
-or $LBFEM_REFERENCE) and the reference program built by `make -C oracle ref`:
+Run in a container that has the reference sources, named by $LBFEM_REFERENCE
+(required), and the reference program built by `make -C oracle ref`:
 
-    python tests/golden/make_golden.py
+    LBFEM_REFERENCE=<lbm-fem tree> python tests/golden/make_golden.py
 
 It writes
   stencils.json       -- assembled stencils of M, C_e, K_e for Q1 and Q2 on a
@@ -33,7 +33,9 @@ import types
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("LBFEM_REFERENCE", "/root/reference")
+REF = os.environ.get("LBFEM_REFERENCE")
+if not REF:
+    sys.exit("make_golden.py: set LBFEM_REFERENCE to the lbm-fem source tree")
 
 
 def load(name, path):

@@ -272,3 +272,15 @@ def test_checkpoint_restart(gpu_lib, oracle_mod, tmp_path, precision):
     a.step(10)
     b.step(10)
     assert rel_l2(b.get_populations(), a.get_populations()) <= (1e-10 if precision == "fp64" else 1e-6)
+
+
+def test_cg_zero_rhs_nonzero_start_gives_zero(gpu_lib, oracle_mod):
+    """As the oracle: an exactly zero right-hand side with a nonzero start
+    returns x = 0 (deal.II's SolverCG would throw NoConvergence at the cap)."""
+    tc, m = tgv(8)
+    prm = make_params(cg_max_iterations=5)
+    x0 = 1e-20 * np.cos(np.arange(m.n_dofs))
+    for h in (_gpu(m, prm), oracle_mod.Oracle(m, prm)):
+        x = h.mass_solve(np.zeros(m.n_dofs), x=x0)
+        assert np.all(x == 0) and h.cg_iterations() == 0
+        h.close()

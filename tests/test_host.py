@@ -107,3 +107,34 @@ def test_run_length_hits_t_end():
     m = cases.build_mesh(tc, 32, 1)
     dt, n = cases.run_length(tc, m, 0.25, 0.25)
     assert n == 166 and abs(n * dt - 0.25 * tc.reference_time()) < 1e-12
+
+
+def test_noalloc_tile_bound_is_implied_by_the_node_bound():
+    """lbfem_gpu_mass_solve_noalloc's fixed array holds the vectors of at most
+    NOALLOC_MAX_NODES nodes and the partial sums of NOALLOC_MAX_TILES tiles. No
+    mesh under the node limit has more tiles than the array holds, for every
+    degree's tile shape (kernels.cuh TileShape<P>), so the node limit is the
+    only one a caller meets."""
+    csrc = os.path.join(ROOT, "lbm-fem_b200", "csrc")
+    kern = open(os.path.join(csrc, "kernels.cuh")).read()
+    src = open(os.path.join(csrc, "lbfem_gpu.cu")).read()
+    max_nodes = 1 << int(re.search(r"NOALLOC_MAX_NODES = 1LL << (\d+)", src).group(1))
+    max_tiles = int(re.search(r"NOALLOC_MAX_TILES = (\d+)", src).group(1))
+    assert (max_nodes, max_tiles) == (131072, 4096)
+    shapes = {int(p): (int(cx), int(cy)) for p, cx, cy in re.findall(
+        r"struct TileShape<(\d)>\s*\{\s*static constexpr int CX = (\d+), CY = (\d+)", kern)}
+    assert sorted(shapes) == [1, 2, 3, 4]
+    worst = {}
+    for p, (cx, cy) in shapes.items():
+        tx, ty = p * cx, p * cy
+        most = 0
+        for ncx in range(1, max_nodes):
+            nfx = p * ncx + 1
+            if nfx * (p + 1) > max_nodes:
+                break
+            # the most cells along y that keep the mesh within the node limit
+            nfy = p * ((max_nodes // nfx - 1) // p) + 1
+            # both orientations of the box
+            most = max(most, -(-nfx // tx) * -(-nfy // ty), -(-nfy // tx) * -(-nfx // ty))
+        worst[p] = most
+    assert worst[1] == 2731 and max(worst.values()) < max_tiles, worst
