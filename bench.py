@@ -435,22 +435,72 @@ def run_ours(args):
     return 0
 
 
+class MT19937_64:
+    """The 64-bit Mersenne Twister of Matsumoto and Nishimura (2000), with the
+    parameters and seeding of C++'s std::mt19937_64: w = 64, n = 312, m = 156,
+    r = 31, a = 0xB5026F5AA96619E9, tempering (u, d) = (29, 0x5555555555555555),
+    (s, b) = (17, 0x71D67FFFEDA60000), (t, c) = (37, 0xFFF7EEE000000000), l = 43,
+    initialisation multiplier f = 6364136223846793005. __call__ returns the
+    engine's next 64-bit output (tests/test_host.py checks the stream against
+    std::mt19937_64 compiled here)."""
+
+    N, M = 312, 156
+    MASK = (1 << 64) - 1
+    UPPER, LOWER = 0xFFFFFFFF80000000, 0x7FFFFFFF
+
+    def __init__(self, seed):
+        self.mt = [seed & self.MASK]
+        for i in range(1, self.N):
+            prev = self.mt[-1]
+            self.mt.append((6364136223846793005 * (prev ^ (prev >> 62)) + i) & self.MASK)
+        self.i = self.N
+
+    def _twist(self):
+        mt = self.mt
+        for k in range(self.N):
+            y = (mt[k] & self.UPPER) | (mt[(k + 1) % self.N] & self.LOWER)
+            v = mt[(k + self.M) % self.N] ^ (y >> 1)
+            mt[k] = v ^ 0xB5026F5AA96619E9 if y & 1 else v
+        self.i = 0
+
+    def __call__(self):
+        if self.i >= self.N:
+            self._twist()
+        y = self.mt[self.i]
+        self.i += 1
+        y ^= (y >> 29) & 0x5555555555555555
+        y ^= (y << 17) & 0x71D67FFFEDA60000
+        y ^= (y << 37) & 0xFFF7EEE000000000
+        y ^= y >> 43
+        return y & self.MASK
+
+    def uniform(self):
+        """A double in [0, 1) from the top 53 bits of one output."""
+        return (self() >> 11) * (1.0 / (1 << 53))
+
+    def choice(self, values):
+        """One of values, uniform: the output modulo len(values) (bias below 1e-18)."""
+        return values[self() % len(values)]
+
+
 def batch_instances(n, seed=20261203):
-    """The batched workload: n independent instances drawn from a seeded
-    generator (numpy MT19937): half lid-driven cavities, half Taylor-Green
-    vortices; mesh edge from {32, 48, 64, 96, 128, 192, 256} cells; degree 1 or
-    2; Re log-uniform in [100, 1000]; U0 uniform in [0.05, 0.1]; mixed precision,
-    consistent mass; Bardow for cavities, Lee-Lin for vortices; CFL 0.4."""
+    """The batched workload: n independent instances drawn from
+    std::mt19937_64(seed) (MT19937_64): half lid-driven cavities, half
+    Taylor-Green vortices (alternating); then per instance, in this order, the
+    mesh edge from {32, 48, 64, 96, 128, 192, 256} cells, the degree 1 or 2,
+    Re log-uniform in [100, 1000] and U0 uniform in [0.05, 0.1] (MT19937_64.choice
+    and .uniform); mixed precision, consistent mass; Bardow for cavities,
+    Lee-Lin for vortices; CFL 0.4."""
     from lbfem_gpu import cases, d2q9, make_params
 
-    rng = np.random.Generator(np.random.MT19937(seed))
+    rng = MT19937_64(seed)
     out = []
     for k in range(n):
         case = "cavity" if k % 2 == 0 else "tgv"
         edge = int(rng.choice([32, 48, 64, 96, 128, 192, 256]))
         p = int(rng.choice([1, 2]))
-        re = float(10 ** rng.uniform(2, 3))
-        u0 = float(rng.uniform(0.05, 0.1))
+        re = float(100.0 * 10 ** rng.uniform())
+        u0 = float(0.05 + 0.05 * rng.uniform())
         if case == "cavity":
             tc = cases.LidDrivenCavity(u0, 1.2)
         else:
@@ -464,11 +514,14 @@ def batch_instances(n, seed=20261203):
 
 
 def batch_measure(n, steps, warmup):
-    """The batched workload of n instances: batched mixed steps (one graph launch per
-    step of all of them), the same instances stepped one at a time in mixed precision
-    and on the plain FP64 path, and each batched mixed instance's relative L2 velocity
-    error against its FP64 run. Host wall clock around calls that each end with one
-    device synchronisation."""
+    """The batched workload of n instances: batched steps (one graph launch per step
+    of all of them) in mixed precision and on the plain FP64 path, the same instances
+    stepped one at a time in both precisions, and each batched mixed instance's
+    relative L2 velocity error against its FP64 run. Device time: CUDA events on the
+    batch stream around the batched launches, and on each instance's stream around
+    its steps one at a time (summed)."""
+    import ctypes as C
+
     import lbfem_gpu
     from lbfem_gpu import d2q9, make_params
 
@@ -488,23 +541,33 @@ def batch_measure(n, steps, warmup):
         return hs
 
     def one_at_a_time(hs):
+        total = 0.0
         for h in hs:
             h.step(warmup)
-        t0 = time.perf_counter()
-        for h in hs:
+            h._call("event_record", h.h, 0)
             h.step(steps)
-        return time.perf_counter() - t0
+            h._call("event_record", h.h, 1)
+            ms = C.c_float()
+            h._call("event_elapsed", h.h, 0, 1, C.byref(ms))
+            total += ms.value * 1e-3
+        return total
+
+    def batched(hs):
+        b = lbfem_gpu.Batch(hs)
+        b.step(warmup)
+        b.step(steps)  # returns after the device finished (one synchronisation)
+        sec = b.last_ms() * 1e-3
+        b.close()
+        return sec
 
     units = 9 * sum(it["mesh"].n_unique() for it in inst) * steps
     hs = make()
-    b = lbfem_gpu.Batch(hs)
-    b.step(warmup)
-    lib.lbfem_gpu_synchronize(hs[0].h)
-    t0 = time.perf_counter()
-    b.step(steps)  # returns after the device finished (one synchronisation)
-    t_batch = time.perf_counter() - t0
-    b.close()
+    t_batch = batched(hs)
     f_mixed = [h.get_populations() for h in hs]  # the batched mixed run's end states
+    for h in hs:
+        h.close()
+    hs = make(fp64=True)
+    t_batch_fp64 = batched(hs)
     for h in hs:
         h.close()
     hs = make()
@@ -526,12 +589,17 @@ def batch_measure(n, steps, warmup):
             "speedup_vs_one_at_a_time": t_single / t_batch,
             "fp64_one_at_a_time": {"value": units / t_fp64, "ms_per_step": 1e3 * t_fp64 / steps},
             "speedup_vs_fp64_one_at_a_time": t_fp64 / t_batch,
+            "fp64_batched": {"value": units / t_batch_fp64, "ms_per_step": 1e3 * t_batch_fp64 / steps},
+            "gain_of_precision_batched": t_batch_fp64 / t_batch,
+            "gain_of_batching_mixed": t_single / t_batch,
+            "gain_of_batching_fp64": t_fp64 / t_batch_fp64,
             "accuracy": {"max_rel_l2_u_mixed_vs_fp64": max(errs), "median": float(np.median(errs)), "target": 1e-5,
                          "note": f"per instance, after {warmup + steps} steps of both runs"},
             "workload": f"{n} instances (cavities and Taylor-Green vortices)",
             "nodes_distinct_total": int(sum(it["mesh"].n_unique() for it in inst)),
             "instances": [{k: it[k] for k in ("case", "edge", "p", "Re", "U0", "scheme")} for it in inst],
-            "timing": "host wall clock around the call (each call ends with a device synchronisation)"}
+            "timing": "device time: CUDA events on the batch stream around the batched graph launches; "
+                      "one at a time, events on each instance's stream around its steps, summed"}
 
 
 def run_batch(args):

@@ -259,6 +259,58 @@ int lbfem_gpu_get_populations_dev(lbfem_gpu_ctx *ctx, double *f, void *stream);
 /* Scheme::step (schemes.h:92-98, 118-124) n_steps times, ordered on the caller's stream. */
 int lbfem_gpu_step_stream(lbfem_gpu_ctx *ctx, int32_t n_steps, void *stream);
 
+/*
+ * One y-strip of a mesh decomposed over several contexts (one per rank), as
+ * the reference distributes its triangulation and vectors over MPI ranks
+ * (discretization.h:71-75) with a ghost exchange inside every operator
+ * application (MatrixFree::loop, advection.h:151-175) and an MPI sum in every
+ * CG dot product (mass.h:204-211).
+ *
+ * The context is created on the rank's local mesh: the cells of its strip
+ * plus one ghost cell layer below (when it has a neighbour below) and the
+ * ghost node row above (when it has a neighbour above), non-periodic in y,
+ * with the walls of those rows. The rank owns the node rows
+ * [ghost_below, n_rows - ghost_above) of the local mesh; the others are
+ * copies of the neighbours' owned rows (ghost_below = degree rows, the
+ * ghost cell layer; ghost_above = 1 row, the neighbour's first owned row).
+ * For a periodic y axis the last rank's ghost row above holds the first
+ * rank's row 0 (the periodic image row is not kept separately).
+ *
+ * comm(user, op, count) is the caller's collective, called by
+ * lbfem_gpu_step (and the operator entries) with the context's stream idle:
+ *  - LBFEM_COMM_EXCHANGE: send_below holds 1 row and send_above `degree` rows
+ *    (count bytes per row), to the neighbour below / above; fill recv_below
+ *    with `degree` rows from the neighbour below and recv_above with 1 row from
+ *    the neighbour above. Sides without a neighbour are skipped.
+ *  - LBFEM_COMM_ALLREDUCE: sum the first count doubles of sums over the ranks,
+ *    in place.
+ * Every rank makes the same calls in the same order. comm returns 0 on
+ * success; anything else fails the step with LBFEM_ERR_ARG. The buffers are
+ * device memory, at least lbfem_gpu_strip_buffer_bytes each (sums: 64
+ * doubles), and stay valid while the context lives. In strip mode steps run
+ * host-driven (no step graphs), CG and conservation sums count the owned rows,
+ * and lbfem_gpu_stream_function is refused. No counterpart in the reference
+ * beyond the MPI decomposition named above.
+ */
+enum { LBFEM_COMM_EXCHANGE = 0, LBFEM_COMM_ALLREDUCE = 1 };
+typedef int (*lbfem_comm_fn)(void *user, int32_t op, int64_t count);
+typedef struct lbfem_strip_desc {
+  int32_t ghost_below;          /* degree (neighbour below) or 0 */
+  int32_t ghost_above;          /* 1 (neighbour above) or 0 */
+  /* y-widths of the neighbours' cells that share the local mesh's bottom and
+   * top node rows (0 where there is none): the mass diagonals of those rows
+   * get the missing cell's share, so that the Jacobi factors of the ghost
+   * rows equal the owner's */
+  double cell_below, cell_above;
+  lbfem_comm_fn comm;
+  void *user;
+  void *send_below, *send_above, *recv_below, *recv_above;
+  double *sums;
+} lbfem_strip_desc;
+/* Bytes each exchange buffer of lbfem_strip_desc needs on this context. */
+int lbfem_gpu_strip_buffer_bytes(const lbfem_gpu_ctx *ctx, int64_t *bytes);
+int lbfem_gpu_set_strip(lbfem_gpu_ctx *ctx, const lbfem_strip_desc *strip);
+
 /* Discretization::node_weight (discretization.h:164-169): the lumped mass diagonal, n_dofs values (1 on periodic images). */
 int lbfem_gpu_node_weight(lbfem_gpu_ctx *ctx, double *w);
 
@@ -329,6 +381,8 @@ typedef struct lbfem_gpu_batch lbfem_gpu_batch;
 int lbfem_gpu_batch_create(lbfem_gpu_ctx *const *ctxs, int32_t n_ctxs, lbfem_gpu_batch **batch);
 int lbfem_gpu_batch_step(lbfem_gpu_batch *batch, int32_t n_steps);
 const char *lbfem_gpu_batch_last_error(const lbfem_gpu_batch *batch);
+/* Device time (CUDA events on the batch stream) of the graph launches of the last batch_step call, in ms. */
+int lbfem_gpu_batch_last_ms(const lbfem_gpu_batch *batch, float *ms);
 int lbfem_gpu_batch_destroy(lbfem_gpu_batch *batch);
 
 /*

@@ -102,7 +102,18 @@ namespace lbfem_gpu
     int ncx, ncy; // cells per axis
     int px, py;
     long long N;
+    // Node rows [oy0, oy1) that this context owns. The whole grid for one
+    // context; a y-strip of a mesh split over several contexts owns its strip,
+    // and its rows outside are ghost copies of the neighbours' (lbfem_gpu_set_strip).
+    // Sums over nodes (CG dot products, conservation) count the owned rows only.
+    int oy0, oy1;
   };
+
+  __device__ __forceinline__ bool
+  owned_row(int j, const Grid &g)
+  {
+    return j >= g.oy0 && j < g.oy1;
+  }
 
   // Everything a kernel needs to know about the discretisation.
   struct Geo

@@ -79,6 +79,9 @@ struct lbfem_gpu_ctx
   int64_t graph_epoch = 0; // counts the invalidations of the step graphs (batch graphs embed them)
   cudaStream_t cap = nullptr;     // captures the loop bodies
   DevStats *d_stats = nullptr, *h_stats = nullptr;
+  // one y-strip of a decomposed mesh (lbfem_gpu_set_strip): ghost rows and the caller's collectives
+  bool strip = false;
+  lbfem_strip_desc sd{};
   std::string err;
 };
 
@@ -211,6 +214,7 @@ namespace
         (st = set_smem(ctx, k_cg_p<P, double, OPK_LAPLACE>, cg_smem<P, double, OPK_LAPLACE>(0))) ||
         (st = set_smem(ctx, k_cg_update<P, double, OPK_LAPLACE>, cg_smem<P, double, OPK_LAPLACE>(2))) ||
         (st = set_smem(ctx, k_cg_start<P, float, float, float>, cg_smem<P, float>(1))) ||
+        (st = set_smem(ctx, k_cg_start<P, float, float, double>, cg_smem<P, float>(1, true))) ||
         (st = set_smem(ctx, k_window_correct<P>, window_smem<P>())) ||
         (st = set_smem(ctx, k_richardson_pass<P, double>, cg_smem<P, double>(0))) ||
         (st = set_smem(ctx, k_richardson_pass<P, float>, cg_smem<P, float>(0))))
@@ -358,6 +362,59 @@ namespace
   }
 
   // The relative tolerance of the mixed-precision mass solve.
+  // ------------------------------------------------ y-strip decomposition
+  // The sums buffer the solvers reduce into: the caller's (summed over the
+  // ranks by its ALLREDUCE) in strip mode, else the context's.
+  double *
+  sums_buf(lbfem_gpu_ctx *ctx)
+  {
+    return ctx->strip ? ctx->sd.sums : ctx->d_sums;
+  }
+
+  // Strip mode: the first n doubles of sums_buf summed over the ranks.
+  int
+  strip_allreduce(lbfem_gpu_ctx *ctx, int n)
+  {
+    if (!ctx->strip)
+      return LBFEM_OK;
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->sd.comm(ctx->sd.user, LBFEM_COMM_ALLREDUCE, n) != 0)
+      return fail(ctx, LBFEM_ERR_ARG, "strip: the allreduce of %d sums failed", n);
+    return LBFEM_OK;
+  }
+
+  // Strip mode: the ghost rows of nb blocks (element size es, block stride N)
+  // of the field at base <- the neighbours' owned rows. Rows are contiguous
+  // in a block, so each side is one strided copy: 1 row down and `degree`
+  // rows up out of the owned rows, `degree` rows below and 1 row above in.
+  int
+  strip_exchange(lbfem_gpu_ctx *ctx, void *base, int nb, size_t es)
+  {
+    if (!ctx->strip)
+      return LBFEM_OK;
+    const Grid &g = ctx->grid;
+    const size_t row = size_t(g.nfx) * es, pitch = size_t(g.N) * es;
+    const int P = ctx->P;
+    char *b = static_cast<char *>(base);
+    const lbfem_strip_desc &sd = ctx->sd;
+    if (sd.ghost_below)
+      CK(cudaMemcpy2DAsync(sd.send_below, row, b + size_t(g.oy0) * row, pitch, row, nb, cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+    if (sd.ghost_above)
+      CK(cudaMemcpy2DAsync(sd.send_above, P * row, b + size_t(g.oy1 - P) * row, pitch, P * row, nb,
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (sd.comm(sd.user, LBFEM_COMM_EXCHANGE, int64_t(nb) * int64_t(row)) != 0)
+      return fail(ctx, LBFEM_ERR_ARG, "strip: the ghost exchange failed");
+    if (sd.ghost_below)
+      CK(cudaMemcpy2DAsync(b + size_t(g.oy0 - P) * row, pitch, sd.recv_below, P * row, P * row, nb,
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+    if (sd.ghost_above)
+      CK(cudaMemcpy2DAsync(b + size_t(g.oy1) * row, pitch, sd.recv_above, row, row, nb, cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+    return LBFEM_OK;
+  }
+
   double
   mixed_tolerance(const lbfem_params &p)
   {
@@ -476,11 +533,12 @@ namespace
     const int nsys = c.nsys;
     CK(cudaMemsetAsync(w.state, 0, sizeof(CgState), ctx->stream));
     int n_tiles = 0, st;
-    if ((st = cg_launch_start(ctx, w, c, &n_tiles)) || (st = reduce_into(ctx, w.partials, w.sums, n_tiles, 3 * NM)))
+    if ((st = cg_launch_start(ctx, w, c, &n_tiles)) || (st = reduce_into(ctx, w.partials, w.sums, n_tiles, 3 * NM)) ||
+        (st = strip_allreduce(ctx, 3 * NM)))
       return st;
     k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 0, tol, max_its);
     LAUNCHED();
-    if ((st = zero_flagged(ctx, c.x_new, w.state, nsys)))
+    if ((st = zero_flagged(ctx, c.x_new, w.state, nsys)) || (st = strip_exchange(ctx, w.r, nsys, sizeof(double))))
       return st;
     int pi = 0;
     for (int it = 0;; ++it)
@@ -496,15 +554,19 @@ namespace
           }
         if (ctx->h_cg->n_active == 0)
           break;
-        if ((st = cg_launch_p(ctx, w, c, pi)) || (st = reduce_into(ctx, w.partials, w.sums, n_tiles, NM)))
+        if ((st = cg_launch_p(ctx, w, c, pi)) || (st = reduce_into(ctx, w.partials, w.sums, n_tiles, NM)) ||
+            (st = strip_allreduce(ctx, NM)))
           return st;
         k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 1, tol, max_its);
         LAUNCHED();
         pi = 1 - pi;
-        if ((st = cg_launch_update(ctx, w, c, pi)) || (st = reduce_into(ctx, w.partials, w.sums, n_tiles, 2 * NM)))
+        if ((st = cg_launch_update(ctx, w, c, pi)) || (st = reduce_into(ctx, w.partials, w.sums, n_tiles, 2 * NM)) ||
+            (st = strip_allreduce(ctx, 2 * NM)))
           return st;
         k_cg_scalars<<<1, 32, 0, ctx->stream>>>(w.state, w.sums, nsys, 2, tol, max_its);
         LAUNCHED();
+        if ((st = strip_exchange(ctx, w.r, nsys, sizeof(double))))
+          return st;
       }
     if (its_out)
       *its_out = ctx->h_cg->total_its;
@@ -518,7 +580,7 @@ namespace
   CgScratch<double>
   ctx_scratch(lbfem_gpu_ctx *ctx)
   {
-    return CgScratch<double>{ctx->d_r, {ctx->d_p[0], ctx->d_p[1]}, ctx->d_partials, ctx->d_sums, ctx->d_cg};
+    return CgScratch<double>{ctx->d_r, {ctx->d_p[0], ctx->d_p[1]}, ctx->d_partials, sums_buf(ctx), ctx->d_cg};
   }
 
   // The context's own work buffers.
@@ -613,8 +675,9 @@ namespace
       LAUNCHED();
       return LBFEM_OK;
     });
-    if (st)
+    if (st || (st = strip_exchange(ctx, ctx->d_r_s, nsys, sizeof(float))))
       return st;
+    double *sums = sums_buf(ctx);
     // the rounds alternate between x_new and x_prev's buffer (free once the start has read it)
     int xi = in, xo = ip;
     float *r_in = ctx->d_r_s, *r_out = ctx->d_p_s[0];
@@ -636,9 +699,32 @@ namespace
           return st;
         std::swap(xi, xo);
         std::swap(r_in, r_out);
-        if ((st = reduce_into(ctx, ctx->d_partials, ctx->d_sums, n_tiles, 2 * NM)))
+        if (ctx->strip)
+          {
+            // The round's residual near the strip's edges saw the locally corrected
+            // ghost rows. With the neighbours' corrected rows in place, the residual
+            // b - A x of the owned rows is formed again (FP64 arithmetic), its ghost
+            // rows exchanged and its sums added over the ranks.
+            float *xs = ctx->d_x_s[xi];
+            if ((st = strip_exchange(ctx, xs, nsys, sizeof(float))))
+              return st;
+            st = with_degree(ctx->P, [&](auto PP) -> int {
+              constexpr int P = decltype(PP)::value;
+              dim3 grid = tile_grid<P>(g);
+              n_tiles = int(grid.x * grid.y);
+              grid.z = nsys;
+              k_cg_start<P, float, float, double><<<grid, THREADS, cg_smem<P, float>(1, true), ctx->stream>>>(
+                geo, b, nullptr, nullptr, xs, r_in, 0, ctx->d_partials, StreamCoef{}, 0);
+              LAUNCHED();
+              return LBFEM_OK;
+            });
+            if (st || (st = reduce_into(ctx, ctx->d_partials, sums, n_tiles, 3 * NM)) ||
+                (st = strip_allreduce(ctx, 2 * NM)) || (st = strip_exchange(ctx, r_in, nsys, sizeof(float))))
+              return st;
+          }
+        else if ((st = reduce_into(ctx, ctx->d_partials, sums, n_tiles, 2 * NM)))
           return st;
-        k_mixed_round<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, ctx->d_sums, nullptr, nsys, tol, max_rounds, 0, 0);
+        k_mixed_round<<<1, 32, 0, ctx->stream>>>(ctx->d_cg, sums, nullptr, nsys, tol, max_rounds, 0, 0);
         LAUNCHED();
         if (round == 0 && (st = zero_flagged(ctx, ctx->d_x_s[xi], ctx->d_cg, nsys)))
           return st; // xi: the round's output after the swap above
@@ -679,10 +765,13 @@ namespace
     R *first = (k % 2) ? scratch : out; // the lumped start, so that the last pass writes out
     k_lumped<R, R><<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo, b, first, nsys);
     LAUNCHED();
+    int st0;
+    if ((st0 = strip_exchange(ctx, first, nsys, sizeof(R))))
+      return st0;
     R *in = first, *to = first == out ? scratch : out;
     for (int j = 0; j < k; ++j)
       {
-        const int st = with_degree(ctx->P, [&](auto PP) -> int {
+        int st = with_degree(ctx->P, [&](auto PP) -> int {
           constexpr int P = decltype(PP)::value;
           dim3 grid = tile_grid<P>(ctx->grid);
           grid.z = nsys;
@@ -690,7 +779,7 @@ namespace
           LAUNCHED();
           return LBFEM_OK;
         });
-        if (st)
+        if (st || (st = strip_exchange(ctx, to, nsys, sizeof(R))))
           return st;
         std::swap(in, to);
       }
@@ -710,7 +799,7 @@ namespace
         LAUNCHED();
         if (its)
           *its = 0;
-        return LBFEM_OK;
+        return strip_exchange(ctx, x_new, nsys, sizeof(double));
       }
     if (ctx->prm.mass == LBFEM_MASS_RICHARDSON)
       {
@@ -965,7 +1054,9 @@ namespace
     else
       k_lumped<double, double><<<nb, THREADS, 0, ctx->stream>>>(geo, ctx->d_rhs, ctx->d_x[ctx->x_cur], NM);
     LAUNCHED();
-    return LBFEM_OK;
+    if (ctx->mixed)
+      return strip_exchange(ctx, ctx->d_x_s[ctx->x_cur], NM, sizeof(float));
+    return strip_exchange(ctx, ctx->d_x[ctx->x_cur], NM, sizeof(double));
   }
 
   // One host-driven step: the solver loops read their state back after every
@@ -1586,7 +1677,9 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
                    m->n_cells_y,
                    m->periodic_x ? 1 : 0,
                    m->periodic_y ? 1 : 0,
-                   N};
+                   N,
+                   0,
+                   nfy};
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   for (auto &e : ctx->ev)
@@ -1921,7 +2014,7 @@ lbfem_gpu_step(lbfem_gpu_ctx *ctx, int32_t n_steps)
     return fail(ctx, LBFEM_ERR_STATE, "step needs the time step");
   const int64_t launches0 = ctx->launches;
   int64_t its_total = 0;
-  if (ctx->trace)
+  if (ctx->trace || ctx->strip)
     {
       // host-driven steps (the solver rounds print their residuals)
       for (int s = 0; s < n_steps; ++s)
@@ -2084,6 +2177,8 @@ lbfem_gpu_stream_function(lbfem_gpu_ctx *ctx, const double *velocity, double *ps
     return st;
   if (!velocity || !psi)
     return fail(ctx, LBFEM_ERR_ARG, "stream_function: null buffer");
+  if (ctx->strip)
+    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "stream_function: not on a strip (gather the velocity on one context)");
   const long long N = ctx->grid.N;
   double *vel = ctx->d_x[ctx->x_new], *b = ctx->d_rhs, *x = ctx->d_rhs + N; // scratch between steps
   if ((st = upload(ctx, velocity, vel, 2)))
@@ -2403,6 +2498,71 @@ lbfem_gpu_step_stream(lbfem_gpu_ctx *ctx, int32_t n_steps, void *stream)
 }
 
 int
+lbfem_gpu_strip_buffer_bytes(const lbfem_gpu_ctx *ctx, int64_t *bytes)
+{
+  if (!ctx || !bytes)
+    return LBFEM_ERR_ARG;
+  // the widest exchange: the 9 FP64 population blocks, `degree` rows
+  *bytes = int64_t(Q) * ctx->P * ctx->grid.nfx * int64_t(sizeof(double));
+  return LBFEM_OK;
+}
+
+int
+lbfem_gpu_set_strip(lbfem_gpu_ctx *ctx, const lbfem_strip_desc *sd)
+{
+  int st;
+  if ((st = check_ctx(ctx)))
+    return st;
+  if (!sd || !sd->comm || !sd->sums)
+    return fail(ctx, LBFEM_ERR_ARG, "set_strip: the collective and the sums buffer are required");
+  const Grid &g = ctx->grid;
+  if (g.py)
+    return fail(ctx, LBFEM_ERR_ARG, "set_strip: the local mesh of a strip is not periodic in y");
+  if ((sd->ghost_below != 0 && sd->ghost_below != ctx->P) || (sd->ghost_above != 0 && sd->ghost_above != 1))
+    return fail(ctx, LBFEM_ERR_ARG, "set_strip: ghost rows are `degree` below and 1 above, or none");
+  if ((sd->ghost_below && (!sd->send_below || !sd->recv_below)) ||
+      (sd->ghost_above && (!sd->send_above || !sd->recv_above)))
+    return fail(ctx, LBFEM_ERR_ARG, "set_strip: missing exchange buffer");
+  const int oy0 = sd->ghost_below, oy1 = g.nfy - sd->ghost_above;
+  // the owned rows must hold whole cells' worth of rows to send `degree` rows up
+  if (oy1 - oy0 < ctx->P + 1)
+    return fail(ctx, LBFEM_ERR_ARG, "set_strip: the strip owns %d node rows, fewer than degree + 1", oy1 - oy0);
+  if (!(sd->cell_below >= 0) || !(sd->cell_above >= 0))
+    return fail(ctx, LBFEM_ERR_ARG, "set_strip: negative cell width");
+  // The end rows of the local mesh lack the neighbours' cell in their mass
+  // diagonals; add its share (M_hat is symmetric under a -> p - a, so a vertex
+  // row's diagonal and row sum scale with the summed width of its two cells).
+  Axis &ay = ctx->ay;
+  const int last = ay.n_nodes - 1;
+  const double fb = (ay.h.front() + sd->cell_below) / ay.h.front(), fa = (ay.h.back() + sd->cell_above) / ay.h.back();
+  ay.diag[0] *= fb;
+  ay.lump[0] *= fb;
+  ay.diag[last] *= fa;
+  ay.lump[last] *= fa;
+  for (int k : {0, last})
+    {
+      ay.invdiag[k] = 1. / ay.diag[k];
+      ay.invlump[k] = 1. / ay.lump[k];
+    }
+  const size_t nb = sizeof(double) * ay.n_nodes;
+  CK(cudaMemcpy(ctx->d_diagy, ay.diag.data(), nb, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_lumpy, ay.lump.data(), nb, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_ijy, ay.invdiag.data(), nb, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_ily, ay.invlump.data(), nb, cudaMemcpyHostToDevice));
+  ctx->sd = *sd;
+  ctx->strip = true;
+  ctx->grid.oy0 = oy0;
+  ctx->grid.oy1 = oy1;
+  // recorded step graphs are not used in strip mode; drop them
+  for (auto &kv : ctx->graphs)
+    if (kv.second.exec)
+      cudaGraphExecDestroy(kv.second.exec);
+  ctx->graphs.clear();
+  ++ctx->graph_epoch;
+  return LBFEM_OK;
+}
+
+int
 lbfem_gpu_node_weight(lbfem_gpu_ctx *ctx, double *w)
 {
   int st;
@@ -2527,6 +2687,8 @@ struct lbfem_gpu_batch
   };
   std::map<std::vector<int>, Entry> graphs; // by the buffer states of the instances
   DevStats *h_stats = nullptr;              // pinned, one per instance
+  cudaEvent_t t0 = nullptr, t1 = nullptr;   // device time of the last batch_step's launches
+  float last_ms = 0.f;
   std::string err;
 };
 
@@ -2653,6 +2815,7 @@ lbfem_gpu_batch_create(lbfem_gpu_ctx *const *ctxs, int32_t n, lbfem_gpu_batch **
   if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreate(&b->t0) != cudaSuccess || cudaEventCreate(&b->t1) != cudaSuccess ||
       cudaHostAlloc(&b->h_stats, sizeof(DevStats) * n, cudaHostAllocDefault) != cudaSuccess)
     {
       cudaGetLastError();
@@ -2667,6 +2830,15 @@ const char *
 lbfem_gpu_batch_last_error(const lbfem_gpu_batch *b)
 {
   return b ? b->err.c_str() : "";
+}
+
+int
+lbfem_gpu_batch_last_ms(const lbfem_gpu_batch *b, float *ms)
+{
+  if (!b || !ms)
+    return LBFEM_ERR_ARG;
+  *ms = b->last_ms;
+  return LBFEM_OK;
 }
 
 int
@@ -2686,6 +2858,10 @@ lbfem_gpu_batch_destroy(lbfem_gpu_batch *b)
     cudaEventDestroy(b->fork);
   if (b->join)
     cudaEventDestroy(b->join);
+  if (b->t0)
+    cudaEventDestroy(b->t0);
+  if (b->t1)
+    cudaEventDestroy(b->t1);
   if (b->stream)
     cudaStreamDestroy(b->stream);
   delete b;
@@ -2713,6 +2889,7 @@ lbfem_gpu_batch_step(lbfem_gpu_batch *b, int32_t n_steps)
   std::vector<RunStart> r0;
   for (size_t k = 0; k < n; ++k)
     r0.push_back(run_start(b->ctxs[k], b->h_stats[k]));
+  BCK(cudaEventRecord(b->t0, b->stream));
   for (int s = 0; s < n_steps; ++s)
     {
       lbfem_gpu_batch::Entry *e;
@@ -2727,9 +2904,11 @@ lbfem_gpu_batch_step(lbfem_gpu_batch *b, int32_t n_steps)
           rotate_after_step(b->ctxs[k]);
         }
     }
+  BCK(cudaEventRecord(b->t1, b->stream));
   for (size_t k = 0; k < n; ++k)
     BCK(cudaMemcpyAsync(&b->h_stats[k], b->ctxs[k]->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost, b->stream));
   BCK(cudaStreamSynchronize(b->stream));
+  BCK(cudaEventElapsedTime(&b->last_ms, b->t0, b->t1));
   int first = LBFEM_OK;
   for (size_t k = 0; k < n; ++k)
     {
@@ -2818,6 +2997,8 @@ lbfem_gpu_mass_solve_noalloc(lbfem_gpu_ctx *ctx, double *x, const double *r)
     return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: needs the structured DoF numbering");
   if (ctx->prm.mass != LBFEM_MASS_CG)
     return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: the consistent mass (CG) only");
+  if (ctx->strip)
+    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: not on a strip");
   if (ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES)
     return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: device ordinal %d too large", ctx->device);
   double *base = nullptr; // check_ctx made ctx's device current

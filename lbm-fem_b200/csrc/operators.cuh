@@ -370,7 +370,7 @@ namespace lbfem_gpu
     LBFEM_GRID_STRIDE(idx, N)
     {
       const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
-      if (is_image(i, j, g))
+      if (is_image(i, j, g) || !owned_row(j, g))
         continue;
       double dr = 0, mx = 0, my = 0;
 #pragma unroll
@@ -402,7 +402,7 @@ namespace lbfem_gpu
     LBFEM_GRID_STRIDE(idx, N)
     {
       const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
-      if (is_image(i, j, g))
+      if (is_image(i, j, g) || !owned_row(j, g))
         continue;
       double v[Q];
 #pragma unroll
@@ -1601,11 +1601,12 @@ namespace lbfem_gpu
       const A rr = -Ax + bb;
       rs[idx] = R(rr);
       if constexpr (SUMS)
-        {
-          part[0] += double(bb) * double(bb);
-          part[1] += double(rr) * double(rr);
-          part[2] += double(rr) * (cg_inv_jacobi<P, OPK>(geo, maps, gx0, gy0, i, j, image) * double(rr));
-        }
+        if (owned_row(gy0 + i, g))
+          {
+            part[0] += double(bb) * double(bb);
+            part[1] += double(rr) * double(rr);
+            part[2] += double(rr) * (cg_inv_jacobi<P, OPK>(geo, maps, gx0, gy0, i, j, image) * double(rr));
+          }
     });
     if constexpr (SUMS)
       {
@@ -1656,7 +1657,8 @@ namespace lbfem_gpu
       else
         pn = s_u[(i + P) * T::PF + j + P];
       posys[idx] = pn;
-      part[0] += double(pn) * double(Ap);
+      if (owned_row(gy0 + i, g))
+        part[0] += double(pn) * double(Ap);
     });
     block_reduce_store<1>(part, partials + (long long)s * nt, tile, NM * nt);
   }
@@ -1705,8 +1707,11 @@ namespace lbfem_gpu
       xs[idx] = (STAGE_XR ? s_x[t] : xs[idx]) + al * pv;
       const R rr = (STAGE_XR ? s_r[t] : rs[idx]) + -al * Ap;
       rs[idx] = rr;
-      part[0] += double(rr) * double(rr);
-      part[1] += double(rr) * (cg_inv_jacobi<P, OPK>(geo, maps, gx0, gy0, i, j, image) * double(rr));
+      if (owned_row(gy0 + i, g))
+        {
+          part[0] += double(rr) * double(rr);
+          part[1] += double(rr) * (cg_inv_jacobi<P, OPK>(geo, maps, gx0, gy0, i, j, image) * double(rr));
+        }
     });
     block_reduce_store<2>(part, partials + (long long)s * nt, tile, NM * nt);
   }
@@ -2091,8 +2096,11 @@ namespace lbfem_gpu
             const double bb = bc[u], rr = bb - ax;
             xo[idx] = float(xv);
             ro[idx] = float(rr);
-            part[0] += bb * bb;
-            part[1] += rr * rr;
+            if (owned_row(gy, g))
+              {
+                part[0] += bb * bb;
+                part[1] += rr * rr;
+              }
           }
         }
       }

@@ -95,6 +95,14 @@ class Batch:
             msg = self.lib.lbfem_gpu_batch_last_error(self.h).decode()
             raise (NoConvergence if st == LBFEM_ERR_NO_CONVERGENCE else LbfemError)(st, f"lbfem_gpu_batch_step: {msg}")
 
+    def last_ms(self):
+        """Device time (CUDA events on the batch stream) of the last step call's launches."""
+        fn = self.lib.lbfem_gpu_batch_last_ms
+        fn.restype, fn.argtypes = C.c_int, [C.c_void_p, C.POINTER(C.c_float)]
+        ms = C.c_float()
+        fn(self.h, C.byref(ms))
+        return ms.value
+
     def close(self):
         if getattr(self, "h", None) is not None:
             fn = self.lib.lbfem_gpu_batch_destroy

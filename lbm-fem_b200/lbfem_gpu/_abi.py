@@ -274,6 +274,8 @@ def declare(lib, prefix):
         "mass_solve_dev": [vp, vp, vp, dp, d, vp], "collide_bgk_dev": [vp, vp, d, vp],
         "compute_equilibrium_dev": [vp, vp, vp, vp], "predictor_corrector_dev": [vp, vp, vp, vp, d, vp],
         "set_populations_dev": [vp, vp, vp], "get_populations_dev": [vp, vp, vp], "step_stream": [vp, i32, vp],
+        # y-strip decomposition (strips.py)
+        "strip_buffer_bytes": [vp, C.POINTER(i64)], "set_strip": [vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(lib, prefix + name, None)

@@ -224,6 +224,11 @@ struct lbfem_oracle
   bool have_ts = false;
   std::vector<double> f, feq, rhs, x0, x1, cg_r, cg_p, cg_v, cg_z;
   int64_t cg_its = 0;
+  // one y-strip of a decomposed mesh (lbfem_oracle_set_strip): owned node rows
+  // [oy0, oy1), the rest ghost copies of the neighbours' rows
+  bool strip = false;
+  int oy0 = 0, oy1 = 0;
+  lbfem_strip_desc sd{};
 
   int64_t
   master(int i, int j) const
@@ -286,6 +291,48 @@ namespace
     for (double v : part)
       s += v;
     return s;
+  }
+
+  // The dot product of the solvers: over the owned rows, summed over the ranks
+  // of a strip decomposition (the MPI sum of deal.II's distributed vectors).
+  int
+  strip_dot(const lbfem_oracle &o, const double *a, const double *b, double *out)
+  {
+    if (!o.strip)
+      {
+        *out = dot(a, b, o.N);
+        return LBFEM_OK;
+      }
+    const int64_t off = int64_t(o.oy0) * o.nfx;
+    o.sd.sums[0] = dot(a + off, b + off, int64_t(o.oy1 - o.oy0) * o.nfx);
+    if (o.sd.comm(o.sd.user, LBFEM_COMM_ALLREDUCE, 1) != 0)
+      return LBFEM_ERR_ARG;
+    *out = o.sd.sums[0];
+    return LBFEM_OK;
+  }
+
+  // The ghost rows of one vector of N values <- the neighbours' owned rows
+  // (1 row down and `degree` rows up out of the owned rows).
+  int
+  strip_exchange(const lbfem_oracle &o, double *v)
+  {
+    if (!o.strip)
+      return LBFEM_OK;
+    const int64_t row = o.nfx;
+    const int P = o.p;
+    double *sb = static_cast<double *>(o.sd.send_below), *sa = static_cast<double *>(o.sd.send_above);
+    double *rb = static_cast<double *>(o.sd.recv_below), *ra = static_cast<double *>(o.sd.recv_above);
+    if (o.sd.ghost_below)
+      std::copy(v + o.oy0 * row, v + (o.oy0 + 1) * row, sb);
+    if (o.sd.ghost_above)
+      std::copy(v + (o.oy1 - P) * row, v + o.oy1 * row, sa);
+    if (o.sd.comm(o.sd.user, LBFEM_COMM_EXCHANGE, row * int64_t(sizeof(double))) != 0)
+      return LBFEM_ERR_ARG;
+    if (o.sd.ghost_below)
+      std::copy(rb, rb + P * row, v + (o.oy0 - P) * row);
+    if (o.sd.ghost_above)
+      std::copy(ra, ra + row, v + o.oy1 * row);
+    return LBFEM_OK;
   }
 
   // ------------------------------------------------------- advection (K1)
@@ -698,7 +745,10 @@ namespace
   {
     const int64_t N = o.N;
     double *r = o.cg_r.data(), *p = o.cg_p.data(), *v = o.cg_v.data(), *z = o.cg_z.data();
-    const double bb = dot(b, b, N);
+    double bb = 0;
+    int sst;
+    if ((sst = strip_dot(o, b, b, &bb)))
+      return sst;
     const double tol = o.prm.cg_tolerance * std::sqrt(bb);
     *its = 0;
     if (bb == 0.)
@@ -722,7 +772,10 @@ namespace
       }
     else
       std::copy(b, b + N, r);
-    double res = std::sqrt(dot(r, r, N));
+    double res = 0;
+    if ((sst = strip_exchange(o, r)) || (sst = strip_dot(o, r, r, &res)))
+      return sst;
+    res = std::sqrt(res);
     int64_t it = 0;
     *its = 0;
     if (std::isnan(res))
@@ -738,7 +791,8 @@ namespace
         for (int64_t i = 0; i < N; ++i)
           z[i] = inv[i] * r[i];
         const double rz_prev = rz;
-        rz = dot(r, z, N);
+        if ((sst = strip_dot(o, r, z, &rz)))
+          return sst;
         const double beta = it > 1 ? rz / rz_prev : 0.;
         if (it > 1)
           {
@@ -749,7 +803,9 @@ namespace
         else
           std::copy(z, z + N, p);
         op_vmult(o, A, v, p);
-        const double pAp = dot(p, v, N);
+        double pAp = 0;
+        if ((sst = strip_dot(o, p, v, &pAp)))
+          return sst;
         const double alpha = rz / pAp;
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < N; ++i)
@@ -757,7 +813,9 @@ namespace
             x[i] += alpha * p[i];
             r[i] += -alpha * v[i];
           }
-        res = std::sqrt(dot(r, r, N));
+        if ((sst = strip_exchange(o, r)) || (sst = strip_dot(o, r, r, &res)))
+          return sst;
+        res = std::sqrt(res);
         *its = it;
         if (std::isnan(res))
           return LBFEM_ERR_NONFINITE;
@@ -777,7 +835,7 @@ namespace
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < o.N; ++i)
           x[i] = inv[i] * r[i];
-        return LBFEM_OK;
+        return strip_exchange(o, x);
       }
     if (o.prm.mass == LBFEM_MASS_RICHARDSON)
       {
@@ -785,13 +843,15 @@ namespace
         const double *inv = o.inv_lumped.data();
         for (int64_t i = 0; i < o.N; ++i)
           x[i] = inv[i] * r[i];
-        for (int k = 0; k < o.prm.richardson; ++k)
+        int sst = strip_exchange(o, x);
+        for (int k = 0; k < o.prm.richardson && !sst; ++k)
           {
             op_vmult(o, A, o.cg_v.data(), x);
             for (int64_t i = 0; i < o.N; ++i)
               x[i] += inv[i] * (r[i] - o.cg_v[i]);
+            sst = strip_exchange(o, x);
           }
-        return LBFEM_OK;
+        return sst;
       }
     int64_t its = 0;
     const int st = cg_solve(o, A, x, r, &its);
@@ -1457,7 +1517,8 @@ lbfem_oracle_conservation(lbfem_oracle *h, double out[5])
   double s[5] = {0, 0, 0, 0, 0};
   for (int64_t i = 0; i < N; ++i)
     {
-      if (h->constrained[i])
+      const int64_t row = i / h->nfx;
+      if (h->constrained[i] || (h->strip && (row < h->oy0 || row >= h->oy1)))
         continue;
       double fi[Q];
       for (int a = 0; a < Q; ++a)
@@ -1476,10 +1537,56 @@ lbfem_oracle_conservation(lbfem_oracle *h, double out[5])
 
 
 int
+lbfem_oracle_strip_buffer_bytes(const lbfem_oracle *h, int64_t *bytes)
+{
+  if (!h || !bytes)
+    return LBFEM_ERR_ARG;
+  *bytes = int64_t(Q) * h->p * h->nfx * int64_t(sizeof(double));
+  return LBFEM_OK;
+}
+
+int
+lbfem_oracle_set_strip(lbfem_oracle *h, const lbfem_strip_desc *sd)
+{
+  if (!h || !sd || !sd->comm || !sd->sums || h->py)
+    return LBFEM_ERR_ARG;
+  if ((sd->ghost_below != 0 && sd->ghost_below != h->p) || (sd->ghost_above != 0 && sd->ghost_above != 1))
+    return LBFEM_ERR_ARG;
+  if ((sd->ghost_below && (!sd->send_below || !sd->recv_below)) ||
+      (sd->ghost_above && (!sd->send_above || !sd->recv_above)))
+    return LBFEM_ERR_ARG;
+  const int oy0 = sd->ghost_below, oy1 = h->nfy - sd->ghost_above;
+  if (oy1 - oy0 < h->p + 1 || !(sd->cell_below >= 0) || !(sd->cell_above >= 0))
+    return LBFEM_ERR_ARG;
+  // the neighbours' cell's share of the mass diagonals of the end rows (a vertex
+  // row's diagonal and row sum scale with the summed width of its two cells)
+  const double fb = (h->vy[1] - h->vy[0] + sd->cell_below) / (h->vy[1] - h->vy[0]);
+  const double fa = (h->vy[h->ncy] - h->vy[h->ncy - 1] + sd->cell_above) / (h->vy[h->ncy] - h->vy[h->ncy - 1]);
+  for (int i = 0; i < h->nfx; ++i)
+    for (const auto &[row, fac] : {std::pair<int, double>{0, fb}, std::pair<int, double>{h->nfy - 1, fa}})
+      {
+        const int64_t k = int64_t(row) * h->nfx + i;
+        if (h->constrained[k])
+          continue;
+        h->jacobi[k] *= fac;
+        h->lumped[k] *= fac;
+        h->inv_jacobi[k] = 1. / h->jacobi[k];
+        h->inv_lumped[k] = 1. / h->lumped[k];
+      }
+  h->sd = *sd;
+  h->strip = true;
+  h->oy0 = oy0;
+  h->oy1 = oy1;
+  return LBFEM_OK;
+}
+
+int
 lbfem_oracle_stream_function(lbfem_oracle *h, const double *velocity, double *psi)
 {
   if (!h || !velocity || !psi)
     return LBFEM_ERR_ARG;
+  if (h->strip)
+    return LBFEM_ERR_UNSUPPORTED;
   int64_t its = 0;
   return stream_function(*h, velocity, velocity + h->N, psi, &its);
 }

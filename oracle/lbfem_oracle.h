@@ -52,6 +52,9 @@ int lbfem_oracle_jacobi_diagonal(lbfem_oracle *h, double *d);
 int lbfem_oracle_conservation(lbfem_oracle *h, double out[5]);
 /* compute_stream_function (io.h:31-95): velocity = (u, v), 2 blocks of n_dofs; psi: n_dofs. */
 int lbfem_oracle_stream_function(lbfem_oracle *h, const double *velocity, double *psi);
+/* One y-strip of a decomposed mesh (lbfem_gpu_set_strip); buffers in host memory. */
+int lbfem_oracle_strip_buffer_bytes(const lbfem_oracle *h, int64_t *bytes);
+int lbfem_oracle_set_strip(lbfem_oracle *h, const lbfem_strip_desc *strip);
 /* 1-D reference data of FE_Q(p): Gauss-Lobatto support points (p+1), Gauss points and weights (p+1). */
 int lbfem_oracle_basis_1d(int32_t p, double *support, double *gauss_points, double *gauss_weights);
 

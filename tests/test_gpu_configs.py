@@ -9,7 +9,12 @@
   and consistent mass, lid 0.1, Re 400, stretch 1.2, CFL 0.4: FP64 against the
   oracle and mixed against FP64 after a few thousand steps.
 
-CG tolerance: the reference default 1e-8 (mass.h:33). Mixed bar: 1e-5."""
+CG tolerance of the FP64 runs: 1e-12, the plain method's (config 0), so that
+the FP64 comparison measures rounding, not where two CG runs of tolerance 1e-8
+happen to stop (at 1e-8 the Couette run ends 7.4e-12 apart after 5000 steps).
+The mixed runs use their own tolerance (LBFEM_MIXED_TOLERANCE). Mixed bar: 1e-5."""
+
+TOL = 1e-12
 import math
 
 import numpy as np
@@ -46,8 +51,8 @@ def test_config1_couette_32x256_5000_steps(gpu_lib, oracle_mod):
     tc.set_reynolds(50)
     m = cases.build_mesh(tc, 32, 1, n_cells_y=256)
     dt, steps = m.time_step(0.25), 5000
-    f_or, w = _run(oracle_mod.Oracle, tc, m, make_params("leelin", "cg"), dt, steps)
-    f64, _ = _run(_gpu, tc, m, make_params("leelin", "cg"), dt, steps)
+    f_or, w = _run(oracle_mod.Oracle, tc, m, make_params("leelin", "cg", cg_tolerance=TOL), dt, steps)
+    f64, _ = _run(_gpu, tc, m, make_params("leelin", "cg", cg_tolerance=TOL), dt, steps)
     fmx, _ = _run(_gpu, tc, m, make_params("leelin", "cg", precision="mixed"), dt, steps)
     assert rel_l2(f64, f_or) <= 1e-12, rel_l2(f64, f_or)
     e_u = rel_l2(_velocity(m, fmx), _velocity(m, f64))
@@ -70,8 +75,8 @@ def test_config2_cavity_128_q2(gpu_lib, oracle_mod, mass, steps):
     m = cases.build_mesh(tc, 128, 2)
     assert m.n_dofs == 66049
     dt = m.time_step(0.4)
-    f_or, _ = _run(oracle_mod.Oracle, tc, m, make_params("bardow", mass), dt, steps)
-    f64, _ = _run(_gpu, tc, m, make_params("bardow", mass), dt, steps)
+    f_or, _ = _run(oracle_mod.Oracle, tc, m, make_params("bardow", mass, cg_tolerance=TOL), dt, steps)
+    f64, _ = _run(_gpu, tc, m, make_params("bardow", mass, cg_tolerance=TOL), dt, steps)
     fmx, _ = _run(_gpu, tc, m, make_params("bardow", mass, precision="mixed"), dt, steps)
     assert rel_l2(f64, f_or) <= 1e-12, rel_l2(f64, f_or)
     e_u = rel_l2(_velocity(m, fmx), _velocity(m, f64))

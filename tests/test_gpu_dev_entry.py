@@ -4,6 +4,8 @@ calls a shim makes when it keeps the reference's Scheme::step and its vectors
 in device memory (advection.h:49-58, mass.h:185, collision.h:105-168). With
 and without a caller DoF numbering. FP64 bar as in the parity tests: relative
 L2 <= 1e-12 (operators, solves), <= 1e-14 element-wise (nodal maps)."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -24,10 +26,13 @@ def _case(name, p):
 
 
 def _perm(m, permuted):
+    """(dof_index, perm, mesh for the context): structured node s is the caller's
+    DoF perm[s]; the context's mesh gives its wall nodes by caller DoF."""
     if not permuted:
-        return None, np.arange(m.n_dofs)
+        return None, np.arange(m.n_dofs), m
     perm = np.random.default_rng(5).permutation(m.n_dofs).astype(np.int64)
-    return perm, perm
+    mc = dataclasses.replace(m, wall_dof=perm[m.wall_dof])
+    return perm, perm, mc
 
 
 @pytest.mark.parametrize("permuted", [False, True], ids=["structured", "permuted"])
@@ -38,9 +43,9 @@ def test_device_operators_match_the_oracle(gpu_lib, oracle_mod, name, p, permute
     import lbfem_gpu
 
     m = _case(name, p)
-    dof_index, perm = _perm(m, permuted)
+    dof_index, perm, mc = _perm(m, permuted)
     prm = make_params("leelin", "cg", cg_tolerance=1e-12)
-    g = lbfem_gpu.Solver(m, prm, dof_index=dof_index)
+    g = lbfem_gpu.Solver(mc, prm, dof_index=dof_index)
     o = oracle_mod.Oracle(m, prm)
     dev = torch.device("cuda:0")
     s = torch.cuda.Stream(device=dev)
@@ -104,20 +109,20 @@ def test_device_populations_and_stream_step(gpu_lib, precision, permuted):
     tc = cases.LidDrivenCavity(0.1, 1.2)
     tc.set_reynolds(400)
     m = cases.build_mesh(tc, 12, 2)
-    dof_index, perm = _perm(m, permuted)
+    dof_index, perm, mc = _perm(m, permuted)
     prm = make_params("bardow", "cg", precision=precision)
     dt, lam = m.time_step(0.4), tc.relaxation_time()
     x, y = m.nodes()
     f0 = tc.initial_populations(x, y, lam)
     fin = np.empty_like(f0)
     fin[:, perm] = f0
-    ref = lbfem_gpu.Solver(m, prm, dof_index=dof_index)
+    ref = lbfem_gpu.Solver(mc, prm, dof_index=dof_index)
     ref.set_time_step(dt, lam)
     ref.set_populations(fin)
     ref.step(7)
     expect = ref.get_populations()
     ref.close()
-    g = lbfem_gpu.Solver(m, prm, dof_index=dof_index)
+    g = lbfem_gpu.Solver(mc, prm, dof_index=dof_index)
     g.set_time_step(dt, lam)
     dev = torch.device("cuda:0")
     s = torch.cuda.Stream(device=dev)

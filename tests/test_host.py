@@ -138,3 +138,27 @@ def test_noalloc_tile_bound_is_implied_by_the_node_bound():
             most = max(most, -(-nfx // tx) * -(-nfy // ty), -(-nfy // tx) * -(-nfx // ty))
         worst[p] = most
     assert worst[1] == 2731 and max(worst.values()) < max_tiles, worst
+
+
+def test_mt19937_64_matches_the_cpp_engine(tmp_path):
+    """The batched workload's generator reproduces std::mt19937_64(20261203)
+    (compiled here with the system C++ compiler): the first 1000 outputs."""
+    import shutil
+    import subprocess
+
+    import bench
+
+    cxx = shutil.which("g++") or shutil.which("c++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    src = tmp_path / "mt.cc"
+    src.write_text("#include <cstdio>\n#include <random>\nint main(){std::mt19937_64 g(20261203ULL);"
+                   "for(int i=0;i<1000;++i)std::printf(\"%llu\\n\",(unsigned long long)g());}\n")
+    exe = tmp_path / "mt"
+    subprocess.run([cxx, "-O1", "-o", str(exe), str(src)], check=True)
+    want = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    rng = bench.MT19937_64(20261203)
+    assert [rng() for _ in range(1000)] == want
+    inst = bench.batch_instances(64)
+    assert sum(i["case"] == "cavity" for i in inst) == 32
+    assert all(100 <= i["Re"] <= 1000 and 0.05 <= i["U0"] <= 0.1 for i in inst)
