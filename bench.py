@@ -21,8 +21,9 @@ A step is one Scheme::step of the whole mesh. Metric: Q.DoF updates/s =
 --impl reference times the CPU implementation of the same path on the host
 cores (the deal.II reference cannot be built here; the FP64 oracle port of its
 algorithm, OpenMP on all cores, stands in for it).
-Under torchrun each rank runs an independent replica (the path is not
-sharded across GPUs yet): value = units of all ranks / max-over-ranks time.
+Under torchrun (N > 1) the mesh is cut into N y-strips, one per rank
+(lbfem_gpu.strips): ghost rows and CG sums over NCCL, value = the mesh's
+units / max-over-ranks device time (strong scaling).
 """
 import argparse
 import json
@@ -331,12 +332,108 @@ def run_precision(args, precision, tc, mesh, dt, lam, f0, local, pg, world, cg_t
     return out
 
 
+def run_strips(args, world, rank, local, pg):
+    """The workload on N GPUs as one mesh cut into N y-strips (lbfem_gpu.strips):
+    each rank steps its strip's context; ghost rows and CG sums move over NCCL
+    (DistComm). Both precisions, device time on each rank's context stream (CUDA
+    events around the K steps, which include the collectives' waits), max over
+    ranks. Strong scaling: the mesh is the same for every N."""
+    import ctypes as C
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import lbfem_gpu
+    from lbfem_gpu import make_params, strips
+
+    torch.cuda.set_device(local)
+    nccl = dist.new_group(backend="nccl", timeout=datetime.timedelta(seconds=120))
+    tc, mesh, dt, lam, f0, cfg = workload(args)
+    lib = lbfem_gpu.library()
+    st = strips.partition(mesh, world)[rank]
+    device = f"cuda:{local}"
+    units = 9 * mesh.n_unique() * args.steps
+    out = {}
+    for precision in ("fp64", "mixed"):
+        prm = make_params(args.scheme, "cg", cg_tolerance=args.cg_tol, precision=precision, device=local)
+        s = strips.StripSolver(mesh, st, prm, lambda mm, pp: lbfem_gpu.Solver(mm, pp), device,
+                               lambda solver: strips.DistComm(st, solver.bufs, nccl))
+        s.set_time_step(dt, lam)
+        s.set_initial_populations(f0)
+        h = s.h
+        s.step(args.warmup)
+        lib.lbfem_gpu_synchronize(h.h)
+        barrier(pg)
+        with Clocks(local) as clocks:
+            h._call("event_record", h.h, 0)
+            s.step(args.steps)
+            h._call("event_record", h.h, 1)
+            lib.lbfem_gpu_synchronize(h.h)
+        ms = C.c_float()
+        h._call("event_elapsed", h.h, 0, 1, C.byref(ms))
+        sec = allreduce_max(pg, ms.value * 1e-3)
+        its, launches = C.c_double(), C.c_int64()
+        h._call("last_step_stats", h.h, C.byref(its), C.byref(launches))
+        r = {"sec": sec, "its": its.value, "launches": int(launches.value), "clocks": clocks.summary()}
+        if precision == "mixed":
+            # end to end through the strip's host-buffer calls: this rank's local
+            # populations in, one step, its owned populations out
+            n_e2e = max(1, min(args.steps, 5))
+            loc = s._local(f0)
+            barrier(pg)
+            t0 = time.perf_counter()
+            for _ in range(n_e2e):
+                h.set_populations(loc)
+                s.step(1)
+                s.owned_populations()
+            r["e2e_sec"] = allreduce_max(pg, time.perf_counter() - t0)
+            r["e2e_steps"] = n_e2e
+            lb = 9 * 8 * st.mesh.n_dofs
+            ob = 9 * 8 * len(st.owned_index(mesh)[0])
+            t = torch.tensor([lb, ob], dtype=torch.float64)
+            if pg is not None:
+                pg.all_reduce(t)
+            r["h2d"], r["d2h"] = int(t[0]), int(t[1])
+        s.close()
+        out[precision] = r
+    if rank != 0:
+        return 0
+    mix, f64 = out["mixed"], out["fp64"]
+    line = {
+        "metric": METRIC, "value": units / mix["sec"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * mix["sec"] / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32 mixed (FP32 deviations, FP32 streaming/collision and FP32 tensor-product window "
+                 "correction; FP64 refinement residuals, dot products and conservation sums)",
+        "data": "synthetic (analytic Taylor-Green initial state)",
+        "config": dict(cfg, precision="mixed (headline) and fp64",
+                       parallelism=f"y-strips x{world} (one mesh; ghost rows and CG sums over NCCL)",
+                       mixed_tolerance=mixed_tol(args.cg_tol),
+                       solver_iterations_per_solve={"mixed (window corrections)": mix["its"],
+                                                    "fp64 (Jacobi-PCG)": f64["its"]}),
+        "fp64": {"value": units / f64["sec"], "ms_per_step": 1e3 * f64["sec"] / args.steps,
+                 "cg_tolerance": args.cg_tol, "gpu_launches": f64["launches"]},
+        "mixed_vs_fp64_speedup": f64["sec"] / mix["sec"],
+        "roofline": None, "cpu_baseline": None,
+        "e2e": {"value": 9 * mesh.n_unique() * mix["e2e_steps"] / mix["e2e_sec"], "unit": UNIT,
+                "h2d_bytes_per_step": mix["h2d"], "d2h_bytes_per_step": mix["d2h"], "steps": mix["e2e_steps"],
+                "call": "each rank: set_populations of its local mesh, one strip step, its owned populations out"},
+        "clocks": mix["clocks"], "gpu_launches": mix["launches"],
+        "timing": "device time per rank (CUDA events on the strip context's stream), max over ranks",
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def run_ours(args):
     import ctypes as C
 
     import lbfem_gpu
 
     world, rank, local, pg = dist_setup()
+    if world > 1:
+        return run_strips(args, world, rank, local, pg)
     tc, mesh, dt, lam, f0, cfg = workload(args)
     lib = lbfem_gpu.library()
     ind = mesh.independent()
@@ -404,8 +501,8 @@ def run_ours(args):
         "dtype": "f32 mixed (FP32 deviations, FP32 streaming/collision and FP32 tensor-product window "
                  "correction; FP64 refinement residuals, dot products and conservation sums)",
         "data": "synthetic (analytic Taylor-Green initial state)",
-        "config": dict(cfg, precision="mixed (headline) and fp64", parallelism=f"replicas x{world}" if world > 1
-                       else "single GPU", mixed_tolerance=mixed_tol(args.cg_tol),
+        "config": dict(cfg, precision="mixed (headline) and fp64", parallelism="single GPU",
+                       mixed_tolerance=mixed_tol(args.cg_tol),
                        solver_iterations_per_solve={"mixed (window corrections)": mix["its"],
                                                     "fp64 (Jacobi-PCG)": f64["its"]}),
         "fp64": {"value": units / f64["sec"], "ms_per_step": 1e3 * f64["sec"] / args.steps,

@@ -1,7 +1,7 @@
 """The N > 1 host path of bench.py on CPU: gloo ranks as the bench's torchrun
-launch makes them (one process per rank, 127.0.0.1 rendezvous). The path runs
-independent replicas, so the only cross-rank steps are the barriers around the
-timed region and the max over ranks of the device time."""
+launch makes them (one process per rank, 127.0.0.1 rendezvous): the barriers
+around the timed region and the max over ranks of the device time. The strips'
+own exchanges and sums over gloo are tested in test_strips.py."""
 import json
 import os
 import socket
