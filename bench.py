@@ -855,6 +855,46 @@ def run_streaming(args):
     return 0
 
 
+def run_contraction_study(args):
+    """The x-pass contraction of the streaming right-hand side alone, on CUDA
+    cores and on tensor cores (lbfem_gpu_contraction_study), degree 2 and 3,
+    FP32 (TF32 three-term split) and FP64 (DMMA), on the node rows of the
+    --cells^2 mesh of each degree. Device time per launch (CUDA events) and the
+    relative difference of the two forms' output checksums."""
+    import ctypes as C
+
+    import lbfem_gpu
+
+    world, rank, local, pg = dist_setup()
+    lib = lbfem_gpu.library()
+    fn = lib.lbfem_gpu_contraction_study
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_int32] * 7 + [C.POINTER(C.c_float), C.POINTER(C.c_double)]
+    out = []
+    for p in (2, 3):
+        rows = p * args.cells + 1
+        for fp64 in (0, 1):
+            res = {}
+            for tensor in (0, 1):
+                ms, cs = C.c_float(), C.c_double()
+                st = fn(local, p, fp64, tensor, rows, args.cells, args.study_reps, C.byref(ms), C.byref(cs))
+                if st != 0:
+                    raise RuntimeError(f"contraction study p={p} fp64={fp64} tensor={tensor}: status {st}")
+                res[tensor] = (ms.value, cs.value)
+            real = 8 if fp64 else 4
+            nbytes = 4 * rows * (p * args.cells + 1) * real  # u, h in; y1, y2 out
+            out.append({"degree": p, "precision": "fp64 (DMMA)" if fp64 else "fp32 (TF32 x3)",
+                        "cuda_core_ms": res[0][0], "tensor_core_ms": res[1][0],
+                        "tensor_over_cuda_time": res[1][0] / res[0][0],
+                        "cuda_core_gbs": nbytes / res[0][0] / 1e6, "tensor_core_gbs": nbytes / res[1][0] / 1e6,
+                        "checksum_rel_diff": abs(res[1][1] - res[0][1]) / abs(res[0][1])})
+    if rank == 0:
+        print(json.dumps({"study": "x-pass sum-factorisation contraction, CUDA cores vs tensor cores",
+                          "grid": f"(p {args.cells} + 1)^2 nodes, two fields in, two assembled rows out",
+                          "reps": args.study_reps, "results": out}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -881,7 +921,12 @@ def main():
                     help="steps of the mixed-vs-FP64 accuracy leg (the throughput scan's 500)")
     ap.add_argument("--cg-tol", type=float, default=1e-8,
                     help="relative CG tolerance of both precisions (MassSettings default 1e-8, mass.h:33)")
+    ap.add_argument("--contraction-study", action="store_true",
+                    help="time the x-pass contraction on CUDA cores and tensor cores instead of the default")
+    ap.add_argument("--study-reps", type=int, default=20)
     args = ap.parse_args()
+    if args.contraction_study:
+        return run_contraction_study(args)
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.batch and args.impl == "ours":

@@ -82,6 +82,17 @@ typedef struct lbfem_mesh_desc {
   int64_t n_walls;
   const int64_t *wall_dof;       /* n_walls caller DoF numbers */
   const double *wall_velocity;   /* 2*n_walls */
+  /*
+   * NULL, or the mapped vertices of a general quadrilateral mesh (the
+   * reference's --distort, TaylorGreenVortex::transform_mesh,
+   * test_cases.h:52-63): vertex (i, j), 0 <= i <= n_cells_x, 0 <= j <= n_cells_y,
+   * at (vertex_xy[2 k], vertex_xy[2 k + 1]), k = j (n_cells_x + 1) + i. Each cell is
+   * the bilinear image of the unit square through its four vertices (MappingQ1),
+   * its support points the images of the Gauss-Lobatto points. vertex_x /
+   * vertex_y still give the box's extent (first and last entries). Supported:
+   * FP64, TG2, either scheme, consistent or lumped mass, no walls.
+   */
+  const double *vertex_xy;
 } lbfem_mesh_desc;
 
 /*
@@ -361,6 +372,17 @@ int lbfem_gpu_advection_resident(lbfem_gpu_ctx *ctx);
  */
 int lbfem_gpu_solve_round_resident(lbfem_gpu_ctx *ctx);
 
+/*
+ * The streaming kernel's tile, chosen at run time: before a mixed-precision
+ * context's first step, each compiled tile shape of its degree (cells per CTA and
+ * per thread's x / y segment) is timed on the context's own buffers, and the
+ * fastest is kept (cached per device, degree, scheme and grid for the process;
+ * LBFEM_TUNE=0 in the environment keeps the default). shape: -1 not yet tuned,
+ * 0 the default shape, 1 the alternative; ms: the two shapes' times per launch.
+ * No counterpart in the reference.
+ */
+int lbfem_gpu_tuning(const lbfem_gpu_ctx *ctx, int32_t *shape, float *ms);
+
 /* Statistics of the last lbfem_gpu_step call: CG iterations per solve (mean) and kernel launches. */
 int lbfem_gpu_last_step_stats(const lbfem_gpu_ctx *ctx, double *cg_iterations_per_solve, int64_t *kernel_launches);
 
@@ -414,6 +436,19 @@ int lbfem_gpu_batch_destroy(lbfem_gpu_batch *batch);
  * lbfem_gpu_cg_iterations.
  */
 int lbfem_gpu_mass_solve_noalloc(lbfem_gpu_ctx *ctx, double *x, const double *r);
+
+/*
+ * The sum-factorisation contraction of the streaming right-hand side's x pass
+ * (the FEEvaluation gradient / integrate pair it replaces is advection.h:100-121),
+ * alone on a rows x (degree * cells + 1) grid of two fields, on CUDA cores
+ * (tensor = 0) or tensor cores (tensor = 1: TF32 mma.sync with a three-term
+ * split for FP32, DMMA for FP64), degree 2 or 3. Times `reps` launches with CUDA
+ * events on the default stream (ms: per launch) and returns a checksum of the
+ * outputs for comparing the two forms. A measurement for the choice between
+ * CUDA and tensor cores; the steps do not use it. No counterpart in the reference.
+ */
+int lbfem_gpu_contraction_study(int32_t device, int32_t degree, int32_t fp64, int32_t tensor, int32_t rows,
+                                int32_t cells, int32_t reps, float *ms, double *checksum);
 
 #ifdef __cplusplus
 }

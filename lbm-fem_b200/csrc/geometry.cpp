@@ -101,6 +101,16 @@ namespace lbfem_gpu
         qx[k] = (t + 1) / 2;
         qw[k] = 1 / ((1 - t * t) * dp * dp);
       }
+    for (int q = 0; q < nq; ++q)
+      {
+        gq[q] = double(qx[q]);
+        gw[q] = double(qw[q]);
+        for (int a = 0; a <= p; ++a)
+          {
+            gS[q][a] = double(L.value(a, qx[q]));
+            gD[q][a] = double(L.deriv(a, qx[q]));
+          }
+      }
     for (int a = 0; a <= p; ++a)
       {
         xi[a] = double(L.x[a]);
@@ -262,5 +272,75 @@ namespace lbfem_gpu
           }
       }
     return out;
+  }
+
+  std::vector<double>
+  quad_geometry(const Basis1D &b, const double *vxy, int ncx, int ncy)
+  {
+    const int n = b.p + 1;
+    std::vector<double> g(size_t(ncx) * ncy * n * n * 5);
+    auto v = [&](int i, int j, int k) { return vxy[(size_t(j) * (ncx + 1) + i) * 2 + k]; };
+    for (int cy = 0; cy < ncy; ++cy)
+      for (int cx = 0; cx < ncx; ++cx)
+        for (int q2 = 0; q2 < n; ++q2)
+          for (int q1 = 0; q1 < n; ++q1)
+            {
+              const double s = b.gq[q1], t = b.gq[q2];
+              double J[2][2];
+              for (int k = 0; k < 2; ++k)
+                {
+                  J[k][0] = (1 - t) * (v(cx + 1, cy, k) - v(cx, cy, k)) + t * (v(cx + 1, cy + 1, k) - v(cx, cy + 1, k));
+                  J[k][1] = (1 - s) * (v(cx, cy + 1, k) - v(cx, cy, k)) + s * (v(cx + 1, cy + 1, k) - v(cx + 1, cy, k));
+                }
+              const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+              double *o = &g[((size_t(cy) * ncx + cx) * n * n + q2 * n + q1) * 5];
+              o[0] = J[1][1] / det;
+              o[1] = -J[0][1] / det;
+              o[2] = -J[1][0] / det;
+              o[3] = J[0][0] / det;
+              o[4] = b.gw[q1] * b.gw[q2] * det;
+            }
+    return g;
+  }
+
+  void
+  quad_diagonals(const Basis1D &b, const std::vector<double> &geo, int ncx, int ncy, bool px, bool py,
+                 std::vector<double> &jacobi, std::vector<double> &lumped)
+  {
+    const int p = b.p, n = p + 1, nfx = p * ncx + 1, nfy = p * ncy + 1;
+    jacobi.assign(size_t(nfx) * nfy, 0.);
+    lumped.assign(size_t(nfx) * nfy, 0.);
+    auto master = [&](int i, int j) {
+      if (px && i == p * ncx)
+        i = 0;
+      if (py && j == p * ncy)
+        j = 0;
+      return size_t(j) * nfx + i;
+    };
+    for (int cy = 0; cy < ncy; ++cy)
+      for (int cx = 0; cx < ncx; ++cx)
+        for (int bb = 0; bb < n; ++bb)
+          for (int aa = 0; aa < n; ++aa)
+            {
+              double sj = 0, sl = 0;
+              for (int q2 = 0; q2 < n; ++q2)
+                for (int q1 = 0; q1 < n; ++q1)
+                  {
+                    const double phi = b.gS[q1][aa] * b.gS[q2][bb];
+                    const double jxw = geo[((size_t(cy) * ncx + cx) * n * n + q2 * n + q1) * 5 + 4];
+                    sj += phi * phi * jxw;
+                    sl += phi * jxw;
+                  }
+              const size_t k = master(cx * p + aa, cy * p + bb);
+              jacobi[k] += sj;
+              lumped[k] += sl;
+            }
+    for (int j = 0; j < nfy; ++j)
+      for (int i = 0; i < nfx; ++i)
+        if ((px && i == p * ncx) || (py && j == p * ncy))
+          {
+            jacobi[size_t(j) * nfx + i] = 1.;
+            lumped[size_t(j) * nfx + i] = 1.;
+          }
   }
 } // namespace lbfem_gpu

@@ -31,8 +31,20 @@ namespace lbfem_gpu
     double Ch[MAXP + 1][MAXP + 1]; // int l_a l_b'
     double Kh[MAXP + 1][MAXP + 1]; // int l_a' l_b'
     double d0[MAXP + 1], d1[MAXP + 1]; // l_a'(0), l_a'(1)
+    double gq[MAXP + 1], gw[MAXP + 1];  // the p + 1 Gauss points and weights on [0,1]
+    double gS[MAXP + 1][MAXP + 1], gD[MAXP + 1][MAXP + 1]; // [q][a] = l_a(x_q), l_a'(x_q)
     explicit Basis1D(int p);
   };
+
+  // General quadrilaterals: the cells are bilinear images (MappingQ1) of the unit
+  // square through the vertices vxy ((ncy+1) x (ncx+1) x 2, vertex (i, j) at
+  // 2 (j (ncx+1) + i)). quad_geometry: per cell (cy ncx + cx) and Gauss point
+  // (q2 (p+1) + q1), the inverse Jacobian row-major and JxW (5 values).
+  std::vector<double> quad_geometry(const Basis1D &b, const double *vxy, int ncx, int ncy);
+  // The Jacobi diagonal and the row sums (lumped diagonal) of the assembled mass
+  // matrix on the structured nodes; a periodic image node gets 1 in both.
+  void quad_diagonals(const Basis1D &b, const std::vector<double> &geo, int ncx, int ncy, bool px, bool py,
+                      std::vector<double> &jacobi, std::vector<double> &lumped);
 
   // The assembled 1-D operators of one axis, as rows of 2p+1 coefficients:
   // row[m][i][k] couples node i to node i+k-p (m: 0 = M, 1 = C, 2 = C^T, 3 = K).

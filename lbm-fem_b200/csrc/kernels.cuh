@@ -76,11 +76,36 @@ namespace lbfem_gpu
     static constexpr int CX = 15, CY = 6, KX = 3, KY = 2;
   };
 
+  // A second shape per degree, for the run-time choice of the streaming kernel's
+  // tile (tune_pair): 8 x-pass warps busy at every degree.
   template <int P>
+  struct TileShapeAlt;
+  template <>
+  struct TileShapeAlt<1>
+  {
+    static constexpr int CX = 48, CY = 24, KX = 6, KY = 6;
+  };
+  template <>
+  struct TileShapeAlt<2>
+  {
+    static constexpr int CX = 24, CY = 12, KX = 3, KY = 3;
+  };
+  template <>
+  struct TileShapeAlt<3>
+  {
+    static constexpr int CX = 16, CY = 8, KX = 2, KY = 2;
+  };
+  template <>
+  struct TileShapeAlt<4>
+  {
+    static constexpr int CX = 16, CY = 6, KX = 2, KY = 2;
+  };
+
+  template <int P, typename S = TileShape<P>>
   struct Tile
   {
-    static constexpr int CX = TileShape<P>::CX, CY = TileShape<P>::CY;
-    static constexpr int KX = TileShape<P>::KX, KY = TileShape<P>::KY;
+    static constexpr int CX = S::CX, CY = S::CY;
+    static constexpr int KX = S::KX, KY = S::KY;
     static constexpr int TX = P * CX, TY = P * CY;         // own nodes
     static constexpr int FX = TX + P + 1, FY = TY + P + 1; // footprint
     static constexpr int PF = FX | 1;                      // odd row pitch: conflict-free column access
@@ -127,6 +152,8 @@ namespace lbfem_gpu
     const double *rowx, *rowy;           // assembled 1-D rows [4][n][2p+1] (M, C, C^T, K), wall faces
     const uint8_t *wall;                 // per node: 0 fluid, k > 0 wall with velocity wall_u[2(k-1)..]; may be null
     const double *wall_u;
+    // general quadrilaterals only (else null): per node lumped diagonal and inverse Jacobi diagonal
+    const double *lump2, *ijac2;
   };
 
   __device__ __constant__ double c_W[Q] = {4. / 9., 1. / 9., 1. / 36., 1. / 9., 1. / 36.,
@@ -190,27 +217,42 @@ namespace lbfem_gpu
     float rho, ux, uy, drho;
   };
 
+  // The D2Q9 directions and weights as compile-time FP32 values: literal
+  // operands in the FP32 kernels instead of constant-bank loads and FP64->FP32
+  // conversions (the weights are the FP64 values rounded to FP32, as before).
+  __device__ constexpr float kEXf[Q] = {0, 1, 1, 0, -1, -1, -1, 0, 1};
+  __device__ constexpr float kEYf[Q] = {0, 0, 1, 1, 1, 0, -1, -1, -1};
+  __device__ constexpr float kWf[Q] = {float(4. / 9.),  float(1. / 9.),  float(1. / 36.), float(1. / 9.), float(1. / 36.),
+                            float(1. / 9.),  float(1. / 36.), float(1. / 9.),  float(1. / 36.)};
+
+  // The momentum sums in the order of the loop over a with e_a in {-1, 0, 1}
+  // (the zero terms dropped: adding +-0 changes no value).
   __device__ __forceinline__ MomF
   moments_dev(const float (&d)[Q])
   {
-    float drho = 0, mx = 0, my = 0;
+    float drho = 0;
 #pragma unroll
     for (int a = 0; a < Q; ++a)
-      {
-        drho += d[a];
-        mx += float(c_EX[a]) * d[a];
-        my += float(c_EY[a]) * d[a];
-      }
+      drho += d[a];
+    const float mx = ((((d[1] + d[2]) - d[4]) - d[5]) - d[6]) + d[8];
+    const float my = ((((d[2] + d[3]) + d[4]) - d[6]) - d[7]) - d[8];
     const float rho = 1.f + drho;
     return {rho, mx / rho, my / rho, drho};
+  }
+
+  // feq - w of the direction (ex, ey) with weight w.
+  __device__ __forceinline__ float
+  feqd(float ex, float ey, float w, const MomF &m)
+  {
+    const float uu = m.ux * m.ux + m.uy * m.uy;
+    const float eu = ex * m.ux + ey * m.uy;
+    return w * (m.drho + m.rho * (3.f * eu + 4.5f * eu * eu - 1.5f * uu));
   }
 
   __device__ __forceinline__ float
   feqd_a(int a, const MomF &m)
   {
-    const float uu = m.ux * m.ux + m.uy * m.uy;
-    const float eu = float(c_EX[a]) * m.ux + float(c_EY[a]) * m.uy;
-    return float(c_W[a]) * (m.drho + m.rho * (3.f * eu + 4.5f * eu * eu - 1.5f * uu));
+    return feqd(kEXf[a], kEYf[a], kWf[a], m);
   }
 
   // What a node imposes on its moments (collision.h:53-72).
@@ -407,22 +449,22 @@ namespace lbfem_gpu
   // Per-CTA tables of the footprint: source column and row offset of every
   // footprint column/row (-1 outside a non-periodic domain), the widths of the
   // CX+1 / CY+1 footprint cells and their inverses (0 outside the domain).
-  template <int P, typename R = double>
+  template <int P, typename R = double, typename S = TileShape<P>>
   struct TileMaps
   {
-    int col[Tile<P>::FX];
-    int rowi[Tile<P>::FY];
-    int row[Tile<P>::FY]; // storage offset of the row (a population array holds fewer than 2^31 nodes)
-    R hx[Tile<P>::CX + 1], hxi[Tile<P>::CX + 1], cx[Tile<P>::CX + 1];
-    R hy[Tile<P>::CY + 1], hyi[Tile<P>::CY + 1], cy[Tile<P>::CY + 1];
-    double ijx[Tile<P>::FX], ijy[Tile<P>::FY]; // inverse Jacobi diagonal factors of the footprint's storage nodes
+    int col[Tile<P, S>::FX];
+    int rowi[Tile<P, S>::FY];
+    int row[Tile<P, S>::FY]; // storage offset of the row (a population array holds fewer than 2^31 nodes)
+    R hx[Tile<P, S>::CX + 1], hxi[Tile<P, S>::CX + 1], cx[Tile<P, S>::CX + 1];
+    R hy[Tile<P, S>::CY + 1], hyi[Tile<P, S>::CY + 1], cy[Tile<P, S>::CY + 1];
+    double ijx[Tile<P, S>::FX], ijy[Tile<P, S>::FY]; // inverse Jacobi diagonal factors of the footprint's storage nodes
   };
 
-  template <int P, typename R>
+  template <int P, typename R, typename S>
   __device__ __forceinline__ void
-  build_maps(TileMaps<P, R> &m, const Geo &geo, int gx0, int gy0)
+  build_maps(TileMaps<P, R, S> &m, const Geo &geo, int gx0, int gy0)
   {
-    using T = Tile<P>;
+    using T = Tile<P, S>;
     const Grid &g = geo.g;
     for (int t = threadIdx.x; t < T::FX; t += blockDim.x)
       {

@@ -6,6 +6,8 @@
 #include "geometry.h"
 #include "operators.cuh"
 #include "stream_pair.cuh"
+#include "contraction_study.cuh"
+#include "quad.cuh"
 
 #include <cuda_runtime.h>
 
@@ -15,8 +17,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <array>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <memory>
 #include <string>
 #include <utility>
@@ -79,6 +83,14 @@ struct lbfem_gpu_ctx
   int64_t graph_epoch = 0; // counts the invalidations of the step graphs (batch graphs embed them)
   cudaStream_t cap = nullptr;     // captures the loop bodies
   DevStats *d_stats = nullptr, *h_stats = nullptr;
+  // the tuned tile shape of the FP32 streaming kernel (tune_pair) and the times it was chosen by
+  int pair_shape = 0;
+  bool pair_tuned = false;
+  float tune_ms[2] = {0.f, 0.f};
+  // general quadrilaterals (lbfem_mesh_desc::vertex_xy): per cell and Gauss point J^-1 and
+  // JxW, and the per-node mass diagonals (inverse Jacobi, lumped and its inverse)
+  bool distorted = false;
+  double *d_qgeo = nullptr, *d_qijac = nullptr, *d_qlump = nullptr, *d_qilump = nullptr;
   // one y-strip of a decomposed mesh (lbfem_gpu_set_strip): ghost rows and the caller's collectives
   bool strip = false;
   lbfem_strip_desc sd{};
@@ -139,6 +151,8 @@ namespace
     g.rowx = ctx->d_rowx;
     g.rowy = ctx->d_rowy;
     g.wall = ctx->d_wall;
+    g.lump2 = ctx->d_qlump;
+    g.ijac2 = ctx->d_qijac;
     g.wall_u = ctx->d_wall_u;
     return g;
   }
@@ -202,6 +216,10 @@ namespace
         (st = set_smem(ctx, k_advection<P, ADV_LEELIN_FUSED, double>, advection_smem<P, ADV_LEELIN_FUSED, double>())) ||
         (st = set_smem(ctx, k_stream_pair<P, PAIR_LEELIN>, pair_smem<P, PAIR_LEELIN>())) ||
         (st = set_smem(ctx, k_stream_pair<P, PAIR_BARDOW>, pair_smem<P, PAIR_BARDOW>())) ||
+        (st = set_smem(ctx, k_stream_pair<P, PAIR_LEELIN, TileShapeAlt<P>>,
+                       pair_smem<P, PAIR_LEELIN, TileShapeAlt<P>>())) ||
+        (st = set_smem(ctx, k_stream_pair<P, PAIR_BARDOW, TileShapeAlt<P>>,
+                       pair_smem<P, PAIR_BARDOW, TileShapeAlt<P>>())) ||
         (st = set_smem(ctx, k_mass_vmult<P>, cg_smem<P, double>(0))) ||
         (st = set_smem(ctx, k_cg_start<P, double, double, double>, cg_smem<P, double>(1))) ||
         (st = set_smem(ctx, k_cg_p<P, double>, cg_smem<P, double>(0))) ||
@@ -244,6 +262,15 @@ namespace
         ac.ey[al] = e[2 * (al + 1) + 1];
       }
     ac.omega = omega;
+    static const double w[5] = {0., 1. / 9., 1. / 36., 1. / 9., 1. / 36.};
+    for (int pr = 0; pr < 4; ++pr)
+      {
+        const double exd = ac.ex[pr], eyd = ac.ey[pr];
+        const double v[8] = {a, b, exd, c * exd * exd, eyd, -2.0 * c * exd * eyd, c * eyd * eyd, c * exd * eyd};
+        for (int k = 0; k < 8; ++k)
+          ac.pk[pr][k] = float(v[k]);
+        ac.pw[pr] = float(w[pr + 1]);
+      }
     return ac;
   }
 
@@ -254,12 +281,23 @@ namespace
     return e;
   }
 
+  int quad_advection(lbfem_gpu_ctx *ctx, const double *f, const double *feq, double *rhs, const AdvCoef &ac);
+  int quad_solve(lbfem_gpu_ctx *ctx, const double *b, double *x, int nsys, int64_t *its);
+  int quad_vmult(lbfem_gpu_ctx *ctx, const double *x, double *y, int nsys);
+
   // ds: the step counters of a step (its kernel does nothing after a failure), null otherwise.
   template <typename R>
   int
   launch_advection(lbfem_gpu_ctx *ctx, int mode, const R *f, const R *feq, R *fout, R *rhs, const AdvCoef &ac,
                    const DevStats *ds = nullptr)
   {
+    if (ctx->distorted)
+      {
+        if constexpr (sizeof(R) == sizeof(double))
+          if (mode == ADV_TG || mode == ADV_LEELIN_FEQ)
+            return quad_advection(ctx, f, mode == ADV_LEELIN_FEQ ? feq : nullptr, rhs, ac);
+        return fail(ctx, LBFEM_ERR_UNSUPPORTED, "general quadrilaterals: the advection of given populations only");
+      }
     const Geo geo = geo_of(ctx);
     return with_degree(ctx->P, [&](auto PP) -> int {
       constexpr int P = decltype(PP)::value;
@@ -289,24 +327,111 @@ namespace
     });
   }
 
-  // The FP32 streaming kernel of the mixed-precision step (pairs of opposite populations).
+  // The FP32 streaming kernel of the mixed-precision step (pairs of opposite
+  // populations), in tile shape `shape` (0: TileShape, 1: TileShapeAlt; -1: the
+  // context's tuned choice).
   int
   launch_pair(lbfem_gpu_ctx *ctx, int mode, const float *d, float *dout, float *rhs, const AdvCoef &ac,
-              const DevStats *ds = nullptr)
+              const DevStats *ds = nullptr, int shape = -1)
   {
     const Geo geo = geo_of(ctx);
+    if (shape < 0)
+      shape = ctx->pair_shape;
     return with_degree(ctx->P, [&](auto PP) -> int {
       constexpr int P = decltype(PP)::value;
-      const dim3 grid = tile_grid<P>(ctx->grid);
-      if (mode == PAIR_BARDOW)
-        k_stream_pair<P, PAIR_BARDOW><<<grid, THREADS, pair_smem<P, PAIR_BARDOW>(), ctx->stream>>>(geo, ds, d, dout, rhs,
-                                                                                                 ac);
+      auto go = [&](auto SS) {
+        using S = decltype(SS);
+        using T = Tile<P, S>;
+        const dim3 grid((ctx->grid.nfx + T::TX - 1) / T::TX, (ctx->grid.nfy + T::TY - 1) / T::TY);
+        if (mode == PAIR_BARDOW)
+          k_stream_pair<P, PAIR_BARDOW, S><<<grid, THREADS, pair_smem<P, PAIR_BARDOW, S>(), ctx->stream>>>(
+            geo, ds, d, dout, rhs, ac);
+        else
+          k_stream_pair<P, PAIR_LEELIN, S><<<grid, THREADS, pair_smem<P, PAIR_LEELIN, S>(), ctx->stream>>>(
+            geo, ds, d, dout, rhs, ac);
+      };
+      if (shape == 1)
+        go(TileShapeAlt<P>{});
       else
-        k_stream_pair<P, PAIR_LEELIN><<<grid, THREADS, pair_smem<P, PAIR_LEELIN>(), ctx->stream>>>(geo, ds, d, dout, rhs,
-                                                                                                 ac);
+        go(TileShape<P>{});
       LAUNCHED();
       return LBFEM_OK;
     });
+  }
+
+  // The run-time choice of the FP32 streaming kernel's tile (cells per CTA and
+  // per x / y segment): each compiled shape is timed on the context's own
+  // buffers (CUDA events, one warm-up and five timed launches) before the first
+  // step records its graph, and the fastest is kept. The choice is cached per
+  // (device, degree, scheme, grid) for the other contexts of the process.
+  // LBFEM_TUNE=0 keeps the default shape, LBFEM_TUNE=alt the alternative (for
+  // tests). Every shape gives bitwise the same
+  // results (the per-node arithmetic does not depend on the tile).
+  struct TuneKey
+  {
+    int dev, P, mode, nfx, nfy;
+    bool
+    operator<(const TuneKey &o) const
+    {
+      return std::tie(dev, P, mode, nfx, nfy) < std::tie(o.dev, o.P, o.mode, o.nfx, o.nfy);
+    }
+  };
+  std::mutex tune_mutex;
+  std::map<TuneKey, std::pair<int, std::array<float, 2>>> tune_cache;
+
+  int
+  tune_pair(lbfem_gpu_ctx *ctx)
+  {
+    if (!ctx->mixed || ctx->pair_tuned || ctx->distorted)
+      return LBFEM_OK;
+    const char *env = std::getenv("LBFEM_TUNE");
+    if (env && (env[0] == '0' || std::strcmp(env, "alt") == 0))
+      {
+        // a fixed shape: the default ("0") or the alternative ("alt")
+        ctx->pair_shape = env[0] == '0' ? 0 : 1;
+        ctx->pair_tuned = true;
+        return LBFEM_OK;
+      }
+    const bool bardow = ctx->prm.scheme == LBFEM_SCHEME_BARDOW;
+    const TuneKey key{ctx->device, ctx->P, bardow ? 1 : 0, ctx->grid.nfx, ctx->grid.nfy};
+    {
+      std::lock_guard<std::mutex> lock(tune_mutex);
+      const auto it = tune_cache.find(key);
+      if (it != tune_cache.end())
+        {
+          ctx->pair_shape = it->second.first;
+          ctx->tune_ms[0] = it->second.second[0];
+          ctx->tune_ms[1] = it->second.second[1];
+          ctx->pair_tuned = true;
+          return LBFEM_OK;
+        }
+    }
+    const double dt = ctx->dt, lam = ctx->lambda, b = -0.5 * dt * dt / lam;
+    const AdvCoef ac = bardow ? adv_coef(-dt, 0., -0.5 * dt * dt, d2q9_e(), dt / (lam + 0.5 * dt))
+                              : adv_coef(-dt - b, b, -0.5 * dt * dt, d2q9_e(), 0.);
+    float *d = ctx->d_fs[ctx->cur], *g = bardow ? ctx->d_fs[1 - ctx->cur] : nullptr;
+    float ms[2] = {0.f, 0.f};
+    int st;
+    for (int shape = 0; shape < 2; ++shape)
+      {
+        if ((st = launch_pair(ctx, bardow ? PAIR_BARDOW : PAIR_LEELIN, d, g, ctx->d_rhs_s, ac, nullptr, shape)))
+          return st;
+        CK(cudaEventRecord(ctx->ev[14], ctx->stream));
+        for (int k = 0; k < 5; ++k)
+          if ((st = launch_pair(ctx, bardow ? PAIR_BARDOW : PAIR_LEELIN, d, g, ctx->d_rhs_s, ac, nullptr, shape)))
+            return st;
+        CK(cudaEventRecord(ctx->ev[15], ctx->stream));
+        CK(cudaEventSynchronize(ctx->ev[15]));
+        CK(cudaEventElapsedTime(&ms[shape], ctx->ev[14], ctx->ev[15]));
+        ms[shape] /= 5.f;
+      }
+    ctx->pair_shape = ms[1] < ms[0] ? 1 : 0;
+    ctx->tune_ms[0] = ms[0];
+    ctx->tune_ms[1] = ms[1];
+    ctx->pair_tuned = true;
+    std::lock_guard<std::mutex> lock(tune_mutex);
+    tune_cache[key] = {ctx->pair_shape, {ms[0], ms[1]}};
+    return LBFEM_OK;
   }
 
   template <typename R>
@@ -792,6 +917,17 @@ namespace
   mass_solve_dev(lbfem_gpu_ctx *ctx, const double *b, double *x_new, bool tg3, const StreamCoef &sc, int64_t *its)
   {
     const int nsys = 1;
+    if (ctx->distorted)
+      {
+        if (tg3)
+          return fail(ctx, LBFEM_ERR_UNSUPPORTED, "general quadrilaterals: no TG3 matrix");
+        int64_t q = 0;
+        const int st = quad_solve(ctx, b, x_new, nsys, &q);
+        if (its)
+          *its = q;
+        ctx->cg_its += q;
+        return st;
+      }
     if (ctx->prm.mass == LBFEM_MASS_LUMPED)
       {
         k_lumped<double, double><<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo_of(ctx), b, x_new,
@@ -1059,6 +1195,243 @@ namespace
     return strip_exchange(ctx, ctx->d_x[ctx->x_cur], NM, sizeof(double));
   }
 
+  // ------------------------------------------------ general quadrilaterals
+  // FP64, host-driven: cell-coloured kernels (quad.cuh) and the CG of the
+  // oracle's order (deal.II SolverCG), one system at a time.
+  template <typename F>
+  int
+  quad_colours(const lbfem_gpu_ctx *ctx, F &&launch)
+  {
+    const Grid &g = ctx->grid;
+    const int nx = (g.px && (g.ncx & 1)) ? 3 : 2, ny = (g.py && (g.ncy & 1)) ? 3 : 2;
+    for (int cy = 0; cy < ny; ++cy)
+      for (int cx = 0; cx < nx; ++cx)
+        {
+          QuadGeo qg{ctx->d_qgeo, cx, cy, g.ncx, g.ncy, nx == 3, ny == 3};
+          int st = launch(qg);
+          if (st)
+            return st;
+        }
+    return LBFEM_OK;
+  }
+
+  long long
+  quad_threads(const lbfem_gpu_ctx *ctx, int per_cell)
+  {
+    const Grid &g = ctx->grid;
+    return (long long)((g.ncx + 1) / 2 + 1) * ((g.ncy + 1) / 2 + 1) * per_cell;
+  }
+
+  // rhs (8 blocks) <- the advection of f (and feq) on the mapped cells
+  int
+  quad_advection(lbfem_gpu_ctx *ctx, const double *f, const double *feq, double *rhs, const AdvCoef &ac)
+  {
+    CK(cudaMemsetAsync(rhs, 0, sizeof(double) * NM * ctx->grid.N, ctx->stream));
+    const Geo geo = geo_of(ctx);
+    const int nb = int((quad_threads(ctx, NM) + 127) / 128);
+    return with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      return quad_colours(ctx, [&](const QuadGeo &qg) -> int {
+        k_quad_advection<P><<<nb, 128, 0, ctx->stream>>>(geo, qg, f, feq, rhs, ac);
+        LAUNCHED();
+        return LBFEM_OK;
+      });
+    });
+  }
+
+  // y <- M x for nsys systems (constrained rows the identity)
+  int
+  quad_vmult(lbfem_gpu_ctx *ctx, const double *x, double *y, int nsys)
+  {
+    CK(cudaMemsetAsync(y, 0, sizeof(double) * nsys * ctx->grid.N, ctx->stream));
+    const Geo geo = geo_of(ctx);
+    const int nb = int((quad_threads(ctx, nsys) + 127) / 128);
+    int st = with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      return quad_colours(ctx, [&](const QuadGeo &qg) -> int {
+        k_quad_mass<P><<<nb, 128, 0, ctx->stream>>>(geo, qg, x, y, nsys);
+        LAUNCHED();
+        return LBFEM_OK;
+      });
+    });
+    if (st)
+      return st;
+    k_quad_images<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(geo, x, y, nsys);
+    LAUNCHED();
+    return LBFEM_OK;
+  }
+
+  int
+  quad_dot(lbfem_gpu_ctx *ctx, const double *a, const double *b, double *out)
+  {
+    const int nb = n_pointwise_blocks(ctx->grid.N);
+    k_quad_dot<<<nb, THREADS, 0, ctx->stream>>>(geo_of(ctx), a, b, ctx->d_partials);
+    LAUNCHED();
+    k_reduce_partials<<<1, 256, 0, ctx->stream>>>(ctx->d_partials, nb, ctx->d_sums);
+    LAUNCHED();
+    CK(cudaMemcpyAsync(out, ctx->d_sums, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return LBFEM_OK;
+  }
+
+  // y = a x + b y (mode 0) or y = x * d (mode 1), one system
+  int
+  quad_axpby(lbfem_gpu_ctx *ctx, double a, const double *x, double b, double *y, const double *d = nullptr)
+  {
+    k_quad_axpby<<<n_pointwise_blocks(ctx->grid.N), THREADS, 0, ctx->stream>>>(ctx->grid.N, a, x, b, y, d,
+                                                                              d ? 1 : 0);
+    LAUNCHED();
+    return LBFEM_OK;
+  }
+
+  // x <- M^{-1} b, Jacobi-PCG from the start in x, in deal.II SolverCG's order of
+  // updates (mass.h:204-211), as the oracle; work vectors r, z, p, v of N values.
+  int
+  quad_cg(lbfem_gpu_ctx *ctx, const double *b, double *x, int64_t *its)
+  {
+    const long long N = ctx->grid.N;
+    double *r = ctx->d_r, *z = ctx->d_r + N, *p = ctx->d_r + 2 * N, *v = ctx->d_r + 3 * N;
+    const double tol0 = ctx->prm.cg_tolerance;
+    int st;
+    double bb = 0, res = 0, rz = 0;
+    *its = 0;
+    if ((st = quad_dot(ctx, b, b, &bb)))
+      return st;
+    const double tol = tol0 * std::sqrt(bb);
+    if (bb == 0.)
+      {
+        // an exactly zero right-hand side: x = 0 (deal.II would iterate toward a tolerance of 0)
+        CK(cudaMemsetAsync(x, 0, sizeof(double) * N, ctx->stream));
+        return LBFEM_OK;
+      }
+    // r = b - A x (A 0 = 0 exactly, so a zero start gives r = b as deal.II's)
+    if ((st = quad_vmult(ctx, x, v, 1)))
+      return st;
+    CK(cudaMemcpyAsync(r, b, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+    if ((st = quad_axpby(ctx, -1., v, 1., r)) || (st = quad_dot(ctx, r, r, &res)))
+      return st;
+    res = std::sqrt(res);
+    if (std::isnan(res))
+      return fail(ctx, LBFEM_ERR_NONFINITE, "CG: non-finite residual");
+    if (res <= tol)
+      return LBFEM_OK;
+    for (int it = 1;; ++it)
+      {
+        if ((st = quad_axpby(ctx, 0., r, 0., z, ctx->d_qijac)))
+          return st;
+        const double rz_prev = rz;
+        if ((st = quad_dot(ctx, r, z, &rz)))
+          return st;
+        if (it > 1)
+          st = quad_axpby(ctx, 1., z, rz / rz_prev, p);
+        else
+          st = cudaMemcpyAsync(p, z, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream) == cudaSuccess
+                 ? LBFEM_OK
+                 : fail(ctx, LBFEM_ERR_CUDA, "CG: copy failed");
+        double pAp = 0;
+        if (st || (st = quad_vmult(ctx, p, v, 1)) || (st = quad_dot(ctx, p, v, &pAp)))
+          return st;
+        const double alpha = rz / pAp;
+        if ((st = quad_axpby(ctx, alpha, p, 1., x)) || (st = quad_axpby(ctx, -alpha, v, 1., r)) ||
+            (st = quad_dot(ctx, r, r, &res)))
+          return st;
+        res = std::sqrt(res);
+        *its = it;
+        if (std::isnan(res))
+          return fail(ctx, LBFEM_ERR_NONFINITE, "CG: non-finite residual");
+        if (res <= tol)
+          return LBFEM_OK;
+        if (it >= ctx->prm.cg_max_iterations)
+          return fail(ctx, LBFEM_ERR_NO_CONVERGENCE, "CG: iteration cap %d reached", ctx->prm.cg_max_iterations);
+      }
+  }
+
+  // The mass solve of nsys systems on the mapped cells: lumped, iterated lumping, or CG
+  // per system from the start in x.
+  int
+  quad_solve(lbfem_gpu_ctx *ctx, const double *b, double *x, int nsys, int64_t *its)
+  {
+    const long long N = ctx->grid.N;
+    int st;
+    *its = 0;
+    if (ctx->prm.mass != LBFEM_MASS_CG)
+      {
+        for (int s = 0; s < nsys; ++s)
+          if ((st = quad_axpby(ctx, 0., b + s * N, 0., x + s * N, ctx->d_qilump)))
+            return st;
+        if (ctx->prm.mass == LBFEM_MASS_RICHARDSON)
+          for (int k = 0; k < ctx->prm.richardson; ++k)
+            for (int s = 0; s < nsys; ++s)
+              {
+                // x += M_L^{-1} (b - M x)
+                double *v = ctx->d_v, *w = ctx->d_v + N;
+                if ((st = quad_vmult(ctx, x + s * N, v, 1)))
+                  return st;
+                CK(cudaMemcpyAsync(w, b + s * N, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+                if ((st = quad_axpby(ctx, -1., v, 1., w)) || (st = quad_axpby(ctx, 0., w, 0., v, ctx->d_qilump)) ||
+                    (st = quad_axpby(ctx, 1., v, 1., x + s * N)))
+                  return st;
+              }
+        return LBFEM_OK;
+      }
+    for (int s = 0; s < nsys; ++s)
+      {
+        int64_t it = 0;
+        if ((st = quad_cg(ctx, b + s * N, x + s * N, &it)))
+          return st;
+        *its += it;
+      }
+    return LBFEM_OK;
+  }
+
+  // Scheme::step on the mapped cells (LeeLin schemes.h:92-98, Bardow 118-124), FP64 TG2.
+  int
+  step_quad(lbfem_gpu_ctx *ctx, int64_t *its)
+  {
+    const Geo geo = geo_of(ctx);
+    const long long N = ctx->grid.N;
+    const int nb = n_pointwise_blocks(N);
+    const double dt = ctx->dt, lam = ctx->lambda;
+    const bool bardow = ctx->prm.scheme == LBFEM_SCHEME_BARDOW;
+    double *f = ctx->d_f[ctx->cur];
+    int st;
+    if (bardow)
+      {
+        k_collide<<<nb, THREADS, 0, ctx->stream>>>(geo, f, dt / (lam + 0.5 * dt));
+        LAUNCHED();
+        st = quad_advection(ctx, f, nullptr, ctx->d_rhs, adv_coef(-dt, 0., -0.5 * dt * dt, d2q9_e(), 0.));
+      }
+    else
+      {
+        k_equilibrium<<<nb, THREADS, 0, ctx->stream>>>(geo, f, ctx->d_feq);
+        LAUNCHED();
+        const double b = -0.5 * dt * dt / lam;
+        st = quad_advection(ctx, f, ctx->d_feq, ctx->d_rhs, adv_coef(-dt - b, b, -0.5 * dt * dt, d2q9_e(), 0.));
+      }
+    if (st)
+      return st;
+    // the CG start 2 x^n - x^{n-1} (TaylorGalerkin::increment, streaming.h:76-80)
+    double *xn = ctx->d_x[ctx->x_new], *xc = ctx->d_x[ctx->x_cur], *xp = ctx->d_x[ctx->x_prev];
+    if (ctx->prm.mass == LBFEM_MASS_CG)
+      {
+        CK(cudaMemcpyAsync(xn, xp, sizeof(double) * NM * N, cudaMemcpyDeviceToDevice, ctx->stream));
+        k_quad_axpby<<<nb, THREADS, 0, ctx->stream>>>(NM * N, 2., xc, -1., xn, nullptr, 0);
+        LAUNCHED();
+      }
+    if ((st = quad_solve(ctx, ctx->d_rhs, xn, NM, its)))
+      return st;
+    const int old_prev = ctx->x_prev;
+    ctx->x_prev = ctx->x_cur;
+    ctx->x_cur = ctx->x_new;
+    ctx->x_new = old_prev;
+    if (bardow)
+      k_add_increment<double><<<nb, THREADS, 0, ctx->stream>>>(geo, nullptr, f, xn, 0);
+    else
+      k_predictor_corrector<<<nb, THREADS, 0, ctx->stream>>>(geo, nullptr, f, ctx->d_feq, xn, dt / lam);
+    LAUNCHED();
+    return LBFEM_OK;
+  }
+
   // One host-driven step: the solver loops read their state back after every
   // iteration (the path of LBFEM_TRACE).
   int
@@ -1067,6 +1440,14 @@ namespace
     int st;
     if (its)
       *its = 0;
+    if (ctx->distorted)
+      {
+        int64_t q = 0;
+        st = step_quad(ctx, &q);
+        if (its)
+          *its = q;
+        return st;
+      }
     for (int s = 0; s < n_sweeps(ctx); ++s)
       {
         if ((st = step_front(ctx, s)))
@@ -1589,7 +1970,7 @@ lbfem_gpu_destroy(lbfem_gpu_ctx *ctx)
                   ctx->d_x[1], ctx->d_x[2], ctx->d_r, ctx->d_p[0], ctx->d_p[1], ctx->d_v, ctx->d_feq, ctx->d_stage,
                   ctx->d_partials, ctx->d_sums, ctx->d_cg, ctx->d_fs[0], ctx->d_fs[1], ctx->d_rhs_s,
                   ctx->d_x_s[0], ctx->d_x_s[1], ctx->d_x_s[2], ctx->d_r_s, ctx->d_p_s[0], ctx->d_p_s[1],
-                  ctx->d_winx, ctx->d_winy};
+                  ctx->d_winx, ctx->d_winy, ctx->d_qgeo, ctx->d_qijac, ctx->d_qlump, ctx->d_qilump};
   for (void *b : bufs)
     if (b)
       cudaFree(b);
@@ -1734,7 +2115,47 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
           for (int c = 0; c <= MAXPD; ++c)
             ref2[q][o][a][c] = make_float2(reff[q][o][a][c], reff[q][o][a][c]);
     CK(cudaMemcpyToSymbol(c_ref2, ref2, sizeof ref2));
+    // the 1-D basis at the Gauss points, for the cell kernels of general quadrilaterals
+    static double gs[MAXPD][MAXPD + 1][MAXPD + 1], gd[MAXPD][MAXPD + 1][MAXPD + 1];
+    std::memset(gs, 0, sizeof gs);
+    std::memset(gd, 0, sizeof gd);
+    for (int q = 1; q <= MAXPD; ++q)
+      {
+        const Basis1D b(q);
+        for (int k = 0; k <= q; ++k)
+          for (int a = 0; a <= q; ++a)
+            {
+              gs[q - 1][k][a] = b.gS[k][a];
+              gd[q - 1][k][a] = b.gD[k][a];
+            }
+      }
+    CK(cudaMemcpyToSymbol(c_gS, gs, sizeof gs));
+    CK(cudaMemcpyToSymbol(c_gD, gd, sizeof gd));
   }
+  if (m->vertex_xy)
+    {
+      // general quadrilaterals: FP64, TG2, no walls (the reference's --distort is a Taylor-Green option)
+      if (prm->precision != LBFEM_PRECISION_FP64 || prm->streaming != LBFEM_STREAMING_TG2 || m->n_walls > 0 ||
+          !m->periodic_x || !m->periodic_y)
+        return fail(ctx, LBFEM_ERR_UNSUPPORTED,
+                    "general quadrilaterals: FP64, TG2, periodic in x and y (no boundary faces) only");
+      ctx->distorted = true;
+      const std::vector<double> qg = quad_geometry(*ctx->basis, m->vertex_xy, m->n_cells_x, m->n_cells_y);
+      std::vector<double> jac, lump;
+      quad_diagonals(*ctx->basis, qg, m->n_cells_x, m->n_cells_y, m->periodic_x != 0, m->periodic_y != 0, jac, lump);
+      for (const double v : qg)
+        if (!std::isfinite(v))
+          return fail(ctx, LBFEM_ERR_ARG, "general quadrilaterals: a degenerate cell");
+      std::vector<double> ijac(jac.size()), ilump(lump.size());
+      for (size_t k = 0; k < jac.size(); ++k)
+        {
+          ijac[k] = 1. / jac[k];
+          ilump[k] = 1. / lump[k];
+        }
+      if ((st = put(&ctx->d_qgeo, qg)) || (st = put(&ctx->d_qijac, ijac)) || (st = put(&ctx->d_qlump, lump)) ||
+          (st = put(&ctx->d_qilump, ilump)))
+        return st;
+    }
 
   // numbering: structured node -> caller DoF, and its inverse for the wall list
   std::vector<long long> node_of_dof;
@@ -2012,9 +2433,11 @@ lbfem_gpu_step(lbfem_gpu_ctx *ctx, int32_t n_steps)
     return fail(ctx, LBFEM_ERR_ARG, "step: negative count");
   if (!ctx->have_ts)
     return fail(ctx, LBFEM_ERR_STATE, "step needs the time step");
+  if ((st = tune_pair(ctx)))
+    return st;
   const int64_t launches0 = ctx->launches;
   int64_t its_total = 0;
-  if (ctx->trace || ctx->strip)
+  if (ctx->trace || ctx->strip || ctx->distorted)
     {
       // host-driven steps (the solver rounds print their residuals)
       for (int s = 0; s < n_steps; ++s)
@@ -2104,12 +2527,16 @@ lbfem_gpu_advection_resident(lbfem_gpu_ctx *ctx)
     return st;
   if (!ctx->have_ts)
     return fail(ctx, LBFEM_ERR_STATE, "advection_resident needs the time step");
+  if (ctx->distorted)
+    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "advection_resident: not on general quadrilaterals");
   const double dt = ctx->dt, lam = ctx->lambda;
   const double b = -0.5 * dt * dt / lam;
   const bool bardow = ctx->prm.scheme == LBFEM_SCHEME_BARDOW;
   const AdvCoef ac = bardow ? adv_coef(-dt, 0., -0.5 * dt * dt, d2q9_e(), dt / (lam + 0.5 * dt))
                             : adv_coef(-dt - b, b, -0.5 * dt * dt, d2q9_e(), 0.);
   const int mode = bardow ? ADV_TG_COLLIDE : ADV_LEELIN_FUSED;
+  if ((st = tune_pair(ctx)))
+    return st;
   if (ctx->mixed)
     return launch_pair(ctx, bardow ? PAIR_BARDOW : PAIR_LEELIN, ctx->d_fs[ctx->cur],
                        bardow ? ctx->d_fs[1 - ctx->cur] : nullptr, ctx->d_rhs_s, ac);
@@ -2177,8 +2604,8 @@ lbfem_gpu_stream_function(lbfem_gpu_ctx *ctx, const double *velocity, double *ps
     return st;
   if (!velocity || !psi)
     return fail(ctx, LBFEM_ERR_ARG, "stream_function: null buffer");
-  if (ctx->strip)
-    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "stream_function: not on a strip (gather the velocity on one context)");
+  if (ctx->strip || ctx->distorted)
+    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "stream_function: not on a strip or on general quadrilaterals");
   const long long N = ctx->grid.N;
   double *vel = ctx->d_x[ctx->x_new], *b = ctx->d_rhs, *x = ctx->d_rhs + N; // scratch between steps
   if ((st = upload(ctx, velocity, vel, 2)))
@@ -2217,6 +2644,12 @@ lbfem_gpu_mass_vmult(lbfem_gpu_ctx *ctx, double *y, const double *x)
     return fail(ctx, LBFEM_ERR_ARG, "mass_vmult: null buffer");
   if ((st = upload(ctx, x, ctx->d_r, 1)))
     return st;
+  if (ctx->distorted)
+    {
+      if ((st = quad_vmult(ctx, ctx->d_r, ctx->d_v, 1)))
+        return st;
+      return download(ctx, ctx->d_v, y, 1);
+    }
   const Geo geo = geo_of(ctx);
   st = with_degree(ctx->P, [&](auto PP) -> int {
     constexpr int P = decltype(PP)::value;
@@ -2498,6 +2931,17 @@ lbfem_gpu_step_stream(lbfem_gpu_ctx *ctx, int32_t n_steps, void *stream)
 }
 
 int
+lbfem_gpu_tuning(const lbfem_gpu_ctx *ctx, int32_t *shape, float *ms)
+{
+  if (!ctx || !shape || !ms)
+    return LBFEM_ERR_ARG;
+  *shape = ctx->pair_tuned ? ctx->pair_shape : -1;
+  ms[0] = ctx->tune_ms[0];
+  ms[1] = ctx->tune_ms[1];
+  return LBFEM_OK;
+}
+
+int
 lbfem_gpu_strip_buffer_bytes(const lbfem_gpu_ctx *ctx, int64_t *bytes)
 {
   if (!ctx || !bytes)
@@ -2516,8 +2960,8 @@ lbfem_gpu_set_strip(lbfem_gpu_ctx *ctx, const lbfem_strip_desc *sd)
   if (!sd || !sd->comm || !sd->sums)
     return fail(ctx, LBFEM_ERR_ARG, "set_strip: the collective and the sums buffer are required");
   const Grid &g = ctx->grid;
-  if (g.py)
-    return fail(ctx, LBFEM_ERR_ARG, "set_strip: the local mesh of a strip is not periodic in y");
+  if (g.py || ctx->distorted)
+    return fail(ctx, LBFEM_ERR_ARG, "set_strip: the local mesh of a strip is an axis-parallel mesh, not periodic in y");
   if ((sd->ghost_below != 0 && sd->ghost_below != ctx->P) || (sd->ghost_above != 0 && sd->ghost_above != 1))
     return fail(ctx, LBFEM_ERR_ARG, "set_strip: ghost rows are `degree` below and 1 above, or none");
   if ((sd->ghost_below && (!sd->send_below || !sd->recv_below)) ||
@@ -2803,7 +3247,7 @@ lbfem_gpu_batch_create(lbfem_gpu_ctx *const *ctxs, int32_t n, lbfem_gpu_batch **
     {
       if (!ctxs[k])
         return LBFEM_ERR_ARG;
-      if (ctxs[k]->device != ctxs[0]->device)
+      if (ctxs[k]->device != ctxs[0]->device || ctxs[k]->distorted || ctxs[k]->strip)
         return LBFEM_ERR_UNSUPPORTED;
       for (int j = 0; j < k; ++j)
         if (ctxs[j] == ctxs[k])
@@ -2882,6 +3326,8 @@ lbfem_gpu_batch_step(lbfem_gpu_batch *b, int32_t n_steps)
       lbfem_gpu_ctx *c = b->ctxs[k];
       if (!c->have_ts)
         return batch_fail(b, LBFEM_ERR_STATE, "instance %zu: step needs the time step", k);
+      if (tune_pair(c) != LBFEM_OK)
+        return batch_fail(b, LBFEM_ERR_CUDA, "instance %zu: %s", k, c->err.c_str());
       // the instance's own queued work first, then its counters
       BCK(cudaStreamSynchronize(c->stream));
       BCK(cudaMemcpy(&b->h_stats[k], c->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost));
@@ -2997,8 +3443,8 @@ lbfem_gpu_mass_solve_noalloc(lbfem_gpu_ctx *ctx, double *x, const double *r)
     return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: needs the structured DoF numbering");
   if (ctx->prm.mass != LBFEM_MASS_CG)
     return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: the consistent mass (CG) only");
-  if (ctx->strip)
-    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: not on a strip");
+  if (ctx->strip || ctx->distorted)
+    return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: not on a strip or on general quadrilaterals");
   if (ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES)
     return fail(ctx, LBFEM_ERR_UNSUPPORTED, "mass_solve_noalloc: device ordinal %d too large", ctx->device);
   double *base = nullptr; // check_ctx made ctx's device current
@@ -3019,4 +3465,88 @@ lbfem_gpu_mass_solve_noalloc(lbfem_gpu_ctx *ctx, double *x, const double *r)
     return solve_st;
   CK(cudaStreamSynchronize(ctx->stream));
   return LBFEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The x-pass contraction on CUDA cores and on tensor cores (a measurement for
+// the choice between the two; no step uses it).
+namespace
+{
+  template <int P, typename R, bool TC>
+  int
+  run_study(int rows, int cells, int reps, float *ms, double *checksum)
+  {
+    using namespace lbfem_gpu::study;
+    const long long n = (long long)rows * (P * cells + 1);
+    R *buf = nullptr;
+    if (cudaMalloc(&buf, sizeof(R) * 4 * n) != cudaSuccess)
+      return LBFEM_ERR_CUDA;
+    R *u = buf, *h = buf + n, *y1 = buf + 2 * n, *y2 = buf + 3 * n;
+    Mats<R> m{};
+    const Basis1D b(P);
+    for (int a = 0; a <= P; ++a)
+      for (int c = 0; c <= P; ++c)
+        {
+          m.M[a][c] = R(b.Mh[a][c]);
+          m.C[a][c] = R(b.Ch[a][c]);
+          m.K[a][c] = R(b.Kh[a][c]);
+        }
+    int st = LBFEM_OK;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const dim3 grid((cells + cells_of<R>() - 1) / cells_of<R>(), (rows + ROWS - 1) / ROWS);
+    auto kernel = k_xpass_study<P, R, TC>;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
+        cudaMemset(y1, 0, sizeof(R) * 2 * n) != cudaSuccess ||
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem<P, R>())) != cudaSuccess)
+      st = LBFEM_ERR_CUDA;
+    if (!st)
+      {
+        k_study_fill<R><<<148 * 8, 256>>>(u, h, n);
+        kernel<<<grid, NT, smem<P, R>()>>>(u, h, y1, y2, rows, cells, m); // warm-up
+        cudaEventRecord(e0);
+        for (int k = 0; k < reps; ++k)
+          kernel<<<grid, NT, smem<P, R>()>>>(u, h, y1, y2, rows, cells, m);
+        cudaEventRecord(e1);
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+          st = LBFEM_ERR_CUDA;
+      }
+    if (!st)
+      {
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        *ms = t / float(reps > 0 ? reps : 1);
+        std::vector<R> hy(2 * n);
+        if (cudaMemcpy(hy.data(), y1, sizeof(R) * 2 * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+          st = LBFEM_ERR_CUDA;
+        double sum = 0;
+        for (long long i = 0; i < 2 * n; ++i)
+          sum += std::fabs(double(hy[i]));
+        *checksum = sum;
+      }
+    if (e0)
+      cudaEventDestroy(e0);
+    if (e1)
+      cudaEventDestroy(e1);
+    cudaFree(buf);
+    return st;
+  }
+} // namespace
+
+extern "C" int
+lbfem_gpu_contraction_study(int32_t device, int32_t degree, int32_t fp64, int32_t tensor, int32_t rows, int32_t cells,
+                            int32_t reps, float *ms, double *checksum)
+{
+  if (degree < 2 || degree > 3 || rows < 1 || cells < 1 || reps < 1 || !ms || !checksum)
+    return LBFEM_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess)
+    return LBFEM_ERR_CUDA;
+  auto pick = [&](auto PP) -> int {
+    constexpr int P = decltype(PP)::value;
+    if (fp64)
+      return tensor ? run_study<P, double, true>(rows, cells, reps, ms, checksum)
+                    : run_study<P, double, false>(rows, cells, reps, ms, checksum);
+    return tensor ? run_study<P, float, true>(rows, cells, reps, ms, checksum)
+                  : run_study<P, float, false>(rows, cells, reps, ms, checksum);
+  };
+  return degree == 2 ? pick(std::integral_constant<int, 2>()) : pick(std::integral_constant<int, 3>());
 }

@@ -301,7 +301,10 @@ namespace lbfem_gpu
     LBFEM_GRID_STRIDE(idx, g.N)
     {
       const int j = int(idx / g.nfx), i = int(idx - (long long)j * g.nfx);
-      w[idx] = is_image(i, j, g) ? 1.0 : which == 0 ? geo.lumpx[i] * geo.lumpy[j] : geo.diagx[i] * geo.diagy[j];
+      if (geo.lump2)
+        w[idx] = which == 0 ? geo.lump2[idx] : 1.0 / geo.ijac2[idx]; // images: 1 in both
+      else
+        w[idx] = is_image(i, j, g) ? 1.0 : which == 0 ? geo.lumpx[i] * geo.lumpy[j] : geo.diagx[i] * geo.diagy[j];
     }
   }
 
@@ -382,7 +385,7 @@ namespace lbfem_gpu
           my += c_EY[a] * v;
         }
       const double rho = 1.0 + dr, ux = mx / rho, uy = my / rho;
-      const double w = geo.lumpx[i] * geo.lumpy[j];
+      const double w = geo.lump2 ? geo.lump2[idx] : geo.lumpx[i] * geo.lumpy[j];
       s[0] += w;
       s[1] += w * rho;
       s[2] += w * mx;
@@ -409,7 +412,7 @@ namespace lbfem_gpu
       for (int a = 0; a < Q; ++a)
         v[a] = f[a * N + idx];
       const Mom m = moments(v);
-      const double w = geo.lumpx[i] * geo.lumpy[j];
+      const double w = geo.lump2 ? geo.lump2[idx] : geo.lumpx[i] * geo.lumpy[j];
       s[0] += w;
       s[1] += w * m.rho;
       s[2] += w * m.rho * m.ux;
@@ -458,6 +461,11 @@ namespace lbfem_gpu
     double a, b, c;        // point operation: value a e.grad f + b e.grad feq, flux c e (e.grad f)
     double ex[NM], ey[NM]; // directions of the moving populations
     double omega;          // BGK rate (ADV_TG_COLLIDE)
+    // FP32 coefficients of the population pairs (a, a + 4), a = 1..4, rounded
+    // once on the host: a, b, ex, c ex^2, ey, -2 c ex ey, c ey^2, c ex ey of
+    // population a, and its weight
+    float pk[4][8];
+    float pw[4];
   };
 
   template <int MODE>

@@ -130,11 +130,11 @@ namespace lbfem_gpu
 
   // Per-cell scales of the footprint, lane-duplicated: width, 1 / width, and 1 / 0 for
   // a cell inside / outside the domain.
-  template <int P>
+  template <int P, typename S = TileShape<P>>
   struct PairScales
   {
-    float2 hx[Tile<P>::CX + 1], hxi[Tile<P>::CX + 1], cx[Tile<P>::CX + 1];
-    float2 hy[Tile<P>::CY + 1], hyi[Tile<P>::CY + 1], cy[Tile<P>::CY + 1];
+    float2 hx[Tile<P, S>::CX + 1], hxi[Tile<P, S>::CX + 1], cx[Tile<P, S>::CX + 1];
+    float2 hy[Tile<P, S>::CY + 1], hyi[Tile<P, S>::CY + 1], cy[Tile<P, S>::CY + 1];
   };
 
   // The pair's coefficients: h = A u + B feq; k1..k6 of the grouped operator.
@@ -149,11 +149,11 @@ namespace lbfem_gpu
     PAIR_BARDOW = 1  // Bardow step: collide_bgk on the fly, write g*, then r of g*
   };
 
-  template <int P, int MODE>
+  template <int P, int MODE, typename S = TileShape<P>>
   constexpr size_t
   pair_smem()
   {
-    using T = Tile<P>;
+    using T = Tile<P, S>;
     // moments [4][NF] float, pair [2][NF] float2 (double-buffered), x-pass outputs [3][NY] float2,
     // Y4 [2][TX] float2, walls [NF] bytes
     return sizeof(float) * 4 * T::NF + sizeof(float2) * (2 * T::NF + 3 * T::NY + 2 * T::TX) +
@@ -181,13 +181,13 @@ namespace lbfem_gpu
 
   // x pass of one footprint row fy and one x segment. CLS: 0 e = (ex, 0), 1 e = (0, ey), 2 diagonal.
   // Each output node's operator rows are formed as they are stored (few live registers).
-  template <int P, int CLS, int MODE>
+  template <int P, int CLS, int MODE, typename S>
   __device__ __forceinline__ void
-  pair_xpass(const float2 *s_u, const float *s_m, float2 *s_y, float2 *s_y4, const PairScales<P> &m,
+  pair_xpass(const float2 *s_u, const float *s_m, float2 *s_y, float2 *s_y4, const PairScales<P, S> &m,
              const PairK &k, float w, float ex, float ey, int fy, int seg, int gx0, int y4_slot, int bx_lo,
              int bx_hi)
   {
-    using T = Tile<P>;
+    using T = Tile<P, S>;
     constexpr bool XC = CLS != 1, YC = CLS != 0, DG = CLS == 2;
     const int base = fy * T::PF;
     const int q0 = seg * T::KX;
@@ -293,12 +293,12 @@ namespace lbfem_gpu
   }
 
   // y pass on column j and y segment seg: emit(own row i, r of the pair).
-  template <int P, int CLS, typename Emit>
+  template <int P, int CLS, typename S, typename Emit>
   __device__ __forceinline__ void
-  pair_ypass(const float2 *s_y, const float2 *s_y4, const PairScales<P> &m, int j, int seg, int gy0, int by_lo,
+  pair_ypass(const float2 *s_y, const float2 *s_y4, const PairScales<P, S> &m, int j, int seg, int gy0, int by_lo,
              int by_hi, Emit &&emit)
   {
-    using T = Tile<P>;
+    using T = Tile<P, S>;
     constexpr bool XC = CLS != 1, YC = CLS != 0, DG = CLS == 2;
     const float2 *y1 = s_y, *y2 = s_y + T::NY, *y3 = s_y + 2 * T::NY;
     const int q0 = seg * T::KY;
@@ -385,14 +385,14 @@ namespace lbfem_gpu
   // rhs_{a-1} <- r_a (a = 1..8) of the scheme's step on FP32 deviations d,
   // pair by pair; PAIR_BARDOW also writes the collided deviations g* to dout.
   // Images get r = 0 (constrained rows).
-  template <int P, int MODE>
+  template <int P, int MODE, typename S = TileShape<P>>
   __global__ void __launch_bounds__(THREADS, 2)
     k_stream_pair(const Geo geo, const DevStats *__restrict__ ds, const float *__restrict__ d,
                   float *__restrict__ dout, float *__restrict__ rhs, const AdvCoef ac)
   {
     if (ds && ds->sticky)
       return; // a step after a failed solve: the populations must stay as they are
-    using T = Tile<P>;
+    using T = Tile<P, S>;
     constexpr bool BARDOW = MODE == PAIR_BARDOW;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     float2 *s_pb = reinterpret_cast<float2 *>(sm_raw);        // [2][NF] the pair, double-buffered
@@ -400,8 +400,8 @@ namespace lbfem_gpu
     float2 *s_y4 = s_y + 3 * T::NY;                           // [2][TX] Y4 on the first / last domain row
     float *s_m = reinterpret_cast<float *>(s_y4 + 2 * T::TX); // [4][NF] moments
     uint8_t *s_wall = reinterpret_cast<uint8_t *>(s_m + 4 * T::NF); // [NF] wall classes (Bardow)
-    __shared__ TileMaps<P, float> maps;
-    __shared__ PairScales<P> sc;
+    __shared__ TileMaps<P, float, S> maps;
+    __shared__ PairScales<P, S> sc;
     const Grid &g = geo.g;
     const long long N = g.N;
     const int gx0 = blockIdx.x * T::TX, gy0 = blockIdx.y * T::TY;
@@ -420,20 +420,38 @@ namespace lbfem_gpu
         sc.cy[t] = bc(maps.cy[t]);
       }
 
+    // Staging walks the footprint a row per warp: a lane's footprint columns
+    // (fx = lane + 32 k) and their source columns are the same for every row
+    // and every population, so they are looked up once; a row's storage offset
+    // is one broadcast load.
+    const int slane = threadIdx.x & 31, swarp = threadIdx.x >> 5;
+    constexpr int NCOL = (T::FX + 31) / 32;
+    int scol[NCOL];
+#pragma unroll
+    for (int k = 0; k < NCOL; ++k)
+      {
+        const int fx = slane + 32 * k;
+        scol[k] = fx < T::FX ? maps.col[fx] : -1;
+      }
+
     // Pair pr of the footprint into buffer pr & 1 by asynchronous copies (one
     // commit group per pair): pair pr + 1 is in flight while pair pr computes.
     auto issue_pair = [&](int pr) {
-      const int a = pr + 1, ab = pr + 5;
+      const float *da = d + (pr + 1) * N, *db = d + (pr + 5) * N;
       float2 *buf = s_pb + (pr & 1) * T::NF;
-      for (int t = threadIdx.x; t < T::FY * T::FX; t += blockDim.x)
+      for (int fy = swarp; fy < T::FY; fy += THREADS / 32)
         {
-          const int fy = t / T::FX, fx = t - fy * T::FX, st = fy * T::PF + fx;
           const int r = maps.row[fy];
-          const int c = maps.col[fx];
-          const bool ok = r >= 0 && c >= 0;
-          const int idx = ok ? r + c : 0;
-          cp_async4(&buf[st].x, d + a * N + idx, ok);
-          cp_async4(&buf[st].y, d + ab * N + idx, ok);
+          float2 *brow = buf + fy * T::PF + slane;
+#pragma unroll
+          for (int k = 0; k < NCOL; ++k)
+            if (slane + 32 * k < T::FX)
+              {
+                const bool ok = r >= 0 && scol[k] >= 0;
+                const int idx = ok ? r + scol[k] : 0;
+                cp_async4(&brow[32 * k].x, da + idx, ok);
+                cp_async4(&brow[32 * k].y, db + idx, ok);
+              }
         }
       cp_async_commit();
     };
@@ -442,70 +460,65 @@ namespace lbfem_gpu
     // moments of every footprint node (Lee-Lin: wall velocity imposed, and the
     // even equilibrium base drho - 1.5 rho u.u; Bardow: the node's own moments
     // and its wall class)
-    {
-      constexpr int NT = T::FY * T::FX;
-      for (int t0 = threadIdx.x; t0 < NT; t0 += 2 * THREADS)
-        {
-          float v[2][Q];
-          int idx[2];
-          int wk[2];
+    // (row per warp as the staging; a lane's loads of all its columns in a row
+    // are issued before the first moment is formed)
+    for (int fy = swarp; fy < T::FY; fy += THREADS / 32)
+      {
+        const int r = maps.row[fy];
+        float v[NCOL][Q];
+        int wk[NCOL];
+        bool ok[NCOL];
 #pragma unroll
-          for (int hh = 0; hh < 2; ++hh)
-            {
-              const int t = t0 + hh * THREADS;
-              idx[hh] = -1;
-              wk[hh] = 0;
-              if (t < NT)
-                {
-                  const int fy = t / T::FX, fx = t - fy * T::FX;
-                  const int r = maps.row[fy];
-                  const int c = maps.col[fx];
-                  if (r >= 0 && c >= 0)
-                    idx[hh] = r + c;
-                }
+        for (int k = 0; k < NCOL; ++k)
+          {
+            ok[k] = r >= 0 && scol[k] >= 0;
+            const int idx = ok[k] ? r + scol[k] : 0;
+            const float *p = d + idx;
 #pragma unroll
-              for (int a = 0; a < Q; ++a)
-                v[hh][a] = idx[hh] >= 0 ? d[a * N + idx[hh]] : 0.f;
-              if (idx[hh] >= 0 && geo.wall)
-                wk[hh] = geo.wall[idx[hh]];
-            }
+            for (int a = 0; a < Q; ++a)
+              v[k][a] = ok[k] ? p[a * N] : 0.f;
+            wk[k] = ok[k] && geo.wall ? geo.wall[idx] : 0;
+          }
+        float *mrow = s_m + fy * T::PF + slane;
 #pragma unroll
-          for (int hh = 0; hh < 2; ++hh)
-            {
-              const int t = t0 + hh * THREADS;
-              if (t >= NT)
+        for (int k = 0; k < NCOL; ++k)
+          {
+            if (slane + 32 * k >= T::FX)
+              continue;
+            float *m = mrow + 32 * k;
+            if (!ok[k])
+              {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                  m[q * T::NF] = 0.f;
+                if constexpr (BARDOW)
+                  s_wall[fy * T::PF + slane + 32 * k] = 0;
                 continue;
-              const int fy = t / T::FX, fx = t - fy * T::FX, st = fy * T::PF + fx;
-              if (idx[hh] < 0)
-                {
-#pragma unroll
-                  for (int q = 0; q < 4; ++q)
-                    s_m[q * T::NF + st] = 0.f;
-                  if constexpr (BARDOW)
-                    s_wall[st] = 0;
-                  continue;
-                }
-              MomF mo = moments_dev(v[hh]);
-              if constexpr (BARDOW)
-                {
-                  s_m[st] = mo.rho;
-                  s_m[T::NF + st] = mo.ux;
-                  s_m[2 * T::NF + st] = mo.uy;
-                  s_m[3 * T::NF + st] = mo.drho;
-                  s_wall[st] = uint8_t(wk[hh]);
-                }
-              else
-                {
-                  mo = impose_class(mo, wk[hh], geo);
-                  s_m[st] = mo.rho;
-                  s_m[T::NF + st] = mo.ux;
-                  s_m[2 * T::NF + st] = mo.uy;
-                  s_m[3 * T::NF + st] = mo.drho - 1.5f * mo.rho * (mo.ux * mo.ux + mo.uy * mo.uy);
-                }
-            }
-        }
-    }
+              }
+            MomF mo = moments_dev(v[k]);
+            if constexpr (BARDOW)
+              {
+                m[0] = mo.rho;
+                m[T::NF] = mo.ux;
+                m[2 * T::NF] = mo.uy;
+                m[3 * T::NF] = mo.drho;
+                s_wall[fy * T::PF + slane + 32 * k] = uint8_t(wk[k]);
+              }
+            else
+              {
+                mo = impose_class(mo, wk[k], geo);
+                m[0] = mo.rho;
+                m[T::NF] = mo.ux;
+                m[2 * T::NF] = mo.uy;
+                m[3 * T::NF] = mo.drho - 1.5f * mo.rho * (mo.ux * mo.ux + mo.uy * mo.uy);
+              }
+          }
+      }
 
+    // a tile of distinct nodes only (no image row or column, nothing past the grid)
+    // writes its results without per-node checks
+    const bool interior =
+      gx0 + T::TX <= (g.px ? g.nux : g.nfx) && gy0 + T::TY <= (g.py ? g.nuy : g.nfy);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int bx_lo = g.px ? -1 : 0, bx_hi = g.px ? -1 : g.nfx - 1;
     const int by_lo = g.py ? -1 : 0, by_hi = g.py ? -1 : g.nfy - 1;
@@ -532,8 +545,8 @@ namespace lbfem_gpu
     for (int pr = 0; pr < 4; ++pr)
       {
         const int a = pr + 1, ab = pr + 5; // opposite populations
-        const float ex = float(ac.ex[a - 1]), ey = float(ac.ey[a - 1]);
-        const float w = float(c_W[a]);
+        const float *pk = ac.pk[pr];
+        const float ex = pk[2], ey = pk[4], w = ac.pw[pr];
         float2 *s_u = s_pb + (pr & 1) * T::NF;
         if (pr < 3)
           {
@@ -560,8 +573,8 @@ namespace lbfem_gpu
                     const MomF mt = impose_class(mo, s_wall[st], geo);
                     // each population's own equilibrium: the collision writes the state, and the
                     // rounding of the even +- odd form accumulates there from step to step
-                    gs.x = feqd_a(a, mt) + (1.f - omega) * (gv.x - feqd_a(a, mo));
-                    gs.y = feqd_a(ab, mt) + (1.f - omega) * (gv.y - feqd_a(ab, mo));
+                    gs.x = feqd(ex, ey, w, mt) + (1.f - omega) * (gv.x - feqd(ex, ey, w, mo));
+                    gs.y = feqd(-ex, -ey, w, mt) + (1.f - omega) * (gv.y - feqd(-ex, -ey, w, mo));
                     const int gx = gx0 - P + fx, gy = gy0 - P + fy;
                     if (fx >= P && fx < P + T::TX && fy >= P && fy < P + T::TY && gx < g.nfx && gy < g.nfy &&
                         !is_image(gx, gy, g))
@@ -575,27 +588,26 @@ namespace lbfem_gpu
           }
         __syncthreads();
         const int cls = ey == 0.f ? 0 : (ex == 0.f ? 1 : 2);
-        const double exd = ac.ex[a - 1], eyd = ac.ey[a - 1];
         PairK k;
-        k.A = bc(float(ac.a));
-        k.B = bc(float(ac.b));
-        k.k1 = make_float2(float(exd), float(-exd));
-        k.k2 = bc(float(ac.c * exd * exd));
-        k.k3 = make_float2(float(eyd), float(-eyd));
-        k.k4 = bc(float(-2.0 * ac.c * exd * eyd));
-        k.k5 = bc(float(ac.c * eyd * eyd));
-        k.k6 = bc(float(ac.c * exd * eyd));
+        k.A = bc(pk[0]);
+        k.B = bc(pk[1]);
+        k.k1 = make_float2(pk[2], -pk[2]);
+        k.k2 = bc(pk[3]);
+        k.k3 = make_float2(pk[4], -pk[4]);
+        k.k4 = bc(pk[5]);
+        k.k5 = bc(pk[6]);
+        k.k6 = bc(pk[7]);
         // x pass: lane = footprint row, warp = x segment
         if (warp < T::NSX && lane < T::FY)
           {
             const int gy = gy0 - P + lane;
             const int y4_slot = gy == by_lo ? 0 : gy == by_hi ? 1 : -1;
             if (cls == 0)
-              pair_xpass<P, 0, MODE>(s_u, s_m, s_y, s_y4, sc, k, w, ex, ey, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
+              pair_xpass<P, 0, MODE, S>(s_u, s_m, s_y, s_y4, sc, k, w, ex, ey, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
             else if (cls == 1)
-              pair_xpass<P, 1, MODE>(s_u, s_m, s_y, s_y4, sc, k, w, ex, ey, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
+              pair_xpass<P, 1, MODE, S>(s_u, s_m, s_y, s_y4, sc, k, w, ex, ey, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
             else
-              pair_xpass<P, 2, MODE>(s_u, s_m, s_y, s_y4, sc, k, w, ex, ey, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
+              pair_xpass<P, 2, MODE, S>(s_u, s_m, s_y, s_y4, sc, k, w, ex, ey, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
           }
         __syncthreads();
         // y pass: lane group = columns, warp group = y segment
@@ -604,22 +616,28 @@ namespace lbfem_gpu
           {
             const int gx = gx0 + j;
             float *oa = rhs + (long long)(a - 1) * N, *ob = rhs + (long long)(ab - 1) * N;
+            float *oac = oa + gx, *obc = ob + gx;
             auto emit = [&](int i, float2 r) {
               const int gy = gy0 + i;
-              if (gx < g.nfx && gy < g.nfy)
+              const int off = gy * g.nfx; // a population array holds fewer than 2^31 nodes
+              if (interior)
                 {
-                  const int idx = gy * g.nfx + gx; // a population array holds fewer than 2^31 nodes
+                  oac[off] = r.x;
+                  obc[off] = r.y;
+                }
+              else if (gx < g.nfx && gy < g.nfy)
+                {
                   const bool img = is_image(gx, gy, g);
-                  oa[idx] = img ? 0.f : r.x;
-                  ob[idx] = img ? 0.f : r.y;
+                  oac[off] = img ? 0.f : r.x;
+                  obc[off] = img ? 0.f : r.y;
                 }
             };
             if (cls == 0)
-              pair_ypass<P, 0>(s_y, s_y4, sc, j, seg, gy0, by_lo, by_hi, emit);
+              pair_ypass<P, 0, S>(s_y, s_y4, sc, j, seg, gy0, by_lo, by_hi, emit);
             else if (cls == 1)
-              pair_ypass<P, 1>(s_y, s_y4, sc, j, seg, gy0, by_lo, by_hi, emit);
+              pair_ypass<P, 1, S>(s_y, s_y4, sc, j, seg, gy0, by_lo, by_hi, emit);
             else
-              pair_ypass<P, 2>(s_y, s_y4, sc, j, seg, gy0, by_lo, by_hi, emit);
+              pair_ypass<P, 2, S>(s_y, s_y4, sc, j, seg, gy0, by_lo, by_hi, emit);
           }
       }
 

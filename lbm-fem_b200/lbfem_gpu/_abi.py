@@ -47,6 +47,7 @@ class MeshDesc(C.Structure):
         ("vertex_x", C.POINTER(C.c_double)), ("vertex_y", C.POINTER(C.c_double)),
         ("n_dofs", C.c_int64), ("dof_index", C.POINTER(C.c_int64)),
         ("n_walls", C.c_int64), ("wall_dof", C.POINTER(C.c_int64)), ("wall_velocity", C.POINTER(C.c_double)),
+        ("vertex_xy", C.POINTER(C.c_double)),
     ]
 
 
@@ -86,11 +87,15 @@ class Handle:
         if dof_index is not None:
             di = np.ascontiguousarray(dof_index, np.int64)
             self._keep.append(di)
+        vxy = None
+        if getattr(mesh, "vertex_xy", None) is not None:
+            vxy = np.ascontiguousarray(mesh.vertex_xy, np.float64).reshape(-1)
+            self._keep.append(vxy)
         desc = MeshDesc(mesh.degree, mesh.n_cells_x, mesh.n_cells_y, int(mesh.periodic_x), int(mesh.periodic_y),
                         _dptr(self._keep[0]), _dptr(self._keep[1]), mesh.n_dofs,
                         di.ctypes.data_as(C.POINTER(C.c_int64)) if di is not None else None,
                         len(self._keep[2]), self._keep[2].ctypes.data_as(C.POINTER(C.c_int64)),
-                        _dptr(self._keep[3]))
+                        _dptr(self._keep[3]), _dptr(vxy))
         self.params = params
         h = C.c_void_p()
         self._call("create", C.byref(desc), C.byref(params), C.byref(h))
@@ -276,6 +281,7 @@ def declare(lib, prefix):
         "set_populations_dev": [vp, vp, vp], "get_populations_dev": [vp, vp, vp], "step_stream": [vp, i32, vp],
         # y-strip decomposition (strips.py)
         "strip_buffer_bytes": [vp, C.POINTER(i64)], "set_strip": [vp, vp],
+        "tuning": [vp, C.POINTER(i32), C.POINTER(C.c_float)],
     }
     for name, args in sig.items():
         fn = getattr(lib, prefix + name, None)

@@ -79,11 +79,19 @@ class TaylorGreenVortex(TestCase):
     n_periodic = 2
     steady = False
 
-    def __init__(self, mach, n1=1, n2=4, shift=(0.0, 0.0), chapman_enskog=True):
+    def __init__(self, mach, n1=1, n2=4, shift=(0.0, 0.0), chapman_enskog=True, distort=0.0):
         super().__init__(mach)
         self.n1, self.n2 = float(n1), float(n2)
         self.shift = shift
         self.chapman_enskog = chapman_enskog
+        self.distort = float(distort)
+
+    def transform_vertices(self, X, Y):
+        """TaylorGreenVortex::transform_mesh (test_cases.h:52-63): every vertex moves by
+        eps L sin(2 pi x / L) sin(2 pi y / L) (1, 1) (zero on the box's sides, so the
+        periodic sides still match); the cells become general quadrilaterals."""
+        d = self.distort * self.L * np.sin(2 * math.pi * X / self.L) * np.sin(2 * math.pi * Y / self.L)
+        return X + d, Y + d
 
     def k1(self):
         return 2 * math.pi * self.n1 / self.L
@@ -196,6 +204,8 @@ class Mesh:
     h_min: float
     wall_dof: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     wall_velocity: np.ndarray = field(default_factory=lambda: np.zeros((0, 2)))
+    # mapped vertices ((n_cells_y + 1) x (n_cells_x + 1) x 2) of a general quadrilateral mesh, or None
+    vertex_xy: np.ndarray | None = None
 
     @property
     def nfx(self):
@@ -216,9 +226,22 @@ class Mesh:
         return np.concatenate([pts, v[-1:]])
 
     def nodes(self):
-        """Support points (x, y) of all structured nodes, node (i, j) at j*nfx + i."""
-        X, Y = np.meshgrid(self.axis_nodes(self.vertex_x), self.axis_nodes(self.vertex_y))
-        return X.ravel(), Y.ravel()
+        """Support points (x, y) of all structured nodes, node (i, j) at j*nfx + i. On a
+        general quadrilateral mesh: the bilinear image (MappingQ1) of each node's
+        Gauss-Lobatto point in its cell."""
+        if self.vertex_xy is None:
+            X, Y = np.meshgrid(self.axis_nodes(self.vertex_x), self.axis_nodes(self.vertex_y))
+            return X.ravel(), Y.ravel()
+        P, xi = self.degree, gauss_lobatto(self.degree)
+        I, J = np.meshgrid(np.arange(self.nfx), np.arange(self.nfy))
+        cx, cy = np.minimum(I // P, self.n_cells_x - 1), np.minimum(J // P, self.n_cells_y - 1)
+        s, t = xi[I - P * cx], xi[J - P * cy]
+        v = self.vertex_xy
+        out = []
+        for k in range(2):
+            out.append(((1 - s) * (1 - t) * v[cy, cx, k] + s * (1 - t) * v[cy, cx + 1, k]
+                        + (1 - s) * t * v[cy + 1, cx, k] + s * t * v[cy + 1, cx + 1, k]).ravel())
+        return out[0], out[1]
 
     def constrained(self):
         """Periodic images (deal.II's constrained DoFs): last column / row of a periodic direction."""
@@ -260,6 +283,10 @@ def build_mesh(tc: TestCase, n_cells_x: int, degree: int = 1, n_cells_y: int | N
     vx, vy, h_min = tc.transform_axes(vx, vy, h_min)
     m = Mesh(degree, n_cells_x, ny, tc.n_periodic >= 1, tc.n_periodic >= 2, np.asarray(vx, float),
              np.asarray(vy, float), h_min)
+    if getattr(tc, "distort", 0.0):
+        VX, VY = np.meshgrid(m.vertex_x, m.vertex_y)
+        TX, TY = tc.transform_vertices(VX, VY)
+        m.vertex_xy = np.stack([TX, TY], axis=-1)
     x, y = m.nodes()
     mask, ux, uy = tc.wall_velocity(x, y)
     m.wall_dof = np.nonzero(mask)[0].astype(np.int64)

@@ -229,6 +229,9 @@ struct lbfem_oracle
   bool strip = false;
   int oy0 = 0, oy1 = 0;
   lbfem_strip_desc sd{};
+  // general quadrilaterals (lbfem_mesh_desc::vertex_xy): the mapped vertices, (ncy+1) x (ncx+1) x 2
+  bool distorted = false;
+  std::vector<double> vxy;
 
   int64_t
   master(int i, int j) const
@@ -335,6 +338,26 @@ namespace
     return LBFEM_OK;
   }
 
+  // MappingQ1 of cell (cx, cy) at the reference point (s, t): the inverse
+  // Jacobian, row-major (Ji[0] = (J^-1)_00, Ji[1] = (J^-1)_01, ...), and det J.
+  double
+  cell_map(const lbfem_oracle &o, int cx, int cy, double s, double t, double (&Ji)[4])
+  {
+    auto v = [&](int i, int j, int k) { return o.vxy[(size_t(j) * (o.ncx + 1) + i) * 2 + k]; };
+    double J[2][2];
+    for (int k = 0; k < 2; ++k)
+      {
+        J[k][0] = (1 - t) * (v(cx + 1, cy, k) - v(cx, cy, k)) + t * (v(cx + 1, cy + 1, k) - v(cx, cy + 1, k));
+        J[k][1] = (1 - s) * (v(cx, cy + 1, k) - v(cx, cy, k)) + s * (v(cx + 1, cy + 1, k) - v(cx + 1, cy, k));
+      }
+    const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    Ji[0] = J[1][1] / det;
+    Ji[1] = -J[0][1] / det;
+    Ji[2] = -J[1][0] / det;
+    Ji[3] = J[0][0] / det;
+    return det;
+  }
+
   // ------------------------------------------------------- advection (K1)
   // rhs (8 blocks) <- cell integrals of the point operation over f (and feq)
   // + wall-face integrals of the surface term.
@@ -361,6 +384,11 @@ namespace
       for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i)
           idx[j][i] = o.master(cx * P + i, cy * P + j);
+      double jinv[n][n][4], jxw[n][n]; // general quadrilaterals: MappingQ1 at the Gauss points
+      if (o.distorted)
+        for (int q2 = 0; q2 < n; ++q2)
+          for (int q1 = 0; q1 < n; ++q1)
+            jxw[q2][q1] = B.qw[q1] * B.qw[q2] * cell_map(o, cx, cy, B.qx[q1], B.qx[q2], jinv[q2][q1]);
       double V[NM][n][n], FX[NM][n][n], FY[NM][n][n]; // at Gauss points [q2][q1]
       for (int al = 0; al < NM; ++al)
         {
@@ -396,21 +424,42 @@ namespace
                         sx += B.S[q2][bb] * tx[bb][q1];
                         sy += B.D[q2][bb] * tv[bb][q1];
                       }
-                    gx[q2][q1] = sx / hx;
-                    gy[q2][q1] = sy / hy;
+                    if (o.distorted)
+                      {
+                        // grad = J^-T (d/dxi, d/deta)
+                        const double *Ji = jinv[q2][q1];
+                        gx[q2][q1] = Ji[0] * sx + Ji[2] * sy;
+                        gy[q2][q1] = Ji[1] * sx + Ji[3] * sy;
+                      }
+                    else
+                      {
+                        gx[q2][q1] = sx / hx;
+                        gy[q2][q1] = sy / hy;
+                      }
                   }
             }
           for (int q2 = 0; q2 < n; ++q2)
             for (int q1 = 0; q1 < n; ++q1)
               {
-                const double JxW = B.qw[q1] * B.qw[q2] * hx * hy;
+                const double JxW = o.distorted ? jxw[q2][q1] : B.qw[q1] * B.qw[q2] * hx * hy;
                 const double s = ex[al] * gxf[q2][q1] + ey[al] * gyf[q2][q1];
                 double val = a * s;
                 if (two)
                   val += b * (ex[al] * gxe[q2][q1] + ey[al] * gye[q2][q1]);
                 V[al][q2][q1] = val * JxW;
-                FX[al][q2][q1] = (c * ex[al]) * s * JxW / hx;
-                FY[al][q2][q1] = (c * ey[al]) * s * JxW / hy;
+                if (o.distorted)
+                  {
+                    // the flux in reference directions: J^-1 F
+                    const double *Ji = jinv[q2][q1];
+                    const double fx = (c * ex[al]) * s * JxW, fy = (c * ey[al]) * s * JxW;
+                    FX[al][q2][q1] = Ji[0] * fx + Ji[1] * fy;
+                    FY[al][q2][q1] = Ji[2] * fx + Ji[3] * fy;
+                  }
+                else
+                  {
+                    FX[al][q2][q1] = (c * ex[al]) * s * JxW / hx;
+                    FY[al][q2][q1] = (c * ey[al]) * s * JxW / hy;
+                  }
               }
         }
       for (int al = 0; al < NM; ++al)
@@ -569,6 +618,12 @@ namespace
       for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i)
           idx[j][i] = o.master(cx * P + i, cy * P + j);
+      auto jxw_at = [&](int q1, int q2) {
+        if (!o.distorted)
+          return B.qw[q1] * B.qw[q2] * hx * hy;
+        double Ji[4];
+        return B.qw[q1] * B.qw[q2] * cell_map(o, cx, cy, B.qx[q1], B.qx[q2], Ji);
+      };
       if (mode == 1)
         {
           for (int bb = 0; bb < n; ++bb)
@@ -579,7 +634,7 @@ namespace
                   for (int q1 = 0; q1 < n; ++q1)
                     {
                       const double phi = B.S[q1][aa] * B.S[q2][bb];
-                      s += phi * phi * (B.qw[q1] * B.qw[q2] * hx * hy);
+                      s += phi * phi * jxw_at(q1, q2);
                     }
                 dst[idx[bb][aa]] += s;
               }
@@ -605,7 +660,7 @@ namespace
             double s = 0;
             for (int bb = 0; bb < n; ++bb)
               s += B.S[q2][bb] * t[bb][q1];
-            vq[q2][q1] = s * (B.qw[q1] * B.qw[q2] * hx * hy);
+            vq[q2][q1] = s * jxw_at(q1, q2);
           }
       double a1[n][n]; // [q1][b]
       for (int q1 = 0; q1 < n; ++q1)
@@ -1253,6 +1308,14 @@ lbfem_oracle_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_ora
     return LBFEM_ERR_ARG;
   o->vx.assign(m->vertex_x, m->vertex_x + o->ncx + 1);
   o->vy.assign(m->vertex_y, m->vertex_y + o->ncy + 1);
+  if (m->vertex_xy)
+    {
+      // general quadrilaterals: TG2, no walls (the reference's --distort is a Taylor-Green option)
+      if (m->n_walls > 0 || prm->streaming != LBFEM_STREAMING_TG2)
+        return LBFEM_ERR_UNSUPPORTED;
+      o->distorted = true;
+      o->vxy.assign(m->vertex_xy, m->vertex_xy + size_t(o->ncx + 1) * (o->ncy + 1) * 2);
+    }
   o->basis = std::make_unique<Basis>(o->p);
   o->prm = *prm;
   const int64_t N = o->N;
@@ -1548,7 +1611,7 @@ lbfem_oracle_strip_buffer_bytes(const lbfem_oracle *h, int64_t *bytes)
 int
 lbfem_oracle_set_strip(lbfem_oracle *h, const lbfem_strip_desc *sd)
 {
-  if (!h || !sd || !sd->comm || !sd->sums || h->py)
+  if (!h || !sd || !sd->comm || !sd->sums || h->py || h->distorted)
     return LBFEM_ERR_ARG;
   if ((sd->ghost_below != 0 && sd->ghost_below != h->p) || (sd->ghost_above != 0 && sd->ghost_above != 1))
     return LBFEM_ERR_ARG;
@@ -1585,7 +1648,7 @@ lbfem_oracle_stream_function(lbfem_oracle *h, const double *velocity, double *ps
 {
   if (!h || !velocity || !psi)
     return LBFEM_ERR_ARG;
-  if (h->strip)
+  if (h->strip || h->distorted)
     return LBFEM_ERR_UNSUPPORTED;
   int64_t its = 0;
   return stream_function(*h, velocity, velocity + h->N, psi, &its);

@@ -500,3 +500,23 @@ def test_ladder_warm_start_on_the_oracle(oracle_mod):
     f0 = hs[0].get_populations()
     for h in hs[1:]:
         assert np.array_equal(h.get_populations(), f0)
+
+
+@pytest.mark.parametrize("eps,expected", [(0.0, 1.73e-2), (0.02, 1.81e-2), (0.04, 2.07e-2)])
+def test_distorted_mesh_error_table(oracle_mod, eps, expected):
+    """docs/results.md:222-233, general quadrilaterals (--distort eps, test_cases.h:52-63,
+    MappingQ1): 48^2, modes (1,4), Re 100, Ma 0.05, TG2 at nominal CFL 0.25, t = t_ref/4,
+    Bardow, consistent mass, Q1, to the printed digits. eps = 0 runs the mapped-vertex
+    path on the undistorted vertices."""
+    tc, m = tgv(48, distort=eps)
+    if eps == 0.0:
+        VX, VY = np.meshgrid(m.vertex_x, m.vertex_y)
+        m.vertex_xy = np.stack([VX, VY], -1)
+    dt, n = cases.run_length(tc, m, 0.25, 0.25)
+    o = setup_case(oracle_mod.Oracle, tc, m, make_params("bardow", "cg"), dt, tc.relaxation_time())
+    o.step(n)
+    err = cases.diagnostics(tc, m, o.node_weight(), o.get_populations(), n * dt)["rel_l2_u"]
+    assert float(f"{err:.2e}") == expected, err
+    # the mapped cells tile the box: the lumped weights of the distinct nodes add up to its area
+    w = o.node_weight()
+    assert abs(w[m.independent()].sum() - 1.0) <= 1e-13
