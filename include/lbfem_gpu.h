@@ -378,8 +378,9 @@ int lbfem_gpu_solve_round_resident(lbfem_gpu_ctx *ctx);
  * per thread's x / y segment) is timed on the context's own buffers, and the
  * fastest is kept (cached per device, degree, scheme and grid for the process;
  * LBFEM_TUNE=0 in the environment keeps the default). shape: -1 not yet tuned,
- * 0 the default shape, 1 the alternative; ms: the two shapes' times per launch.
- * No counterpart in the reference.
+ * 0 the default shape, 1 the alternative (8 x-pass warps), 2 the small one
+ * (shared memory and registers for 3 CTAs per SM); ms: the three shapes' times
+ * per launch (3 floats). No counterpart in the reference.
  */
 int lbfem_gpu_tuning(const lbfem_gpu_ctx *ctx, int32_t *shape, float *ms);
 

@@ -59,21 +59,25 @@ namespace lbfem_gpu
   struct TileShape<1>
   {
     static constexpr int CX = 64, CY = 24, KX = 8, KY = 6;
+    static constexpr int MIN_CTAS = 2; // CTAs per SM the streaming kernel's registers are sized for
   };
   template <>
   struct TileShape<2>
   {
     static constexpr int CX = 32, CY = 12, KX = 4, KY = 3;
+    static constexpr int MIN_CTAS = 2; // CTAs per SM the streaming kernel's registers are sized for
   };
   template <>
   struct TileShape<3>
   {
     static constexpr int CX = 21, CY = 8, KX = 3, KY = 2;
+    static constexpr int MIN_CTAS = 2; // CTAs per SM the streaming kernel's registers are sized for
   };
   template <>
   struct TileShape<4>
   {
     static constexpr int CX = 15, CY = 6, KX = 3, KY = 2;
+    static constexpr int MIN_CTAS = 2; // CTAs per SM the streaming kernel's registers are sized for
   };
 
   // A second shape per degree, for the run-time choice of the streaming kernel's
@@ -84,21 +88,54 @@ namespace lbfem_gpu
   struct TileShapeAlt<1>
   {
     static constexpr int CX = 48, CY = 24, KX = 6, KY = 6;
+    static constexpr int MIN_CTAS = 2; // CTAs per SM the streaming kernel's registers are sized for
   };
   template <>
   struct TileShapeAlt<2>
   {
     static constexpr int CX = 24, CY = 12, KX = 3, KY = 3;
+    static constexpr int MIN_CTAS = 2; // CTAs per SM the streaming kernel's registers are sized for
   };
   template <>
   struct TileShapeAlt<3>
   {
     static constexpr int CX = 16, CY = 8, KX = 2, KY = 2;
+    static constexpr int MIN_CTAS = 2; // CTAs per SM the streaming kernel's registers are sized for
   };
   template <>
   struct TileShapeAlt<4>
   {
     static constexpr int CX = 16, CY = 6, KX = 2, KY = 2;
+    static constexpr int MIN_CTAS = 2; // CTAs per SM the streaming kernel's registers are sized for
+  };
+
+  // A third shape: fewer rows, shared memory for 3 CTAs per SM (degrees 1-3)
+  // and registers capped to match.
+  template <int P>
+  struct TileShapeSmall;
+  template <>
+  struct TileShapeSmall<1>
+  {
+    static constexpr int CX = 48, CY = 16, KX = 6, KY = 4;
+    static constexpr int MIN_CTAS = 3;
+  };
+  template <>
+  struct TileShapeSmall<2>
+  {
+    static constexpr int CX = 24, CY = 8, KX = 3, KY = 2;
+    static constexpr int MIN_CTAS = 3;
+  };
+  template <>
+  struct TileShapeSmall<3>
+  {
+    static constexpr int CX = 16, CY = 6, KX = 2, KY = 2;
+    static constexpr int MIN_CTAS = 3;
+  };
+  template <>
+  struct TileShapeSmall<4>
+  {
+    static constexpr int CX = 16, CY = 4, KX = 2, KY = 1;
+    static constexpr int MIN_CTAS = 2;
   };
 
   template <int P, typename S = TileShape<P>>

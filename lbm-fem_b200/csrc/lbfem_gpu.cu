@@ -86,7 +86,7 @@ struct lbfem_gpu_ctx
   // the tuned tile shape of the FP32 streaming kernel (tune_pair) and the times it was chosen by
   int pair_shape = 0;
   bool pair_tuned = false;
-  float tune_ms[2] = {0.f, 0.f};
+  float tune_ms[3] = {0.f, 0.f, 0.f};
   // general quadrilaterals (lbfem_mesh_desc::vertex_xy): per cell and Gauss point J^-1 and
   // JxW, and the per-node mass diagonals (inverse Jacobi, lumped and its inverse)
   bool distorted = false;
@@ -220,6 +220,10 @@ namespace
                        pair_smem<P, PAIR_LEELIN, TileShapeAlt<P>>())) ||
         (st = set_smem(ctx, k_stream_pair<P, PAIR_BARDOW, TileShapeAlt<P>>,
                        pair_smem<P, PAIR_BARDOW, TileShapeAlt<P>>())) ||
+        (st = set_smem(ctx, k_stream_pair<P, PAIR_LEELIN, TileShapeSmall<P>>,
+                       pair_smem<P, PAIR_LEELIN, TileShapeSmall<P>>())) ||
+        (st = set_smem(ctx, k_stream_pair<P, PAIR_BARDOW, TileShapeSmall<P>>,
+                       pair_smem<P, PAIR_BARDOW, TileShapeSmall<P>>())) ||
         (st = set_smem(ctx, k_mass_vmult<P>, cg_smem<P, double>(0))) ||
         (st = set_smem(ctx, k_cg_start<P, double, double, double>, cg_smem<P, double>(1))) ||
         (st = set_smem(ctx, k_cg_p<P, double>, cg_smem<P, double>(0))) ||
@@ -328,8 +332,8 @@ namespace
   }
 
   // The FP32 streaming kernel of the mixed-precision step (pairs of opposite
-  // populations), in tile shape `shape` (0: TileShape, 1: TileShapeAlt; -1: the
-  // context's tuned choice).
+  // populations), in tile shape `shape` (0: TileShape, 1: TileShapeAlt,
+  // 2: TileShapeSmall; -1: the context's tuned choice).
   int
   launch_pair(lbfem_gpu_ctx *ctx, int mode, const float *d, float *dout, float *rhs, const AdvCoef &ac,
               const DevStats *ds = nullptr, int shape = -1)
@@ -352,6 +356,8 @@ namespace
       };
       if (shape == 1)
         go(TileShapeAlt<P>{});
+      else if (shape == 2)
+        go(TileShapeSmall<P>{});
       else
         go(TileShape<P>{});
       LAUNCHED();
@@ -364,8 +370,8 @@ namespace
   // buffers (CUDA events, one warm-up and five timed launches) before the first
   // step records its graph, and the fastest is kept. The choice is cached per
   // (device, degree, scheme, grid) for the other contexts of the process.
-  // LBFEM_TUNE=0 keeps the default shape, LBFEM_TUNE=alt the alternative (for
-  // tests). Every shape gives bitwise the same
+  // LBFEM_TUNE=0 keeps the default shape; LBFEM_TUNE=alt / small fix the other
+  // two (for tests). Every shape gives bitwise the same
   // results (the per-node arithmetic does not depend on the tile).
   struct TuneKey
   {
@@ -377,7 +383,8 @@ namespace
     }
   };
   std::mutex tune_mutex;
-  std::map<TuneKey, std::pair<int, std::array<float, 2>>> tune_cache;
+  constexpr int N_SHAPES = 3;
+  std::map<TuneKey, std::pair<int, std::array<float, N_SHAPES>>> tune_cache;
 
   int
   tune_pair(lbfem_gpu_ctx *ctx)
@@ -385,10 +392,10 @@ namespace
     if (!ctx->mixed || ctx->pair_tuned || ctx->distorted)
       return LBFEM_OK;
     const char *env = std::getenv("LBFEM_TUNE");
-    if (env && (env[0] == '0' || std::strcmp(env, "alt") == 0))
+    if (env && (env[0] == '0' || std::strcmp(env, "alt") == 0 || std::strcmp(env, "small") == 0))
       {
-        // a fixed shape: the default ("0") or the alternative ("alt")
-        ctx->pair_shape = env[0] == '0' ? 0 : 1;
+        // a fixed shape: the default ("0"), the alternative ("alt") or the small one ("small")
+        ctx->pair_shape = env[0] == '0' ? 0 : env[0] == 'a' ? 1 : 2;
         ctx->pair_tuned = true;
         return LBFEM_OK;
       }
@@ -400,8 +407,8 @@ namespace
       if (it != tune_cache.end())
         {
           ctx->pair_shape = it->second.first;
-          ctx->tune_ms[0] = it->second.second[0];
-          ctx->tune_ms[1] = it->second.second[1];
+          for (int k = 0; k < N_SHAPES; ++k)
+            ctx->tune_ms[k] = it->second.second[k];
           ctx->pair_tuned = true;
           return LBFEM_OK;
         }
@@ -410,9 +417,9 @@ namespace
     const AdvCoef ac = bardow ? adv_coef(-dt, 0., -0.5 * dt * dt, d2q9_e(), dt / (lam + 0.5 * dt))
                               : adv_coef(-dt - b, b, -0.5 * dt * dt, d2q9_e(), 0.);
     float *d = ctx->d_fs[ctx->cur], *g = bardow ? ctx->d_fs[1 - ctx->cur] : nullptr;
-    float ms[2] = {0.f, 0.f};
+    std::array<float, N_SHAPES> ms{};
     int st;
-    for (int shape = 0; shape < 2; ++shape)
+    for (int shape = 0; shape < N_SHAPES; ++shape)
       {
         if ((st = launch_pair(ctx, bardow ? PAIR_BARDOW : PAIR_LEELIN, d, g, ctx->d_rhs_s, ac, nullptr, shape)))
           return st;
@@ -425,12 +432,16 @@ namespace
         CK(cudaEventElapsedTime(&ms[shape], ctx->ev[14], ctx->ev[15]));
         ms[shape] /= 5.f;
       }
-    ctx->pair_shape = ms[1] < ms[0] ? 1 : 0;
-    ctx->tune_ms[0] = ms[0];
-    ctx->tune_ms[1] = ms[1];
+    ctx->pair_shape = 0;
+    for (int k = 0; k < N_SHAPES; ++k)
+      {
+        ctx->tune_ms[k] = ms[k];
+        if (ms[k] < ms[ctx->pair_shape])
+          ctx->pair_shape = k;
+      }
     ctx->pair_tuned = true;
     std::lock_guard<std::mutex> lock(tune_mutex);
-    tune_cache[key] = {ctx->pair_shape, {ms[0], ms[1]}};
+    tune_cache[key] = {ctx->pair_shape, ms};
     return LBFEM_OK;
   }
 
@@ -2936,8 +2947,8 @@ lbfem_gpu_tuning(const lbfem_gpu_ctx *ctx, int32_t *shape, float *ms)
   if (!ctx || !shape || !ms)
     return LBFEM_ERR_ARG;
   *shape = ctx->pair_tuned ? ctx->pair_shape : -1;
-  ms[0] = ctx->tune_ms[0];
-  ms[1] = ctx->tune_ms[1];
+  for (int k = 0; k < N_SHAPES; ++k)
+    ms[k] = ctx->tune_ms[k];
   return LBFEM_OK;
 }
 

@@ -386,7 +386,7 @@ namespace lbfem_gpu
   // pair by pair; PAIR_BARDOW also writes the collided deviations g* to dout.
   // Images get r = 0 (constrained rows).
   template <int P, int MODE, typename S = TileShape<P>>
-  __global__ void __launch_bounds__(THREADS, 2)
+  __global__ void __launch_bounds__(THREADS, S::MIN_CTAS)
     k_stream_pair(const Geo geo, const DevStats *__restrict__ ds, const float *__restrict__ d,
                   float *__restrict__ dout, float *__restrict__ rhs, const AdvCoef ac)
   {

@@ -1,6 +1,6 @@
-"""The run-time choice of the streaming kernel's tile (lbfem_gpu_tuning): both
-compiled shapes give bitwise the same steps, and a mixed context's first step
-times both and keeps the faster."""
+"""The run-time choice of the streaming kernel's tile (lbfem_gpu_tuning): the
+three compiled shapes give bitwise the same steps, and a mixed context's first
+step times them and keeps the fastest."""
 import ctypes as C
 import os
 
@@ -24,7 +24,7 @@ def _run(tc, m, prm, dt, steps, tune):
     try:
         h = setup_case(lbfem_gpu.Solver, tc, m, prm, dt, tc.relaxation_time())
         h.step(steps)
-        shape, ms = C.c_int32(), (C.c_float * 2)()
+        shape, ms = C.c_int32(), (C.c_float * 3)()
         h._call("tuning", h.h, C.byref(shape), ms)
         f = h.get_populations()
         h.close()
@@ -51,8 +51,9 @@ def test_tile_shapes_agree_bitwise(gpu_lib, p, case, scheme):
     dt = m.time_step(cfl)
     f0, s0, _ = _run(tc, m, prm, dt, 12, "0")
     f1, s1, _ = _run(tc, m, prm, dt, 12, "alt")
-    assert (s0, s1) == (0, 1)
-    assert np.array_equal(f0, f1)
+    f2, s2, _ = _run(tc, m, prm, dt, 12, "small")
+    assert (s0, s1, s2) == (0, 1, 2)
+    assert np.array_equal(f0, f1) and np.array_equal(f0, f2)
     ft, st, ms = _run(tc, m, prm, dt, 12, None)
-    assert st in (0, 1) and min(ms) > 0 and ms[st] == min(ms)
+    assert st in (0, 1, 2) and min(ms) > 0 and ms[st] == min(ms)
     assert np.array_equal(ft, f0)
