@@ -659,25 +659,39 @@ def batch_measure(n, steps, warmup, accuracy_steps=1000):
             total += ms.value * 1e-3
         return total
 
-    def batched(hs, more=0):
-        b = lbfem_gpu.Batch(hs)
+    def batched(hs, more=0, grouped=True):
+        # LBFEM_BATCH_GROUP is read when the batch is created
+        old = os.environ.get("LBFEM_BATCH_GROUP")
+        os.environ["LBFEM_BATCH_GROUP"] = "1" if grouped else "0"
+        try:
+            b = lbfem_gpu.Batch(hs)
+        finally:
+            if old is None:
+                del os.environ["LBFEM_BATCH_GROUP"]
+            else:
+                os.environ["LBFEM_BATCH_GROUP"] = old
         b.step(warmup)
         b.step(steps)  # returns after the device finished (one synchronisation)
         sec = b.last_ms() * 1e-3
+        launches = b.last_launches()
         if more:
             b.step(more)  # untimed: the longer run of the accuracy check
         b.close()
-        return sec
+        return sec, launches
 
     units = 9 * sum(it["mesh"].n_unique() for it in inst) * steps
     more = max(0, accuracy_steps - warmup - steps)
     hs = make()
-    t_batch = batched(hs, more)
+    t_batch, n_launch = batched(hs, more)
     f_mixed = [h.get_populations() for h in hs]  # the batched mixed run's end states
     for h in hs:
         h.close()
+    hs = make()
+    t_branches, n_launch_branches = batched(hs, grouped=False)
+    for h in hs:
+        h.close()
     hs = make(fp64=True)
-    t_batch_fp64 = batched(hs, more)
+    t_batch_fp64, _ = batched(hs, more)
     f_fp64 = [h.get_populations() for h in hs]  # the batched FP64 run (bitwise the one-at-a-time run)
     for h in hs:
         h.close()
@@ -696,6 +710,11 @@ def batch_measure(n, steps, warmup, accuracy_steps=1000):
         _, uxr, uyr = d2q9.moments(fr[:, ind])
         errs.append(float(np.linalg.norm(np.stack([uxm - uxr, uym - uyr])) / np.linalg.norm(np.stack([uxr, uyr]))))
     return {"value": units / t_batch, "ms_per_step": 1e3 * t_batch / steps, "steps": steps, "warmup": warmup,
+            "gpu_launches": n_launch,
+            "branches": {"value": units / t_branches, "ms_per_step": 1e3 * t_branches / steps,
+                         "gpu_launches": n_launch_branches,
+                         "note": "every instance a graph branch of its own step graph (LBFEM_BATCH_GROUP=0)"},
+            "gain_of_grouping": t_branches / t_batch,
             "one_at_a_time": {"value": units / t_single, "ms_per_step": 1e3 * t_single / steps},
             "speedup_vs_one_at_a_time": t_single / t_batch,
             "fp64_one_at_a_time": {"value": units / t_fp64, "ms_per_step": 1e3 * t_fp64 / steps},
@@ -709,6 +728,8 @@ def batch_measure(n, steps, warmup, accuracy_steps=1000):
             "workload": f"{n} instances (cavities and Taylor-Green vortices)",
             "nodes_distinct_total": int(sum(it["mesh"].n_unique() for it in inst)),
             "instances": [{k: it[k] for k in ("case", "edge", "p", "Re", "U0", "scheme")} for it in inst],
+            "grouping": "the mixed instances' steps run as grouped kernels, each over the tiles of all "
+                        "instances of its degree (one solver loop for all); the FP64 batch is graph branches",
             "timing": "device time: CUDA events on the batch stream around the batched graph launches; "
                       "one at a time, events on each instance's stream around its steps, summed"}
 
@@ -725,6 +746,8 @@ def run_batch(args):
                 "one_at_a_time": r["one_at_a_time"], "speedup_vs_one_at_a_time": r["speedup_vs_one_at_a_time"],
                 "fp64_one_at_a_time": r["fp64_one_at_a_time"],
                 "speedup_vs_fp64_one_at_a_time": r["speedup_vs_fp64_one_at_a_time"], "accuracy": r["accuracy"],
+                "gpu_launches": r["gpu_launches"], "branches": r["branches"],
+                "gain_of_grouping": r["gain_of_grouping"], "grouping": r["grouping"],
                 "dtype": "f32 mixed", "data": "synthetic",
                 "config": {"workload": r["workload"], "nodes_distinct_total": r["nodes_distinct_total"],
                            "instances": r["instances"]},

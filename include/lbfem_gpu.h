@@ -391,9 +391,14 @@ int lbfem_gpu_last_step_stats(const lbfem_gpu_ctx *ctx, double *cg_iterations_pe
  * Batched stepping of independent instances (contexts of any mesh, degree,
  * scheme and precision on one device). lbfem_gpu_batch_step advances every
  * instance by n_steps steps; each step of all instances is one CUDA graph
- * launch, whose independent branches are the instances' own step graphs, so
- * small instances run side by side on the GPU. Results are those of
- * lbfem_gpu_step on each context. A solver failure in any instance is returned
+ * launch. The mixed-precision instances with consistent mass and TG2
+ * streaming on Cartesian whole meshes are stepped by grouped kernels: each
+ * kernel of the step runs over the tiles of all these instances (of one
+ * degree), and the solve loops while any of them is active. Every other
+ * instance is an independent branch of the graph running its own step graph.
+ * Small instances thus share launches or run side by side on the GPU. Results
+ * are bitwise those of lbfem_gpu_step on each context (LBFEM_BATCH_GROUP=0 in
+ * the environment at batch creation makes every instance a branch). A solver failure in any instance is returned
  * (the lowest instance index, its message in lbfem_gpu_batch_last_error); that
  * instance stays as before its failing step, the others complete all steps.
  * The contexts must have their time step set and must not be stepped through
@@ -406,6 +411,8 @@ int lbfem_gpu_batch_step(lbfem_gpu_batch *batch, int32_t n_steps);
 const char *lbfem_gpu_batch_last_error(const lbfem_gpu_batch *batch);
 /* Device time (CUDA events on the batch stream) of the graph launches of the last batch_step call, in ms. */
 int lbfem_gpu_batch_last_ms(const lbfem_gpu_batch *batch, float *ms);
+/* Kernels launched by the last batch_step call, all instances and the grouped launches. */
+int lbfem_gpu_batch_last_launches(const lbfem_gpu_batch *batch, int64_t *launches);
 int lbfem_gpu_batch_destroy(lbfem_gpu_batch *batch);
 
 /*

@@ -426,10 +426,13 @@ namespace lbfem_gpu
 
   // One CTA per quantity q: out[q] = sum_b partials[q * n_blocks + b], in a fixed order.
   __global__ void
-  k_reduce_partials(const double *__restrict__ partials, int n_blocks, double *__restrict__ out)
+  k_reduce_partials(const double *__restrict__ partials, int n_blocks, double *__restrict__ out);
+
+  // Quantity q of the partials (one CTA; the body of k_reduce_partials and of its batched form).
+  __device__ __forceinline__ void
+  reduce_partials_q(const double *__restrict__ partials, int n_blocks, double *__restrict__ out, int q)
   {
     __shared__ double red[32];
-    const int q = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double s = 0;
     for (int b = threadIdx.x; b < n_blocks; b += blockDim.x)
@@ -449,6 +452,12 @@ namespace lbfem_gpu
         if (lane == 0)
           out[q] = s;
       }
+  }
+
+  __global__ void
+  k_reduce_partials(const double *__restrict__ partials, int n_blocks, double *__restrict__ out)
+  {
+    reduce_partials_q(partials, n_blocks, out, blockIdx.x);
   }
 
   // ------------------------------------------------------ asynchronous copies

@@ -8,6 +8,7 @@
 #include "stream_pair.cuh"
 #include "contraction_study.cuh"
 #include "quad.cuh"
+#include "batch_group.cuh"
 
 #include <cuda_runtime.h>
 
@@ -238,6 +239,10 @@ namespace
         (st = set_smem(ctx, k_cg_start<P, float, float, float>, cg_smem<P, float>(1))) ||
         (st = set_smem(ctx, k_cg_start<P, float, float, double>, cg_smem<P, float>(1, true))) ||
         (st = set_smem(ctx, k_window_correct<P>, window_smem<P>())) ||
+        (st = set_smem(ctx, kg_stream_pair<P, PAIR_LEELIN>, pair_smem<P, PAIR_LEELIN>())) ||
+        (st = set_smem(ctx, kg_stream_pair<P, PAIR_BARDOW>, pair_smem<P, PAIR_BARDOW>())) ||
+        (st = set_smem(ctx, kg_cg_start<P>, cg_smem<P, float>(1))) ||
+        (st = set_smem(ctx, kg_window<P>, window_smem<P>())) ||
         (st = set_smem(ctx, k_richardson_pass<P, double>, cg_smem<P, double>(0))) ||
         (st = set_smem(ctx, k_richardson_pass<P, float>, cg_smem<P, float>(0))))
       return st;
@@ -445,12 +450,29 @@ namespace
     return LBFEM_OK;
   }
 
+  FaceCoef face_coef(const lbfem_gpu_ctx *ctx, const double *e, double dt, bool remove);
+
   template <typename R>
   int
   launch_wall_faces(lbfem_gpu_ctx *ctx, const R *f, R *rhs, const double *e, double dt, bool remove)
   {
     if (ctx->n_bnodes == 0)
       return LBFEM_OK;
+    const FaceCoef fc = face_coef(ctx, e, dt, remove);
+    const Geo geo = geo_of(ctx);
+    return with_degree(ctx->P, [&](auto PP) -> int {
+      constexpr int P = decltype(PP)::value;
+      k_wall_faces<P, R><<<(ctx->n_bnodes + 127) / 128, 128, 0, ctx->stream>>>(geo, f, rhs, ctx->d_bnode,
+                                                                           ctx->n_bnodes, fc);
+      LAUNCHED();
+      return LBFEM_OK;
+    });
+  }
+
+  // The wall-face coefficients of directions e (9 x 2) and time step dt.
+  FaceCoef
+  face_coef(const lbfem_gpu_ctx *ctx, const double *e, double dt, bool remove)
+  {
     FaceCoef fc{};
     fc.half_dt2 = 0.5 * dt * dt;
     for (int al = 0; al < NM; ++al)
@@ -468,14 +490,7 @@ namespace
     fc.hx1 = ctx->ax.h_last;
     fc.hy0 = ctx->ay.h_first;
     fc.hy1 = ctx->ay.h_last;
-    const Geo geo = geo_of(ctx);
-    return with_degree(ctx->P, [&](auto PP) -> int {
-      constexpr int P = decltype(PP)::value;
-      k_wall_faces<P, R><<<(ctx->n_bnodes + 127) / 128, 128, 0, ctx->stream>>>(geo, f, rhs, ctx->d_bnode,
-                                                                           ctx->n_bnodes, fc);
-      LAUNCHED();
-      return LBFEM_OK;
-    });
+    return fc;
   }
 
   // ------------------------------------------------------ mass solve (K2-K4)
@@ -1118,18 +1133,36 @@ namespace
   // Sweep s of the front of a step: the streaming right-hand side of the sweep's
   // directions. The first sweep of Bardow collides on the fly into the other
   // population buffer; the second split sweep streams that buffer as it stands.
+  struct FrontCoef
+  {
+    double e[2 * Q]; // the sweep's directions
+    AdvCoef ac;      // the streaming right-hand side's coefficients
+    bool bardow, remove;
+  };
+
+  FrontCoef
+  front_coef(const lbfem_gpu_ctx *ctx, int sweep)
+  {
+    FrontCoef fr;
+    const double dt = ctx->dt, lam = ctx->lambda;
+    sweep_directions(ctx, sweep, fr.e);
+    const int rm = ctx->prm.remove_wall_mass_flux;
+    fr.bardow = ctx->prm.scheme == LBFEM_SCHEME_BARDOW;
+    const double b = -0.5 * dt * dt / lam;
+    fr.ac = fr.bardow ? adv_coef(-dt, 0., -0.5 * dt * dt, fr.e, dt / (lam + 0.5 * dt))
+                      : adv_coef(-dt - b, b, -0.5 * dt * dt, fr.e, 0.);
+    fr.remove = rm < 0 ? fr.bardow : rm != 0;
+    return fr;
+  }
+
   int
   step_front(lbfem_gpu_ctx *ctx, int sweep = 0)
   {
-    const double dt = ctx->dt, lam = ctx->lambda;
-    double e[2 * Q];
-    sweep_directions(ctx, sweep, e);
-    const int rm = ctx->prm.remove_wall_mass_flux;
-    const bool bardow = ctx->prm.scheme == LBFEM_SCHEME_BARDOW;
-    const double b = -0.5 * dt * dt / lam;
-    const AdvCoef ac = bardow ? adv_coef(-dt, 0., -0.5 * dt * dt, e, dt / (lam + 0.5 * dt))
-                              : adv_coef(-dt - b, b, -0.5 * dt * dt, e, 0.);
-    const bool remove = rm < 0 ? bardow : rm != 0;
+    const FrontCoef fr = front_coef(ctx, sweep);
+    const double dt = ctx->dt;
+    const double *e = fr.e;
+    const AdvCoef &ac = fr.ac;
+    const bool bardow = fr.bardow, remove = fr.remove;
     int st;
     if (ctx->mixed)
       {
@@ -3139,11 +3172,29 @@ struct lbfem_gpu_batch
     cudaGraphExec_t exec = nullptr;
     std::vector<int64_t> epochs;      // the time-step epochs of the instances it was recorded with
     std::vector<int64_t> fixed, body; // per instance: kernels outside the loops, per loop body
+    void *d_group = nullptr;          // the grouped launches' instance table and tile lists
+    int64_t group_fixed = 0, group_body = 0; // the grouped launches outside the loop, per loop body
   };
   std::map<std::vector<int>, Entry> graphs; // by the buffer states of the instances
+  // the instances stepped by grouped launches (mixed precision, consistent mass,
+  // TG2, Cartesian, whole mesh), largest first; the others are graph branches
+  std::vector<size_t> grouped;
+  cudaStream_t gstream = nullptr, gcap = nullptr; // the grouped launches' capture streams
+  static constexpr int MAX_CLASSES = 8;           // (degree, scheme) pairs
+  cudaStream_t cs[MAX_CLASSES] = {}, bs[MAX_CLASSES] = {}; // class branches outside and inside the loop
+  cudaEvent_t gfork = nullptr, gjoin = nullptr;
+  unsigned long long *d_loops = nullptr;          // loop bodies the grouped solve ran
+  unsigned long long *h_loops = nullptr;          // pinned copy
+  // LBFEM_TRACE: the grouped step is launched kernel by kernel with its loop on
+  // the host (the graph holds the other instances' branches only)
+  bool trace = false;
+  int *d_flag = nullptr;          // the host-driven loop's condition
+  void *d_trace_plan = nullptr;   // the host-driven step's argument lists
+  size_t trace_plan_bytes = 0;
   DevStats *h_stats = nullptr;              // pinned, one per instance
   cudaEvent_t t0 = nullptr, t1 = nullptr;   // device time of the last batch_step's launches
   float last_ms = 0.f;
+  int64_t last_launches = 0; // kernels launched by the last batch_step (all instances)
   std::string err;
 };
 
@@ -3169,6 +3220,338 @@ namespace
         return batch_fail(b, LBFEM_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
     }                                                                                                     \
   while (0)
+
+  // ------------------------------------------------------- grouped launches
+  // The instances whose step the grouped kernels of batch_group.cuh run.
+  bool
+  groupable(const lbfem_gpu_ctx *c)
+  {
+    return c->mixed && c->prm.mass == LBFEM_MASS_CG && n_sweeps(c) == 1 &&
+           c->prm.streaming == LBFEM_STREAMING_TG2 && !c->distorted && !c->strip;
+  }
+
+  // A class of grouped instances: one degree and one scheme, a contiguous range
+  // [i0, i1) of the instance table, and the (instance, tile) or (instance, node
+  // chunk) references of its launches (instance indices into the whole table).
+  struct GroupClass
+  {
+    int P = 1, mode = PAIR_LEELIN;
+    int i0 = 0, i1 = 0;
+    size_t pair_off = 0, wall_off = 0, start_off = 0, win_off = 0, chunk_off = 0;
+    int pair_n = 0;  // streaming tiles (Tile<P>)
+    int wall_n = 0;  // (instance, first boundary node) per 128 wall nodes
+    int start_n = 0; // start tiles (Tile<P>)
+    int win_n = 0;   // window tiles (WinShape<P>)
+    int chunk_n = 0; // node chunks of GROUP_CHUNK nodes
+  };
+
+  // The argument lists of the grouped launches for the instances' current
+  // buffer states, laid out for one device allocation: the instance table
+  // (sorted by class, largest instances first within a class), then the
+  // reference lists of every class.
+  struct GroupPlan
+  {
+    std::vector<unsigned char> bytes;
+    int n = 0;      // instances
+    size_t tab = 0; // offset of the instance table
+    std::vector<GroupClass> cls;
+  };
+
+  template <typename T>
+  size_t
+  plan_put(std::vector<unsigned char> &bytes, const std::vector<T> &v)
+  {
+    const size_t off = (bytes.size() + 15) & ~size_t(15);
+    bytes.resize(off + sizeof(T) * v.size());
+    if (!v.empty())
+      std::memcpy(bytes.data() + off, v.data(), sizeof(T) * v.size());
+    return off;
+  }
+
+  // The arguments of the instances b->grouped, as record_step would pass them
+  // to the single-instance kernels of a mixed-precision step (step_front,
+  // mixed_graph, step_back).
+  GroupPlan
+  group_plan(const lbfem_gpu_batch *b)
+  {
+    GroupPlan gp;
+    std::vector<size_t> idx = b->grouped; // largest first
+    auto class_of = [&](size_t k) {
+      const lbfem_gpu_ctx *c = b->ctxs[k];
+      return 2 * c->P + (c->prm.scheme == LBFEM_SCHEME_BARDOW ? 1 : 0);
+    };
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t x, size_t y) { return class_of(x) < class_of(y); });
+    gp.n = int(idx.size());
+    std::vector<GroupInst> tab(idx.size());
+    struct Lists
+    {
+      std::vector<TileRef> pair, start, win;
+      std::vector<int2> wall, chunks;
+    };
+    std::vector<Lists> lists;
+    for (size_t j = 0; j < idx.size(); ++j)
+      {
+        const lbfem_gpu_ctx *c = b->ctxs[idx[j]];
+        const FrontCoef fr = front_coef(c, 0);
+        const int k = int(j), mode = fr.bardow ? PAIR_BARDOW : PAIR_LEELIN;
+        GroupInst &I = tab[j];
+        I.geo = geo_of(c);
+        I.ds = c->d_stats;
+        I.ac = fr.ac;
+        I.fc = face_coef(c, fr.e, c->dt, fr.remove);
+        I.bnode = c->d_bnode;
+        I.n_bnodes = int(c->n_bnodes);
+        I.bardow = fr.bardow ? 1 : 0;
+        I.f = c->d_fs[c->cur];
+        I.g = fr.bardow ? c->d_fs[1 - c->cur] : nullptr;
+        I.rhs = c->d_rhs_s;
+        I.xc = c->d_x_s[c->x_cur];
+        I.xp = c->d_x_s[c->x_prev];
+        I.xn = c->d_x_s[c->x_new];
+        I.r0 = c->d_r_s;
+        I.r1 = c->d_p_s[0];
+        I.winx = c->d_winx;
+        I.winy = c->d_winy;
+        I.cg = c->d_cg;
+        I.partials = c->d_partials;
+        I.sums = c->d_sums;
+        I.tol = mixed_tolerance(c->prm);
+        I.max_rounds = c->prm.cg_max_iterations;
+        I.theta = c->dt / c->lambda;
+        I.N = c->grid.N;
+        with_degree(c->P, [&](auto PP) -> int {
+          constexpr int P = decltype(PP)::value;
+          const dim3 tg = tile_grid<P>(c->grid);
+          using S = WinShape<P>;
+          I.nb_start_x = int(tg.x);
+          I.nb_start_y = int(tg.y);
+          I.nb_win_x = (c->grid.nfx + S::TX - 1) / S::TX;
+          I.nb_win_y = (c->grid.nfy + S::TY - 1) / S::TY;
+          return 0;
+        });
+        if (gp.cls.empty() || gp.cls.back().P != c->P || gp.cls.back().mode != mode)
+          {
+            GroupClass gc;
+            gc.P = c->P;
+            gc.mode = mode;
+            gc.i0 = k;
+            gp.cls.push_back(gc);
+            lists.emplace_back();
+          }
+        gp.cls.back().i1 = k + 1;
+        Lists &L = lists.back();
+        for (int by = 0; by < I.nb_start_y; ++by)
+          for (int bx = 0; bx < I.nb_start_x; ++bx)
+            {
+              L.pair.push_back({k, bx, by});
+              L.start.push_back({k, bx, by});
+            }
+        for (int by = 0; by < I.nb_win_y; ++by)
+          for (int bx = 0; bx < I.nb_win_x; ++bx)
+            L.win.push_back({k, bx, by});
+        for (int t = 0; t < I.n_bnodes; t += 128)
+          L.wall.push_back(make_int2(k, t));
+        for (long long ch = 0; ch * GROUP_CHUNK < I.N; ++ch)
+          L.chunks.push_back(make_int2(k, int(ch)));
+      }
+    gp.tab = plan_put(gp.bytes, tab);
+    for (size_t q = 0; q < gp.cls.size(); ++q)
+      {
+        GroupClass &gc = gp.cls[q];
+        const Lists &L = lists[q];
+        gc.pair_off = plan_put(gp.bytes, L.pair);
+        gc.pair_n = int(L.pair.size());
+        gc.wall_off = plan_put(gp.bytes, L.wall);
+        gc.wall_n = int(L.wall.size());
+        gc.start_off = plan_put(gp.bytes, L.start);
+        gc.start_n = int(L.start.size());
+        gc.win_off = plan_put(gp.bytes, L.win);
+        gc.win_n = int(L.win.size());
+        gc.chunk_off = plan_put(gp.bytes, L.chunks);
+        gc.chunk_n = int(L.chunks.size());
+      }
+    return gp;
+  }
+
+  // The grouped step of the instances b->grouped: the kernel sequence of
+  // record_step for a mixed-precision step, each kernel over the tiles of all
+  // instances of one class (degree and scheme). The classes run as concurrent
+  // branches (streams b->cs, and b->bs inside the loop body) that join only for
+  // the loop condition, so the launches of small classes overlap. The solve's
+  // loop runs while any instance is active; a round of an instance that has
+  // stopped carries its solution and residual over and counts nothing (the
+  // single-instance loop's bodies after convergence), so each instance's
+  // results are those of its own step. Recorded on b->gstream, which is being
+  // captured, with the loop as a conditional WHILE node; or (host_driven)
+  // launched from b->stream with the loop on the host, which reads the loop
+  // condition after every body (the path of LBFEM_TRACE, whose kernels
+  // profilers can see one by one). *fixed, *body: the kernels outside the loop
+  // and per loop body.
+  int
+  record_group(lbfem_gpu_batch *b, const GroupPlan &gp, const void *d_plan, bool host_driven, int64_t *fixed,
+               int64_t *body)
+  {
+    const unsigned char *base = static_cast<const unsigned char *>(d_plan);
+    const GroupInst *tab = reinterpret_cast<const GroupInst *>(base + gp.tab);
+    auto tiles = [&](size_t off) { return reinterpret_cast<const TileRef *>(base + off); };
+    auto refs = [&](size_t off) { return reinterpret_cast<const int2 *>(base + off); };
+    cudaStream_t s = host_driven ? b->stream : b->gstream;
+    const int nc = int(gp.cls.size());
+    int64_t n_fixed = 0, n_body = 0;
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t graph = nullptr;
+    cudaGraphConditionalHandle h = 0;
+    if (!host_driven)
+      {
+        BCK(cudaStreamGetCaptureInfo_v3(s, &cs, nullptr, &graph, nullptr, nullptr, nullptr));
+        BCK(cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault)); // 0 at every launch
+      }
+    const int use_h = host_driven ? 0 : 1;
+    int *flag = host_driven ? b->d_flag : nullptr;
+
+    // the class streams q[0..nc) wait for the work queued on `from`; `to` waits for theirs
+    auto fork = [&](cudaStream_t from, cudaStream_t *q) -> cudaError_t {
+      cudaError_t e = cudaEventRecord(b->gfork, from);
+      for (int c = 0; c < nc && e == cudaSuccess; ++c)
+        e = cudaStreamWaitEvent(q[c], b->gfork, 0);
+      return e;
+    };
+    auto join = [&](cudaStream_t *q, cudaStream_t to) -> cudaError_t {
+      cudaError_t e = cudaSuccess;
+      for (int c = 0; c < nc && e == cudaSuccess; ++c)
+        if ((e = cudaEventRecord(b->gjoin, q[c])) == cudaSuccess)
+          e = cudaStreamWaitEvent(to, b->gjoin, 0);
+      return e;
+    };
+    // one round of the mixed solve for class gc on stream q: the window
+    // correction (phase: the buffer roles of kg_window), the sums, the bookkeeping
+    auto round = [&](const GroupClass &gc, cudaStream_t q, int phase, int all) -> int64_t {
+      with_degree(gc.P, [&](auto PP) -> int {
+        constexpr int P = decltype(PP)::value;
+        kg_window<P><<<dim3(gc.win_n, NM), WinShape<P>::THREADS, window_smem<P>(), q>>>(tab, tiles(gc.win_off),
+                                                                                       phase, all);
+        return 0;
+      });
+      kg_reduce<<<(gc.i1 - gc.i0) * 2 * NM, 256, 0, q>>>(tab + gc.i0, 2 * NM);
+      kg_mixed_round<<<gc.i1 - gc.i0, 32, 0, q>>>(tab + gc.i0);
+      return 3;
+    };
+
+    // per class: the front (step_front), the solve's start, round 0 and the zero
+    // rule (mixed_graph); then the loop condition of all classes
+    kg_clear<<<gp.n, 64, 0, s>>>(tab);
+    ++n_fixed;
+    BCK(cudaGetLastError());
+    BCK(fork(s, b->cs));
+    for (int c = 0; c < nc; ++c)
+      {
+        const GroupClass &gc = gp.cls[c];
+        cudaStream_t q = b->cs[c];
+        with_degree(gc.P, [&](auto PP) -> int {
+          constexpr int P = decltype(PP)::value;
+          if (gc.mode == PAIR_BARDOW)
+            kg_stream_pair<P, PAIR_BARDOW><<<gc.pair_n, THREADS, pair_smem<P, PAIR_BARDOW>(), q>>>(
+              tab, tiles(gc.pair_off));
+          else
+            kg_stream_pair<P, PAIR_LEELIN><<<gc.pair_n, THREADS, pair_smem<P, PAIR_LEELIN>(), q>>>(
+              tab, tiles(gc.pair_off));
+          if (gc.wall_n)
+            kg_wall_faces<P><<<gc.wall_n, 128, 0, q>>>(tab, refs(gc.wall_off));
+          kg_cg_start<P><<<dim3(gc.start_n, NM), THREADS, cg_smem<P, float>(1), q>>>(tab, tiles(gc.start_off));
+          return 0;
+        });
+        n_fixed += gc.wall_n ? 3 : 2;
+        n_fixed += round(gc, q, 0, 1);
+        kg_zero<<<dim3(gc.chunk_n, NM), THREADS, 0, q>>>(tab, refs(gc.chunk_off));
+        ++n_fixed;
+      }
+    BCK(cudaGetLastError());
+    BCK(join(b->cs, s));
+    kg_control<<<1, 256, 0, s>>>(tab, gp.n, h, use_h, nullptr, flag);
+    ++n_fixed;
+    BCK(cudaGetLastError());
+
+    // the loop: one body is two rounds of every class (x_prev -> x_new -> x_prev)
+    if (host_driven)
+      {
+        int any = 0;
+        for (;;)
+          {
+            BCK(cudaMemcpyAsync(&any, b->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+            BCK(cudaStreamSynchronize(s));
+            if (!any)
+              break;
+            BCK(fork(s, b->cs));
+            n_body = 1;
+            for (int c = 0; c < nc; ++c)
+              n_body += round(gp.cls[c], b->cs[c], 1, 0) + round(gp.cls[c], b->cs[c], 0, 0);
+            BCK(cudaGetLastError());
+            BCK(join(b->cs, s));
+            kg_control<<<1, 256, 0, s>>>(tab, gp.n, h, 0, b->d_loops, flag);
+            BCK(cudaGetLastError());
+          }
+      }
+    else
+      {
+        const cudaGraphNode_t *deps = nullptr;
+        size_t nd = 0;
+        BCK(cudaStreamGetCaptureInfo_v3(s, &cs, nullptr, &graph, &deps, nullptr, &nd));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        BCK(cudaGraphAddNode(&node, graph, deps, nd, &np));
+        BCK(cudaStreamBeginCaptureToGraph(b->gcap, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal));
+        cudaError_t le = fork(b->gcap, b->bs);
+        n_body = 1;
+        for (int c = 0; c < nc && le == cudaSuccess; ++c)
+          n_body += round(gp.cls[c], b->bs[c], 1, 0) + round(gp.cls[c], b->bs[c], 0, 0);
+        if (le == cudaSuccess)
+          le = cudaGetLastError();
+        if (le == cudaSuccess)
+          le = join(b->bs, b->gcap);
+        if (le == cudaSuccess)
+          {
+            kg_control<<<1, 256, 0, b->gcap>>>(tab, gp.n, h, 1, b->d_loops, nullptr);
+            le = cudaGetLastError();
+          }
+        cudaGraph_t bg = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(b->gcap, &bg);
+        BCK(le);
+        BCK(ee);
+        BCK(cudaStreamUpdateCaptureDependencies_v2(s, &node, nullptr, 1, cudaStreamSetCaptureDependencies));
+      }
+
+    // per class: the nodal update (step_back)
+    BCK(fork(s, b->cs));
+    for (int c = 0; c < nc; ++c)
+      {
+        const GroupClass &gc = gp.cls[c];
+        if (gc.mode == PAIR_BARDOW)
+          kg_nodal<PAIR_BARDOW><<<gc.chunk_n, THREADS, 0, b->cs[c]>>>(tab, refs(gc.chunk_off));
+        else
+          kg_nodal<PAIR_LEELIN><<<gc.chunk_n, THREADS, 0, b->cs[c]>>>(tab, refs(gc.chunk_off));
+        ++n_fixed;
+      }
+    BCK(cudaGetLastError());
+    BCK(join(b->cs, s));
+    *fixed = n_fixed;
+    *body = n_body;
+    return LBFEM_OK;
+  }
+
+  bool
+  create_class_streams(lbfem_gpu_batch *b)
+  {
+    for (int c = 0; c < lbfem_gpu_batch::MAX_CLASSES; ++c)
+      if (cudaStreamCreateWithFlags(&b->cs[c], cudaStreamNonBlocking) != cudaSuccess ||
+          cudaStreamCreateWithFlags(&b->bs[c], cudaStreamNonBlocking) != cudaSuccess)
+        return false;
+    return true;
+  }
 
   // The batch graph of the instances' current buffer states: one capture in
   // which every instance's step is recorded on its own stream, forked from and
@@ -3197,9 +3580,33 @@ namespace
       }
     e.fixed.assign(b->ctxs.size(), 0);
     e.body.assign(b->ctxs.size(), 0);
+    GroupPlan gp;
+    const bool group = !b->grouped.empty() && !b->trace;
+    if (group)
+      {
+        // the argument lists of the grouped launches, uploaded before the capture
+        if (e.d_group)
+          {
+            BCK(cudaStreamSynchronize(b->stream)); // a launch of the previous graph may still read them
+            BCK(cudaFree(e.d_group));
+            e.d_group = nullptr;
+          }
+        gp = group_plan(b);
+        BCK(cudaMalloc(&e.d_group, gp.bytes.size()));
+        BCK(cudaMemcpy(e.d_group, gp.bytes.data(), gp.bytes.size(), cudaMemcpyHostToDevice));
+      }
+    std::vector<char> in_group(b->ctxs.size(), 0);
+    for (size_t k : b->grouped)
+      in_group[k] = 1;
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     int st = LBFEM_OK;
     cudaError_t ce = cudaEventRecord(b->fork, b->stream);
+    if (ce == cudaSuccess && group && (ce = cudaStreamWaitEvent(b->gstream, b->fork, 0)) == cudaSuccess)
+      {
+        st = record_group(b, gp, e.d_group, false, &e.group_fixed, &e.group_body);
+        if (!st && (ce = cudaEventRecord(b->join, b->gstream)) == cudaSuccess)
+          ce = cudaStreamWaitEvent(b->stream, b->join, 0);
+      }
     // the largest instances are recorded first, so that their branches start first;
     // results and failure indices stay those of the instance order
     std::vector<size_t> order(b->ctxs.size());
@@ -3210,6 +3617,8 @@ namespace
     for (size_t o = 0; o < order.size() && !st && ce == cudaSuccess; ++o)
       {
         const size_t k = order[o];
+        if (in_group[k])
+          continue;
         lbfem_gpu_ctx *c = b->ctxs[k];
         ce = cudaStreamWaitEvent(c->stream, b->fork, 0);
         if (ce != cudaSuccess)
@@ -3267,11 +3676,31 @@ lbfem_gpu_batch_create(lbfem_gpu_ctx *const *ctxs, int32_t n, lbfem_gpu_batch **
   auto b = std::make_unique<lbfem_gpu_batch>();
   b->device = ctxs[0]->device;
   b->ctxs.assign(ctxs, ctxs + n);
+  b->trace = std::getenv("LBFEM_TRACE") != nullptr;
+  // LBFEM_BATCH_GROUP=0 steps every instance as a graph branch of its own
+  const char *genv = std::getenv("LBFEM_BATCH_GROUP");
+  if (!(genv && genv[0] == '0'))
+    {
+      for (int k = 0; k < n; ++k)
+        if (groupable(ctxs[k]))
+          b->grouped.push_back(size_t(k));
+      // largest first: their tiles lead the grouped launches' lists
+      std::stable_sort(b->grouped.begin(), b->grouped.end(),
+                       [&](size_t x, size_t y) { return ctxs[x]->grid.N > ctxs[y]->grid.N; });
+    }
   if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->gstream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->gcap, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->gfork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->gjoin, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&b->t0) != cudaSuccess || cudaEventCreate(&b->t1) != cudaSuccess ||
-      cudaHostAlloc(&b->h_stats, sizeof(DevStats) * n, cudaHostAllocDefault) != cudaSuccess)
+      cudaHostAlloc(&b->h_stats, sizeof(DevStats) * n, cudaHostAllocDefault) != cudaSuccess ||
+      cudaHostAlloc(&b->h_loops, sizeof(unsigned long long), cudaHostAllocDefault) != cudaSuccess ||
+      cudaMalloc(&b->d_loops, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMemset(b->d_loops, 0, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&b->d_flag, sizeof(int)) != cudaSuccess || !create_class_streams(b.get()))
     {
       cudaGetLastError();
       lbfem_gpu_batch_destroy(b.release());
@@ -3297,6 +3726,15 @@ lbfem_gpu_batch_last_ms(const lbfem_gpu_batch *b, float *ms)
 }
 
 int
+lbfem_gpu_batch_last_launches(const lbfem_gpu_batch *b, int64_t *launches)
+{
+  if (!b || !launches)
+    return LBFEM_ERR_ARG;
+  *launches = b->last_launches;
+  return LBFEM_OK;
+}
+
+int
 lbfem_gpu_batch_destroy(lbfem_gpu_batch *b)
 {
   if (!b)
@@ -3305,10 +3743,37 @@ lbfem_gpu_batch_destroy(lbfem_gpu_batch *b)
   if (b->stream)
     cudaStreamSynchronize(b->stream);
   for (auto &kv : b->graphs)
-    if (kv.second.exec)
-      cudaGraphExecDestroy(kv.second.exec);
+    {
+      if (kv.second.exec)
+        cudaGraphExecDestroy(kv.second.exec);
+      if (kv.second.d_group)
+        cudaFree(kv.second.d_group);
+    }
   if (b->h_stats)
     cudaFreeHost(b->h_stats);
+  if (b->h_loops)
+    cudaFreeHost(b->h_loops);
+  if (b->d_loops)
+    cudaFree(b->d_loops);
+  if (b->d_flag)
+    cudaFree(b->d_flag);
+  if (b->d_trace_plan)
+    cudaFree(b->d_trace_plan);
+  if (b->gstream)
+    cudaStreamDestroy(b->gstream);
+  if (b->gcap)
+    cudaStreamDestroy(b->gcap);
+  for (int c = 0; c < lbfem_gpu_batch::MAX_CLASSES; ++c)
+    {
+      if (b->cs[c])
+        cudaStreamDestroy(b->cs[c]);
+      if (b->bs[c])
+        cudaStreamDestroy(b->bs[c]);
+    }
+  if (b->gfork)
+    cudaEventDestroy(b->gfork);
+  if (b->gjoin)
+    cudaEventDestroy(b->gjoin);
   if (b->fork)
     cudaEventDestroy(b->fork);
   if (b->join)
@@ -3337,7 +3802,8 @@ lbfem_gpu_batch_step(lbfem_gpu_batch *b, int32_t n_steps)
       lbfem_gpu_ctx *c = b->ctxs[k];
       if (!c->have_ts)
         return batch_fail(b, LBFEM_ERR_STATE, "instance %zu: step needs the time step", k);
-      if (tune_pair(c) != LBFEM_OK)
+      // (the grouped launches use the default streaming tile)
+      if (std::find(b->grouped.begin(), b->grouped.end(), k) == b->grouped.end() && tune_pair(c) != LBFEM_OK)
         return batch_fail(b, LBFEM_ERR_CUDA, "instance %zu: %s", k, c->err.c_str());
       // the instance's own queued work first, then its counters
       BCK(cudaStreamSynchronize(c->stream));
@@ -3346,26 +3812,60 @@ lbfem_gpu_batch_step(lbfem_gpu_batch *b, int32_t n_steps)
   std::vector<RunStart> r0;
   for (size_t k = 0; k < n; ++k)
     r0.push_back(run_start(b->ctxs[k], b->h_stats[k]));
+  BCK(cudaMemcpyAsync(b->h_loops, b->d_loops, sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  const unsigned long long loops0 = *b->h_loops;
+  int64_t group_fixed = 0, group_body = 0; // kernels of the grouped launches
   BCK(cudaEventRecord(b->t0, b->stream));
   for (int s = 0; s < n_steps; ++s)
     {
-      lbfem_gpu_batch::Entry *e;
       int st;
-      if ((st = batch_graph(b, &e)))
-        return st;
-      BCK(cudaGraphLaunch(e->exec, b->stream));
-      for (size_t k = 0; k < n; ++k)
+      if (!b->trace || b->grouped.size() < n)
         {
-          r0[k].fixed += e->fixed[k];
-          r0[k].body = e->body[k];
-          rotate_after_step(b->ctxs[k]);
+          lbfem_gpu_batch::Entry *e;
+          if ((st = batch_graph(b, &e)))
+            return st;
+          BCK(cudaGraphLaunch(e->exec, b->stream));
+          group_fixed += e->group_fixed;
+          group_body = e->group_body;
+          for (size_t k = 0; k < n; ++k)
+            {
+              r0[k].fixed += e->fixed[k];
+              r0[k].body = e->body[k];
+            }
         }
+      if (b->trace && !b->grouped.empty())
+        {
+          const GroupPlan gp = group_plan(b);
+          if (gp.bytes.size() > b->trace_plan_bytes)
+            {
+              BCK(cudaStreamSynchronize(b->stream));
+              if (b->d_trace_plan)
+                BCK(cudaFree(b->d_trace_plan));
+              b->d_trace_plan = nullptr;
+              BCK(cudaMalloc(&b->d_trace_plan, gp.bytes.size()));
+              b->trace_plan_bytes = gp.bytes.size();
+            }
+          // the previous step's launches read the table until the stream gets here
+          BCK(cudaMemcpyAsync(b->d_trace_plan, gp.bytes.data(), gp.bytes.size(), cudaMemcpyHostToDevice, b->stream));
+          BCK(cudaStreamSynchronize(b->stream));
+          int64_t f = 0, bd = 0;
+          if ((st = record_group(b, gp, b->d_trace_plan, true, &f, &bd)))
+            return st;
+          group_fixed += f;
+          if (bd)
+            group_body = bd;
+        }
+      for (size_t k = 0; k < n; ++k)
+        rotate_after_step(b->ctxs[k]);
     }
   BCK(cudaEventRecord(b->t1, b->stream));
   for (size_t k = 0; k < n; ++k)
     BCK(cudaMemcpyAsync(&b->h_stats[k], b->ctxs[k]->d_stats, sizeof(DevStats), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaMemcpyAsync(b->h_loops, b->d_loops, sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->stream));
   BCK(cudaStreamSynchronize(b->stream));
   BCK(cudaEventElapsedTime(&b->last_ms, b->t0, b->t1));
+  b->last_launches = group_fixed + int64_t(*b->h_loops - loops0) * group_body;
   int first = LBFEM_OK;
   for (size_t k = 0; k < n; ++k)
     {
@@ -3374,7 +3874,8 @@ lbfem_gpu_batch_step(lbfem_gpu_batch *b, int32_t n_steps)
       const int st = finish_run(c, r0[k], b->h_stats[k], &its, &launched);
       c->cg_its += its;
       c->launches += launched;
-      c->last_launches = launched;
+      c->last_launches = launched; // 0 for a grouped instance (its kernels are the grouped launches)
+      b->last_launches += launched;
       c->last_its_per_solve = n_steps > 0 ? double(its) / (double(n_steps) * NM) : 0.0;
       if (st && first == LBFEM_OK)
         {

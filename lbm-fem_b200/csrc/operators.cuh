@@ -160,15 +160,11 @@ namespace lbfem_gpu
   //   feq_a(fhat) - feq_a(f) = w_a (d rho + 3 e.dJ + 4.5 d[(e.J)^2 / rho] - 1.5 d[J.J / rho]),
   // each difference written out in the small changes. No difference of two
   // O(1e-2) equilibria is rounded (the reason the corrector once ran in FP64).
-  __global__ void __launch_bounds__(THREADS, 4)
-  k_predictor_corrector_dev(const Geo geo, DevStats *__restrict__ ds, float *__restrict__ d,
-                            const float *__restrict__ x, double theta)
+  // Node i of the kernel below (also the body of its batched form).
+  __device__ __forceinline__ void
+  pc_dev_node(const Geo &geo, float *__restrict__ d, const float *__restrict__ x, float th, float inv, long long i)
   {
-    if (step_skipped(ds))
-      return;
     const long long N = geo.g.N;
-    const float th = float(theta), inv = float(1. / (1. + theta));
-    LBFEM_GRID_STRIDE(i, N)
     {
       float di[Q], xa[Q];
 #pragma unroll
@@ -217,6 +213,17 @@ namespace lbfem_gpu
           d[a * N + i] = di[a] + fmaf(th, float(c_W[a]) * dq, up);
         }
     }
+  }
+
+  __global__ void __launch_bounds__(THREADS, 4)
+  k_predictor_corrector_dev(const Geo geo, DevStats *__restrict__ ds, float *__restrict__ d,
+                            const float *__restrict__ x, double theta)
+  {
+    if (step_skipped(ds))
+      return;
+    const float th = float(theta), inv = float(1. / (1. + theta));
+    LBFEM_GRID_STRIDE(i, geo.g.N)
+    pc_dev_node(geo, d, x, th, inv, i);
   }
 
   // Bardow's initial transform on deviations: d + scale (d - (feq - w)).
@@ -966,12 +973,15 @@ namespace lbfem_gpu
   template <int P, typename R>
   __global__ void
   k_wall_faces(const Geo geo, const R *__restrict__ f, R *__restrict__ rhs, const int4 *__restrict__ bnode,
-               int n_bnodes, const FaceCoef fc)
+               int n_bnodes, const FaceCoef fc);
+
+  // Boundary node t of the kernel below (also the body of its batched form).
+  template <int P, typename R>
+  __device__ __forceinline__ void
+  wall_face_node(const Geo &geo, const R *__restrict__ f, R *__restrict__ rhs, const int4 *__restrict__ bnode,
+                 const FaceCoef &fc, int t)
   {
     constexpr int K = 2 * P + 1;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_bnodes)
-      return;
     const Grid &g = geo.g;
     const long long N = g.N;
     const int4 bn = bnode[t];
@@ -1040,6 +1050,16 @@ namespace lbfem_gpu
 #pragma unroll
     for (int al = 0; al < NM; ++al)
       rhs[al * N + idx] = R(double(rhs[al * N + idx]) + Rs[al]);
+  }
+
+  template <int P, typename R>
+  __global__ void
+  k_wall_faces(const Geo geo, const R *__restrict__ f, R *__restrict__ rhs, const int4 *__restrict__ bnode,
+               int n_bnodes, const FaceCoef fc)
+  {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n_bnodes)
+      wall_face_node<P, R>(geo, f, rhs, bnode, fc, t);
   }
 
   // ------------------------------------------------------ mass matrix (K2)
@@ -1550,11 +1570,13 @@ namespace lbfem_gpu
   // FP32 storage and the register-bound TG3 / Laplace operators stage b in shared
   // memory (the FP32 start runs 8 CTAs per SM at 32 registers); the FP64 mass start
   // reads it in place, which leaves room for 6 CTAs per SM.
-  template <int P, typename R, typename X = R, typename A = R, int OPK = OPK_MASS>
-  __global__ void __launch_bounds__(THREADS, OPK != OPK_MASS ? 2 : sizeof(R) == sizeof(float) ? 8 : 6)
-    k_cg_start(const Geo geo, const R *__restrict__ b, const X *__restrict__ x_cur, const X *__restrict__ x_prev,
-               X *__restrict__ x_new, R *__restrict__ r, int extrapolate, double *__restrict__ partials,
-               const StreamCoef sc, int skip)
+  // Tile (bx, by) of system bz, of an nbx x nby tile grid (the kernel below, and
+  // the body of its batched form).
+  template <int P, typename R, typename X, typename A, int OPK>
+  __device__ __forceinline__ void
+  cg_start_tile(const Geo &geo, const R *__restrict__ b, const X *__restrict__ x_cur, const X *__restrict__ x_prev,
+                X *__restrict__ x_new, R *__restrict__ r, int extrapolate, double *__restrict__ partials,
+                const StreamCoef &sc, int skip, int bx, int by, int bz, int nbx, int nby)
   {
     using T = Tile<P>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -1563,18 +1585,18 @@ namespace lbfem_gpu
     __shared__ TileMaps<P, A> maps;
     const Grid &g = geo.g;
     const long long N = g.N;
-    const int s = blockIdx.z;
+    const int s = bz;
     if ((skip >> s) & 1)
       {
         if (threadIdx.x == 0)
           {
-            const int nt = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
+            const int nt = nbx * nby, tile = by * nbx + bx;
             for (int q = 0; q < 3; ++q)
               partials[(long long)(q * NM + s) * nt + tile] = 0.0;
           }
         return;
       }
-    const int gx0 = blockIdx.x * T::TX, gy0 = blockIdx.y * T::TY;
+    const int gx0 = bx * T::TX, gy0 = by * T::TY;
     build_maps<P>(maps, geo, gx0, gy0);
     __syncthreads();
     const long long o = s * N;
@@ -1618,10 +1640,20 @@ namespace lbfem_gpu
     });
     if constexpr (SUMS)
       {
-        const int nt = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
+        const int nt = nbx * nby, tile = by * nbx + bx;
         // partial (quantity k of system s) at [(k*NM + s) * n_tiles + tile]
         block_reduce_store<3>(part, partials + (long long)s * nt, tile, NM * nt);
       }
+  }
+
+  template <int P, typename R, typename X = R, typename A = R, int OPK = OPK_MASS>
+  __global__ void __launch_bounds__(THREADS, OPK != OPK_MASS ? 2 : sizeof(R) == sizeof(float) ? 8 : 6)
+    k_cg_start(const Geo geo, const R *__restrict__ b, const X *__restrict__ x_cur, const X *__restrict__ x_prev,
+               X *__restrict__ x_new, R *__restrict__ r, int extrapolate, double *__restrict__ partials,
+               const StreamCoef sc, int skip)
+  {
+    cg_start_tile<P, R, X, A, OPK>(geo, b, x_cur, x_prev, x_new, r, extrapolate, partials, sc, skip, blockIdx.x,
+                                   blockIdx.y, blockIdx.z, gridDim.x, gridDim.y);
   }
 
   // p <- D^{-1} r + beta p (p <- D^{-1} r on the first iteration); partial p.Ap. One system per CTA.
@@ -1910,11 +1942,11 @@ namespace lbfem_gpu
   // round in the same buffers. x and r are never updated in place (the halos
   // read the inputs). Periodic images have identity rows.
   template <int P>
-  __global__ void __launch_bounds__(WinShape<P>::THREADS, WinShape<P>::MIN_CTAS)
-    k_window_correct(const Geo geo, const float *__restrict__ lx, const float *__restrict__ ly,
-                     const float *__restrict__ r_in, const float *__restrict__ x_in, const float *__restrict__ b,
-                     float *__restrict__ x_out, float *__restrict__ r_out, const CgState *__restrict__ st, int all,
-                     double *__restrict__ partials)
+  __device__ __forceinline__ void
+  window_correct_tile(const Geo &geo, const float *__restrict__ lx, const float *__restrict__ ly,
+                      const float *__restrict__ r_in, const float *__restrict__ x_in, const float *__restrict__ b,
+                      float *__restrict__ x_out, float *__restrict__ r_out, const CgState *__restrict__ st, int all,
+                      double *__restrict__ partials, int bx, int by, int bz, int nbx, int nby)
   {
     using S = WinShape<P>;
     constexpr int W = S::W, FX = S::FX, FY = S::FY, PF = S::PF, NC = S::NC, K = S::K, NT = S::THREADS;
@@ -1924,12 +1956,12 @@ namespace lbfem_gpu
     __shared__ __align__(16) float s_lx[FX * NC], s_ly[FY * NC];     // factors (apart from the window: no aliasing)
     __shared__ int s_col[FX], s_row[FY];                             // storage column / row, -1 outside the grid
     __shared__ int s_rowoff[FY];                                     // storage offset of a window row, -1 outside
-    const int s = blockIdx.z;
+    const int s = bz;
     const Grid &g = geo.g;
     const long long N = g.N;
-    const int gx0 = blockIdx.x * S::TX, gy0 = blockIdx.y * S::TY;
+    const int gx0 = bx * S::TX, gy0 = by * S::TY;
     const int tid = threadIdx.x;
-    const int n_tiles = gridDim.x * gridDim.y, tile = blockIdx.y * gridDim.x + blockIdx.x;
+    const int n_tiles = nbx * nby, tile = by * nbx + bx;
     const float *rs = r_in + (long long)s * N, *xs = x_in + (long long)s * N, *bs = b + (long long)s * N;
     float *xo = x_out + (long long)s * N, *ro = r_out + (long long)s * N;
     double part[2] = {0, 0};
@@ -1950,7 +1982,7 @@ namespace lbfem_gpu
         block_reduce_store_n<2, NT>(part, partials + (long long)s * n_tiles, tile, NM * n_tiles);
         return;
       }
-    const float *lxt = lx + (size_t)blockIdx.x * FX * NC, *lyt = ly + (size_t)blockIdx.y * FY * NC;
+    const float *lxt = lx + (size_t)bx * FX * NC, *lyt = ly + (size_t)by * FY * NC;
     for (int t = tid; t < FX * NC; t += NT)
       s_lx[t] = lxt[t];
     for (int t = tid; t < FY * NC; t += NT)
@@ -2115,6 +2147,17 @@ namespace lbfem_gpu
     block_reduce_store_n<2, NT>(part, partials + (long long)s * n_tiles, tile, NM * n_tiles);
   }
 
+  template <int P>
+  __global__ void __launch_bounds__(WinShape<P>::THREADS, WinShape<P>::MIN_CTAS)
+    k_window_correct(const Geo geo, const float *__restrict__ lx, const float *__restrict__ ly,
+                     const float *__restrict__ r_in, const float *__restrict__ x_in, const float *__restrict__ b,
+                     float *__restrict__ x_out, float *__restrict__ r_out, const CgState *__restrict__ st, int all,
+                     double *__restrict__ partials)
+  {
+    window_correct_tile<P>(geo, lx, ly, r_in, x_in, b, x_out, r_out, st, all, partials, blockIdx.x, blockIdx.y,
+                           blockIdx.z, gridDim.x, gridDim.y);
+  }
+
   // The scalar work of one CG phase, one thread per system, from the reduced sums.
   // phase 0 (after start): sums = [bb, rr, rz]; phase 1 (after p): [pAp];
   // phase 2 (after update): [rr, rz].
@@ -2216,9 +2259,9 @@ namespace lbfem_gpu
   // active residual means the tolerance lies below the FP32 resolution of the
   // solution (status 4); round max_rounds is the cap (status 2). Corrections
   // are counted; use_h: sets the graph loop condition.
-  __global__ void
-  k_mixed_round(CgState *__restrict__ st, const double *__restrict__ sums, DevStats *__restrict__ ds, int nsys,
-                double tol, int max_rounds, cudaGraphConditionalHandle h, int use_h)
+  __device__ __forceinline__ void
+  mixed_round_body(CgState *__restrict__ st, const double *__restrict__ sums, DevStats *__restrict__ ds, int nsys,
+                   double tol, int max_rounds)
   {
     __shared__ int corrected[NM], progress[NM];
     const int s = threadIdx.x;
@@ -2274,8 +2317,15 @@ namespace lbfem_gpu
             if (st->status != 0 && ds->sticky == 0)
               ds->sticky = st->status;
           }
-        if (use_h)
-          cudaGraphSetConditional(h, st->n_active > 0 ? 1u : 0u);
       }
+  }
+
+  __global__ void
+  k_mixed_round(CgState *__restrict__ st, const double *__restrict__ sums, DevStats *__restrict__ ds, int nsys,
+                double tol, int max_rounds, cudaGraphConditionalHandle h, int use_h)
+  {
+    mixed_round_body(st, sums, ds, nsys, tol, max_rounds);
+    if (use_h && threadIdx.x == 0)
+      cudaGraphSetConditional(h, st->n_active > 0 ? 1u : 0u);
   }
 } // namespace lbfem_gpu

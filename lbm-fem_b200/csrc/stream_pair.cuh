@@ -385,10 +385,12 @@ namespace lbfem_gpu
   // rhs_{a-1} <- r_a (a = 1..8) of the scheme's step on FP32 deviations d,
   // pair by pair; PAIR_BARDOW also writes the collided deviations g* to dout.
   // Images get r = 0 (constrained rows).
-  template <int P, int MODE, typename S = TileShape<P>>
-  __global__ void __launch_bounds__(THREADS, S::MIN_CTAS)
-    k_stream_pair(const Geo geo, const DevStats *__restrict__ ds, const float *__restrict__ d,
-                  float *__restrict__ dout, float *__restrict__ rhs, const AdvCoef ac)
+  // The tile (bx, by) of the kernel below (also the body of its batched form, one
+  // launch over the tiles of many instances).
+  template <int P, int MODE, typename S>
+  __device__ __forceinline__ void
+  stream_pair_tile(const Geo &geo, const DevStats *__restrict__ ds, const float *__restrict__ d,
+                   float *__restrict__ dout, float *__restrict__ rhs, const AdvCoef &ac, int bx, int by)
   {
     if (ds && ds->sticky)
       return; // a step after a failed solve: the populations must stay as they are
@@ -404,7 +406,7 @@ namespace lbfem_gpu
     __shared__ PairScales<P, S> sc;
     const Grid &g = geo.g;
     const long long N = g.N;
-    const int gx0 = blockIdx.x * T::TX, gy0 = blockIdx.y * T::TY;
+    const int gx0 = bx * T::TX, gy0 = by * T::TY;
     build_maps<P>(maps, geo, gx0, gy0);
     __syncthreads();
     for (int t = threadIdx.x; t <= T::CX; t += blockDim.x)
@@ -661,5 +663,13 @@ namespace lbfem_gpu
               dout[q * N + idx] = v[q];
           }
       }
+  }
+
+  template <int P, int MODE, typename S = TileShape<P>>
+  __global__ void __launch_bounds__(THREADS, S::MIN_CTAS)
+    k_stream_pair(const Geo geo, const DevStats *__restrict__ ds, const float *__restrict__ d,
+                  float *__restrict__ dout, float *__restrict__ rhs, const AdvCoef ac)
+  {
+    stream_pair_tile<P, MODE, S>(geo, ds, d, dout, rhs, ac, blockIdx.x, blockIdx.y);
   }
 } // namespace lbfem_gpu

@@ -103,6 +103,14 @@ class Batch:
         fn(self.h, C.byref(ms))
         return ms.value
 
+    def last_launches(self):
+        """Kernels launched by the last step call (all instances and the grouped launches)."""
+        fn = self.lib.lbfem_gpu_batch_last_launches
+        fn.restype, fn.argtypes = C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]
+        n = C.c_int64()
+        fn(self.h, C.byref(n))
+        return int(n.value)
+
     def close(self):
         if getattr(self, "h", None) is not None:
             fn = self.lib.lbfem_gpu_batch_destroy

@@ -137,3 +137,98 @@ def test_ladder_batched_equals_one_at_a_time(gpu_lib):
     driver.batched_ladder(b, 5, batch=False)
     for x, y in zip(a, b):
         assert np.array_equal(x.get_populations(), y.get_populations())
+
+
+def _grouped_instances():
+    """Mixed-precision instances of every degree, both schemes and uneven sizes
+    (the grouped launches), with two FP64 instances (graph branches beside them)."""
+    out = []
+    table = [("cavity", 24, 1, "bardow", "mixed"), ("tgv", 12, 2, "leelin", "mixed"), ("cavity", 6, 3, "bardow", "mixed"),
+             ("tgv", 8, 4, "leelin", "mixed"), ("tgv", 30, 1, "leelin", "mixed"), ("cavity", 10, 2, "leelin", "mixed"),
+             ("tgv", 6, 3, "bardow", "mixed"), ("cavity", 9, 1, "bardow", "fp64"), ("cavity", 5, 4, "bardow", "mixed"),
+             ("tgv", 7, 2, "leelin", "fp64")]
+    for k, (case, n, p, scheme, precision) in enumerate(table):
+        if case == "tgv":
+            tc = cases.TaylorGreenVortex((0.03 + 0.01 * k) / math.sqrt(d2q9.CS2), 1, 1, shift=(0.25, 0.25),
+                                         chapman_enskog=False)
+            tc.set_reynolds(100 + 50 * k)
+        else:
+            tc = cases.LidDrivenCavity(0.05 + 0.01 * k, 1.2)
+            tc.set_reynolds(200 + 40 * k)
+        m = cases.build_mesh(tc, n, p)
+        # uneven tolerances: the instances' solves stop after different numbers of rounds
+        tol = [1e-6, 1e-5, 1e-6, 1e-4][k % 4] if precision == "mixed" else 1e-10
+        out.append((tc, m, make_params(scheme, "cg", cg_tolerance=tol, precision=precision), m.time_step(0.4)))
+    return out
+
+
+def _run(grouped, monkeypatch, n_first=4, n_second=3, host_driven=False):
+    import lbfem_gpu
+
+    monkeypatch.setenv("LBFEM_BATCH_GROUP", "1" if grouped else "0")
+    hs = [setup_case(lbfem_gpu.Solver, tc, m, prm, dt, tc.relaxation_time()) for tc, m, prm, dt in _grouped_instances()]
+    if host_driven:
+        monkeypatch.setenv("LBFEM_TRACE", "1")  # read at batch creation: the grouped kernels one by one
+    b = lbfem_gpu.Batch(hs)
+    monkeypatch.delenv("LBFEM_TRACE", raising=False)
+    b.step(n_first)
+    # a new time step for two instances: the batch graph and its grouped tables are recorded again
+    for k in (1, 7):
+        tc, m, _, dt = _grouped_instances()[k]
+        hs[k].set_time_step(0.9 * dt, tc.relaxation_time())
+    b.step(n_second)
+    launches = b.last_launches()
+    b.close()
+    return [h.get_populations() for h in hs], launches
+
+
+def test_grouped_batch_matches_single_instances(gpu_lib, monkeypatch):
+    """The grouped launches give every instance bitwise the populations of its own
+    steps, and of the batch without grouping, with fewer kernel launches."""
+    import lbfem_gpu
+
+    singles = []
+    for k, (tc, m, prm, dt) in enumerate(_grouped_instances()):
+        h = setup_case(lbfem_gpu.Solver, tc, m, prm, dt, tc.relaxation_time())
+        h.step(4)
+        if k in (1, 7):
+            h.set_time_step(0.9 * dt, tc.relaxation_time())
+        h.step(3)
+        singles.append(h.get_populations())
+    grouped, n_grouped = _run(True, monkeypatch)
+    branches, n_branches = _run(False, monkeypatch)
+    host, n_host = _run(True, monkeypatch, host_driven=True)
+    for k, (fg, fb, fh, fs) in enumerate(zip(grouped, branches, host, singles)):
+        assert np.array_equal(fg, fs), k
+        assert np.array_equal(fb, fs), k
+        assert np.array_equal(fh, fs), k
+    assert 0 < n_grouped < n_branches
+    assert n_host == n_grouped
+
+
+def test_grouped_batch_failure_of_one_instance(gpu_lib, monkeypatch):
+    """A grouped instance whose solve stops at its round cap is reported and left as
+    before its failing step; the other grouped instances complete all steps."""
+    import lbfem_gpu
+
+    monkeypatch.setenv("LBFEM_BATCH_GROUP", "1")
+    inst = _grouped_instances()[:4]
+    handles, refs = [], []
+    for k, (tc, m, prm, dt) in enumerate(inst):
+        if k == 2:  # a tolerance below the FP32 resolution: stagnates (or meets its cap) at its first step
+            prm = make_params("bardow", "cg", cg_tolerance=1e-12, mixed_tolerance=1e-12, cg_max_iterations=4,
+                              precision="mixed")
+        handles.append(setup_case(lbfem_gpu.Solver, tc, m, prm, dt, tc.relaxation_time()))
+        r = setup_case(lbfem_gpu.Solver, tc, m, prm, dt, tc.relaxation_time())
+        if k != 2:
+            r.step(3)
+        refs.append(r)
+    before = handles[2].get_populations()
+    b = lbfem_gpu.Batch(handles)
+    with pytest.raises(lbfem_gpu.NoConvergence) as ei:
+        b.step(3)
+    assert "instance 2" in str(ei.value)
+    assert np.array_equal(handles[2].get_populations(), before)
+    for k in (0, 1, 3):
+        assert np.array_equal(handles[k].get_populations(), refs[k].get_populations()), k
+    b.close()
