@@ -738,7 +738,7 @@ def run_batch(args):
     """Aggregate throughput of the batched instances, against stepping them one at a
     time, in mixed precision and on the plain FP64 path."""
     world, rank, local, pg = dist_setup()
-    r = batch_measure(args.batch, args.steps, args.warmup)
+    r = batch_measure(args.batch, args.steps, args.warmup, args.batch_accuracy_steps)
     if rank == 0:
         line = {"metric": "aggregate Q·DoF updates/s of batched independent instances (one graph launch per step)",
                 "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -748,6 +748,9 @@ def run_batch(args):
                 "speedup_vs_fp64_one_at_a_time": r["speedup_vs_fp64_one_at_a_time"], "accuracy": r["accuracy"],
                 "gpu_launches": r["gpu_launches"], "branches": r["branches"],
                 "gain_of_grouping": r["gain_of_grouping"], "grouping": r["grouping"],
+                "fp64_batched": r["fp64_batched"], "gain_of_precision_batched": r["gain_of_precision_batched"],
+                "gain_of_batching_mixed": r["gain_of_batching_mixed"],
+                "gain_of_batching_fp64": r["gain_of_batching_fp64"],
                 "dtype": "f32 mixed", "data": "synthetic",
                 "config": {"workload": r["workload"], "nodes_distinct_total": r["nodes_distinct_total"],
                            "instances": r["instances"]},
@@ -944,6 +947,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-workload leg (64 instances, mixed batched vs one at a time and FP64)")
+    ap.add_argument("--batch-accuracy-steps", type=int, default=10000,
+                    help="steps per instance of the --batch leg's mixed-vs-FP64 accuracy check (both batched)")
     ap.add_argument("--batch", type=int, default=0,
                     help="time N batched independent instances (the batched workload) instead of the default")
     ap.add_argument("--ladder", type=int, default=0,
