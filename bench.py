@@ -194,10 +194,10 @@ def run_reference(args):
 
 
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the default
-# workload's kernels, from ncu captures on the Q3 512^2 case scaled by the stored nodes
-# (x 3.997); the profiles/ summaries give the commands.
-STREAMING_TRAFFIC = {"fp64": 1147e6, "mixed": 482e6}
-WINDOW_TRAFFIC = 1349e6
+# workload's kernels, from one-pass ncu captures of a launch on the 1024^2 Q3 mesh itself
+# (profiles/traffic_tgv_q3_1024.md gives the commands and the read / write split).
+STREAMING_TRAFFIC = {"fp64": 1147e6, "mixed": 608.9e6}
+WINDOW_TRAFFIC = 1490.1e6
 
 
 def mixed_tol(cg_tol):

@@ -3280,7 +3280,14 @@ namespace
       const lbfem_gpu_ctx *c = b->ctxs[k];
       return 2 * c->P + (c->prm.scheme == LBFEM_SCHEME_BARDOW ? 1 : 0);
     };
-    std::stable_sort(idx.begin(), idx.end(), [&](size_t x, size_t y) { return class_of(x) < class_of(y); });
+    // the classes with the most nodes first: their branches are recorded, and start, first
+    std::map<int, long long> class_nodes;
+    for (size_t k : idx)
+      class_nodes[class_of(k)] += b->ctxs[k]->grid.N;
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t x, size_t y) {
+      const int cx = class_of(x), cy = class_of(y);
+      return cx != cy && (class_nodes[cx] != class_nodes[cy] ? class_nodes[cx] > class_nodes[cy] : cx < cy);
+    });
     gp.n = int(idx.size());
     std::vector<GroupInst> tab(idx.size());
     struct Lists
