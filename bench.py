@@ -196,7 +196,7 @@ def run_reference(args):
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the default
 # workload's kernels, from one-pass ncu captures of a launch on the 1024^2 Q3 mesh itself
 # (profiles/traffic_tgv_q3_1024.md gives the commands and the read / write split).
-STREAMING_TRAFFIC = {"fp64": 1147e6, "mixed": 608.9e6}
+STREAMING_TRAFFIC = {"fp64": 1269.1e6, "mixed": 608.9e6}
 WINDOW_TRAFFIC = 1490.1e6
 
 
