@@ -261,6 +261,27 @@ namespace lbfem_gpu
   __device__ constexpr float kEYf[Q] = {0, 0, 1, 1, 1, 0, -1, -1, -1};
   __device__ constexpr float kWf[Q] = {float(4. / 9.),  float(1. / 9.),  float(1. / 36.), float(1. / 9.), float(1. / 36.),
                             float(1. / 9.),  float(1. / 36.), float(1. / 9.),  float(1. / 36.)};
+  // The weights' FP32 rounding errors (w - kWf, rounded to FP32). All nine FP32
+  // weights are 4 / 9, 1 / 9 and 1 / 36 rounded up by the same relative 7.45e-9, so
+  // their sum and their second moments exceed 1 and 1 / 3 by that much. A
+  // product w t rounded once from kWf t would give every equilibrium that excess
+  // of mass and momentum: a bias that the collisions add up step after step,
+  // about 7.5e-9 of the velocity per step. Formed as fma(kWf, t, kWlf t), the
+  // product is the exact weight's, rounded once, with no common bias.
+  constexpr double kW64[Q] = {4. / 9., 1. / 9., 1. / 36., 1. / 9., 1. / 36., 1. / 9., 1. / 36., 1. / 9., 1. / 36.};
+  __device__ constexpr float kWlf[Q] = {
+    float(kW64[0] - double(float(kW64[0]))), float(kW64[1] - double(float(kW64[1]))),
+    float(kW64[2] - double(float(kW64[2]))), float(kW64[3] - double(float(kW64[3]))),
+    float(kW64[4] - double(float(kW64[4]))), float(kW64[5] - double(float(kW64[5]))),
+    float(kW64[6] - double(float(kW64[6]))), float(kW64[7] - double(float(kW64[7]))),
+    float(kW64[8] - double(float(kW64[8])))};
+
+  // w t for the weight w = wh + wl (wh its FP32 rounding, wl the rest), rounded once
+  __device__ __forceinline__ float
+  wmul(float wh, float wl, float t)
+  {
+    return fmaf(wh, t, wl * t);
+  }
 
   // The momentum sums in the order of the loop over a with e_a in {-1, 0, 1}
   // (the zero terms dropped: adding +-0 changes no value).
@@ -277,19 +298,19 @@ namespace lbfem_gpu
     return {rho, mx / rho, my / rho, drho};
   }
 
-  // feq - w of the direction (ex, ey) with weight w.
+  // feq - w of the direction (ex, ey) with weight w = wh + wl.
   __device__ __forceinline__ float
-  feqd(float ex, float ey, float w, const MomF &m)
+  feqd(float ex, float ey, float wh, float wl, const MomF &m)
   {
     const float uu = m.ux * m.ux + m.uy * m.uy;
     const float eu = ex * m.ux + ey * m.uy;
-    return w * (m.drho + m.rho * (3.f * eu + 4.5f * eu * eu - 1.5f * uu));
+    return wmul(wh, wl, m.drho + m.rho * (3.f * eu + 4.5f * eu * eu - 1.5f * uu));
   }
 
   __device__ __forceinline__ float
   feqd_a(int a, const MomF &m)
   {
-    return feqd(kEXf[a], kEYf[a], kWf[a], m);
+    return feqd(kEXf[a], kEYf[a], kWf[a], kWlf[a], m);
   }
 
   // What a node imposes on its moments (collision.h:53-72).

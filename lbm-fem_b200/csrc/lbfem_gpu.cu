@@ -279,6 +279,7 @@ namespace
         for (int k = 0; k < 8; ++k)
           ac.pk[pr][k] = float(v[k]);
         ac.pw[pr] = float(w[pr + 1]);
+        ac.pwl[pr] = float(w[pr + 1] - double(ac.pw[pr]));
       }
     return ac;
   }

@@ -163,7 +163,7 @@ namespace lbfem_gpu
   // u and h = A u + B feq of the pair at footprint index t (Lee-Lin), or u and A u.
   template <int MODE>
   __device__ __forceinline__ void
-  pair_uh(const float2 *s_u, const float *s_m, int nf, int t, float w, float ex, float ey, const PairK &k,
+  pair_uh(const float2 *s_u, const float *s_m, int nf, int t, float w, float wl, float ex, float ey, const PairK &k,
           float2 &u, float2 &h)
   {
     u = s_u[t];
@@ -172,7 +172,7 @@ namespace lbfem_gpu
         // staged: rho, ux, uy, base = drho - 1.5 rho u.u (wall velocity imposed)
         const float rho = s_m[t], ux = s_m[nf + t], uy = s_m[2 * nf + t], base = s_m[3 * nf + t];
         const float eu = fmaf(ey, uy, ex * ux), reu = rho * eu;
-        const float E = w * fmaf(4.5f * reu, eu, base), O = 3.f * w * reu;
+        const float E = wmul(w, wl, fmaf(4.5f * reu, eu, base)), O = 3.f * wmul(w, wl, reu);
         h = fma2(k.B, make_float2(E + O, E - O), mul2(k.A, u));
       }
     else
@@ -184,8 +184,8 @@ namespace lbfem_gpu
   template <int P, int CLS, int MODE, typename S>
   __device__ __forceinline__ void
   pair_xpass(const float2 *s_u, const float *s_m, float2 *s_y, float2 *s_y4, const PairScales<P, S> &m,
-             const PairK &k, float w, float ex, float ey, int fy, int seg, int gx0, int y4_slot, int bx_lo,
-             int bx_hi)
+             const PairK &k, float w, float wl, float ex, float ey, int fy, int seg, int gx0, int y4_slot,
+             int bx_lo, int bx_hi)
   {
     using T = Tile<P, S>;
     constexpr bool XC = CLS != 1, YC = CLS != 0, DG = CLS == 2;
@@ -194,7 +194,7 @@ namespace lbfem_gpu
     float2 u[P + 1], h[P + 1];
 #pragma unroll
     for (int b = 0; b <= P; ++b)
-      pair_uh<MODE>(s_u, s_m, T::NF, base + q0 * P + b, w, ex, ey, k, u[b], h[b]);
+      pair_uh<MODE>(s_u, s_m, T::NF, base + q0 * P + b, w, wl, ex, ey, k, u[b], h[b]);
     // pending right-vertex contributions of the previous cell
     float2 pCh{}, pKu{}, pMh{}, pCu{}, pMu{};
     if constexpr (XC)
@@ -219,7 +219,7 @@ namespace lbfem_gpu
         h[0] = h[P];
 #pragma unroll
         for (int b = 1; b <= P; ++b)
-          pair_uh<MODE>(s_u, s_m, T::NF, base + qc * P + b, w, ex, ey, k, u[b], h[b]);
+          pair_uh<MODE>(s_u, s_m, T::NF, base + qc * P + b, w, wl, ex, ey, k, u[b], h[b]);
         const float2 sc = m.cx[qc], sh = m.hx[qc], shi = m.hxi[qc];
         const int j0 = (qc - 1) * P;
 #pragma unroll
@@ -548,7 +548,7 @@ namespace lbfem_gpu
       {
         const int a = pr + 1, ab = pr + 5; // opposite populations
         const float *pk = ac.pk[pr];
-        const float ex = pk[2], ey = pk[4], w = ac.pw[pr];
+        const float ex = pk[2], ey = pk[4], w = ac.pw[pr], wl = ac.pwl[pr];
         float2 *s_u = s_pb + (pr & 1) * T::NF;
         if (pr < 3)
           {
@@ -575,8 +575,8 @@ namespace lbfem_gpu
                     const MomF mt = impose_class(mo, s_wall[st], geo);
                     // each population's own equilibrium: the collision writes the state, and the
                     // rounding of the even +- odd form accumulates there from step to step
-                    gs.x = feqd(ex, ey, w, mt) + (1.f - omega) * (gv.x - feqd(ex, ey, w, mo));
-                    gs.y = feqd(-ex, -ey, w, mt) + (1.f - omega) * (gv.y - feqd(-ex, -ey, w, mo));
+                    gs.x = feqd(ex, ey, w, wl, mt) + (1.f - omega) * (gv.x - feqd(ex, ey, w, wl, mo));
+                    gs.y = feqd(-ex, -ey, w, wl, mt) + (1.f - omega) * (gv.y - feqd(-ex, -ey, w, wl, mo));
                     const int gx = gx0 - P + fx, gy = gy0 - P + fy;
                     if (fx >= P && fx < P + T::TX && fy >= P && fy < P + T::TY && gx < g.nfx && gy < g.nfy &&
                         !is_image(gx, gy, g))
@@ -605,11 +605,11 @@ namespace lbfem_gpu
             const int gy = gy0 - P + lane;
             const int y4_slot = gy == by_lo ? 0 : gy == by_hi ? 1 : -1;
             if (cls == 0)
-              pair_xpass<P, 0, MODE, S>(s_u, s_m, s_y, s_y4, sc, k, w, ex, ey, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
+              pair_xpass<P, 0, MODE, S>(s_u, s_m, s_y, s_y4, sc, k, w, wl, ex, ey, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
             else if (cls == 1)
-              pair_xpass<P, 1, MODE, S>(s_u, s_m, s_y, s_y4, sc, k, w, ex, ey, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
+              pair_xpass<P, 1, MODE, S>(s_u, s_m, s_y, s_y4, sc, k, w, wl, ex, ey, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
             else
-              pair_xpass<P, 2, MODE, S>(s_u, s_m, s_y, s_y4, sc, k, w, ex, ey, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
+              pair_xpass<P, 2, MODE, S>(s_u, s_m, s_y, s_y4, sc, k, w, wl, ex, ey, lane, warp, gx0, y4_slot, bx_lo, bx_hi);
           }
         __syncthreads();
         // y pass: lane group = columns, warp group = y segment
