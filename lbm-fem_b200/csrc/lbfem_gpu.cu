@@ -2152,6 +2152,32 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
         for (int a = 0; a <= MAXPD; ++a)
           for (int c = 0; c <= MAXPD; ++c)
             reff[q][o][a][c] = float(ref[q][o][a][c]);
+    // The rows of the derivative and stiffness matrices sum to zero: they
+    // annihilate constants. Their FP32 roundings do not (row sums up to 1.5e-7 at
+    // p = 2..4), and the streaming kernel would then give the slowly varying part
+    // of the deviations a small coherent source every step. Each row's entries,
+    // largest first, take up the FP32 row sum until it is exactly zero (entries
+    // change by at most 7e-8 of the row's largest).
+    for (int q = 0; q < MAXPD; ++q)
+      for (int o : {int(OP_C), int(OP_K)})
+        for (int a = 0; a <= q + 1; ++a)
+          {
+            float *row = reff[q][o][a];
+            int order[MAXPD + 1];
+            for (int c = 0; c <= q + 1; ++c)
+              order[c] = c;
+            std::stable_sort(order, order + q + 2,
+                             [&](int x, int y) { return std::fabs(row[x]) > std::fabs(row[y]); });
+            for (int k = 0; k <= q + 1; ++k)
+              {
+                double sum = 0; // exact: a few FP32 values
+                for (int c = 0; c <= q + 1; ++c)
+                  sum += double(row[c]);
+                if (sum == 0.0)
+                  break;
+                row[order[k]] = float(double(row[order[k]]) - sum);
+              }
+          }
     CK(cudaMemcpyToSymbol(c_reff, reff, sizeof reff));
     static float2 ref2[MAXPD][3][MAXPD + 1][MAXPD + 1];
     for (int q = 0; q < MAXPD; ++q)
