@@ -32,7 +32,8 @@ namespace lbfem_gpu
     double *partials, *sums;
     double tol;
     int max_rounds;
-    int nb_start_x, nb_start_y; // tile grid of the start (Tile<P>)
+    int nb_pair_x, nb_pair_y;   // tile grid of the streaming kernel (Tile<P>)
+    int nb_start_x, nb_start_y; // tile grid of the start (StartShape<P>)
     int nb_win_x, nb_win_y;     // tile grid of the window rounds (WinShape<P>)
     double theta;
     long long N;
@@ -81,14 +82,14 @@ namespace lbfem_gpu
       wall_face_node<P, float>(I.geo, I.bardow ? I.g : I.f, I.rhs, I.bnode, I.fc, t);
   }
 
+  // blockIdx.y: system
   template <int P>
-  __global__ void __launch_bounds__(THREADS, 8)
-    kg_cg_start(const GroupInst *__restrict__ tab, const TileRef *__restrict__ tiles)
+  __global__ void __launch_bounds__(StartShape<P>::THREADS)
+    kg_mixed_start(const GroupInst *__restrict__ tab, const TileRef *__restrict__ tiles)
   {
     const TileRef t = tiles[blockIdx.x];
     const GroupInst &I = load_inst(tab, t.inst);
-    cg_start_tile<P, float, float, float, OPK_MASS>(I.geo, I.rhs, I.xc, I.xp, I.xn, I.r0, 1, I.partials, StreamCoef{},
-                                                    0, t.bx, t.by, blockIdx.y, I.nb_start_x, I.nb_start_y);
+    mixed_start_tile<P>(I.geo, I.rhs, I.xc, I.xp, I.xn, I.r0, t.bx, t.by, blockIdx.y);
   }
 
   // phase 0: r0, x_new -> x_prev, r1; phase 1: r1, x_prev -> x_new, r0 (the rounds of mixed_graph)

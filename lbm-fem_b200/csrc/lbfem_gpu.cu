@@ -172,6 +172,15 @@ namespace
     return dim3((g.nfx + Tile<P>::TX - 1) / Tile<P>::TX, (g.nfy + Tile<P>::TY - 1) / Tile<P>::TY);
   }
 
+  // the tiles of the mixed solve's start for nsys systems
+  template <int P>
+  dim3
+  start_grid(const Grid &g, int nsys)
+  {
+    using S = StartShape<P>;
+    return dim3((g.nfx + S::TX - 1) / S::TX, (g.nfy + S::TY - 1) / S::TY, nsys);
+  }
+
   template <typename F>
   int
   with_degree(int P, F &&f)
@@ -236,12 +245,10 @@ namespace
                        cg_smem<P, double, OPK_LAPLACE>(1))) ||
         (st = set_smem(ctx, k_cg_p<P, double, OPK_LAPLACE>, cg_smem<P, double, OPK_LAPLACE>(0))) ||
         (st = set_smem(ctx, k_cg_update<P, double, OPK_LAPLACE>, cg_smem<P, double, OPK_LAPLACE>(2))) ||
-        (st = set_smem(ctx, k_cg_start<P, float, float, float>, cg_smem<P, float>(1))) ||
         (st = set_smem(ctx, k_cg_start<P, float, float, double>, cg_smem<P, float>(1, true))) ||
         (st = set_smem(ctx, k_window_correct<P>, window_smem<P>())) ||
         (st = set_smem(ctx, kg_stream_pair<P, PAIR_LEELIN>, pair_smem<P, PAIR_LEELIN>())) ||
         (st = set_smem(ctx, kg_stream_pair<P, PAIR_BARDOW>, pair_smem<P, PAIR_BARDOW>())) ||
-        (st = set_smem(ctx, kg_cg_start<P>, cg_smem<P, float>(1))) ||
         (st = set_smem(ctx, kg_window<P>, window_smem<P>())) ||
         (st = set_smem(ctx, k_richardson_pass<P, double>, cg_smem<P, double>(0))) ||
         (st = set_smem(ctx, k_richardson_pass<P, float>, cg_smem<P, float>(0))))
@@ -819,11 +826,9 @@ namespace
     CK(cudaMemsetAsync(ctx->d_cg, 0, sizeof(CgState), ctx->stream));
     int st = with_degree(ctx->P, [&](auto PP) -> int {
       constexpr int P = decltype(PP)::value;
-      dim3 grid = tile_grid<P>(g);
-      grid.z = nsys;
       // FP32 arithmetic: r0 only feeds the FP32 correction (the rounds form the FP64 residuals)
-      k_cg_start<P, float, float, float><<<grid, THREADS, cg_smem<P, float>(1), ctx->stream>>>(
-        geo, b, ctx->d_x_s[ic], ctx->d_x_s[ip], ctx->d_x_s[in], ctx->d_r_s, 1, ctx->d_partials, StreamCoef{}, 0);
+      k_mixed_start<P><<<start_grid<P>(g, nsys), StartShape<P>::THREADS, 0, ctx->stream>>>(
+        geo, b, ctx->d_x_s[ic], ctx->d_x_s[ip], ctx->d_x_s[in], ctx->d_r_s);
       LAUNCHED();
       return LBFEM_OK;
     });
@@ -1633,10 +1638,8 @@ namespace
     CK(cudaMemsetAsync(ctx->d_cg, 0, sizeof(CgState), ctx->stream));
     int st = with_degree(ctx->P, [&](auto PP) -> int {
       constexpr int P = decltype(PP)::value;
-      dim3 grid = tile_grid<P>(g);
-      grid.z = NM;
-      k_cg_start<P, float, float, float><<<grid, THREADS, cg_smem<P, float>(1), ctx->stream>>>(
-        geo, b, xc, xp, xn, ctx->d_r_s, 1, ctx->d_partials, StreamCoef{}, 0);
+      k_mixed_start<P><<<start_grid<P>(g, NM), StartShape<P>::THREADS, 0, ctx->stream>>>(geo, b, xc, xp, xn,
+                                                                                       ctx->d_r_s);
       LAUNCHED();
       return LBFEM_OK;
     });
@@ -3267,7 +3270,7 @@ namespace
     size_t pair_off = 0, wall_off = 0, start_off = 0, win_off = 0, chunk_off = 0;
     int pair_n = 0;  // streaming tiles (Tile<P>)
     int wall_n = 0;  // (instance, first boundary node) per 128 wall nodes
-    int start_n = 0; // start tiles (Tile<P>)
+    int start_n = 0; // start tiles (StartShape<P>)
     int win_n = 0;   // window tiles (WinShape<P>)
     int chunk_n = 0; // node chunks of GROUP_CHUNK nodes
   };
@@ -3355,10 +3358,12 @@ namespace
         I.N = c->grid.N;
         with_degree(c->P, [&](auto PP) -> int {
           constexpr int P = decltype(PP)::value;
-          const dim3 tg = tile_grid<P>(c->grid);
+          const dim3 tg = tile_grid<P>(c->grid), sg = start_grid<P>(c->grid, 1);
           using S = WinShape<P>;
-          I.nb_start_x = int(tg.x);
-          I.nb_start_y = int(tg.y);
+          I.nb_pair_x = int(tg.x);
+          I.nb_pair_y = int(tg.y);
+          I.nb_start_x = int(sg.x);
+          I.nb_start_y = int(sg.y);
           I.nb_win_x = (c->grid.nfx + S::TX - 1) / S::TX;
           I.nb_win_y = (c->grid.nfy + S::TY - 1) / S::TY;
           return 0;
@@ -3374,12 +3379,12 @@ namespace
           }
         gp.cls.back().i1 = k + 1;
         Lists &L = lists.back();
+        for (int by = 0; by < I.nb_pair_y; ++by)
+          for (int bx = 0; bx < I.nb_pair_x; ++bx)
+            L.pair.push_back({k, bx, by});
         for (int by = 0; by < I.nb_start_y; ++by)
           for (int bx = 0; bx < I.nb_start_x; ++bx)
-            {
-              L.pair.push_back({k, bx, by});
-              L.start.push_back({k, bx, by});
-            }
+            L.start.push_back({k, bx, by});
         for (int by = 0; by < I.nb_win_y; ++by)
           for (int bx = 0; bx < I.nb_win_x; ++bx)
             L.win.push_back({k, bx, by});
@@ -3491,7 +3496,7 @@ namespace
               tab, tiles(gc.pair_off));
           if (gc.wall_n)
             kg_wall_faces<P><<<gc.wall_n, 128, 0, q>>>(tab, refs(gc.wall_off));
-          kg_cg_start<P><<<dim3(gc.start_n, NM), THREADS, cg_smem<P, float>(1), q>>>(tab, tiles(gc.start_off));
+          kg_mixed_start<P><<<dim3(gc.start_n, NM), StartShape<P>::THREADS, 0, q>>>(tab, tiles(gc.start_off));
           return 0;
         });
         n_fixed += gc.wall_n ? 3 : 2;

@@ -1762,6 +1762,149 @@ namespace lbfem_gpu
   // decay exponentially, so M^{-1} r at the own nodes of a tile follows from
   // banded LDL^T solves on a window of W nodes around the tile in each direction
   // (factors from window_ldl on the host), to a few 1e-6 of |r|.
+  // ------------------------------------------------ start of the mixed solve
+  // x0 = 2 x_cur - x_prev (the extrapolated start, rounded to FP32 and stored in
+  // x_new) and r0 = b - A x0 in FP32 arithmetic, for one tile of TX x TY nodes of
+  // one system. A = My (x) Mx on the assembled 1-D rows (rounded to FP32);
+  // periodic images have identity rows. x0 is staged with a halo of P nodes; a
+  // thread owns one column: the x pass of its column on the tile's rows and halo
+  // (kept in registers), then the y pass. r0 only feeds the first FP32
+  // correction; the rounds form the residuals in FP64.
+  template <int P>
+  struct StartShape
+  {
+    static constexpr int TX = 128, TY = 16, THREADS = 128;
+    static constexpr int FX = TX + 2 * P, FY = TY + 2 * P; // staged x0
+    static constexpr int K = 2 * P + 1;                   // entries of an assembled 1-D row
+  };
+
+  __device__ __forceinline__ float
+  extrapolated(const float *__restrict__ x_cur, const float *__restrict__ x_prev, long long idx)
+  {
+    return fmaf(2.f, x_cur[idx], -x_prev[idx]);
+  }
+
+  template <int P>
+  __device__ __forceinline__ void
+  mixed_start_tile(const Geo &geo, const float *__restrict__ b, const float *__restrict__ x_cur,
+                   const float *__restrict__ x_prev, float *__restrict__ x_new, float *__restrict__ r, int bx, int by,
+                   int s)
+  {
+    using S = StartShape<P>;
+    constexpr int K = S::K, FX = S::FX, FY = S::FY;
+    __shared__ float s_x[FY * FX], s_p[FY * FX]; // x_cur, then x0; x_prev
+    __shared__ int s_col[FX], s_rowoff[FY];
+    __shared__ float s_my[S::TY][K + 1];
+    const Grid &g = geo.g;
+    const long long o = (long long)s * g.N;
+    const float *xc = x_cur + o, *xp = x_prev + o, *bs = b + o;
+    float *xn = x_new + o, *rs = r + o;
+    const int gx0 = bx * S::TX, gy0 = by * S::TY, tid = threadIdx.x;
+    for (int t = tid; t < FX; t += S::THREADS)
+      s_col[t] = wrap(gx0 - P + t, g.px, g.nux, g.nfx);
+    for (int t = tid; t < FY; t += S::THREADS)
+      {
+        const int row = wrap(gy0 - P + t, g.py, g.nuy, g.nfy);
+        s_rowoff[t] = row < 0 ? -1 : row * g.nfx;
+      }
+    for (int t = tid; t < S::TY * (K + 1); t += S::THREADS)
+      {
+        const int i = t / (K + 1), k = t - i * (K + 1), gy = gy0 + i;
+        s_my[i][k] = (k < K && gy < g.nfy && !(g.py && gy == g.nuy)) ? float(geo.rowy[(long long)gy * K + k]) : 0.f;
+      }
+    __syncthreads();
+    // x_cur and x_prev on the tile and its halo: asynchronous copies, all in flight
+    // at once (zero outside the grid)
+    for (int c = tid; c < FX; c += S::THREADS)
+      {
+        const int col = s_col[c];
+#pragma unroll 8
+        for (int q = 0; q < FY; ++q)
+          {
+            const int ro = s_rowoff[q];
+            const bool ok = ro >= 0 && col >= 0;
+            const long long at = ok ? ro + col : 0;
+            cp_async4(&s_x[q * FX + c], xc + at, ok);
+            cp_async4(&s_p[q * FX + c], xp + at, ok);
+          }
+      }
+    const int j = tid, gx = gx0 + j;
+    const bool col_in = gx < g.nfx;
+    const bool img_col = g.px && gx == g.nux;
+    float mx[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      mx[k] = (col_in && !img_col) ? float(geo.rowx[(long long)gx * K + k]) : 0.f;
+    // this column's b, loaded while the copies land
+    const int rows_in = g.nfy - gy0;
+    float bv[S::TY];
+#pragma unroll
+    for (int i = 0; i < S::TY; ++i)
+      bv[i] = (col_in && i < rows_in) ? bs[(long long)(gy0 + i) * g.nfx + gx] : 0.f;
+    cp_async_wait_all();
+    __syncthreads();
+    for (int t = tid; t < FY * FX; t += S::THREADS)
+      s_x[t] = fmaf(2.f, s_x[t], -s_p[t]);
+    __syncthreads();
+    if (!col_in)
+      return; // no barrier follows
+    // (Mx x0) of this column on the tile's rows and a halo of P rows
+    float t[FY];
+#pragma unroll
+    for (int q = 0; q < FY; ++q)
+      {
+        const float *w = &s_x[q * FX + j]; // columns gx - P .. gx + P
+        float a0 = mx[0] * w[0], a1 = mx[1] * w[1];
+#pragma unroll
+        for (int k = 2; k < K; k += 2)
+          {
+            a0 = fmaf(mx[k], w[k], a0);
+            if (k + 1 < K)
+              a1 = fmaf(mx[k + 1], w[k + 1], a1);
+          }
+        t[q] = a0 + a1;
+      }
+#pragma unroll
+    for (int i = 0; i < S::TY; ++i)
+      {
+        if (i >= rows_in)
+          break;
+        const int gy = gy0 + i;
+        const long long idx = (long long)gy * g.nfx + gx;
+        const bool image = img_col || (g.py && gy == g.nuy);
+        float x0, ax;
+        if (image)
+          {
+            x0 = extrapolated(xc, xp, idx);
+            ax = x0; // identity row
+          }
+        else
+          {
+            x0 = s_x[(i + P) * FX + j + P];
+            float a0 = s_my[i][0] * t[i], a1 = s_my[i][1] * t[i + 1];
+#pragma unroll
+            for (int k = 2; k < K; k += 2)
+              {
+                a0 = fmaf(s_my[i][k], t[i + k], a0);
+                if (k + 1 < K)
+                  a1 = fmaf(s_my[i][k + 1], t[i + k + 1], a1);
+              }
+            ax = a0 + a1;
+          }
+        xn[idx] = x0;
+        rs[idx] = bv[i] - ax;
+      }
+  }
+
+  // grid (x tiles, y tiles, systems)
+  template <int P>
+  __global__ void __launch_bounds__(StartShape<P>::THREADS)
+    k_mixed_start(const Geo geo, const float *__restrict__ b, const float *__restrict__ x_cur,
+                  const float *__restrict__ x_prev, float *__restrict__ x_new, float *__restrict__ r)
+  {
+    mixed_start_tile<P>(geo, b, x_cur, x_prev, x_new, r, blockIdx.x, blockIdx.y, blockIdx.z);
+  }
+
   template <int P>
   struct WinShape
   {
