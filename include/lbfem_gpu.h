@@ -138,6 +138,16 @@ const char *lbfem_gpu_last_error(const lbfem_gpu_ctx *ctx);
 int lbfem_gpu_device_count(void);
 
 /*
+ * The reference element matrix op (0 mass, 1 derivative int l_a l_b', 2
+ * stiffness) of FE_Q(degree) on [0, 1], row-major (degree + 1)^2 entries: in
+ * FP64 (ref64) and as the FP32 kernels use it (ref32; either may be null). The
+ * FP32 derivative and stiffness rows sum exactly to zero, as the FP64 rows do
+ * in exact arithmetic. Needs no GPU. The reference's counterpart is deal.II's
+ * FE_Q shape data behind FEEvaluation (advection.h:100-121).
+ */
+int lbfem_gpu_reference_matrix(int32_t degree, int32_t op, double *ref64, float *ref32);
+
+/*
  * Creates a context: exports the discretisation to flat device arrays and
  * builds the operators (Discretization::reinit + Scheme constructor,
  * discretization.h:78-144, schemes.h:85-90,111-116, streaming.h:41-60).

@@ -207,6 +207,64 @@ namespace
            sizeof(R) * own * T::TX * T::TY;
   }
 
+  // The reference element matrices of every degree (FE_Q(p) on [0, 1]) in FP64,
+  // and the FP32 copies the FP32 kernels use. The rows of the derivative and
+  // stiffness matrices sum to zero: they annihilate constants. Their FP32
+  // roundings do not (row sums up to 1.5e-7 at p = 2..4), and the streaming
+  // kernel would then give the slowly varying part of the deviations a small
+  // coherent source every step. Each row's entries, largest first, take up the
+  // FP32 row sum until it is exactly zero (entries move by at most 7e-8 of the
+  // row's largest).
+  void
+  reference_matrices(double (&ref)[MAXPD][3][MAXPD + 1][MAXPD + 1], float (&reff)[MAXPD][3][MAXPD + 1][MAXPD + 1])
+  {
+    std::memset(ref, 0, sizeof ref);
+    for (int q = 1; q <= MAXPD; ++q)
+      {
+        const Basis1D b(q);
+        for (int a = 0; a <= q; ++a)
+          for (int c = 0; c <= q; ++c)
+            {
+              ref[q - 1][OP_M][a][c] = b.Mh[a][c];
+              ref[q - 1][OP_C][a][c] = b.Ch[a][c];
+              ref[q - 1][OP_K][a][c] = b.Kh[a][c];
+            }
+      }
+    for (int q = 0; q < MAXPD; ++q)
+      for (int o = 0; o < 3; ++o)
+        for (int a = 0; a <= MAXPD; ++a)
+          {
+            double big = 0;
+            for (int c = 0; c <= MAXPD; ++c)
+              big = std::max(big, std::fabs(ref[q][o][a][c]));
+            // entries that are zero but for the quadrature's rounding (1e-20 beside
+            // O(1)) become zero, so that the FP64 sums of a row's FP32 entries below
+            // are exact
+            for (int c = 0; c <= MAXPD; ++c)
+              reff[q][o][a][c] = std::fabs(ref[q][o][a][c]) <= 1e-14 * big ? 0.f : float(ref[q][o][a][c]);
+          }
+    for (int q = 0; q < MAXPD; ++q)
+      for (int o : {int(OP_C), int(OP_K)})
+        for (int a = 0; a <= q + 1; ++a)
+          {
+            float *row = reff[q][o][a];
+            int order[MAXPD + 1];
+            for (int c = 0; c <= q + 1; ++c)
+              order[c] = c;
+            std::stable_sort(order, order + q + 2,
+                             [&](int x, int y) { return std::fabs(row[x]) > std::fabs(row[y]); });
+            for (int k = 0; k <= q + 1; ++k)
+              {
+                double sum = 0; // exact: a few FP32 values
+                for (int c = 0; c <= q + 1; ++c)
+                  sum += double(row[c]);
+                if (sum == 0.0)
+                  break;
+                row[order[k]] = float(double(row[order[k]]) - sum);
+              }
+          }
+  }
+
   template <typename K>
   int
   set_smem(lbfem_gpu_ctx *ctx, K kernel, size_t bytes)
@@ -1985,6 +2043,26 @@ lbfem_gpu_device_count(void)
   return n;
 }
 
+int
+lbfem_gpu_reference_matrix(int32_t degree, int32_t op, double *ref64, float *ref32)
+{
+  if (degree < 1 || degree > MAXPD || op < 0 || op > 2)
+    return LBFEM_ERR_ARG;
+  static double ref[MAXPD][3][MAXPD + 1][MAXPD + 1];
+  static float reff[MAXPD][3][MAXPD + 1][MAXPD + 1];
+  static std::once_flag once;
+  std::call_once(once, [] { reference_matrices(ref, reff); });
+  for (int a = 0; a <= degree; ++a)
+    for (int c = 0; c <= degree; ++c)
+      {
+        if (ref64)
+          ref64[a * (degree + 1) + c] = ref[degree - 1][op][a][c];
+        if (ref32)
+          ref32[a * (degree + 1) + c] = reff[degree - 1][op][a][c];
+      }
+  return LBFEM_OK;
+}
+
 void *
 lbfem_gpu_host_alloc(size_t bytes)
 {
@@ -2136,51 +2214,9 @@ lbfem_gpu_create(const lbfem_mesh_desc *m, const lbfem_params *prm, lbfem_gpu_ct
   {
     // reference element matrices of every degree, into constant memory
     static double ref[MAXPD][3][MAXPD + 1][MAXPD + 1];
-    std::memset(ref, 0, sizeof ref);
-    for (int q = 1; q <= MAXPD; ++q)
-      {
-        const Basis1D b(q);
-        for (int a = 0; a <= q; ++a)
-          for (int c = 0; c <= q; ++c)
-            {
-              ref[q - 1][OP_M][a][c] = b.Mh[a][c];
-              ref[q - 1][OP_C][a][c] = b.Ch[a][c];
-              ref[q - 1][OP_K][a][c] = b.Kh[a][c];
-            }
-      }
-    CK(cudaMemcpyToSymbol(c_ref, ref, sizeof ref));
     static float reff[MAXPD][3][MAXPD + 1][MAXPD + 1];
-    for (int q = 0; q < MAXPD; ++q)
-      for (int o = 0; o < 3; ++o)
-        for (int a = 0; a <= MAXPD; ++a)
-          for (int c = 0; c <= MAXPD; ++c)
-            reff[q][o][a][c] = float(ref[q][o][a][c]);
-    // The rows of the derivative and stiffness matrices sum to zero: they
-    // annihilate constants. Their FP32 roundings do not (row sums up to 1.5e-7 at
-    // p = 2..4), and the streaming kernel would then give the slowly varying part
-    // of the deviations a small coherent source every step. Each row's entries,
-    // largest first, take up the FP32 row sum until it is exactly zero (entries
-    // change by at most 7e-8 of the row's largest).
-    for (int q = 0; q < MAXPD; ++q)
-      for (int o : {int(OP_C), int(OP_K)})
-        for (int a = 0; a <= q + 1; ++a)
-          {
-            float *row = reff[q][o][a];
-            int order[MAXPD + 1];
-            for (int c = 0; c <= q + 1; ++c)
-              order[c] = c;
-            std::stable_sort(order, order + q + 2,
-                             [&](int x, int y) { return std::fabs(row[x]) > std::fabs(row[y]); });
-            for (int k = 0; k <= q + 1; ++k)
-              {
-                double sum = 0; // exact: a few FP32 values
-                for (int c = 0; c <= q + 1; ++c)
-                  sum += double(row[c]);
-                if (sum == 0.0)
-                  break;
-                row[order[k]] = float(double(row[order[k]]) - sum);
-              }
-          }
+    reference_matrices(ref, reff);
+    CK(cudaMemcpyToSymbol(c_ref, ref, sizeof ref));
     CK(cudaMemcpyToSymbol(c_reff, reff, sizeof reff));
     static float2 ref2[MAXPD][3][MAXPD + 1][MAXPD + 1];
     for (int q = 0; q < MAXPD; ++q)

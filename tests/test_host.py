@@ -162,3 +162,51 @@ def test_mt19937_64_matches_the_cpp_engine(tmp_path):
     inst = bench.batch_instances(64)
     assert sum(i["case"] == "cavity" for i in inst) == 32
     assert all(100 <= i["Re"] <= 1000 and 0.05 <= i["U0"] <= 0.1 for i in inst)
+
+
+def _element_matrices(p):
+    """FE_Q(p) on [0, 1] at the Gauss-Lobatto points: mass, derivative and
+    stiffness matrices by exact Gauss quadrature (numpy, independent of the
+    library's geometry code)."""
+    x = cases.gauss_lobatto(p)
+    n = p + 1
+    coef = np.linalg.inv(np.vander(x, n, increasing=True))  # l_a(t) = sum_k coef[k, a] t^k
+    g, w = np.polynomial.legendre.leggauss(n + 1)
+    t, w = (g + 1) / 2, w / 2
+    l = np.vander(t, n, increasing=True) @ coef
+    dv = np.zeros((len(t), n))
+    for k in range(1, n):
+        dv[:, k] = k * t ** (k - 1)
+    dl = dv @ coef
+    return [(l * w[:, None]).T @ l, (l * w[:, None]).T @ dl, (dl * w[:, None]).T @ dl]
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_fp32_element_matrices_annihilate_constants(p):
+    """The FP32 element matrices of the FP32 kernels: the mass matrix is the
+    FP64 one rounded; the derivative and stiffness rows sum exactly to zero (their
+    plain FP32 roundings do not from p = 2 on), each entry within 1.2e-7 of its
+    row's largest."""
+    import lbfem_gpu
+
+    lib = lbfem_gpu.library()
+    fn = lib.lbfem_gpu_reference_matrix
+    fn.restype, fn.argtypes = C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_float)]
+    exact = _element_matrices(p)
+    n = p + 1
+    for op in range(3):
+        r64 = np.zeros(n * n)
+        r32 = np.zeros(n * n, dtype=np.float32)
+        assert fn(p, op, r64.ctypes.data_as(C.POINTER(C.c_double)), r32.ctypes.data_as(C.POINTER(C.c_float))) == 0
+        r64, r32 = r64.reshape(n, n), r32.reshape(n, n)
+        assert np.allclose(r64, exact[op], rtol=0, atol=1e-13 * np.abs(exact[op]).max())
+        tiny = np.abs(r64) <= 1e-14 * np.abs(r64).max(axis=1, keepdims=True)  # exact zeros but for rounding
+        if op == 0:
+            assert np.array_equal(r32, np.where(tiny, 0.0, r64).astype(np.float32))
+            continue
+        assert np.all(r32[tiny] == 0)
+        for a in range(n):
+            row = [float(v) for v in r32[a]]
+            assert sum(row) == 0.0  # exact in FP64: a few FP32 values
+            assert np.abs(r32[a].astype(np.float64) - r64[a]).max() <= 1.2e-7 * np.abs(r64[a]).max()
+    assert fn(0, 0, None, None) != 0 and fn(p, 3, None, None) != 0
