@@ -178,7 +178,7 @@ namespace
   start_grid(const Grid &g, int nsys)
   {
     using S = StartShape<P>;
-    return dim3((g.nfx + S::TX - 1) / S::TX, (g.nfy + S::TY - 1) / S::TY, nsys);
+    return dim3(tiles_along(g.nfx, g.nux, g.px, S::TX), tiles_along(g.nfy, g.nuy, g.py, S::TY), nsys);
   }
 
   template <typename F>
@@ -902,7 +902,7 @@ namespace
         st = with_degree(ctx->P, [&](auto PP) -> int {
           constexpr int P = decltype(PP)::value;
           using S = WinShape<P>;
-          const dim3 grid((g.nfx + S::TX - 1) / S::TX, (g.nfy + S::TY - 1) / S::TY, nsys);
+          const dim3 grid(tiles_along(g.nfx, g.nux, g.px, S::TX), tiles_along(g.nfy, g.nuy, g.py, S::TY), nsys);
           n_tiles = int(grid.x * grid.y);
           k_window_correct<P><<<grid, S::THREADS, window_smem<P>(), ctx->stream>>>(
             geo, ctx->d_winx, ctx->d_winy, r_in, ctx->d_x_s[xi], b, ctx->d_x_s[xo], r_out, ctx->d_cg, round == 0,
@@ -1708,7 +1708,7 @@ namespace
       int s2 = with_degree(ctx->P, [&](auto PP) -> int {
         constexpr int P = decltype(PP)::value;
         using S = WinShape<P>;
-        const dim3 grid((g.nfx + S::TX - 1) / S::TX, (g.nfy + S::TY - 1) / S::TY, NM);
+        const dim3 grid(tiles_along(g.nfx, g.nux, g.px, S::TX), tiles_along(g.nfy, g.nuy, g.py, S::TY), NM);
         n_tiles = int(grid.x * grid.y);
         k_window_correct<P><<<grid, S::THREADS, window_smem<P>(), ctx->stream>>>(
           geo, ctx->d_winx, ctx->d_winy, r_in, x_in, b, x_out, r_out, ctx->d_cg, all, ctx->d_partials);
@@ -2667,7 +2667,7 @@ lbfem_gpu_solve_round_resident(lbfem_gpu_ctx *ctx)
   return with_degree(ctx->P, [&](auto PP) -> int {
     constexpr int P = decltype(PP)::value;
     using S = WinShape<P>;
-    const dim3 grid((g.nfx + S::TX - 1) / S::TX, (g.nfy + S::TY - 1) / S::TY, NM);
+    const dim3 grid(tiles_along(g.nfx, g.nux, g.px, S::TX), tiles_along(g.nfy, g.nuy, g.py, S::TY), NM);
     k_window_correct<P><<<grid, S::THREADS, window_smem<P>(), ctx->stream>>>(
       geo, ctx->d_winx, ctx->d_winy, ctx->d_r_s, ctx->d_x_s[ctx->x_cur], ctx->d_rhs_s, ctx->d_p_s[1], ctx->d_p_s[0],
       ctx->d_cg, 1, ctx->d_partials);
@@ -3400,8 +3400,8 @@ namespace
           I.nb_pair_y = int(tg.y);
           I.nb_start_x = int(sg.x);
           I.nb_start_y = int(sg.y);
-          I.nb_win_x = (c->grid.nfx + S::TX - 1) / S::TX;
-          I.nb_win_y = (c->grid.nfy + S::TY - 1) / S::TY;
+          I.nb_win_x = tiles_along(c->grid.nfx, c->grid.nux, c->grid.px, S::TX);
+          I.nb_win_y = tiles_along(c->grid.nfy, c->grid.nuy, c->grid.py, S::TY);
           return 0;
         });
         if (gp.cls.empty() || gp.cls.back().P != c->P || gp.cls.back().mode != mode)

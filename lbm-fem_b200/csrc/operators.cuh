@@ -1762,6 +1762,15 @@ namespace lbfem_gpu
   // decay exponentially, so M^{-1} r at the own nodes of a tile follows from
   // banded LDL^T solves on a window of W nodes around the tile in each direction
   // (factors from window_ldl on the host), to a few 1e-6 of |r|.
+  // Tiles of T nodes along an axis of nf stored nodes (nu distinct). On a periodic
+  // axis whose distinct nodes fill whole tiles, the image node (the last stored
+  // node) gets no tile of its own: the last tile takes it.
+  __host__ __device__ constexpr int
+  tiles_along(int nf, int nu, int periodic, int T)
+  {
+    return (periodic && nu % T == 0) ? nu / T : (nf + T - 1) / T;
+  }
+
   // ------------------------------------------------ start of the mixed solve
   // x0 = 2 x_cur - x_prev (the extrapolated start, rounded to FP32 and stored in
   // x_new) and r0 = b - A x0 in FP32 arithmetic, for one tile of TX x TY nodes of
@@ -1894,6 +1903,25 @@ namespace lbfem_gpu
         xn[idx] = x0;
         rs[idx] = bv[i] - ax;
       }
+    // a periodic axis's image column (row) beyond the last tile (tiles_along): identity rows
+    auto image_start = [&](int x, int y) {
+      const long long idx = (long long)y * g.nfx + x;
+      const float v = extrapolated(xc, xp, idx);
+      xn[idx] = v;
+      rs[idx] = bs[idx] - v;
+    };
+    const int nbx = tiles_along(g.nfx, g.nux, g.px, S::TX), nby = tiles_along(g.nfy, g.nuy, g.py, S::TY);
+    const bool ext_x = g.px && g.nux % S::TX == 0 && bx == nbx - 1;
+    const bool ext_y = g.py && g.nuy % S::TY == 0 && by == nby - 1;
+    if (ext_y)
+      image_start(gx, g.nuy);
+    if (ext_x && j == 0)
+      {
+        for (int i = 0; i < S::TY && gy0 + i < g.nfy; ++i)
+          image_start(g.nux, gy0 + i);
+        if (ext_y)
+          image_start(g.nux, g.nuy);
+      }
   }
 
   // grid (x tiles, y tiles, systems)
@@ -1924,6 +1952,7 @@ namespace lbfem_gpu
     static constexpr int KP = K + 1;                       // row pitch of the My rows (16-byte pairs)
     static constexpr int THREADS = 160;
     static_assert(FY <= THREADS && TX + 2 * P <= THREADS, "one thread per window row and per own-plus-halo column");
+    static_assert(TX < THREADS, "a spare thread for an image column");
     static_assert(FX % 8 == 0 && FY % 4 == 0 && W - P >= 3, "whole chunks; the backward sweeps stop at W - P");
   };
 
@@ -2108,20 +2137,33 @@ namespace lbfem_gpu
     const float *rs = r_in + (long long)s * N, *xs = x_in + (long long)s * N, *bs = b + (long long)s * N;
     float *xo = x_out + (long long)s * N, *ro = r_out + (long long)s * N;
     double part[2] = {0, 0};
+    // A periodic axis whose distinct nodes fill whole tiles has no tile for its
+    // image column (row) alone: the last tile takes it (identity rows).
+    const bool ext_x = g.px && g.nux % S::TX == 0 && bx == nbx - 1;
+    const bool ext_y = g.py && g.nuy % S::TY == 0 && by == nby - 1;
     if (!all && !st->active[s])
       {
         // converged: carried over to the output buffers
+        auto copy = [&](int gx, int gy) {
+          const long long idx = (long long)gy * g.nfx + gx;
+          xo[idx] = xs[idx];
+          ro[idx] = rs[idx];
+        };
         for (int t = tid; t < S::TX * S::TY; t += NT)
           {
             const int i = t / S::TX, j = t - i * S::TX;
             const int gx = gx0 + j, gy = gy0 + i;
             if (gx < g.nfx && gy < g.nfy)
-              {
-                const long long idx = (long long)gy * g.nfx + gx;
-                xo[idx] = xs[idx];
-                ro[idx] = rs[idx];
-              }
+              copy(gx, gy);
           }
+        if (ext_y)
+          for (int j = tid; j < S::TX; j += NT)
+            if (gx0 + j < g.nfx)
+              copy(gx0 + j, g.nuy);
+        if (ext_x)
+          for (int i = tid; i < S::TY + (ext_y ? 1 : 0); i += NT)
+            if (gy0 + i < g.nfy)
+              copy(g.nux, gy0 + i);
         block_reduce_store_n<2, NT>(part, partials + (long long)s * n_tiles, tile, NM * n_tiles);
         return;
       }
@@ -2286,6 +2328,28 @@ namespace lbfem_gpu
               }
           }
         }
+      }
+    // the image row and column a tile takes beyond its own nodes (identity rows, as above)
+    auto image_node = [&](int gx, int gy) {
+      const long long idx = (long long)gy * g.nfx + gx;
+      const double xv = double(xs[idx]) + double(rs[idx]);
+      const double bb = bs[idx], rr = bb - xv;
+      xo[idx] = float(xv);
+      ro[idx] = float(rr);
+      if (owned_row(gy, g))
+        {
+          part[0] += bb * bb;
+          part[1] += rr * rr;
+        }
+    };
+    if (ext_y && tid < S::TX && gx0 + tid < g.nfx)
+      image_node(gx0 + tid, g.nuy);
+    if (ext_x && tid == S::TX)
+      {
+        for (int i = 0; i < S::TY && gy0 + i < g.nfy; ++i)
+          image_node(g.nux, gy0 + i);
+        if (ext_y)
+          image_node(g.nux, g.nuy);
       }
     block_reduce_store_n<2, NT>(part, partials + (long long)s * n_tiles, tile, NM * n_tiles);
   }
