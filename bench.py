@@ -197,7 +197,7 @@ def run_reference(args):
 # workload's kernels, from one-pass ncu captures of a launch on the 1024^2 Q3 mesh itself
 # (profiles/traffic_tgv_q3_1024.md gives the commands and the read / write split).
 STREAMING_TRAFFIC = {"fp64": 1269.1e6, "mixed": 608.9e6}
-WINDOW_TRAFFIC = 1490.1e6
+WINDOW_TRAFFIC = 1476.0e6
 
 
 def mixed_tol(cg_tol):
