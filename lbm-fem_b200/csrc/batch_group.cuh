@@ -70,16 +70,15 @@ namespace lbfem_gpu
     stream_pair_tile<P, MODE, TileShape<P>>(I.geo, I.ds, I.f, I.g, I.rhs, I.ac, t.bx, t.by);
   }
 
-  // refs: (instance, first boundary node) per CTA of 128 threads
+  // refs: (instance, first boundary node) per CTA of 128 threads, 8 per node
   template <int P>
   __global__ void
   kg_wall_faces(const GroupInst *__restrict__ tab, const int2 *__restrict__ refs)
   {
     const int2 rf = refs[blockIdx.x];
     const GroupInst &I = load_inst(tab, rf.x);
-    const int t = rf.y + threadIdx.x;
-    if (t < I.n_bnodes)
-      wall_face_node<P, float>(I.geo, I.bardow ? I.g : I.f, I.rhs, I.bnode, I.fc, t);
+    const int t = rf.y + (threadIdx.x >> 3);
+    wall_face_pop<P, float>(I.geo, I.bardow ? I.g : I.f, I.rhs, I.bnode, I.fc, t, threadIdx.x & 7, t < I.n_bnodes);
   }
 
   // blockIdx.y: system

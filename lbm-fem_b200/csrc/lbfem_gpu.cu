@@ -528,7 +528,7 @@ namespace
     const Geo geo = geo_of(ctx);
     return with_degree(ctx->P, [&](auto PP) -> int {
       constexpr int P = decltype(PP)::value;
-      k_wall_faces<P, R><<<(ctx->n_bnodes + 127) / 128, 128, 0, ctx->stream>>>(geo, f, rhs, ctx->d_bnode,
+      k_wall_faces<P, R><<<(ctx->n_bnodes * 8 + 127) / 128, 128, 0, ctx->stream>>>(geo, f, rhs, ctx->d_bnode,
                                                                            ctx->n_bnodes, fc);
       LAUNCHED();
       return LBFEM_OK;
@@ -3305,7 +3305,7 @@ namespace
     int i0 = 0, i1 = 0;
     size_t pair_off = 0, wall_off = 0, start_off = 0, win_off = 0, chunk_off = 0;
     int pair_n = 0;  // streaming tiles (Tile<P>)
-    int wall_n = 0;  // (instance, first boundary node) per 128 wall nodes
+    int wall_n = 0;  // (instance, first boundary node) per 16 wall nodes
     int start_n = 0; // start tiles (StartShape<P>)
     int win_n = 0;   // window tiles (WinShape<P>)
     int chunk_n = 0; // node chunks of GROUP_CHUNK nodes
@@ -3424,7 +3424,7 @@ namespace
         for (int by = 0; by < I.nb_win_y; ++by)
           for (int bx = 0; bx < I.nb_win_x; ++bx)
             L.win.push_back({k, bx, by});
-        for (int t = 0; t < I.n_bnodes; t += 128)
+        for (int t = 0; t < I.n_bnodes; t += 16) // 8 threads per node, 128 per CTA
           L.wall.push_back(make_int2(k, t));
         for (long long ch = 0; ch * GROUP_CHUNK < I.N; ++ch)
           L.chunks.push_back(make_int2(k, int(ch)));

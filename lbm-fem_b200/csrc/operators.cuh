@@ -968,50 +968,55 @@ namespace lbfem_gpu
   };
 
   // rhs += int_wall phi (dt^2/2)(n.e)(e.grad f) (advection.h:126-146,182-199) at the
-  // boundary nodes of the non-periodic sides; one thread per boundary node
-  // (bnode = (i, j, side mask: 1 bottom, 2 top, 4 left, 8 right)).
+  // boundary nodes of the non-periodic sides; 8 threads per boundary node, one per
+  // moving population (bnode = (i, j, side mask: 1 bottom, 2 top, 4 left, 8 right)).
   template <int P, typename R>
   __global__ void
   k_wall_faces(const Geo geo, const R *__restrict__ f, R *__restrict__ rhs, const int4 *__restrict__ bnode,
                int n_bnodes, const FaceCoef fc);
 
-  // Boundary node t of the kernel below (also the body of its batched form).
+  // Boundary node t, population al + 1, of the kernel below (also the body of its
+  // batched form): 8 consecutive lanes take the 8 moving populations of one node,
+  // and every lane of the warp calls it (valid: the lane has a node). Each
+  // population's sum over the node's sides is that of the reference's loop; the
+  // mass-flux removal sums the 8 populations' terms in the order al = 0..7 on
+  // every lane of the group.
   template <int P, typename R>
   __device__ __forceinline__ void
-  wall_face_node(const Geo &geo, const R *__restrict__ f, R *__restrict__ rhs, const int4 *__restrict__ bnode,
-                 const FaceCoef &fc, int t)
+  wall_face_pop(const Geo &geo, const R *__restrict__ f, R *__restrict__ rhs, const int4 *__restrict__ bnode,
+                const FaceCoef &fc, int t, int al, bool valid)
   {
     constexpr int K = 2 * P + 1;
     const Grid &g = geo.g;
     const long long N = g.N;
-    const int4 bn = bnode[t];
-    const int i = bn.x, j = bn.y, sides = bn.z;
-    double Rs[NM];
-#pragma unroll
-    for (int al = 0; al < NM; ++al)
-      Rs[al] = 0;
-    for (int side = 0; side < 4; ++side)
+    double Rs = 0;
+    int i = 0, j = 0;
+    if (valid)
       {
-        if (!(sides & (1 << side)))
-          continue;
-        const bool horizontal = side < 2;
-        const double *rows = horizontal ? geo.rowx : geo.rowy;
-        const int n_nodes = horizontal ? g.nfx : g.nfy;
-        const int per = horizontal ? g.px : g.py, nu = horizontal ? g.nux : g.nuy;
-        const int tpos = horizontal ? i : j;
-        const double *dn = (side == 0 || side == 2) ? fc.d0 : fc.d1;
-        const double hn = side == 0 ? fc.hy0 : side == 1 ? fc.hy1 : side == 2 ? fc.hx0 : fc.hx1;
-        const int base = (side == 0 || side == 2) ? 0 : (horizontal ? g.nfy : g.nfx) - 1 - P; // first normal layer
-        const int line = (side == 0) ? 0 : (side == 1) ? g.nfy - 1 : (side == 2) ? 0 : g.nfx - 1;
-        for (int al = 0; al < NM; ++al)
+        const int4 bn = bnode[t];
+        i = bn.x;
+        j = bn.y;
+        const int sides = bn.z;
+        const double ex = fc.ex[al], ey = fc.ey[al];
+        const R *u = f + (long long)(al + 1) * N;
+        for (int side = 0; side < 4; ++side)
           {
-            const double ex = fc.ex[al], ey = fc.ey[al];
+            if (!(sides & (1 << side)))
+              continue;
             const double en = side == 0 ? -ey : side == 1 ? ey : side == 2 ? -ex : ex;
             if (en == 0.0)
               continue;
+            const bool horizontal = side < 2;
+            const double *rows = horizontal ? geo.rowx : geo.rowy;
+            const int n_nodes = horizontal ? g.nfx : g.nfy;
+            const int per = horizontal ? g.px : g.py, nu = horizontal ? g.nux : g.nuy;
+            const int tpos = horizontal ? i : j;
+            const double *dn = (side == 0 || side == 2) ? fc.d0 : fc.d1;
+            const double hn = side == 0 ? fc.hy0 : side == 1 ? fc.hy1 : side == 2 ? fc.hx0 : fc.hx1;
+            const int base = (side == 0 || side == 2) ? 0 : (horizontal ? g.nfy : g.nfx) - 1 - P; // first normal layer
+            const int line = (side == 0) ? 0 : (side == 1) ? g.nfy - 1 : (side == 2) ? 0 : g.nfx - 1;
             const double et = horizontal ? ex : ey;  // tangential component
             const double enn = horizontal ? ey : ex; // normal component (derivative direction)
-            const R *u = f + (long long)(al + 1) * N;
             double tang = 0, norm = 0;
             for (int k = 0; k < K; ++k)
               {
@@ -1022,44 +1027,44 @@ namespace lbfem_gpu
                 const double cC = rows[((long long)1 * n_nodes + tpos) * K + k];
                 double d = 0;
 #pragma unroll
-                for (int b = 0; b <= P; ++b)
+                for (int bb = 0; bb <= P; ++bb)
                   {
                     const long long id =
-                      horizontal ? (long long)(base + b) * g.nfx + s : (long long)s * g.nfx + base + b;
-                    d += dn[b] * u[id];
+                      horizontal ? (long long)(base + bb) * g.nfx + s : (long long)s * g.nfx + base + bb;
+                    d += dn[bb] * u[id];
                   }
                 d /= hn;
                 const long long il = horizontal ? (long long)line * g.nfx + s : (long long)s * g.nfx + line;
                 tang += cC * u[il];
                 norm += cM * d;
               }
-            Rs[al] += fc.half_dt2 * en * (et * tang + enn * norm);
+            Rs += fc.half_dt2 * en * (et * tang + enn * norm);
           }
       }
     if (fc.remove)
       {
+        const int lane0 = (threadIdx.x & 31) & ~7;
         double flux = 0;
 #pragma unroll
-        for (int al = 0; al < NM; ++al)
-          flux += Rs[al];
-#pragma unroll
-        for (int al = 0; al < NM; ++al)
-          Rs[al] -= (c_W[al + 1] / (1. - c_W[0])) * flux;
+        for (int a = 0; a < NM; ++a)
+          flux += __shfl_sync(0xffffffffu, Rs, lane0 + a);
+        Rs -= (c_W[al + 1] / (1. - c_W[0])) * flux;
       }
-    const long long idx = (long long)j * g.nfx + i;
-#pragma unroll
-    for (int al = 0; al < NM; ++al)
-      rhs[al * N + idx] = R(double(rhs[al * N + idx]) + Rs[al]);
+    if (valid)
+      {
+        const long long idx = (long long)j * g.nfx + i;
+        rhs[al * N + idx] = R(double(rhs[al * N + idx]) + Rs);
+      }
   }
 
+  // blockDim a multiple of 32: thread 8 t + al takes node t, population al + 1
   template <int P, typename R>
   __global__ void
   k_wall_faces(const Geo geo, const R *__restrict__ f, R *__restrict__ rhs, const int4 *__restrict__ bnode,
                int n_bnodes, const FaceCoef fc)
   {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n_bnodes)
-      wall_face_node<P, R>(geo, f, rhs, bnode, fc, t);
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    wall_face_pop<P, R>(geo, f, rhs, bnode, fc, q >> 3, q & 7, (q >> 3) < n_bnodes);
   }
 
   // ------------------------------------------------------ mass matrix (K2)

@@ -126,3 +126,17 @@ def test_mixed_equilibria_conserve_mass_and_momentum(gpu_lib):
     ur, _ = _velocity(m, ref.get_populations())
     um, _ = _velocity(m, mix.get_populations())
     assert rel_l2(um, ur) <= 1e-6
+
+
+def test_mixed_image_rows_taken_by_the_last_tiles(gpu_lib):
+    """TGV Q2 on 64^2 cells, Lee-Lin: 128 distinct nodes per periodic axis fill
+    whole window tiles (128 x 64) and start tiles (128 x 16), so the last tiles
+    also take the image column and row. All nine population arrays, images
+    included, follow the FP64 run (deviations from the rest state)."""
+    tc = cases.TaylorGreenVortex(0.05 / math.sqrt(d2q9.CS2), 1, 1, shift=(0.25, 0.25), chapman_enskog=False)
+    tc.set_reynolds(100)
+    m = cases.build_mesh(tc, 64, 2)
+    assert (m.nfx - 1) % 128 == 0 and (m.nfy - 1) % 64 == 0
+    ref, mix = _pair(tc, m, "leelin", "cg", m.time_step(0.4), 60)
+    w = d2q9.W[:, None]
+    assert rel_l2(mix.get_populations() - w, ref.get_populations() - w) <= 1e-5
