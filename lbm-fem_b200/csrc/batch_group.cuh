@@ -4,9 +4,9 @@
 // instance, for one state of the buffer rotation) and a list of (instance,
 // tile) references drive each launch; the tile bodies are those of the
 // single-instance kernels, with the instance's own tile grid, so every
-// instance computes bitwise what its own step computes. Instances of one
-// degree share the tile kernels; the streaming kernel and the nodal update
-// also split by scheme.
+// instance computes bitwise what its own step computes. The instances fall in
+// classes of one degree and one scheme; each class's launches form one branch
+// of the step's graph (record_group in lbfem_gpu.cu).
 #pragma once
 
 #include "stream_pair.cuh"
