@@ -1828,20 +1828,40 @@ namespace lbfem_gpu
       }
     __syncthreads();
     // x_cur and x_prev on the tile and its halo: asynchronous copies, all in flight
-    // at once (zero outside the grid)
-    for (int c = tid; c < FX; c += S::THREADS)
+    // at once (zero outside the grid). A tile whose staged rows and columns neither
+    // leave the grid nor cross a periodic seam addresses them directly.
+    const bool inner = gx0 - P >= 0 && gx0 - P + FX <= (g.px ? g.nux : g.nfx) && gy0 - P >= 0 &&
+                       gy0 - P + FY <= (g.py ? g.nuy : g.nfy);
+    if (inner)
       {
-        const int col = s_col[c];
-#pragma unroll 8
-        for (int q = 0; q < FY; ++q)
+        const long long first = (long long)(gy0 - P) * g.nfx + gx0 - P;
+        for (int c = tid; c < FX; c += S::THREADS)
           {
-            const int ro = s_rowoff[q];
-            const bool ok = ro >= 0 && col >= 0;
-            const long long at = ok ? ro + col : 0;
-            cp_async4(&s_x[q * FX + c], xc + at, ok);
-            cp_async4(&s_p[q * FX + c], xp + at, ok);
+            const float *pc = xc + first + c, *pp = xp + first + c;
+#pragma unroll 11
+            for (int q = 0; q < FY; ++q)
+              {
+                cp_async4(&s_x[q * FX + c], pc, true);
+                cp_async4(&s_p[q * FX + c], pp, true);
+                pc += g.nfx;
+                pp += g.nfx;
+              }
           }
       }
+    else
+      for (int c = tid; c < FX; c += S::THREADS)
+        {
+          const int col = s_col[c];
+#pragma unroll 8
+          for (int q = 0; q < FY; ++q)
+            {
+              const int ro = s_rowoff[q];
+              const bool ok = ro >= 0 && col >= 0;
+              const long long at = ok ? ro + col : 0;
+              cp_async4(&s_x[q * FX + c], xc + at, ok);
+              cp_async4(&s_p[q * FX + c], xp + at, ok);
+            }
+        }
     const int j = tid, gx = gx0 + j;
     const bool col_in = gx < g.nfx;
     const bool img_col = g.px && gx == g.nux;
